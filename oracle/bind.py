@@ -1,0 +1,423 @@
+"""TEST INFRASTRUCTURE ONLY -- ctypes bindings for the CPU checkers.
+
+* ``liboracle.so``: the plain-C restatement of LibAPR's path (apr_oracle.c).
+* ``_ref/libaprref.so``: LibAPR's own CPU code compiled from its headers
+  (strict IEEE flags); ``_ref/libaprref_fast.so`` the same at the reference's
+  Release flags (-O3 -ffast-math), used only for timing.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module.  Images are numpy arrays of shape (z, x, y) in C order, i.e. the
+reference's PixelData memory order (y fastest).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+MAXL = 32
+
+
+class OrcParams(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("dx", "dy", "dz", "psfx", "psfy", "psfz", "Ip_th", "lambda_",
+                                         "rel_error", "sigma_th", "sigma_th_max", "grad_th")] + \
+               [(n, C.c_int) for n in ("reflect_bc_lis", "neighborhood_optimization", "constant_intensity_scale")]
+
+
+class OrcAccess(C.Structure):
+    _fields_ = [("l_min", C.c_int), ("l_max", C.c_int), ("org", C.c_int * 3),
+                ("y_num", C.c_int * MAXL), ("x_num", C.c_int * MAXL), ("z_num", C.c_int * MAXL),
+                ("level_xz", C.c_uint64 * (MAXL + 2)), ("n_xz", C.c_uint64),
+                ("xz_end", C.POINTER(C.c_uint64)), ("P", C.c_uint64), ("y_vec", C.POINTER(C.c_uint16))]
+
+
+def make_params(lambda_=3.0, rel_error=0.1, Ip_th=0.0, sigma_th=0.0, sigma_th_max=0.0, grad_th=0.0,
+                dx=1.0, dy=1.0, dz=1.0, psfx=2.0, psfy=2.0, psfz=2.0, reflect_bc_lis=1,
+                neighborhood_optimization=1, constant_intensity_scale=0):
+    return OrcParams(dx, dy, dz, psfx, psfy, psfz, Ip_th, lambda_, rel_error, sigma_th, sigma_th_max,
+                     grad_th, reflect_bc_lis, neighborhood_optimization, constant_intensity_scale)
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(C.POINTER(t))
+
+
+_lib = None
+_ref = {}
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        L = C.CDLL(os.path.join(HERE, "liboracle.so"))
+        L.orc_get_apr.argtypes = [C.POINTER(C.c_uint16), C.c_int, C.c_int, C.c_int, C.POINTER(OrcParams),
+                                  C.c_int, C.POINTER(C.c_void_p)]
+        L.orc_get_apr_custom.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int,
+                                         C.POINTER(OrcParams), C.POINTER(C.c_void_p)]
+        L.orc_free.argtypes = [C.c_void_p]
+        L.orc_get_access.argtypes = [C.c_void_p]
+        L.orc_get_access.restype = C.POINTER(OrcAccess)
+        L.orc_copy_intermediate.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_float), C.c_size_t]
+        L.orc_bspline_offset.argtypes = [C.c_void_p]
+        L.orc_bspline_offset.restype = C.c_float
+        L.orc_sample_image.argtypes = [C.POINTER(OrcAccess), C.POINTER(C.c_uint16), C.POINTER(C.c_uint16)]
+        L.orc_tree_init.argtypes = [C.POINTER(OrcAccess), C.POINTER(OrcAccess)]
+        L.orc_access_free.argtypes = [C.POINTER(OrcAccess)]
+        L.orc_fill_tree_mean.argtypes = [C.POINTER(OrcAccess), C.POINTER(OrcAccess), C.POINTER(C.c_float),
+                                         C.POINTER(C.c_float)]
+        L.orc_downsampled_stencils.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int,
+                                               C.POINTER(C.c_float), C.POINTER(C.c_int)]
+        L.orc_convolve.argtypes = [C.POINTER(OrcAccess), C.POINTER(OrcAccess), C.POINTER(C.c_float),
+                                   C.POINTER(C.c_int), C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                   C.c_int, C.POINTER(C.c_uint64)]
+        L.orc_richardson_lucy.argtypes = [C.POINTER(OrcAccess), C.POINTER(OrcAccess), C.POINTER(C.c_uint16),
+                                          C.c_void_p, C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int, C.c_int,
+                                          C.c_int, C.c_int]
+        L.orc_bspline_axis.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int]
+        L.orc_bspline_axis.restype = C.c_uint64
+        _lib = L
+    return _lib
+
+
+def ref_available(fast=False):
+    return os.path.exists(os.path.join(HERE, "_ref", "libaprref_fast.so" if fast else "libaprref.so"))
+
+
+def ref(fast=False):
+    if fast not in _ref:
+        R = C.CDLL(os.path.join(HERE, "_ref", "libaprref_fast.so" if fast else "libaprref.so"))
+        vp = C.c_void_p
+        R.ref_get_apr.argtypes = [C.POINTER(C.c_uint16), C.c_int, C.c_int, C.c_int, C.POINTER(OrcParams), C.c_int,
+                                  C.POINTER(vp)]
+        R.ref_get_apr_plain.argtypes = R.ref_get_apr.argtypes
+        R.ref_get_apr_custom.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int,
+                                         C.POINTER(OrcParams), C.POINTER(vp)]
+        R.ref_free.argtypes = [vp]
+        R.ref_apr_info.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_uint64),
+                                   C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_float)]
+        R.ref_apr_copy.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint16)]
+        R.ref_copy_intermediate.argtypes = [vp, C.c_int, C.POINTER(C.c_float), C.c_size_t]
+        R.ref_apr_from_arrays.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_uint64), C.c_uint64,
+                                          C.POINTER(C.c_uint64), C.c_uint64, C.POINTER(C.c_uint16), C.c_uint64]
+        R.ref_apr_from_arrays.restype = vp
+        R.ref_sample_image.argtypes = [vp, C.POINTER(C.c_uint16), C.POINTER(C.c_uint16)]
+        R.ref_tree_info.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        R.ref_tree_copy.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint16)]
+        R.ref_fill_tree_mean.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        R.ref_convolve_pencil.argtypes = [vp, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_float),
+                                          C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int]
+        R.ref_richardson_lucy.argtypes = [vp, C.POINTER(C.c_uint16), vp, C.POINTER(C.c_float), C.c_int, C.c_int,
+                                          C.c_int, C.c_int, C.c_int, C.c_int]
+        R.ref_smooth.argtypes = [C.POINTER(C.c_uint16), C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, C.c_float,
+                                 C.POINTER(C.c_float)]
+        _ref[fast] = R
+    return _ref[fast]
+
+
+class Access:
+    """A linear access structure held as numpy arrays (LinearAccess.hpp:33-35)."""
+
+    def __init__(self, org, l_min, l_max, y_num, x_num, z_num, level_xz, xz_end, y_vec):
+        self.org = tuple(int(v) for v in org)
+        self.l_min, self.l_max = int(l_min), int(l_max)
+        self.y_num, self.x_num, self.z_num = list(y_num), list(x_num), list(z_num)
+        self.level_xz = np.ascontiguousarray(level_xz, dtype=np.uint64)
+        self.xz_end = np.ascontiguousarray(xz_end, dtype=np.uint64)
+        self.y_vec = np.ascontiguousarray(y_vec, dtype=np.uint16)
+
+    @property
+    def P(self):
+        return int(self.xz_end[-1]) if len(self.xz_end) else 0
+
+    def c(self):
+        s = OrcAccess()
+        s.l_min, s.l_max = self.l_min, self.l_max
+        for i in range(3):
+            s.org[i] = self.org[i]
+        for l in range(MAXL):
+            s.y_num[l] = self.y_num[l] if l < len(self.y_num) else 0
+            s.x_num[l] = self.x_num[l] if l < len(self.x_num) else 0
+            s.z_num[l] = self.z_num[l] if l < len(self.z_num) else 0
+        for i in range(min(len(self.level_xz), MAXL + 2)):
+            s.level_xz[i] = int(self.level_xz[i])
+        s.n_xz = len(self.xz_end)
+        s.xz_end = _ptr(self.xz_end, C.c_uint64)
+        s.P = self.P
+        s.y_vec = _ptr(self.y_vec, C.c_uint16) if len(self.y_vec) else _ptr(np.zeros(1, np.uint16), C.c_uint16)
+        s._keep = (self.xz_end, self.y_vec)
+        return s
+
+    @staticmethod
+    def from_c(s):
+        L = s.l_max
+        return Access([s.org[i] for i in range(3)], s.l_min, L, [s.y_num[i] for i in range(MAXL)],
+                      [s.x_num[i] for i in range(MAXL)], [s.z_num[i] for i in range(MAXL)],
+                      np.array([s.level_xz[i] for i in range(L + 2)], dtype=np.uint64),
+                      np.ctypeslib.as_array(s.xz_end, shape=(s.n_xz,)).copy(),
+                      np.ctypeslib.as_array(s.y_vec, shape=(max(s.P, 1),))[: s.P].copy())
+
+    def rows(self, level):
+        """(z, x, begin, end) for every row of a level."""
+        base = int(self.level_xz[level])
+        xn, zn = self.x_num[level], self.z_num[level]
+        e = self.xz_end[base: base + xn * zn]
+        b = self.xz_end[base - 1: base - 1 + xn * zn]
+        return b.astype(np.int64), e.astype(np.int64)
+
+    def particle_coords(self):
+        """Per particle (level, z, x, y) arrays in linear order."""
+        lev = np.zeros(self.P, np.int32)
+        zz = np.zeros(self.P, np.int32)
+        xx = np.zeros(self.P, np.int32)
+        for l in range(self.l_min, self.l_max + 1):
+            b, e = self.rows(l)
+            xn = self.x_num[l]
+            cnt = e - b
+            idx = np.repeat(np.arange(len(cnt)), cnt)
+            sl = slice(int(b[0]) if len(b) else 0, int(e[-1]) if len(e) else 0)
+            lev[sl] = l
+            zz[sl] = idx // xn
+            xx[sl] = idx % xn
+        return lev, zz, xx, self.y_vec.astype(np.int32)
+
+
+def orc_get_apr(img, params, image_type=1, keep=True):
+    """Returns (Access, offset, intermediates dict) from the C restatement."""
+    L = lib()
+    img = np.ascontiguousarray(img, dtype=np.uint16)
+    z, x, y = img.shape
+    h = C.c_void_p()
+    e = L.orc_get_apr(_ptr(img, C.c_uint16), y, x, z, C.byref(params), image_type, C.byref(h))
+    if e != 0:
+        return e, None, None
+    acc = Access.from_c(L.orc_get_access(h).contents)
+    off = L.orc_bspline_offset(h)
+    inter = {}
+    if keep:
+        yd, xd, zd = (y + 1) // 2, (x + 1) // 2, (z + 1) // 2
+        for w in range(7):
+            shp = (z, x, y) if w == 0 else (zd, xd, yd)
+            a = np.zeros(shp, np.float32)
+            if L.orc_copy_intermediate(h, w, _ptr(a, C.c_float), a.size) == 0:
+                inter[w] = a
+    L.orc_free(h)
+    return 0, acc, (off, inter)
+
+
+def orc_get_apr_custom(grad, lis, shape_zxy, params):
+    L = lib()
+    z, x, y = shape_zxy
+    g = np.ascontiguousarray(grad, dtype=np.float32)
+    s = np.ascontiguousarray(lis, dtype=np.float32)
+    h = C.c_void_p()
+    e = L.orc_get_apr_custom(_ptr(g, C.c_float), _ptr(s, C.c_float), y, x, z, C.byref(params), C.byref(h))
+    assert e == 0
+    acc = Access.from_c(L.orc_get_access(h).contents)
+    L.orc_free(h)
+    return acc
+
+
+def orc_sample(acc, img):
+    out = np.zeros(acc.P, np.uint16)
+    img = np.ascontiguousarray(img, dtype=np.uint16)
+    lib().orc_sample_image(C.byref(acc.c()), _ptr(img, C.c_uint16), _ptr(out, C.c_uint16))
+    return out
+
+
+def orc_tree(acc):
+    L = lib()
+    t = OrcAccess()
+    ca = acc.c()
+    assert L.orc_tree_init(C.byref(ca), C.byref(t)) == 0
+    tr = Access.from_c(t)
+    L.orc_access_free(C.byref(t))
+    return tr
+
+
+def orc_tree_mean(acc, tree, parts):
+    out = np.zeros(max(tree.P, 1), np.float32)
+    p = np.ascontiguousarray(parts, dtype=np.float32)
+    lib().orc_fill_tree_mean(C.byref(acc.c()), C.byref(tree.c()), _ptr(p, C.c_float), _ptr(out, C.c_float))
+    return out[: tree.P]
+
+
+def orc_stencils(stencil, nlevels, normalize):
+    st = np.ascontiguousarray(stencil, dtype=np.float32).ravel()
+    ks = int(round(st.size ** (1 / 3)))
+    out = np.zeros(ks ** 3 * (nlevels + 1) + 64, np.float32)
+    sides = np.zeros(MAXL, np.int32)
+    n = lib().orc_downsampled_stencils(_ptr(st, C.c_float), ks, nlevels, int(normalize), _ptr(out, C.c_float),
+                                       _ptr(sides, C.c_int))
+    return out[:n].copy(), sides[: max(nlevels, 1)].copy()
+
+
+def orc_convolve(acc, tree, stencil, parts, reflect=True, use_stencil_ds=True, normalize=False):
+    nlev = max(acc.l_max - acc.l_min, 1) if use_stencil_ds else 1
+    st, sides = orc_stencils(stencil, nlev, normalize)
+    p = np.ascontiguousarray(parts, dtype=np.float32)
+    out = np.zeros(acc.P, np.float32)
+    stale = C.c_uint64()
+    lib().orc_convolve(C.byref(acc.c()), C.byref(tree.c()), _ptr(st, C.c_float), _ptr(sides, C.c_int), len(sides),
+                       _ptr(p, C.c_float), _ptr(out, C.c_float), int(reflect), C.byref(stale))
+    return out, int(stale.value)
+
+
+def orc_richardson_lucy(acc, tree, parts_u16, psf, niter, use_stencil_ds=True, normalize=False, use_double=False,
+                        init=None):
+    p = np.ascontiguousarray(parts_u16, dtype=np.uint16)
+    st = np.ascontiguousarray(psf, dtype=np.float32).ravel()
+    ks = int(round(st.size ** (1 / 3)))
+    dt = np.float64 if use_double else np.float32
+    out = np.ones(acc.P, dt) if init is None else np.ascontiguousarray(init, dtype=dt).copy()
+    lib().orc_richardson_lucy(C.byref(acc.c()), C.byref(tree.c()), _ptr(p, C.c_uint16), out.ctypes.data_as(C.c_void_p),
+                              _ptr(st, C.c_float), ks, niter, int(use_stencil_ds), int(normalize),
+                              int(init is not None), int(use_double))
+    return out
+
+
+# ----------------------------------------------------------------------------- reference (oracle/_ref)
+
+def _ref_access(R, h):
+    lmin, lmax = C.c_int(), C.c_int()
+    nl, nx, P = C.c_uint64(), C.c_uint64(), C.c_uint64()
+    off = C.c_float()
+    R.ref_apr_info(h, C.byref(lmin), C.byref(lmax), C.byref(nl), C.byref(nx), C.byref(P), C.byref(off))
+    lx = np.zeros(nl.value, np.uint64)
+    xe = np.zeros(nx.value, np.uint64)
+    yv = np.zeros(max(P.value, 1), np.uint16)
+    R.ref_apr_copy(h, _ptr(lx, C.c_uint64), _ptr(xe, C.c_uint64), _ptr(yv, C.c_uint16))
+    return lmin.value, lmax.value, lx, xe, yv[: P.value], off.value
+
+
+class RefAPR:
+    """Handle on an APR held by the reference library."""
+
+    def __init__(self, h, shape_zxy, fast=False):
+        self.h, self.shape, self.fast = h, shape_zxy, fast
+        self.R = ref(fast)
+
+    def __del__(self):
+        try:
+            self.R.ref_free(self.h)
+        except Exception:
+            pass
+
+    def access(self):
+        lmin, lmax, lx, xe, yv, _ = _ref_access(self.R, self.h)
+        z, x, y = self.shape
+        a = Access((y, x, z), lmin, lmax, [0] * MAXL, [0] * MAXL, [0] * MAXL, lx, xe, yv)
+        ref_geom(a)
+        return a
+
+    def offset(self):
+        return _ref_access(self.R, self.h)[5]
+
+    def intermediate(self, which):
+        z, x, y = self.shape
+        a = np.zeros(((z + 1) // 2, (x + 1) // 2, (y + 1) // 2), np.float32)
+        assert self.R.ref_copy_intermediate(self.h, which, _ptr(a, C.c_float), a.size) == 0
+        return a
+
+    def sample(self, img):
+        out = np.zeros(max(self.access().P, 1), np.uint16)
+        img = np.ascontiguousarray(img, dtype=np.uint16)
+        self.R.ref_sample_image(self.h, _ptr(img, C.c_uint16), _ptr(out, C.c_uint16))
+        return out
+
+    def tree(self):
+        nl, nx, P = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        self.R.ref_tree_info(self.h, C.byref(nl), C.byref(nx), C.byref(P))
+        lx = np.zeros(nl.value, np.uint64)
+        xe = np.zeros(nx.value, np.uint64)
+        yv = np.zeros(max(P.value, 1), np.uint16)
+        self.R.ref_tree_copy(self.h, _ptr(lx, C.c_uint64), _ptr(xe, C.c_uint64), _ptr(yv, C.c_uint16))
+        z, x, y = self.shape
+        t = Access((y, x, z), 0, len(lx) - 2, [0] * MAXL, [0] * MAXL, [0] * MAXL, lx, xe, yv[: P.value])
+        ref_geom(t, tree=True)
+        return t
+
+    def tree_mean(self, parts):
+        t = self.tree()
+        out = np.zeros(max(t.P, 1), np.float32)
+        p = np.ascontiguousarray(parts, dtype=np.float32)
+        self.R.ref_fill_tree_mean(self.h, _ptr(p, C.c_float), _ptr(out, C.c_float))
+        return out[: t.P]
+
+    def convolve(self, stencil, parts, reflect=True, use_stencil_ds=True, normalize=False):
+        st = np.ascontiguousarray(stencil, dtype=np.float32).ravel()
+        ks = int(round(st.size ** (1 / 3)))
+        p = np.ascontiguousarray(parts, dtype=np.float32)
+        out = np.zeros(len(p), np.float32)
+        self.R.ref_convolve_pencil(self.h, _ptr(st, C.c_float), ks, _ptr(p, C.c_float), _ptr(out, C.c_float),
+                                   int(reflect), int(use_stencil_ds), int(normalize))
+        return out
+
+    def richardson_lucy(self, parts_u16, psf, niter, use_stencil_ds=True, normalize=False, use_double=False,
+                        init=None):
+        p = np.ascontiguousarray(parts_u16, dtype=np.uint16)
+        st = np.ascontiguousarray(psf, dtype=np.float32).ravel()
+        ks = int(round(st.size ** (1 / 3)))
+        dt = np.float64 if use_double else np.float32
+        out = np.ones(len(p), dt) if init is None else np.ascontiguousarray(init, dtype=dt).copy()
+        self.R.ref_richardson_lucy(self.h, _ptr(p, C.c_uint16), out.ctypes.data_as(C.c_void_p), _ptr(st, C.c_float),
+                                   ks, niter, int(use_stencil_ds), int(normalize), int(init is not None),
+                                   int(use_double))
+        return out
+
+
+def ref_geom(a, tree=False):
+    """Fills y/x/z_num of an Access from its org dims (GenInfo.hpp:33-98)."""
+    import math
+    y, x, z = a.org
+    md = max(x, y, z)
+    lm = math.ceil(math.log2(md))
+    if not tree:
+        lm = max(1, lm)
+        for l in range(1, lm + 1):
+            cell = round(2.0 ** (lm - l))
+            a.y_num[l], a.x_num[l], a.z_num[l] = (math.ceil(y / cell), math.ceil(x / cell), math.ceil(z / cell))
+    else:
+        tl = max(lm - 1, 0)
+        for l in range(0, tl + 1):
+            cell = round(2.0 ** (tl - l + 1))
+            a.y_num[l], a.x_num[l], a.z_num[l] = (math.ceil(y / cell), math.ceil(x / cell), math.ceil(z / cell))
+
+
+def ref_get_apr(img, params, image_type=1, staged=True, fast=False):
+    R = ref(fast)
+    img = np.ascontiguousarray(img, dtype=np.uint16)
+    z, x, y = img.shape
+    h = C.c_void_p()
+    fn = R.ref_get_apr if staged else R.ref_get_apr_plain
+    e = fn(_ptr(img, C.c_uint16), y, x, z, C.byref(params), image_type, C.byref(h))
+    if e != 0:
+        return e, None
+    return 0, RefAPR(h.value, img.shape, fast)
+
+
+def ref_get_apr_custom(grad, lis, shape_zxy, params):
+    R = ref()
+    z, x, y = shape_zxy
+    g = np.ascontiguousarray(grad, dtype=np.float32)
+    s = np.ascontiguousarray(lis, dtype=np.float32)
+    h = C.c_void_p()
+    R.ref_get_apr_custom(_ptr(g, C.c_float), _ptr(s, C.c_float), y, x, z, C.byref(params), C.byref(h))
+    return RefAPR(h.value, shape_zxy)
+
+
+def ref_from_access(acc, shape_zxy):
+    R = ref()
+    z, x, y = shape_zxy
+    h = R.ref_apr_from_arrays(y, x, z, _ptr(acc.level_xz, C.c_uint64), len(acc.level_xz),
+                              _ptr(acc.xz_end, C.c_uint64), len(acc.xz_end),
+                              _ptr(acc.y_vec if len(acc.y_vec) else np.zeros(1, np.uint16), C.c_uint16), acc.P)
+    return RefAPR(h, shape_zxy)
+
+
+def ref_smooth(img, lambda_, image_type, offset):
+    R = ref()
+    img = np.ascontiguousarray(img, dtype=np.uint16)
+    z, x, y = img.shape
+    out = np.zeros(img.shape, np.float32)
+    e = R.ref_smooth(_ptr(img, C.c_uint16), y, x, z, lambda_, image_type, offset, _ptr(out, C.c_float))
+    return e, out
