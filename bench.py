@@ -1,0 +1,399 @@
+"""Benchmark: get_apr (+ particle sampling) on the 2048x2048x512 uint16 volume,
+then APR isotropic 3x3x3 and 5x5x5 convolution over its particles.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  A step is one get_apr + sample_image pass over one
+seeded synthetic volume (background 100, 60000 Gaussian blobs sigma U[2,8] px,
+amplitude U[500,6000], Poisson noise; APR parameters lambda=3, E=0.1,
+Ip_th=0, sigma_th=50, grad_th=10, ImageType uint16).  ``value`` is whole-job
+GVox/s with the input resident in HBM; ``e2e`` is the same through the
+host-buffer C ABI (image host->device and particles device->host inside the
+timed region).  Under torchrun every rank converts its own volume (different
+seed): the volumes are independent, so scaling is weak and no collective runs
+on the data path.  The input (4 GiB) is larger than L2, so no L2 flush is
+needed between steps.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SHAPE = (512, 2048, 2048)  # z, x, y
+BLOBS = 60000
+SIGMA = (2.0, 8.0)
+AMP = (500.0, 6000.0)
+BG = 100.0
+PARAMS = dict(lambda_=3.0, rel_error=0.1, Ip_th=0.0, sigma_th=50.0, grad_th=10.0)
+METRIC = "get_apr GVox/s + APR conv Gpart/s vs HBM roofline; RL time-to-1e-3 learned vs plain"
+CPU_SLAB_Z = 64  # bounded CPU sample: z-slab of the same volume
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu = gpu
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in open(self.f.name).read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(n)
+            except Exception:
+                pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def lib_params():
+    import libapr_b200 as A
+    p = A.APRParameters()
+    for k, v in PARAMS.items():
+        setattr(p, k, v)
+    return p
+
+
+def algorithmic_bytes(stage, N, Nd, P, T):
+    """Minimum HBM bytes of one launch of a stage (uint16 ImageType)."""
+    return {
+        "bspline_y": 2 * 2 * N, "bspline_x": 2 * 2 * N, "bspline_z": 2 * 2 * N,
+        "gradient_ds": 2 * N + 6 * Nd, "inv_bspline": 8 * Nd, "local_intensity_scale": 8 * Nd,
+        "levels": 14 * Nd, "offset": 2 * N, "sample_image": 2 * N + 4 * P,
+        "convolve": 10 * P + 10 * T, "fill_tree_mean": 6 * P + 6 * T,
+    }.get(stage)
+
+
+def cpu_baseline(host_img, steps=2):
+    """The reference's own CPU get_apr + sample_image (oracle/_ref, Release
+    flags) on a z-slab of the volume, all host threads."""
+    from oracle import bind as B
+    if not B.ref_available(fast=True):
+        return None
+    slab = np.ascontiguousarray(host_img[:CPU_SLAB_Z])
+    p = B.make_params(**PARAMS)
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        e, r = B.ref_get_apr(slab, p, 1, staged=False, fast=True)
+        r.sample(slab)
+        ts.append(time.perf_counter() - t0)
+        del r
+    t = min(ts)
+    return {"value": slab.size / t / 1e9, "unit": "GVox/s", "cores": os.cpu_count(), "kind": "reference",
+            "sample": "get_apr + sample_image on a %dx%dx%d z-slab of the volume, best of %d" % (
+                slab.shape[0], slab.shape[1], slab.shape[2], steps), "seconds": t}
+
+
+def run_reference(args):
+    """--impl reference: the reference CPU implementation, rank 0 only."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    from oracle import bind as B
+    import libapr_b200.synth as S
+    if not B.ref_available(fast=True):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (needs the LibAPR tree)"}))
+        return 0
+    slab_shape = (CPU_SLAB_Z, SHAPE[1], SHAPE[2])
+    frac = CPU_SLAB_Z / SHAPE[0]
+    img = None
+    try:
+        import torch
+        import libapr_b200 as A
+        if torch.cuda.is_available():
+            d = torch.empty(slab_shape, dtype=torch.int16, device="cuda")
+            A.synth_blobs_device(d, int(BLOBS * frac), SIGMA, AMP, BG, seed=1000)
+            img = d.cpu().numpy().view(np.uint16)
+    except Exception:
+        img = None
+    if img is None:
+        img = S.blob_volume(slab_shape, int(BLOBS * frac), SIGMA, AMP, BG, seed=1000)
+    p = B.make_params(**PARAMS)
+    times = []
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        e, r = B.ref_get_apr(img, p, 1, staged=False, fast=True)
+        r.sample(img)
+        dt = time.perf_counter() - t0
+        del r
+        if i >= args.warmup:
+            times.append(dt)
+    t = sum(times) / len(times)
+    v = img.size / t / 1e9
+    line = {"metric": METRIC, "value": v, "unit": "GVox/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+            "config": {"workload": "get_apr + sample_image, uint16 2048x2048x512 blob volume (each step a "
+                                   "2048x2048x%d z-slab of it)" % CPU_SLAB_Z, "image_type": "uint16", **PARAMS},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "GVox/s", "cores": os.cpu_count(), "kind": "reference",
+                             "sample": "z-slab %s per step, LibAPR CPU get_apr_cpu + sample_image at Release "
+                                       "flags (-O3 -ffast-math), OpenMP" % (slab_shape,)},
+            "e2e": {"value": v, "unit": "GVox/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--shape", default=None, help="z,x,y override (debugging only)")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-conv", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    import torch.distributed as dist
+    import libapr_b200 as A
+    from libapr_b200 import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    shape = tuple(int(v) for v in args.shape.split(",")) if args.shape else SHAPE
+    z, x, y = shape
+    N = z * x * y
+    L = _lib.lib()
+    stream = torch.cuda.current_stream()
+    sptr = C.c_void_p(stream.cuda_stream)
+
+    img = torch.empty(shape, dtype=torch.int16, device="cuda")
+    A.synth_blobs_device(img, int(BLOBS * N / (SHAPE[0] * SHAPE[1] * SHAPE[2])), SIGMA, AMP, BG,
+                         seed=1000 + rank, stream=stream)
+    torch.cuda.synchronize()
+    conv = A.APRConverter("uint16")
+    par = lib_params().c()
+    iptr = C.c_void_p(img.data_ptr())
+
+    def get_apr_dev():
+        h = C.c_void_p()
+        _lib.check(L.aprb_get_apr_device(conv._h, C.byref(par), iptr, y, x, z, sptr, C.byref(h)))
+        return h
+
+    # learn P, allocate particle output
+    h0 = get_apr_dev()
+    info = _lib.aprb_apr_info()
+    _lib.check(L.aprb_apr_get_info(h0, C.byref(info)))
+    P = int(info.total_number_particles)
+    parts = torch.empty(max(P, 1), dtype=torch.int16, device="cuda")
+    pptr = C.c_void_p(parts.data_ptr())
+    L.aprb_apr_free(h0)
+
+    def step(keep):
+        h = get_apr_dev()
+        _lib.check(L.aprb_sample_image_device(h, iptr, pptr, sptr))
+        keep.append(h)
+
+    hs = []
+    for _ in range(args.warmup):
+        step(hs)
+    torch.cuda.synchronize()
+    for h in hs:
+        L.aprb_apr_free(h)
+    hs = []
+
+    clocks = Clocks(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    L.aprb_profile_reset()
+    L.aprb_profile_enable(1)
+    launches0 = L.aprb_kernel_launch_count()
+    if rank == 0:
+        clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step(hs)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ck = clocks.stop() if rank == 0 else None
+    launches = L.aprb_kernel_launch_count() - launches0
+    L.aprb_profile_enable(0)
+    ms = ev0.elapsed_time(ev1) / args.steps
+    names = (C.c_char_p * 64)()
+    tms = (C.c_double * 64)()
+    cnts = (C.c_uint64 * 64)()
+    ns = L.aprb_profile_read(names, tms, cnts, 64)
+    stages = {names[i].decode(): (tms[i], int(cnts[i])) for i in range(ns)}
+    L.aprb_profile_reset()
+    t_max = torch.tensor([ms], device="cuda", dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_all = float(t_max.item())
+    last = hs[-1]
+    for h in hs[:-1]:
+        L.aprb_apr_free(h)
+
+    Nd = ((z + 1) // 2) * ((x + 1) // 2) * ((y + 1) // 2)
+    hbm, peak_kind = peaks()
+    out = {}
+    if rank == 0:
+        # dominant stage and its roofline (algorithmic bytes / mean launch time)
+        dom = max(stages.items(), key=lambda kv: kv[1][0])
+        dname, (dms, dcnt) = dom
+        per = dms / dcnt / 1e3
+        ab = algorithmic_bytes(dname, N, Nd, P, 0)
+        achieved = ab / per / 1e9 if ab else None
+        out["roofline"] = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                           "frac": achieved / hbm if achieved else None, "traffic": None,
+                           "peak_source": peak_kind, "algorithmic_bytes_per_launch": ab,
+                           "launch_ms": per * 1e3}
+        pipe_b = 10 * N + 4 * P
+        out["pipeline_roofline"] = {"algorithmic_bytes": pipe_b, "achieved_gbs": pipe_b / (ms_all / 1e3) / 1e9,
+                                    "frac": pipe_b / (ms_all / 1e3) / 1e9 / hbm}
+        out["stages_ms_per_step"] = {k: v[0] / args.steps for k, v in stages.items()}
+
+    # --- convolution over the particles of the last step (float intensities)
+    conv_res = {}
+    if not args.no_conv:
+        pf = parts[:P].to(torch.int32).bitwise_and(0xFFFF).to(torch.float32).contiguous()
+        outp = torch.empty_like(pf)
+        _lib.check(L.aprb_apr_init_tree(last))
+        _lib.check(L.aprb_apr_get_info(last, C.byref(info)))
+        T = int(info.tree_total_number_particles)
+        rng = np.random.default_rng(7)
+        for ks in (3, 5):
+            st = rng.uniform(-1, 1, ks ** 3).astype(np.float32)
+            st = (st / st.sum()).astype(np.float32)
+            stp = C.c_void_p(st.ctypes.data)
+
+            def run_conv():
+                _lib.check(L.aprb_convolve_device(last, stp, ks, C.c_void_p(pf.data_ptr()),
+                                                  C.c_void_p(outp.data_ptr()), 1, 1, 0, sptr))
+
+            for _ in range(2):
+                run_conv()
+            torch.cuda.synchronize()
+            L.aprb_profile_reset()
+            L.aprb_profile_enable(1)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = max(2, args.steps)
+            e0.record(stream)
+            for _ in range(reps):
+                run_conv()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            L.aprb_profile_enable(0)
+            L.aprb_profile_reset()
+            cms = e0.elapsed_time(e1) / reps
+            ab = 10 * P + 10 * T
+            flops = 2 * (ks ** 3) * P
+            conv_res["conv%d%d%d" % (ks, ks, ks)] = {
+                "value": P / (cms / 1e3) / 1e9, "unit": "Gpart/s", "ms": cms, "particles": P, "tree_nodes": T,
+                "roofline": {"bound": "hbm", "achieved": ab / (cms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                             "frac": ab / (cms / 1e3) / 1e9 / hbm, "algorithmic_bytes": ab},
+                "gflops": flops / (cms / 1e3) / 1e9}
+        del pf, outp
+    L.aprb_apr_free(last)
+
+    # --- end to end through the host-buffer C ABI
+    e2e = None
+    if rank == 0:
+        host = torch.empty(shape, dtype=torch.int16, pin_memory=True)
+        host.copy_(img)
+        hparts = torch.empty(max(P, 1), dtype=torch.int16, pin_memory=True)
+        hp = C.c_void_p(host.data_ptr())
+        hpp = C.c_void_p(hparts.data_ptr())
+
+        def e2e_step():
+            h = C.c_void_p()
+            _lib.check(L.aprb_get_apr(conv._h, C.byref(par), hp, y, x, z, C.byref(h)))
+            _lib.check(L.aprb_sample_image(h, hp, hpp))
+            L.aprb_apr_free(h)
+
+        e2e_step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        torch.cuda.synchronize()
+        te = (time.perf_counter() - t0) / args.steps
+        e2e = {"value": N * world / te / 1e9, "unit": "GVox/s", "h2d_bytes_per_step": 4 * N,
+               "d2h_bytes_per_step": 2 * P, "ms_per_step": te * 1e3}
+        cpu = None
+        if not args.no_cpu:
+            cpu = cpu_baseline(host.numpy().view(np.uint16))
+        line = {"metric": METRIC, "value": N * world / (ms_all / 1e3) / 1e9, "unit": "GVox/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_all, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+                "config": {"workload": "get_apr + sample_image, uint16 %dx%dx%d (y,x,z) blob volume, "
+                                       "60000 blobs per 2048x2048x512, per GPU" % (y, x, z),
+                           "image_type": "uint16", **PARAMS, "particles": P,
+                           "l2": "input 4 GiB > L2, no flush needed",
+                           "parallelism": "independent volume per GPU" if world > 1 else "1 GPU"},
+                "gpu_launches": int(launches), "e2e": e2e, "cpu_baseline": cpu, **out, **conv_res}
+        if ck:
+            line["clocks"] = ck
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

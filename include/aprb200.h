@@ -1,0 +1,182 @@
+/*
+ * aprb200 -- B200-native (sm_100a) APR construction and filtering.
+ *
+ * C ABI of libaprb200.so.  Plain pointers and sizes only; every entry point
+ * returns an aprb_status and never throws.  Each declaration names the LibAPR
+ * interface it replaces (file:line in the LibAPR source tree).
+ *
+ * Conventions
+ *  - Dense images are y-fastest, then x, then z (LibAPR PixelData order:
+ *    index = z*x_num*y_num + x*y_num + y), dimensions passed as (y, x, z).
+ *  - Functions without the _device suffix take HOST buffers, copy them to the
+ *    GPU, run, copy results back and return when the results are on the host
+ *    (the reference's calls are blocking too).  The _device variants take
+ *    device pointers and a cudaStream_t (passed as void*), enqueue work on that
+ *    stream and return without waiting, except where noted (a structure whose
+ *    size is data-dependent reads its particle count back once).
+ *  - The particle structure is the reference's linear access structure
+ *    (LinearAccess.hpp:33-35): level_xz (uint64, l_max+2 entries), xz_end
+ *    (uint64, inclusive particle counts per (level, z, x) row, entry 0 is a
+ *    zero guard), y_vec (uint16 per particle); particle order is level
+ *    ascending, then z, x, y.
+ *  - One GPU, the calling thread's current CUDA device.  Handles are not
+ *    thread-safe: one converter / APR handle per host thread, as one
+ *    APRConverter object is not re-entrant in the reference.
+ */
+#ifndef APRB200_H
+#define APRB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    APRB_OK = 0,
+    APRB_ERR_INVALID_ARGUMENT = 1,   /* null pointer, bad enum, size mismatch            */
+    APRB_ERR_DIMENSIONS = 2,         /* input dimension check failed (APRConverter.hpp:86-91)  */
+    APRB_ERR_INTEGER_OVERFLOW = 3,   /* uint16 IIR under/overflow (ComputeGradient.hpp:409-412) */
+    APRB_ERR_UNSUPPORTED = 4,        /* e.g. stencil side not 3 or 5 (APRNumericsGPU.cu:201-203) */
+    APRB_ERR_OUT_OF_MEMORY = 5,
+    APRB_ERR_CUDA = 6,               /* a CUDA runtime call failed                        */
+    APRB_ERR_NO_DEVICE = 7,          /* no usable sm_100 device                           */
+    APRB_ERR_INCOMPLETE_NEIGHBOURHOOD = 8 /* filter read a cell no particle covers (invalid APR) */
+} aprb_status;
+
+/* Mirror of the APRParameters fields the path reads (APRParameters.hpp:14-41). */
+typedef struct {
+    float dx, dy, dz;
+    float psfx, psfy, psfz;
+    float Ip_th, lambda, rel_error, sigma_th, sigma_th_max, grad_th;
+    int reflect_bc_lis;              /* default 1 */
+    int neighborhood_optimization;   /* default 1 */
+    int constant_intensity_scale;    /* default 0 */
+    int check_input;                 /* default 0 (APRConverter.hpp:86) */
+    int swap_dimensions;             /* default 0 */
+} aprb_params;
+
+/* ImageType of APRConverter<ImageType> */
+enum { APRB_IMAGE_FLOAT = 0, APRB_IMAGE_U16 = 1 };
+
+/* Intermediates kept by a converter for stage-level checks. */
+enum {
+    APRB_STAGE_SMOOTHED = 0,        /* full-res B-spline coefficients (IT values as float)    */
+    APRB_STAGE_GRADIENT = 1,        /* ds gradient magnitude after get_gradient               */
+    APRB_STAGE_DS_IMAGE = 2,        /* ds inverse-bspline image (local_scale_temp2)           */
+    APRB_STAGE_LOCAL_SCALE = 3,     /* ds local intensity scale                               */
+    APRB_STAGE_GRADIENT_APPLIED = 4,/* ds gradient after applyParameters                      */
+    APRB_STAGE_SCALE_APPLIED = 5,   /* ds scale after applyParameters                         */
+    APRB_STAGE_LEVELS = 6           /* ds particle-cell levels (compute_level_for_array)      */
+};
+
+typedef struct aprb_converter aprb_converter;
+typedef struct aprb_apr aprb_apr;
+
+typedef struct {
+    int l_min, l_max;
+    int org_dims[3];                 /* y, x, z */
+    int y_num[32], x_num[32], z_num[32];
+    uint64_t total_number_particles;
+    uint64_t n_level_xz;             /* l_max + 2 */
+    uint64_t n_xz;                   /* entries of xz_end */
+    float bspline_offset;
+    /* tree (valid after aprb_apr_init_tree) */
+    int tree_l_min, tree_l_max;
+    uint64_t tree_total_number_particles, tree_n_level_xz, tree_n_xz;
+} aprb_apr_info;
+
+const char *aprb_status_string(aprb_status s);
+/* Text of the last error on this thread ("" when none). */
+const char *aprb_last_error(void);
+
+/* APRParameters defaults (APRParameters.hpp:14-41). */
+void aprb_default_params(aprb_params *p);
+
+/* --- construction: APRConverter<ImageType> (APRConverter.hpp:35-134) ---------- */
+aprb_status aprb_converter_create(int image_type, aprb_converter **out);
+aprb_status aprb_converter_destroy(aprb_converter *c);
+/* keep_intermediates != 0 keeps the APRB_STAGE_* buffers after get_apr */
+aprb_status aprb_converter_keep_intermediates(aprb_converter *c, int keep);
+
+/* APRConverter<IT>::get_apr(APR&, PixelData<uint16_t>&) (APRConverter.hpp:591-600 -> get_apr_cpu :535-582) */
+aprb_status aprb_get_apr(aprb_converter *c, const aprb_params *p, const uint16_t *img, int y_num, int x_num,
+                         int z_num, aprb_apr **out);
+/* same, image already on the device; enqueued on stream, returns after the particle count is known */
+aprb_status aprb_get_apr_device(aprb_converter *c, const aprb_params *p, const uint16_t *img_dev, int y_num,
+                                int x_num, int z_num, void *stream, aprb_apr **out);
+/* copy one APRB_STAGE_* intermediate of the last get_apr to the host (n = element count) */
+aprb_status aprb_converter_intermediate(const aprb_converter *c, int stage, float *dst, size_t n);
+
+/* --- the APR object ------------------------------------------------------------ */
+aprb_status aprb_apr_free(aprb_apr *a);
+aprb_status aprb_apr_get_info(const aprb_apr *a, aprb_apr_info *info);
+/* LinearAccess arrays to host (any pointer may be NULL) */
+aprb_status aprb_apr_export(const aprb_apr *a, uint64_t *level_xz, uint64_t *xz_end, uint16_t *y_vec);
+/* device pointers of the LinearAccess arrays (owned by the APR) */
+aprb_status aprb_apr_device_arrays(const aprb_apr *a, const uint64_t **level_xz, const uint64_t **xz_end,
+                                   const uint16_t **y_vec);
+/* build an APR from host LinearAccess arrays (e.g. read from a .apr file) */
+aprb_status aprb_apr_from_arrays(int y_num, int x_num, int z_num, const uint64_t *level_xz, uint64_t n_level_xz,
+                                 const uint64_t *xz_end, uint64_t n_xz, const uint16_t *y_vec, uint64_t n_particles,
+                                 aprb_apr **out);
+
+/* --- particle sampling: ParticleData::sample_image (ParticleData.hpp:123-127) --- */
+aprb_status aprb_sample_image(const aprb_apr *a, const uint16_t *img, uint16_t *parts);
+aprb_status aprb_sample_image_device(const aprb_apr *a, const uint16_t *img_dev, uint16_t *parts_dev, void *stream);
+
+/* --- APR tree: APR::initialize_tree_dense (APR.hpp:633-689) ---------------------- */
+aprb_status aprb_apr_init_tree(aprb_apr *a);
+aprb_status aprb_apr_export_tree(aprb_apr *a, uint64_t *level_xz, uint64_t *xz_end, uint16_t *y_vec);
+/* APRTreeNumerics::fill_tree_mean (APRTreeNumerics.hpp:63-203) */
+aprb_status aprb_fill_tree_mean(aprb_apr *a, const float *parts, float *tree);
+aprb_status aprb_fill_tree_mean_device(aprb_apr *a, const float *parts_dev, float *tree_dev, void *stream);
+
+/* --- APR isotropic convolution --------------------------------------------------
+ * APRFilter::convolve_pencil(apr, stencil, in, out, reflect, use_stencil_downsample, normalize)
+ * (APRFilter.hpp:139-149, :1094-1216), and the GPU isotropic_convolve_333/555
+ * (APRIsoConvGPU333.hpp:37-51, APRIsoConvGPU555.hpp:38-52) which it replaces.
+ * stencil: ksize^3 floats in PixelData order; ksize 3 or 5.  Every level,
+ * l_min included, is filtered (the CPU semantics). */
+aprb_status aprb_convolve(aprb_apr *a, const float *stencil, int ksize, const float *in, float *out, int reflect,
+                          int use_stencil_downsample, int normalize);
+aprb_status aprb_convolve_device(aprb_apr *a, const float *stencil, int ksize, const float *in_dev, float *out_dev,
+                                 int reflect, int use_stencil_downsample, int normalize, void *stream);
+
+/* --- APR Richardson-Lucy --------------------------------------------------------
+ * APRNumerics::richardson_lucy (APRNumerics.hpp:576-593) /
+ * APRNumericsGPU::richardson_lucy (APRNumericsGPU.hpp:105-108).  psf: ksize^3
+ * floats; out holds the estimate (read as the start value when resume). */
+aprb_status aprb_richardson_lucy(aprb_apr *a, const uint16_t *in, float *out, const float *psf, int ksize, int niter,
+                                 int use_stencil_downsample, int normalize, int resume);
+aprb_status aprb_richardson_lucy_device(aprb_apr *a, const uint16_t *in_dev, float *out_dev, const float *psf,
+                                        int ksize, int niter, int use_stencil_downsample, int normalize, int resume,
+                                        void *stream);
+
+/* --- synthetic data (benchmark inputs; no reference counterpart) ----------------
+ * Background + n_blobs isotropic Gaussians (centre uniform, sigma and peak
+ * uniform in the given ranges) + Poisson noise, rounded and clipped to
+ * uint16, written to a device buffer of y*x*z elements. Deterministic for a
+ * seed. */
+aprb_status aprb_synth_blobs_u16(uint16_t *img_dev, int y_num, int x_num, int z_num, int n_blobs, float sigma_lo,
+                                 float sigma_hi, float amp_lo, float amp_hi, float background, uint64_t seed,
+                                 void *stream);
+
+/* number of kernel launches this thread issued through the library so far */
+uint64_t aprb_kernel_launch_count(void);
+
+/* --- stage timing (the reference's APRTimer stages, APRConverter.hpp:61-65,
+ * measured with CUDA events on the launching stream) -------------------------
+ * When enabled, every pipeline stage records an event pair on its stream.
+ * aprb_profile_read waits for the recorded events and returns, per stage
+ * name (in first-seen order), the summed device milliseconds and the number
+ * of recordings; it returns the number of stages (at most max). */
+aprb_status aprb_profile_enable(int on);
+aprb_status aprb_profile_reset(void);
+int aprb_profile_read(const char **names, double *ms, uint64_t *count, int max);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,369 @@
+"""libapr_b200 -- B200-native APR construction and filtering.
+
+Python mirror of LibAPR's interface for the hot path, over the C ABI of
+libaprb200.so (include/aprb200.h):
+
+* ``APRParameters``            -- src/algorithm/APRParameters.hpp:11-50
+* ``APRConverter(image_type)`` -- src/algorithm/APRConverter.hpp:35-134;
+  ``get_apr(apr, img)`` returns False on a failed dimension check and raises
+  ``ValueError`` on uint16 smoothing overflow (the reference throws
+  std::invalid_argument, ComputeGradient.hpp:409-412)
+* ``APR``                      -- src/data_structures/APR/APR.hpp (linear access)
+* ``ParticleData``             -- sample_image (ParticleData.hpp:123-127)
+* ``APRTreeNumerics.fill_tree_mean`` (APRTreeNumerics.hpp:63-203)
+* ``APRFilter.convolve_pencil`` (APRFilter.hpp:139-149) and
+  ``isotropic_convolve_333/555`` (APRIsoConvGPU333/555.hpp)
+* ``APRNumerics.richardson_lucy`` (APRNumerics.hpp:576-593); stencils other
+  than 3^3 / 5^3 raise RuntimeError as in APRNumericsGPU.cu:201-203
+* ``APRStencil.create_gaussian_filter`` (APRStencil.hpp:174-228)
+
+Images are numpy arrays of shape (z, x, y) (C order, y fastest: the
+reference's PixelData order) on the host, or CUDA tensors of the same layout
+(torch) for the device entry points.  All computation runs on the GPU; there
+is no CPU fallback.
+"""
+import ctypes as C
+import math
+
+import numpy as np
+
+from . import _lib
+from ._lib import APRBError, check, lib
+
+__all__ = ["APRParameters", "APRConverter", "APR", "ParticleData", "APRFilter", "APRNumerics", "APRTreeNumerics",
+           "APRStencil", "APRBError", "isotropic_convolve_333", "isotropic_convolve_555"]
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data)
+
+
+def _dptr(t):
+    """Device pointer of a CUDA tensor-like object (torch.Tensor)."""
+    return C.c_void_p(int(t.data_ptr()))
+
+
+def _stream(stream):
+    if stream is None:
+        return None
+    return C.c_void_p(int(getattr(stream, "cuda_stream", stream)))
+
+
+class APRParameters:
+    """APRParameters (src/algorithm/APRParameters.hpp:11-50).  ``lambda`` is a
+    Python keyword: use ``par.lambda_`` or ``setattr(par, 'lambda', v)``."""
+
+    _FIELDS = ("dx", "dy", "dz", "psfx", "psfy", "psfz", "Ip_th", "lambda_", "rel_error", "sigma_th",
+               "sigma_th_max", "grad_th", "reflect_bc_lis", "neighborhood_optimization", "constant_intensity_scale",
+               "check_input", "swap_dimensions")
+
+    def __init__(self, **kw):
+        p = _lib.aprb_params()
+        lib().aprb_default_params(C.byref(p))
+        for f in self._FIELDS:
+            v = getattr(p, f)
+            object.__setattr__(self, f, bool(v) if f in ("reflect_bc_lis", "neighborhood_optimization",
+                                                           "constant_intensity_scale", "check_input",
+                                                           "swap_dimensions") else float(v))
+        for k, v in kw.items():
+            setattr(self, k, v)
+
+    def __setattr__(self, k, v):
+        if k == "lambda":
+            k = "lambda_"
+        if k not in self._FIELDS:
+            raise AttributeError("APRParameters has no field %r" % k)
+        object.__setattr__(self, k, v)
+
+    def __getattr__(self, k):
+        if k == "lambda":
+            return self.lambda_
+        raise AttributeError(k)
+
+    def c(self):
+        p = _lib.aprb_params()
+        for f in self._FIELDS:
+            setattr(p, f, getattr(self, f))
+        return p
+
+
+class APR:
+    """An APR: the linear access structure, resident on the GPU."""
+
+    def __init__(self):
+        self._h = None
+        self._info = None
+
+    def _set(self, h):
+        self._free()
+        self._h = C.c_void_p(h) if not isinstance(h, C.c_void_p) else h
+        self._info = None
+
+    def _free(self):
+        if self._h is not None and self._h.value:
+            lib().aprb_apr_free(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self._free()
+        except Exception:
+            pass
+
+    @classmethod
+    def from_arrays(cls, shape_zxy, level_xz, xz_end, y_vec):
+        z, x, y = shape_zxy
+        lx = np.ascontiguousarray(level_xz, np.uint64)
+        xe = np.ascontiguousarray(xz_end, np.uint64)
+        yv = np.ascontiguousarray(y_vec, np.uint16)
+        h = C.c_void_p()
+        check(lib().aprb_apr_from_arrays(y, x, z, _ptr(lx), len(lx), _ptr(xe), len(xe),
+                                         _ptr(yv) if len(yv) else None, int(xe[-1]), C.byref(h)))
+        a = cls()
+        a._set(h)
+        return a
+
+    def info(self):
+        if self._info is None or not self._info.tree_n_xz:
+            i = _lib.aprb_apr_info()
+            check(lib().aprb_apr_get_info(self._h, C.byref(i)))
+            self._info = i
+        return self._info
+
+    def level_min(self):
+        return self.info().l_min
+
+    def level_max(self):
+        return self.info().l_max
+
+    def total_number_particles(self):
+        return int(self.info().total_number_particles)
+
+    def org_dims(self, d):
+        return self.info().org_dims[d]
+
+    def y_num(self, l):
+        return self.info().y_num[l]
+
+    def x_num(self, l):
+        return self.info().x_num[l]
+
+    def z_num(self, l):
+        return self.info().z_num[l]
+
+    def bspline_offset(self):
+        return float(self.info().bspline_offset)
+
+    def linear_access(self):
+        """(level_xz, xz_end, y_vec) numpy copies of LinearAccess (LinearAccess.hpp:33-35)."""
+        i = self.info()
+        lx = np.zeros(i.n_level_xz, np.uint64)
+        xe = np.zeros(i.n_xz, np.uint64)
+        yv = np.zeros(max(i.total_number_particles, 1), np.uint16)
+        check(lib().aprb_apr_export(self._h, _ptr(lx), _ptr(xe), _ptr(yv)))
+        return lx, xe, yv[: i.total_number_particles]
+
+    def init_tree(self):
+        check(lib().aprb_apr_init_tree(self._h))
+        self._info = None
+
+    def tree_access(self):
+        self.init_tree()
+        i = self.info()
+        lx = np.zeros(i.tree_n_level_xz, np.uint64)
+        xe = np.zeros(i.tree_n_xz, np.uint64)
+        yv = np.zeros(max(i.tree_total_number_particles, 1), np.uint16)
+        check(lib().aprb_apr_export_tree(self._h, _ptr(lx), _ptr(xe), _ptr(yv)))
+        return lx, xe, yv[: i.tree_total_number_particles]
+
+    def total_number_tree_particles(self):
+        self.init_tree()
+        return int(self.info().tree_total_number_particles)
+
+
+class APRConverter:
+    """APRConverter<ImageType> (src/algorithm/APRConverter.hpp:35-134)."""
+
+    def __init__(self, image_type="uint16"):
+        it = {"uint16": 1, "uint16_t": 1, np.uint16: 1, "float": 0, "float32": 0, np.float32: 0}[image_type]
+        self.image_type = it
+        self.par = APRParameters()
+        h = C.c_void_p()
+        check(lib().aprb_converter_create(it, C.byref(h)))
+        self._h = h
+        self.bspline_offset = 0.0
+
+    def __del__(self):
+        try:
+            if self._h is not None:
+                lib().aprb_converter_destroy(self._h)
+        except Exception:
+            pass
+
+    def keep_intermediates(self, keep=True):
+        check(lib().aprb_converter_keep_intermediates(self._h, int(keep)))
+
+    def _finish(self, st, h, apr):
+        if st == 2:  # dimension check failed: the reference returns false
+            return False
+        if st == 3:
+            raise ValueError(lib().aprb_last_error().decode())
+        check(st)
+        apr._set(h)
+        self.bspline_offset = apr.bspline_offset()
+        return True
+
+    def get_apr(self, apr, img):
+        """APRConverter::get_apr (APRConverter.hpp:591-600): img is a (z, x, y)
+        uint16 numpy array, or a CUDA tensor for the device path."""
+        p = self.par.c()
+        h = C.c_void_p()
+        if hasattr(img, "data_ptr"):
+            z, x, y = img.shape
+            st = lib().aprb_get_apr_device(self._h, C.byref(p), _dptr(img), y, x, z, None, C.byref(h))
+        else:
+            a = np.ascontiguousarray(img, np.uint16)
+            z, x, y = a.shape
+            st = lib().aprb_get_apr(self._h, C.byref(p), _ptr(a), y, x, z, C.byref(h))
+        return self._finish(st, h, apr)
+
+    def intermediate(self, stage, shape_zxy):
+        """Copy of one APRB_STAGE_* buffer of the last get_apr (needs keep_intermediates)."""
+        out = np.zeros(shape_zxy, np.float32)
+        check(lib().aprb_converter_intermediate(self._h, int(stage), _ptr(out), out.size))
+        return out
+
+
+class ParticleData:
+    """ParticleData<T> (ParticleData.hpp:26-218): ``data`` is a numpy array."""
+
+    def __init__(self, data=None):
+        self.data = data
+
+    def __len__(self):
+        return 0 if self.data is None else len(self.data)
+
+    def sample_image(self, apr, img):
+        a = np.ascontiguousarray(img, np.uint16)
+        out = np.zeros(max(apr.total_number_particles(), 1), np.uint16)
+        check(lib().aprb_sample_image(apr._h, _ptr(a), _ptr(out)))
+        self.data = out[: apr.total_number_particles()]
+        return self
+
+
+class APRTreeNumerics:
+    @staticmethod
+    def fill_tree_mean(apr, particle_data, tree_data=None):
+        parts = np.ascontiguousarray(getattr(particle_data, "data", particle_data), np.float32)
+        apr.init_tree()
+        out = np.zeros(max(apr.total_number_tree_particles(), 1), np.float32)
+        check(lib().aprb_fill_tree_mean(apr._h, _ptr(parts), _ptr(out)))
+        res = out[: apr.total_number_tree_particles()]
+        if tree_data is not None:
+            tree_data.data = res
+        return res
+
+
+class APRFilter:
+    @staticmethod
+    def convolve_pencil(apr, stencil, particle_input, particle_output=None, reflect_boundary=True,
+                        use_stencil_downsample=True, normalize=False):
+        st = np.ascontiguousarray(stencil, np.float32).ravel()
+        ks = int(round(st.size ** (1.0 / 3.0)))
+        if ks ** 3 != st.size:
+            raise ValueError("stencil must be cubic")
+        parts = np.ascontiguousarray(getattr(particle_input, "data", particle_input), np.float32)
+        out = np.zeros(max(len(parts), 1), np.float32)
+        st_ = lib().aprb_convolve(apr._h, _ptr(st), ks, _ptr(parts), _ptr(out), int(reflect_boundary),
+                                  int(use_stencil_downsample), int(normalize))
+        check(st_)
+        res = out[: len(parts)]
+        if particle_output is not None:
+            particle_output.data = res
+        return res
+
+    convolve = convolve_pencil
+
+
+def isotropic_convolve_333(apr, particle_input, stencil, reflective_bc=True, use_stencil_downsample=True,
+                           normalize_stencil=False):
+    """isotropic_convolve_333 (APRIsoConvGPU333.hpp:37-51); unlike the reference
+    GPU kernel the coarsest level l_min is filtered too (the CPU semantics)."""
+    st = np.asarray(stencil, np.float32)
+    if st.size != 27:
+        raise ValueError("isotropic_convolve_333 needs a 3x3x3 stencil")
+    return APRFilter.convolve_pencil(apr, st, particle_input, None, reflective_bc, use_stencil_downsample,
+                                     normalize_stencil)
+
+
+def isotropic_convolve_555(apr, particle_input, stencil, reflective_bc=True, use_stencil_downsample=True,
+                           normalize_stencil=False):
+    st = np.asarray(stencil, np.float32)
+    if st.size != 125:
+        raise ValueError("isotropic_convolve_555 needs a 5x5x5 stencil")
+    return APRFilter.convolve_pencil(apr, st, particle_input, None, reflective_bc, use_stencil_downsample,
+                                     normalize_stencil)
+
+
+class APRNumerics:
+    @staticmethod
+    def richardson_lucy(apr, particle_input, particle_output, psf, number_iterations, use_stencil_downsample=True,
+                        normalize=False, resume=False):
+        st = np.ascontiguousarray(psf, np.float32).ravel()
+        ks = int(round(st.size ** (1.0 / 3.0)))
+        if ks ** 3 != st.size or ks not in (3, 5):
+            raise RuntimeError("APR RL: stencil side must be 3 or 5")
+        parts = np.ascontiguousarray(getattr(particle_input, "data", particle_input), np.uint16)
+        n = len(parts)
+        if resume and getattr(particle_output, "data", None) is not None:
+            out = np.ascontiguousarray(particle_output.data, np.float32).copy()
+        else:
+            out = np.zeros(max(n, 1), np.float32)
+        out = np.resize(out, max(n, 1)).astype(np.float32)
+        check(lib().aprb_richardson_lucy(apr._h, _ptr(parts), _ptr(out), _ptr(st), ks, int(number_iterations),
+                                         int(use_stencil_downsample), int(normalize), int(resume)))
+        res = out[:n]
+        if particle_output is not None:
+            particle_output.data = res
+        return res
+
+
+class APRStencil:
+    @staticmethod
+    def create_gaussian_filter(sigma=(1.0, 1.0, 1.0), size=(5, 5, 5), normalize=True):
+        """APRStencil::create_gaussian_filter<float> (APRStencil.hpp:174-228),
+        float arithmetic as the reference (expf, sqrtf of 2*pi)."""
+        f32 = np.float32
+
+        def g1(s, n):
+            if n <= 1:
+                return np.ones(1, f32)
+            i = np.arange(-(n // 2), n // 2 + 1)
+            num = np.exp((-(i * i) / (2 * f32(s) * f32(s))).astype(f32)).astype(f32)
+            den = f32(s) * f32(math.sqrt(np.float32(2 * math.pi)))
+            return (num / den).astype(f32)
+
+        gy, gx, gz = g1(sigma[0], size[0]), g1(sigma[1], size[1]), g1(sigma[2], size[2])
+        st = np.zeros((size[2], size[1], size[0]), f32)
+        s = f32(0)
+        for i in range(size[0]):
+            for j in range(size[1]):
+                for k in range(size[2]):
+                    v = f32(f32(gy[i] * gx[j]) * gz[k])
+                    st[k, j, i] = v
+                    s = f32(s + v)
+        if normalize:
+            st = (st / s).astype(f32)
+        return st
+
+
+def kernel_launch_count():
+    return int(lib().aprb_kernel_launch_count())
+
+
+def synth_blobs_device(out_tensor, n_blobs, sigma=(2.0, 6.0), amp=(800.0, 4000.0), background=100.0, seed=0,
+                       stream=None):
+    """Fills a (z, x, y) uint16 CUDA tensor with the seeded blob + Poisson model."""
+    z, x, y = out_tensor.shape
+    check(lib().aprb_synth_blobs_u16(_dptr(out_tensor), y, x, z, int(n_blobs), sigma[0], sigma[1], amp[0], amp[1],
+                                     background, int(seed), _stream(stream)))

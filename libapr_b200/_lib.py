@@ -1,0 +1,96 @@
+"""ctypes binding of libaprb200.so (the C ABI declared in include/aprb200.h).
+
+The library is built in-tree by libapr_b200/build.py.  There is no fallback:
+importing this module raises if the CUDA library is missing, and every call
+that fails returns its aprb_status, which the Python layer turns into an
+exception.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libaprb200.so")
+
+APRB_OK = 0
+STATUS = {
+    0: "ok", 1: "invalid argument", 2: "input dimension check failed", 3: "integer overflow",
+    4: "unsupported", 5: "out of memory", 6: "CUDA error", 7: "no sm_100 device", 8: "incomplete neighbourhood",
+}
+
+
+class aprb_params(C.Structure):
+    _fields_ = [(n, C.c_float) for n in ("dx", "dy", "dz", "psfx", "psfy", "psfz", "Ip_th", "lambda_", "rel_error",
+                                         "sigma_th", "sigma_th_max", "grad_th")] + \
+               [(n, C.c_int) for n in ("reflect_bc_lis", "neighborhood_optimization", "constant_intensity_scale",
+                                       "check_input", "swap_dimensions")]
+
+
+class aprb_apr_info(C.Structure):
+    _fields_ = [("l_min", C.c_int), ("l_max", C.c_int), ("org_dims", C.c_int * 3),
+                ("y_num", C.c_int * 32), ("x_num", C.c_int * 32), ("z_num", C.c_int * 32),
+                ("total_number_particles", C.c_uint64), ("n_level_xz", C.c_uint64), ("n_xz", C.c_uint64),
+                ("bspline_offset", C.c_float),
+                ("tree_l_min", C.c_int), ("tree_l_max", C.c_int), ("tree_total_number_particles", C.c_uint64),
+                ("tree_n_level_xz", C.c_uint64), ("tree_n_xz", C.c_uint64)]
+
+
+# Every exported entry point and its C signature (include/aprb200.h).
+_vp, _u64, _i, _f = C.c_void_p, C.c_uint64, C.c_int, C.c_float
+SIGNATURES = {
+    "aprb_status_string": ([C.c_int], C.c_char_p),
+    "aprb_last_error": ([], C.c_char_p),
+    "aprb_default_params": ([C.POINTER(aprb_params)], None),
+    "aprb_converter_create": ([_i, C.POINTER(_vp)], _i),
+    "aprb_converter_destroy": ([_vp], _i),
+    "aprb_converter_keep_intermediates": ([_vp, _i], _i),
+    "aprb_get_apr": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, C.POINTER(_vp)], _i),
+    "aprb_get_apr_device": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, _vp, C.POINTER(_vp)], _i),
+    "aprb_converter_intermediate": ([_vp, _i, _vp, C.c_size_t], _i),
+    "aprb_apr_free": ([_vp], _i),
+    "aprb_apr_get_info": ([_vp, C.POINTER(aprb_apr_info)], _i),
+    "aprb_apr_export": ([_vp, _vp, _vp, _vp], _i),
+    "aprb_apr_device_arrays": ([_vp, _vp, _vp, _vp], _i),
+    "aprb_apr_from_arrays": ([_i, _i, _i, _vp, _u64, _vp, _u64, _vp, _u64, C.POINTER(_vp)], _i),
+    "aprb_sample_image": ([_vp, _vp, _vp], _i),
+    "aprb_sample_image_device": ([_vp, _vp, _vp, _vp], _i),
+    "aprb_apr_init_tree": ([_vp], _i),
+    "aprb_apr_export_tree": ([_vp, _vp, _vp, _vp], _i),
+    "aprb_fill_tree_mean": ([_vp, _vp, _vp], _i),
+    "aprb_fill_tree_mean_device": ([_vp, _vp, _vp, _vp], _i),
+    "aprb_convolve": ([_vp, _vp, _i, _vp, _vp, _i, _i, _i], _i),
+    "aprb_convolve_device": ([_vp, _vp, _i, _vp, _vp, _i, _i, _i, _vp], _i),
+    "aprb_richardson_lucy": ([_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i], _i),
+    "aprb_richardson_lucy_device": ([_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp], _i),
+    "aprb_synth_blobs_u16": ([_vp, _i, _i, _i, _i, _f, _f, _f, _f, _f, _u64, _vp], _i),
+    "aprb_kernel_launch_count": ([], _u64),
+    "aprb_profile_enable": ([_i], _i),
+    "aprb_profile_reset": ([], _i),
+    "aprb_profile_read": ([C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_uint64), _i], _i),
+}
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libaprb200.so is not built (run libapr_b200/build.py or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+class APRBError(RuntimeError):
+    def __init__(self, status, detail):
+        super().__init__("%s: %s" % (STATUS.get(status, status), detail))
+        self.status = status
+
+
+def check(status):
+    if status != APRB_OK:
+        raise APRBError(status, lib().aprb_last_error().decode())

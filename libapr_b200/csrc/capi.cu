@@ -1,0 +1,735 @@
+// C ABI of libaprb200 (include/aprb200.h): handle management, host<->device
+// staging and the stage order of APRConverter::get_apr_cpu
+// (APRConverter.hpp:535-582).  No exception crosses the ABI: every entry
+// point returns an aprb_status.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace aprb {
+
+static thread_local std::string g_last_error;
+static thread_local uint64_t g_launches = 0;
+
+void set_error(const std::string &msg) { g_last_error = msg; }
+void count_launch(uint64_t n) { g_launches += n; }
+
+struct ProfRec {
+    const char *name;
+    cudaEvent_t a, b;
+};
+static thread_local bool g_prof_on = false;
+static thread_local std::vector<ProfRec> g_prof;
+static thread_local std::vector<size_t> g_prof_open;
+
+void prof_record(const char *name, cudaStream_t s, bool begin) {
+    if (!g_prof_on) return;
+    if (begin) {
+        ProfRec r{name, nullptr, nullptr};
+        cudaEventCreate(&r.a);
+        cudaEventCreate(&r.b);
+        cudaEventRecord(r.a, s);
+        g_prof.push_back(r);
+        g_prof_open.push_back(g_prof.size() - 1);
+    } else {
+        if (g_prof_open.empty()) return;
+        const size_t i = g_prof_open.back();
+        g_prof_open.pop_back();
+        cudaEventRecord(g_prof[i].b, s);
+    }
+}
+
+static void require_device() {
+    static int ok = -1;
+    if (ok < 0) {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+            cudaGetLastError();
+            ok = 0;
+        } else {
+            int dev = 0, major = 0;
+            cudaGetDevice(&dev);
+            cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+            ok = major == 10 ? 1 : 0;
+        }
+    }
+    if (!ok) {
+        set_error("no sm_100 CUDA device available");
+        throw Error{APRB_ERR_NO_DEVICE};
+    }
+}
+
+#define ARG_CHECK(cond, msg)                         \
+    do {                                             \
+        if (!(cond)) {                               \
+            set_error(msg);                          \
+            throw Error{APRB_ERR_INVALID_ARGUMENT};  \
+        }                                            \
+    } while (0)
+
+template <typename F>
+static aprb_status guarded(F &&f) {
+    try {
+        f();
+        return APRB_OK;
+    } catch (const Error &e) {
+        return e.status;
+    } catch (const std::bad_alloc &) {
+        set_error("host allocation failed");
+        return APRB_ERR_OUT_OF_MEMORY;
+    } catch (...) {
+        set_error("unexpected exception");
+        return APRB_ERR_CUDA;
+    }
+}
+
+}  // namespace aprb
+
+using namespace aprb;
+
+struct aprb_apr {
+    Geom g{};
+    int org[3] = {0, 0, 0};
+    uint64_t n_xz = 0, P = 0;
+    float offset = 0;
+    DevBuf xz_end, y_vec, level_xz;
+    // tree
+    bool tree_built = false;
+    Geom tg{};
+    uint64_t t_n_xz = 0, T = 0;
+    DevBuf t_xz_end, t_y_vec, t_flags;
+    // filter work
+    DevBuf scan_tmp, tree_vals, pyr, parts_f, parts_u16, out_f, rb, stencils, stencils_f, io_in, io_out;
+    FilterBuffers fb;
+    uint64_t last_stale = 0;
+};
+
+struct aprb_converter {
+    int image_type = APRB_IMAGE_U16;
+    int keep = 0;
+    int dims[3] = {0, 0, 0};  // y, x, z of the last call
+    DevBuf img, work, grad, grad_keep, ids_raw, ids, lis, lis_keep, pyr_status, pyr_level, mm, offset, err;
+    DevBuf scan_tmp;
+    LisBuffers lisb;
+    bool have = false;
+};
+
+extern "C" {
+
+const char *aprb_status_string(aprb_status s) {
+    switch (s) {
+        case APRB_OK: return "ok";
+        case APRB_ERR_INVALID_ARGUMENT: return "invalid argument";
+        case APRB_ERR_DIMENSIONS: return "input dimension check failed";
+        case APRB_ERR_INTEGER_OVERFLOW: return "integer under-/overflow in the B-spline smoothing";
+        case APRB_ERR_UNSUPPORTED: return "unsupported configuration";
+        case APRB_ERR_OUT_OF_MEMORY: return "out of memory";
+        case APRB_ERR_CUDA: return "CUDA error";
+        case APRB_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+        case APRB_ERR_INCOMPLETE_NEIGHBOURHOOD: return "filter neighbourhood not covered by particles";
+    }
+    return "unknown status";
+}
+
+const char *aprb_last_error(void) { return g_last_error.c_str(); }
+uint64_t aprb_kernel_launch_count(void) { return g_launches; }
+
+aprb_status aprb_profile_enable(int on) {
+    g_prof_on = on != 0;
+    return APRB_OK;
+}
+
+aprb_status aprb_profile_reset(void) {
+    for (auto &r : g_prof) {
+        cudaEventSynchronize(r.b);
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    g_prof.clear();
+    g_prof_open.clear();
+    return APRB_OK;
+}
+
+int aprb_profile_read(const char **names, double *ms, uint64_t *count, int max) {
+    std::vector<const char *> order;
+    std::vector<double> tot;
+    std::vector<uint64_t> cnt;
+    for (auto &r : g_prof) {
+        cudaEventSynchronize(r.b);
+        float t = 0;
+        if (cudaEventElapsedTime(&t, r.a, r.b) != cudaSuccess) {
+            cudaGetLastError();
+            t = 0;
+        }
+        size_t j = 0;
+        while (j < order.size() && std::strcmp(order[j], r.name) != 0) ++j;
+        if (j == order.size()) {
+            order.push_back(r.name);
+            tot.push_back(0);
+            cnt.push_back(0);
+        }
+        tot[j] += t;
+        cnt[j] += 1;
+    }
+    int n = (int)order.size() < max ? (int)order.size() : max;
+    for (int i = 0; i < n; ++i) {
+        if (names) names[i] = order[i];
+        if (ms) ms[i] = tot[i];
+        if (count) count[i] = cnt[i];
+    }
+    return n;
+}
+
+void aprb_default_params(aprb_params *p) {
+    if (!p) return;
+    std::memset(p, 0, sizeof(*p));
+    p->dx = p->dy = p->dz = 1;
+    p->psfx = p->psfy = p->psfz = 2;
+    p->Ip_th = 0;
+    p->lambda = 3.0f;
+    p->rel_error = 0.1f;
+    p->sigma_th = 0;
+    p->sigma_th_max = 0;
+    p->grad_th = 0;
+    p->reflect_bc_lis = 1;
+    p->neighborhood_optimization = 1;
+    p->constant_intensity_scale = 0;
+    p->check_input = 0;
+    p->swap_dimensions = 0;
+}
+
+aprb_status aprb_converter_create(int image_type, aprb_converter **out) {
+    return guarded([&] {
+        ARG_CHECK(out, "null output pointer");
+        ARG_CHECK(image_type == APRB_IMAGE_U16 || image_type == APRB_IMAGE_FLOAT, "image_type must be 0 or 1");
+        auto *c = new aprb_converter();
+        c->image_type = image_type;
+        *out = c;
+    });
+}
+
+aprb_status aprb_converter_destroy(aprb_converter *c) {
+    delete c;
+    return APRB_OK;
+}
+
+aprb_status aprb_converter_keep_intermediates(aprb_converter *c, int keep) {
+    return guarded([&] {
+        ARG_CHECK(c, "null converter");
+        c->keep = keep != 0;
+    });
+}
+
+}  // extern "C"
+
+namespace {
+
+// APRConverter::check_input_dimensions (APRConverter.hpp:606-640)
+bool check_dims(const aprb_params &p, int &y, int &x, int &z) {
+    const int nd = (x > 1) + (y > 1) + (z > 1);
+    if (nd == 0) return false;
+    if (nd == 3) return true;
+    if (y > 1) return true;
+    if (p.swap_dimensions) {
+        if (x > 1)
+            std::swap(x, y);
+        else
+            std::swap(z, y);
+        return true;
+    }
+    return false;
+}
+
+template <typename IT>
+void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, int yn, int xn, int zn,
+                 cudaStream_t s, aprb_apr *a) {
+    Geom &g = a->g;
+    a->n_xz = apr_geometry(yn, xn, zn, g);
+    a->org[0] = yn;
+    a->org[1] = xn;
+    a->org[2] = zn;
+    const int L = g.l_max;
+    const int yd = (yn + 1) / 2, xd = (xn + 1) / 2, zd = (zn + 1) / 2;
+    const uint64_t n = (uint64_t)yn * xn * zn, nd = (uint64_t)yd * xd * zd;
+    const bool is_u16 = sizeof(IT) == 2;
+
+    unsigned *mm = c->mm.as<unsigned>(2);
+    float *d_off = c->offset.as<float>(1);
+    unsigned *d_err = c->err.as<unsigned>(1);
+    APRB_CUDA(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
+    launch_minmax_offset(img, n, mm, d_off, is_u16 && p.lambda > 0, s);
+
+    IT *work = c->work.as<IT>(n);
+    launch_smooth<IT>(img, work, yn, xn, zn, p.lambda, d_off, d_err, s);
+
+    IT *grad = c->grad.as<IT>(nd);
+    float *ids_raw = c->ids_raw.as<float>(nd);
+    float *ids = c->ids.as<float>(nd);
+    launch_gradient<IT>(work, yn, xn, zn, grad, ids_raw, ids, yd, xd, zd, p, s);
+
+    float *lis = c->lis.as<float>(nd);
+    launch_local_intensity_scale(ids, lis, yd, xd, zd, p, c->lisb, s);
+    if (c->keep) {
+        APRB_CUDA(cudaMemcpyAsync(c->grad_keep.as<IT>(nd), grad, nd * sizeof(IT), cudaMemcpyDeviceToDevice, s));
+        APRB_CUDA(cudaMemcpyAsync(c->lis_keep.as<float>(nd), lis, nd * sizeof(float), cudaMemcpyDeviceToDevice, s));
+    }
+
+    // particle-cell pyramid: pct levels l_min..L-1 (PullingScheme.hpp:92-104)
+    Pyramid pm;
+    const int top = L - 1;
+    uint64_t tot = 0, off[32] = {};
+    for (int l = g.l_min; l <= top; ++l) {
+        off[l] = tot;
+        tot += ((uint64_t)g.y_num[l] * g.x_num[l] * g.z_num[l] + 15) & ~uint64_t(15);
+    }
+    uint8_t *st = c->pyr_status.as<uint8_t>(tot ? tot : 16);
+    uint8_t *lv = c->pyr_level.as<uint8_t>(tot ? tot : 16);
+    for (int l = g.l_min; l <= top; ++l) {
+        pm.status[l] = st + off[l];
+        pm.level[l] = lv + off[l];
+    }
+    uint8_t scratch_status_dummy = 0;
+    (void)scratch_status_dummy;
+    if (top >= g.l_min) {
+        launch_levels<IT>(grad, lis, ids, nd, d_off, p, L, top, pm.level[top], pm.status[top], c->keep, s);
+    } else {
+        uint8_t *lvl = c->pyr_level.as<uint8_t>(nd), *sts = c->pyr_status.as<uint8_t>(nd);
+        launch_levels<IT>(grad, lis, ids, nd, d_off, p, L, top, lvl, sts, c->keep, s);
+    }
+
+    uint64_t *xz_end = a->xz_end.as<uint64_t>(a->n_xz);
+    const int min_type = p.neighborhood_optimization ? 1 : 2;
+    unsigned h_err = 0;
+    if (L <= 2) {
+        APRB_CUDA(cudaMemsetAsync(xz_end, 0, a->n_xz * sizeof(uint64_t), s));
+        launch_full_resolution_structure(g, xz_end, nullptr, s);
+        a->P = (uint64_t)g.y_num[L] * g.x_num[L] * g.z_num[L];
+        APRB_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaStreamSynchronize(s));
+        if (h_err) {
+            set_error("integer under-/overflow encountered in the B-spline smoothing");
+            throw Error{APRB_ERR_INTEGER_OVERFLOW};
+        }
+        uint16_t *yv = a->y_vec.as<uint16_t>(a->P);
+        launch_full_resolution_structure(g, xz_end, yv, s);
+    } else {
+        launch_pulling_scheme(g, pm, s);
+        APRB_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        a->P = launch_linear_counts(g, pm, xz_end, a->n_xz, min_type, c->scan_tmp, s);
+        if (h_err) {
+            set_error("integer under-/overflow encountered in the B-spline smoothing");
+            throw Error{APRB_ERR_INTEGER_OVERFLOW};
+        }
+        uint16_t *yv = a->y_vec.as<uint16_t>(a->P ? a->P : 1);
+        launch_linear_fill(g, pm, xz_end, yv, min_type, s);
+    }
+    APRB_CUDA(cudaMemcpyAsync(&a->offset, d_off, sizeof(float), cudaMemcpyDeviceToHost, s));
+    APRB_CUDA(cudaStreamSynchronize(s));
+    c->dims[0] = yn;
+    c->dims[1] = xn;
+    c->dims[2] = zn;
+    c->have = true;
+}
+
+void get_apr_impl(aprb_converter *c, const aprb_params *p, const uint16_t *img_dev, int y, int x, int z,
+                  cudaStream_t s, aprb_apr **out) {
+    require_device();
+    ARG_CHECK(c && p && img_dev && out, "null argument");
+    ARG_CHECK(y >= 1 && x >= 1 && z >= 1, "dimensions must be positive");
+    ARG_CHECK(y <= 65535 && x <= 65535 && z <= 65535, "each dimension must fit the uint16 coordinates");
+    aprb_params par = *p;
+    if (par.check_input && !check_dims(par, y, x, z)) {
+        set_error("Input dimension check failed");
+        throw Error{APRB_ERR_DIMENSIONS};
+    }
+    ARG_CHECK(par.rel_error > 0, "rel_error must be positive");
+    std::unique_ptr<aprb_apr> a(new aprb_apr());
+    if (c->image_type == APRB_IMAGE_U16)
+        run_get_apr<uint16_t>(c, par, img_dev, y, x, z, s, a.get());
+    else
+        run_get_apr<float>(c, par, img_dev, y, x, z, s, a.get());
+    *out = a.release();
+}
+
+}  // namespace
+
+extern "C" {
+
+aprb_status aprb_get_apr_device(aprb_converter *c, const aprb_params *p, const uint16_t *img_dev, int y_num,
+                                int x_num, int z_num, void *stream, aprb_apr **out) {
+    return guarded([&] { get_apr_impl(c, p, img_dev, y_num, x_num, z_num, (cudaStream_t)stream, out); });
+}
+
+aprb_status aprb_get_apr(aprb_converter *c, const aprb_params *p, const uint16_t *img, int y_num, int x_num,
+                         int z_num, aprb_apr **out) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(c && img, "null argument");
+        const uint64_t n = (uint64_t)y_num * x_num * z_num;
+        cudaStream_t s = cudaStreamPerThread;
+        uint16_t *d = c->img.as<uint16_t>(n);
+        APRB_CUDA(cudaMemcpyAsync(d, img, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+        get_apr_impl(c, p, d, y_num, x_num, z_num, s, out);
+    });
+}
+
+aprb_status aprb_converter_intermediate(const aprb_converter *c, int stage, float *dst, size_t n) {
+    return guarded([&] {
+        ARG_CHECK(c && dst, "null argument");
+        ARG_CHECK(c->have && c->keep, "no intermediates kept (enable aprb_converter_keep_intermediates first)");
+        const int y = c->dims[0], x = c->dims[1], z = c->dims[2];
+        const uint64_t full = (uint64_t)y * x * z;
+        const uint64_t nd = (uint64_t)((y + 1) / 2) * ((x + 1) / 2) * ((z + 1) / 2);
+        const bool u16 = c->image_type == APRB_IMAGE_U16;
+        const void *src = nullptr;
+        int kind = 0;  // 0 IT, 1 float, 2 uint8
+        uint64_t cnt = nd;
+        switch (stage) {
+            case APRB_STAGE_SMOOTHED: src = c->work.p; cnt = full; kind = 0; break;
+            case APRB_STAGE_GRADIENT: src = c->grad_keep.p; kind = 0; break;
+            case APRB_STAGE_DS_IMAGE: src = c->ids.p; kind = 1; break;
+            case APRB_STAGE_LOCAL_SCALE: src = c->lis_keep.p; kind = 1; break;
+            case APRB_STAGE_GRADIENT_APPLIED: src = c->grad.p; kind = 0; break;
+            case APRB_STAGE_SCALE_APPLIED: src = c->lis.p; kind = 1; break;
+            case APRB_STAGE_LEVELS: {
+                Geom g;
+                apr_geometry(y, x, z, g);
+                const int top = g.l_max - 1;
+                uint64_t o = 0;
+                for (int l = g.l_min; l < top; ++l) o += ((uint64_t)g.y_num[l] * g.x_num[l] * g.z_num[l] + 15) & ~uint64_t(15);
+                src = (const uint8_t *)c->pyr_level.p + (top >= g.l_min ? o : 0);
+                kind = 2;
+                break;
+            }
+            default: ARG_CHECK(false, "unknown stage");
+        }
+        ARG_CHECK(n == cnt, "element count does not match the stage size");
+        if (kind == 1) {
+            APRB_CUDA(cudaMemcpy(dst, src, cnt * sizeof(float), cudaMemcpyDeviceToHost));
+        } else if (kind == 2) {
+            std::vector<uint8_t> h(cnt);
+            APRB_CUDA(cudaMemcpy(h.data(), src, cnt, cudaMemcpyDeviceToHost));
+            for (uint64_t i = 0; i < cnt; ++i) dst[i] = (float)h[i];
+        } else if (u16) {
+            std::vector<uint16_t> h(cnt);
+            APRB_CUDA(cudaMemcpy(h.data(), src, cnt * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+            for (uint64_t i = 0; i < cnt; ++i) dst[i] = (float)h[i];
+        } else {
+            APRB_CUDA(cudaMemcpy(dst, src, cnt * sizeof(float), cudaMemcpyDeviceToHost));
+        }
+    });
+}
+
+aprb_status aprb_apr_free(aprb_apr *a) {
+    delete a;
+    return APRB_OK;
+}
+
+aprb_status aprb_apr_get_info(const aprb_apr *a, aprb_apr_info *info) {
+    return guarded([&] {
+        ARG_CHECK(a && info, "null argument");
+        std::memset(info, 0, sizeof(*info));
+        info->l_min = a->g.l_min;
+        info->l_max = a->g.l_max;
+        for (int i = 0; i < 3; ++i) info->org_dims[i] = a->org[i];
+        for (int l = 0; l < 32; ++l) {
+            info->y_num[l] = a->g.y_num[l];
+            info->x_num[l] = a->g.x_num[l];
+            info->z_num[l] = a->g.z_num[l];
+        }
+        info->total_number_particles = a->P;
+        info->n_level_xz = (uint64_t)a->g.l_max + 2;
+        info->n_xz = a->n_xz;
+        info->bspline_offset = a->offset;
+        if (a->tree_built) {
+            info->tree_l_min = a->tg.l_min;
+            info->tree_l_max = a->tg.l_max;
+            info->tree_total_number_particles = a->T;
+            info->tree_n_level_xz = (uint64_t)a->tg.l_max + 2;
+            info->tree_n_xz = a->t_n_xz;
+        }
+    });
+}
+
+aprb_status aprb_apr_export(const aprb_apr *a, uint64_t *level_xz, uint64_t *xz_end, uint16_t *y_vec) {
+    return guarded([&] {
+        ARG_CHECK(a, "null apr");
+        if (level_xz) std::memcpy(level_xz, a->g.level_xz, sizeof(uint64_t) * (a->g.l_max + 2));
+        if (xz_end) APRB_CUDA(cudaMemcpy(xz_end, a->xz_end.p, a->n_xz * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+        if (y_vec && a->P) APRB_CUDA(cudaMemcpy(y_vec, a->y_vec.p, a->P * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+    });
+}
+
+aprb_status aprb_apr_device_arrays(const aprb_apr *a, const uint64_t **level_xz, const uint64_t **xz_end,
+                                   const uint16_t **y_vec) {
+    return guarded([&] {
+        ARG_CHECK(a, "null apr");
+        if (level_xz) *level_xz = nullptr;  // level offsets are host-side geometry (aprb_apr_export)
+        if (xz_end) *xz_end = (const uint64_t *)a->xz_end.p;
+        if (y_vec) *y_vec = (const uint16_t *)a->y_vec.p;
+    });
+}
+
+aprb_status aprb_apr_from_arrays(int y_num, int x_num, int z_num, const uint64_t *level_xz, uint64_t n_level_xz,
+                                 const uint64_t *xz_end, uint64_t n_xz, const uint16_t *y_vec, uint64_t n_particles,
+                                 aprb_apr **out) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(level_xz && xz_end && out, "null argument");
+        std::unique_ptr<aprb_apr> a(new aprb_apr());
+        a->n_xz = apr_geometry(y_num, x_num, z_num, a->g);
+        ARG_CHECK(n_level_xz == (uint64_t)a->g.l_max + 2, "level_xz length does not match the dimensions");
+        ARG_CHECK(n_xz == a->n_xz, "xz_end length does not match the dimensions");
+        for (uint64_t i = 0; i < n_level_xz; ++i)
+            ARG_CHECK(level_xz[i] == a->g.level_xz[i], "level_xz does not match the dimensions");
+        ARG_CHECK(xz_end[n_xz - 1] == n_particles, "xz_end total does not match the particle count");
+        a->org[0] = y_num;
+        a->org[1] = x_num;
+        a->org[2] = z_num;
+        a->P = n_particles;
+        APRB_CUDA(cudaMemcpy(a->xz_end.as<uint64_t>(n_xz), xz_end, n_xz * sizeof(uint64_t), cudaMemcpyHostToDevice));
+        uint16_t *yv = a->y_vec.as<uint16_t>(n_particles ? n_particles : 1);
+        if (n_particles) {
+            ARG_CHECK(y_vec, "null y_vec");
+            APRB_CUDA(cudaMemcpy(yv, y_vec, n_particles * sizeof(uint16_t), cudaMemcpyHostToDevice));
+        }
+        *out = a.release();
+    });
+}
+
+aprb_status aprb_sample_image_device(const aprb_apr *a, const uint16_t *img_dev, uint16_t *parts_dev, void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && img_dev && parts_dev, "null argument");
+        aprb_apr *m = const_cast<aprb_apr *>(a);
+        launch_sample(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, img_dev, parts_dev, m->pyr,
+                      (cudaStream_t)stream);
+    });
+}
+
+aprb_status aprb_sample_image(const aprb_apr *a, const uint16_t *img, uint16_t *parts) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && img && parts, "null argument");
+        aprb_apr *m = const_cast<aprb_apr *>(a);
+        cudaStream_t s = cudaStreamPerThread;
+        const uint64_t n = (uint64_t)a->org[0] * a->org[1] * a->org[2];
+        uint16_t *di = m->io_in.as<uint16_t>(n);
+        uint16_t *dp = m->parts_u16.as<uint16_t>(a->P ? a->P : 1);
+        APRB_CUDA(cudaMemcpyAsync(di, img, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+        launch_sample(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, di, dp, m->pyr, s);
+        if (a->P) APRB_CUDA(cudaMemcpyAsync(parts, dp, a->P * sizeof(uint16_t), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+}  // extern "C"
+
+namespace {
+
+void ensure_tree(aprb_apr *a, cudaStream_t s) {
+    if (a->tree_built) return;
+    a->t_n_xz = tree_geometry(a->org[0], a->org[1], a->org[2], a->tg);
+    uint64_t *txz = a->t_xz_end.as<uint64_t>(a->t_n_xz);
+    a->T = launch_tree_build(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg, txz,
+                             a->t_n_xz, a->t_flags, a->scan_tmp, s);
+    uint16_t *ty = a->t_y_vec.as<uint16_t>(a->T ? a->T : 1);
+    launch_tree_fill(a->tg, a->t_flags, txz, ty, s);
+    APRB_CUDA(cudaStreamSynchronize(s));
+    a->t_flags.release();
+    a->tree_built = true;
+}
+
+// stencil set of APRFilter::convolve_pencil(apr, stencil, ..., use_stencil_downsample, normalize)
+// (APRFilter.hpp:139-149): one stencil per level below l_max when downsampling
+ConvPlan make_plan(const aprb_apr *a, const float *stencil, int ks, int ds, int normalize, int reflect,
+                   std::vector<float> &host) {
+    if (ks != 3 && ks != 5) {
+        set_error("stencil side must be 3 or 5");
+        throw Error{APRB_ERR_UNSUPPORTED};
+    }
+    ConvPlan plan;
+    const int nlev = ds ? std::max(a->g.l_max - a->g.l_min, 1) : 1;
+    host = downsampled_stencils(stencil, ks, nlev, normalize != 0, plan.sides);
+    plan.nstencils = (int)plan.sides.size();
+    int o = 0;
+    for (int sd : plan.sides) {
+        plan.offsets.push_back(o);
+        o += sd * sd * sd;
+    }
+    plan.reflect = reflect != 0;
+    return plan;
+}
+
+void convolve_impl(aprb_apr *a, const float *stencil, int ks, const float *in, float *out, int reflect, int ds,
+                   int normalize, cudaStream_t s) {
+    ensure_tree(a, s);
+    std::vector<float> host;
+    ConvPlan plan = make_plan(a, stencil, ks, ds, normalize, reflect, host);
+    float *dst = a->stencils.as<float>(host.size());
+    APRB_CUDA(cudaMemcpyAsync(dst, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    float *tree = a->tree_vals.as<float>(a->T ? a->T : 1);
+    filter_apply(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
+                 (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, in, tree, &plan, dst, out, 0,
+                 nullptr, a->fb, s);
+    a->last_stale = filter_stale_count(a->fb, s);
+}
+
+__global__ void fill_kernel(float *p, uint64_t n, float v) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+void rl_impl(aprb_apr *a, const uint16_t *in, float *out, const float *psf, int ks, int niter, int ds, int normalize,
+             int resume, cudaStream_t s) {
+    ensure_tree(a, s);
+    const int n0 = ks * ks * ks;
+    std::vector<float> flipped(n0);
+    for (int i = 0; i < n0; ++i) flipped[i] = psf[n0 - 1 - i];
+    std::vector<float> hp, hf;
+    ConvPlan plan = make_plan(a, psf, ks, ds, normalize, 1, hp);
+    ConvPlan plan_f = make_plan(a, flipped.data(), ks, ds, normalize, 1, hf);
+    float *dp = a->stencils.as<float>(hp.size());
+    float *df = a->stencils_f.as<float>(hf.size());
+    APRB_CUDA(cudaMemcpyAsync(dp, hp.data(), hp.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    APRB_CUDA(cudaMemcpyAsync(df, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    if (!resume && a->P) {
+        fill_kernel<<<blocks_for(a->P, 256), 256, 0, s>>>(out, a->P, 1.0f);
+        count_launch();
+        APRB_CHECK_LAUNCH();
+    }
+    float *tree = a->tree_vals.as<float>(a->T ? a->T : 1);
+    float *rb = a->rb.as<float>(a->P ? a->P : 1);
+    const uint64_t *xz = (const uint64_t *)a->xz_end.p;
+    const uint16_t *yv = (const uint16_t *)a->y_vec.p;
+    const uint64_t *txz = (const uint64_t *)a->t_xz_end.p;
+    const uint16_t *tyv = (const uint16_t *)a->t_y_vec.p;
+    for (int it = 0; it < niter; ++it) {
+        // rb = in / conv(psf_flipped, out); out = out * conv(psf, rb)  (APRNumerics.hpp:565-570)
+        filter_apply(a->g, xz, yv, a->tg, txz, tyv, out, tree, &plan_f, df, rb, 1, in, a->fb, s);
+        filter_apply(a->g, xz, yv, a->tg, txz, tyv, rb, tree, &plan, dp, out, 2, nullptr, a->fb, s);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+aprb_status aprb_apr_init_tree(aprb_apr *a) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a, "null apr");
+        ensure_tree(a, cudaStreamPerThread);
+    });
+}
+
+aprb_status aprb_apr_export_tree(aprb_apr *a, uint64_t *level_xz, uint64_t *xz_end, uint16_t *y_vec) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a, "null apr");
+        ensure_tree(a, cudaStreamPerThread);
+        if (level_xz) std::memcpy(level_xz, a->tg.level_xz, sizeof(uint64_t) * (a->tg.l_max + 2));
+        if (xz_end) APRB_CUDA(cudaMemcpy(xz_end, a->t_xz_end.p, a->t_n_xz * sizeof(uint64_t), cudaMemcpyDeviceToHost));
+        if (y_vec && a->T) APRB_CUDA(cudaMemcpy(y_vec, a->t_y_vec.p, a->T * sizeof(uint16_t), cudaMemcpyDeviceToHost));
+    });
+}
+
+aprb_status aprb_fill_tree_mean_device(aprb_apr *a, const float *parts_dev, float *tree_dev, void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && parts_dev && tree_dev, "null argument");
+        cudaStream_t s = (cudaStream_t)stream;
+        ensure_tree(a, s);
+        filter_apply(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
+                     (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, parts_dev, tree_dev, nullptr,
+                     nullptr, nullptr, 0, nullptr, a->fb, s);
+    });
+}
+
+aprb_status aprb_fill_tree_mean(aprb_apr *a, const float *parts, float *tree) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && parts && tree, "null argument");
+        cudaStream_t s = cudaStreamPerThread;
+        ensure_tree(a, s);
+        float *dp = a->parts_f.as<float>(a->P ? a->P : 1);
+        float *dt = a->out_f.as<float>(a->T ? a->T : 1);
+        APRB_CUDA(cudaMemcpyAsync(dp, parts, a->P * sizeof(float), cudaMemcpyHostToDevice, s));
+        filter_apply(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
+                     (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, dp, dt, nullptr, nullptr,
+                     nullptr, 0, nullptr, a->fb, s);
+        APRB_CUDA(cudaMemcpyAsync(tree, dt, a->T * sizeof(float), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+aprb_status aprb_convolve_device(aprb_apr *a, const float *stencil, int ksize, const float *in_dev, float *out_dev,
+                                 int reflect, int use_stencil_downsample, int normalize, void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && stencil && in_dev && out_dev, "null argument");
+        convolve_impl(a, stencil, ksize, in_dev, out_dev, reflect, use_stencil_downsample, normalize,
+                      (cudaStream_t)stream);
+    });
+}
+
+aprb_status aprb_convolve(aprb_apr *a, const float *stencil, int ksize, const float *in, float *out, int reflect,
+                          int use_stencil_downsample, int normalize) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && stencil && in && out, "null argument");
+        cudaStream_t s = cudaStreamPerThread;
+        float *di = a->parts_f.as<float>(a->P ? a->P : 1);
+        float *dout = a->out_f.as<float>(a->P ? a->P : 1);
+        APRB_CUDA(cudaMemcpyAsync(di, in, a->P * sizeof(float), cudaMemcpyHostToDevice, s));
+        convolve_impl(a, stencil, ksize, di, dout, reflect, use_stencil_downsample, normalize, s);
+        APRB_CUDA(cudaMemcpyAsync(out, dout, a->P * sizeof(float), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+aprb_status aprb_richardson_lucy_device(aprb_apr *a, const uint16_t *in_dev, float *out_dev, const float *psf,
+                                        int ksize, int niter, int use_stencil_downsample, int normalize, int resume,
+                                        void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && in_dev && out_dev && psf && niter >= 0, "invalid argument");
+        rl_impl(a, in_dev, out_dev, psf, ksize, niter, use_stencil_downsample, normalize, resume,
+                (cudaStream_t)stream);
+    });
+}
+
+aprb_status aprb_richardson_lucy(aprb_apr *a, const uint16_t *in, float *out, const float *psf, int ksize, int niter,
+                                 int use_stencil_downsample, int normalize, int resume) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && in && out && psf && niter >= 0, "invalid argument");
+        cudaStream_t s = cudaStreamPerThread;
+        uint16_t *di = a->parts_u16.as<uint16_t>(a->P ? a->P : 1);
+        float *dout = a->out_f.as<float>(a->P ? a->P : 1);
+        APRB_CUDA(cudaMemcpyAsync(di, in, a->P * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+        if (resume) APRB_CUDA(cudaMemcpyAsync(dout, out, a->P * sizeof(float), cudaMemcpyHostToDevice, s));
+        rl_impl(a, di, dout, psf, ksize, niter, use_stencil_downsample, normalize, resume, s);
+        APRB_CUDA(cudaMemcpyAsync(out, dout, a->P * sizeof(float), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+aprb_status aprb_synth_blobs_u16(uint16_t *img_dev, int y_num, int x_num, int z_num, int n_blobs, float sigma_lo,
+                                 float sigma_hi, float amp_lo, float amp_hi, float background, uint64_t seed,
+                                 void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(img_dev && y_num > 0 && x_num > 0 && z_num > 0 && n_blobs >= 0, "invalid argument");
+        static thread_local DevBuf buf;
+        launch_synth_blobs(img_dev, y_num, x_num, z_num, n_blobs, sigma_lo, sigma_hi, amp_lo, amp_hi, background,
+                           seed, buf, (cudaStream_t)stream);
+    });
+}
+
+}  // extern "C"

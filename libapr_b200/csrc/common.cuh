@@ -1,0 +1,121 @@
+// Shared device helpers and host plumbing for libaprb200.
+//
+// Every kernel in this library is compiled for sm_100a with -fmad=false and
+// IEEE division/sqrt, so each float operation rounds where the reference's
+// strict-IEEE CPU build rounds.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "../../include/aprb200.h"
+
+namespace aprb {
+
+// ------------------------------------------------------------------ errors
+void set_error(const std::string &msg);
+struct Error {
+    aprb_status status;
+};
+#define APRB_CUDA(call)                                                                        \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) {                                                               \
+            ::aprb::set_error(std::string(#call) + ": " + cudaGetErrorString(e_));             \
+            throw ::aprb::Error{e_ == cudaErrorMemoryAllocation ? APRB_ERR_OUT_OF_MEMORY       \
+                                                                : APRB_ERR_CUDA};              \
+        }                                                                                      \
+    } while (0)
+#define APRB_CHECK_LAUNCH() APRB_CUDA(cudaGetLastError())
+
+void count_launch(uint64_t n = 1);
+
+// Stage timing: a scope that records a CUDA event pair on the stream when
+// profiling is enabled (aprb_profile_enable).
+void prof_record(const char *name, cudaStream_t s, bool begin);
+struct ProfScope {
+    const char *name;
+    cudaStream_t s;
+    ProfScope(const char *n, cudaStream_t st) : name(n), s(st) { prof_record(name, s, true); }
+    ~ProfScope() { prof_record(name, s, false); }
+};
+#define APRB_PROF_CAT2(a, b) a##b
+#define APRB_PROF_CAT(a, b) APRB_PROF_CAT2(a, b)
+#define APRB_PROF(name, s) ::aprb::ProfScope APRB_PROF_CAT(prof_scope_, __LINE__)(name, s)
+
+inline unsigned blocks_for(uint64_t n, unsigned threads) {
+    uint64_t b = (n + threads - 1) / threads;
+    return (unsigned)(b == 0 ? 1 : b);
+}
+
+// ------------------------------------------------------------------ device buffers
+// A device allocation that grows on demand and is reused across calls, as the
+// reference converter keeps its scratch images as members.
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+    void *get(size_t bytes) {
+        if (bytes > cap) {
+            if (p) cudaFree(p);
+            p = nullptr;
+            cap = 0;
+            size_t want = bytes ? bytes : 16;
+            APRB_CUDA(cudaMalloc(&p, want));
+            cap = want;
+        }
+        return p;
+    }
+    template <typename T>
+    T *as(size_t n) {
+        return (T *)get(n * sizeof(T));
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+    }
+    ~DevBuf() { release(); }
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+};
+
+// ------------------------------------------------------------------ conversions
+// ImageType = uint16 stores convert like the reference's x86-64 build:
+// truncate toward zero to 32 bit, keep the low 16 bits; NaN and out-of-range
+// give 0.
+__host__ __device__ __forceinline__ float cvt_u16(float v) {
+    if (!(v > -2147483648.0f && v < 2147483648.0f)) return 0.0f;
+    return (float)(uint16_t)(int32_t)v;
+}
+__host__ __device__ __forceinline__ float cvt_u16d(double v) {
+    if (!(v > -2147483648.0 && v < 2147483648.0)) return 0.0f;
+    return (float)(uint16_t)(int32_t)v;
+}
+// round<T> (ComputeGradient.hpp:220-244): std::round then range check.
+__device__ __forceinline__ float round_u16(float v, unsigned &err) {
+    v = roundf(v);
+    if (v < 0.0f || v > 65535.0f) err++;
+    return cvt_u16(v);
+}
+// float -> uint32 as the x86-64 build converts (64-bit truncation, low 32 bits).
+__device__ __forceinline__ uint32_t cvt_u32(float v) {
+    if (!(v > -9223372036854775808.0f && v < 9223372036854775808.0f)) return 0u;
+    return (uint32_t)(long long)v;
+}
+
+__host__ __device__ __forceinline__ size_t idx3(int y, int x, int z, int yn, int xn) {
+    return ((size_t)z * (size_t)xn + (size_t)x) * (size_t)yn + (size_t)y;
+}
+
+// Level geometry of GenInfo (GenInfo.hpp:33-98), shared host/device.
+struct Geom {
+    int l_min, l_max;
+    int y_num[32], x_num[32], z_num[32];
+    uint64_t level_xz[34];
+};
+
+}  // namespace aprb

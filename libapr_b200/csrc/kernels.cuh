@@ -1,0 +1,92 @@
+// Declarations shared by the kernel translation units of libaprb200.
+#pragma once
+
+#include <algorithm>
+#include <cmath>
+
+#include "common.cuh"
+#include "host_params.hpp"
+
+namespace aprb {
+
+constexpr int kMaxK0 = 256;  // longest folded recursive-filter boundary vector
+
+// particle-cell status codes (PullingScheme.hpp:16-22) and the
+// equivalence-optimisation seed (LinearAccess.hpp:265)
+constexpr uint8_t kEmpty = 0, kSeed = 1, kBoundary = 2, kFiller = 3, kUpsamplingSeed = 4, kAscendant = 8,
+                  kPropagate = 15, kAscendantNeighbour = 16;
+
+struct IIRDev {
+    float b1, b2, norm;
+    int minLen;
+};
+
+struct LisBuffers {
+    DevBuf padded, a, c, scalars;
+};
+
+// ---- pipeline.cu
+void launch_minmax_offset(const uint16_t *img, uint64_t n, unsigned *mm, float *offset, int apply, cudaStream_t s);
+template <typename IT>
+void launch_smooth(const uint16_t *img, IT *work, int yn, int xn, int zn, float lambda, const float *d_offset,
+                   unsigned *d_err, cudaStream_t s);
+template <typename IT>
+void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *ids_raw, float *ids, int yd, int xd,
+                     int zd, const aprb_params &p, cudaStream_t s);
+void launch_local_intensity_scale(const float *ids, float *lis, int yd, int xd, int zd, const aprb_params &p,
+                                  LisBuffers &b, cudaStream_t s);
+template <typename IT>
+void launch_levels(IT *grad, float *lis, const float *ids, uint64_t nd, const float *d_offset, const aprb_params &p,
+                   int apr_l_max, int top_level, uint8_t *level, uint8_t *status, int keep, cudaStream_t s);
+
+// ---- structure.cu
+// Particle-cell pyramid: status[l] for pct levels l_min..l_max-1 (dims of
+// Geom level l); status[l_max-1] and level_top are filled by launch_levels.
+struct Pyramid {
+    uint8_t *status[32] = {};
+    uint8_t *level[32] = {};
+};
+void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s);
+// Linear access structure: writes row counts into xz_end (n_xz entries) and
+// scans them; returns the particle count (synchronises the stream once).
+uint64_t launch_linear_counts(const Geom &g, Pyramid &pm, uint64_t *xz_end, uint64_t n_xz, int min_type,
+                              DevBuf &scan_tmp, cudaStream_t s);
+void launch_linear_fill(const Geom &g, const Pyramid &pm, const uint64_t *xz_end, uint16_t *y_vec, int min_type,
+                        cudaStream_t s);
+void launch_full_resolution_structure(const Geom &g, uint64_t *xz_end, uint16_t *y_vec, cudaStream_t s);
+void inclusive_scan_u64(uint64_t *data, uint64_t n, DevBuf &tmp, cudaStream_t s);
+
+// sampling (ParticleData.hpp:222-261)
+void launch_sample(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const uint16_t *img,
+                   uint16_t *parts, DevBuf &pyr, cudaStream_t s);
+
+// tree (APR.hpp:633-689)
+uint64_t launch_tree_build(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
+                           uint64_t *t_xz_end, uint64_t t_n_xz, DevBuf &flags, DevBuf &scan_tmp, cudaStream_t s);
+void launch_tree_fill(const Geom &tg, const DevBuf &flags, const uint64_t *t_xz_end, uint16_t *t_y_vec,
+                      cudaStream_t s);
+
+// ---- filter.cu
+struct FilterBuffers {
+    DevBuf dense, type, stale, stencils;
+};
+// APRTreeNumerics::fill_tree_mean, or (stencil != null) APRFilter::convolve_pencil
+// whose epilogue is: mode 0 out = conv; mode 1 out = in_u16 / conv (RL ratio);
+// mode 2 out = out * conv (RL update).
+struct ConvPlan {
+    int nstencils = 0;
+    std::vector<int> sides;
+    std::vector<int> offsets;
+    int reflect = 1;
+};
+void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
+                  const uint64_t *t_xz_end, const uint16_t *t_y_vec, const float *in, float *tree,
+                  const ConvPlan *plan, const float *d_stencils, float *out, int mode, const uint16_t *rl_in,
+                  FilterBuffers &fb, cudaStream_t s);
+uint64_t filter_stale_count(FilterBuffers &fb, cudaStream_t s);
+
+// ---- synth.cu
+void launch_synth_blobs(uint16_t *img, int yn, int xn, int zn, int n_blobs, float slo, float shi, float alo,
+                        float ahi, float bg, uint64_t seed, DevBuf &blobs, cudaStream_t s);
+
+}  // namespace aprb

@@ -1,0 +1,817 @@
+// Pixel stages of get_apr on the GPU: offset, smoothing-spline recursive
+// filters along y/x/z, gradient magnitude fused with the 2x max and mean
+// down-sampling, inverse B-spline at ds resolution, local intensity scale,
+// and the fused applyParameters + computeLevels + top-level seeding.
+//
+// Bit-exactness: each kernel performs the reference's float operations in the
+// reference's order (ComputeGradient.hpp, LocalIntensityScale.hpp,
+// LocalParticleCellSet.hpp, APRConverter.hpp); recurrences that the reference
+// runs sequentially along a line run sequentially in one thread here.
+#include "kernels.cuh"
+
+namespace aprb {
+
+__constant__ float c_bc[4][kMaxK0];
+
+// ---------------------------------------------------------------------------
+// a1: compute_bspline_offset (AutoParameters.hpp:164-197) -- min/max reduction
+// then the clamped offset, kept on the device.
+// ---------------------------------------------------------------------------
+__global__ void minmax_u16_kernel(const uint16_t *__restrict__ img, uint64_t n, unsigned *mm) {
+    unsigned mn = 0xffffu, mx = 0u;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        unsigned v = img[i];
+        mn = v < mn ? v : mn;
+        mx = v > mx ? v : mx;
+    }
+    mn = __reduce_min_sync(0xffffffffu, mn);
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&mm[0], mn);
+        atomicMax(&mm[1], mx);
+    }
+}
+
+__global__ void offset_kernel(const unsigned *mm, float *offset, int apply) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (!apply) {
+        *offset = 0.0f;
+        return;
+    }
+    int mn = (int)mm[0], mx = (int)mm[1];
+    float off = (float)((65535 - (mx - mn)) / 2 - mn);
+    off = off < 100.f ? off : 100.f;
+    *offset = off > -100.f ? off : -100.f;
+}
+
+// Working-image value of the raw input: image_temp = IT(input + offset) for
+// integer IT, a plain copy for float IT (APRConverter.hpp:218-223).
+template <typename IT>
+__device__ __forceinline__ float raw_to_it(uint16_t v, float off);
+template <>
+__device__ __forceinline__ float raw_to_it<uint16_t>(uint16_t v, float off) {
+    return cvt_u16((float)v + off);
+}
+template <>
+__device__ __forceinline__ float raw_to_it<float>(uint16_t v, float) {
+    return (float)v;
+}
+
+template <typename IT>
+__device__ __forceinline__ float rnd_it(float v, unsigned &err);
+template <>
+__device__ __forceinline__ float rnd_it<uint16_t>(float v, unsigned &err) {
+    return round_u16(v, err);
+}
+template <>
+__device__ __forceinline__ float rnd_it<float>(float v, unsigned &) {
+    return v;
+}
+template <typename IT>
+__device__ __forceinline__ float store_cvt(float v);
+template <>
+__device__ __forceinline__ float store_cvt<uint16_t>(float v) {
+    return cvt_u16(v);
+}
+template <>
+__device__ __forceinline__ float store_cvt<float>(float v) {
+    return v;
+}
+template <typename IT>
+__device__ __forceinline__ IT to_it(float v) {
+    return (IT)v;
+}
+
+// ---------------------------------------------------------------------------
+// a2 (y): bspline_filt_rec_y (ComputeGradient.hpp:249-413).
+// One thread owns one y-line (the recurrence is sequential); a warp owns 32
+// consecutive lines and moves them through shared memory in 32x32 tiles so
+// global loads and stores are coalesced.  The forward pass stores its values,
+// the backward pass reads them back through L2 (__ldcg).
+// ---------------------------------------------------------------------------
+constexpr int kTile = 32;
+constexpr int kYWarps = 4;
+
+template <typename IT>
+__global__ void __launch_bounds__(kYWarps * 32) iir_y_kernel(const uint16_t *__restrict__ src, IT *__restrict__ dst,
+                                                              int yn, uint64_t nlines, IIRDev c,
+                                                              const float *__restrict__ d_offset, unsigned *err_out) {
+    __shared__ float tile[kYWarps][kTile][kTile + 1];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t line0 = ((uint64_t)blockIdx.x * kYWarps + w) * kTile;
+    if (line0 >= nlines) return;
+    const uint64_t myline = line0 + lane;
+    const bool valid = myline < nlines;
+    const float off = d_offset ? *d_offset : 0.0f;
+    float(*T)[kTile + 1] = tile[w];
+    unsigned err = 0;
+
+    float t1 = 0, t2 = 0, t3 = 0, t4 = 0;
+    if (valid) {
+        const uint16_t *L = src + myline * (uint64_t)yn;
+        for (int k = 0; k < c.minLen; ++k) {
+            float v = raw_to_it<IT>(L[k], off);
+            t1 = t1 + c_bc[0][k] * v;
+            t2 = t2 + c_bc[1][k] * v;
+        }
+        for (int k = 0; k < c.minLen; ++k) {
+            float v = raw_to_it<IT>(L[yn - 1 - k], off);
+            t3 = t3 + c_bc[2][k] * v;
+            t4 = t4 + c_bc[3][k] * v;
+        }
+    }
+    // forward (causal) pass
+    for (int y0 = 0; y0 < yn; y0 += kTile) {
+        for (int j = 0; j < kTile; ++j) {
+            uint64_t ln = line0 + j;
+            if (ln < nlines && y0 + lane < yn) T[j][lane] = raw_to_it<IT>(src[ln * (uint64_t)yn + y0 + lane], off);
+        }
+        __syncwarp();
+        if (valid) {
+            const int kend = min(kTile, yn - y0);
+            for (int k = 0; k < kend; ++k) {
+                const int y = y0 + k;
+                float out;
+                if (y == 0) {
+                    out = store_cvt<IT>(t2);
+                } else if (y == 1) {
+                    out = store_cvt<IT>(t1);
+                } else {
+                    float temp = t1 * c.b1 + t2 * c.b2 + T[lane][k];
+                    out = rnd_it<IT>(temp, err);
+                    t2 = t1;
+                    t1 = temp;
+                }
+                if (y == yn - 2) out = rnd_it<IT>(t3 * c.norm, err);
+                if (y == yn - 1) out = rnd_it<IT>(t4 * c.norm, err);
+                T[lane][k] = out;
+            }
+        }
+        __syncwarp();
+        for (int j = 0; j < kTile; ++j) {
+            uint64_t ln = line0 + j;
+            if (ln < nlines && y0 + lane < yn) dst[ln * (uint64_t)yn + y0 + lane] = to_it<IT>(T[j][lane]);
+        }
+        __syncwarp();
+    }
+    // backward (anti-causal) pass
+    float b2v = 0, b1v = 0;
+    if (valid) {
+        const IT *L = dst + myline * (uint64_t)yn;
+        b2v = (float)__ldcg(&L[yn - 1]) / c.norm;
+        b1v = (float)__ldcg(&L[yn - 2]) / c.norm;
+    }
+    const int last0 = ((yn - 1) / kTile) * kTile;
+    for (int y0 = last0; y0 >= 0; y0 -= kTile) {
+        for (int j = 0; j < kTile; ++j) {
+            uint64_t ln = line0 + j;
+            if (ln < nlines && y0 + lane < yn) T[j][lane] = (float)__ldcg(&dst[ln * (uint64_t)yn + y0 + lane]);
+        }
+        __syncwarp();
+        if (valid) {
+            const int kend = min(kTile, yn - y0);
+            for (int k = kend - 1; k >= 0; --k) {
+                const int y = y0 + k;
+                if (y > yn - 3) continue;
+                float temp = b1v * c.b1 + b2v * c.b2 + T[lane][k];
+                T[lane][k] = rnd_it<IT>(temp * c.norm, err);
+                b2v = b1v;
+                b1v = temp;
+            }
+        }
+        __syncwarp();
+        for (int j = 0; j < kTile; ++j) {
+            uint64_t ln = line0 + j;
+            if (ln < nlines && y0 + lane < yn) dst[ln * (uint64_t)yn + y0 + lane] = to_it<IT>(T[j][lane]);
+        }
+        __syncwarp();
+    }
+    if (err) atomicAdd(err_out, err);
+}
+
+// ---------------------------------------------------------------------------
+// a2 (x, z): bspline_filt_rec_x (ComputeGradient.hpp:602-779) and
+// bspline_filt_rec_z (:416-599).  One thread per line along the strided axis;
+// neighbouring threads own neighbouring y so every step is a coalesced row.
+// In place.
+// ---------------------------------------------------------------------------
+template <typename IT>
+__global__ void iir_strided_kernel(IT *__restrict__ im, int yn, int n, uint64_t stride, uint64_t outer_stride,
+                                   uint64_t nlines, IIRDev c, unsigned *err_out) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nlines) return;
+    const uint64_t y = g % (uint64_t)yn, o = g / (uint64_t)yn;
+    IT *L = im + o * outer_stride + y;
+    unsigned err = 0;
+    float v1 = 0, v2 = 0, v3 = 0, v4 = 0;
+    for (int i = 0; i < c.minLen; ++i) {
+        float a = (float)L[(uint64_t)i * stride];
+        float b = (float)L[(uint64_t)(n - 1 - i) * stride];
+        v1 = v1 + c_bc[0][i] * a;
+        v2 = v2 + c_bc[1][i] * a;
+        v3 = v3 + c_bc[2][i] * b;
+        v4 = v4 + c_bc[3][i] * b;
+    }
+    L[0] = to_it<IT>(rnd_it<IT>(v2, err));
+    L[stride] = to_it<IT>(rnd_it<IT>(v1, err));
+    constexpr int U = 8;
+    int i = 2;
+    for (; i + U <= n; i += U) {
+        float buf[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) buf[u] = (float)L[(uint64_t)(i + u) * stride];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            float nv = rnd_it<IT>(buf[u] + c.b1 * v1 + c.b2 * v2, err);
+            v2 = v1;
+            v1 = nv;
+            buf[u] = nv;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) L[(uint64_t)(i + u) * stride] = to_it<IT>(buf[u]);
+    }
+    for (; i < n; ++i) {
+        float nv = rnd_it<IT>((float)L[(uint64_t)i * stride] + c.b1 * v1 + c.b2 * v2, err);
+        v2 = v1;
+        v1 = nv;
+        L[(uint64_t)i * stride] = to_it<IT>(nv);
+    }
+    L[(uint64_t)(n - 1) * stride] = to_it<IT>(rnd_it<IT>(v4 * c.norm, err));
+    L[(uint64_t)(n - 2) * stride] = to_it<IT>(rnd_it<IT>(v3 * c.norm, err));
+    int j = n - 3;
+    for (; j - U + 1 >= 0; j -= U) {
+        float buf[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) buf[u] = (float)L[(uint64_t)(j - u) * stride];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            float temp = (buf[u] + c.b1 * v3 + c.b2 * v4);
+            buf[u] = rnd_it<IT>(temp * c.norm, err);
+            v4 = v3;
+            v3 = temp;
+        }
+#pragma unroll
+        for (int u = 0; u < U; ++u) L[(uint64_t)(j - u) * stride] = to_it<IT>(buf[u]);
+    }
+    for (; j >= 0; --j) {
+        float temp = ((float)L[(uint64_t)j * stride] + c.b1 * v3 + c.b2 * v4);
+        L[(uint64_t)j * stride] = to_it<IT>(rnd_it<IT>(temp * c.norm, err));
+        v4 = v3;
+        v3 = temp;
+    }
+    if (err) atomicAdd(err_out, err);
+}
+
+// Copy of the offset input when no smoothing runs (lambda <= 0 or y too short).
+template <typename IT>
+__global__ void offset_copy_kernel(const uint16_t *__restrict__ src, IT *__restrict__ dst, uint64_t n,
+                                   const float *__restrict__ d_offset) {
+    const float off = d_offset ? *d_offset : 0.0f;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = to_it<IT>(raw_to_it<IT>(src[i], off));
+}
+
+// ---------------------------------------------------------------------------
+// a3 + a4: calc_bspline_fd_ds_mag (ComputeGradient.hpp:976-1051) fused with
+// downsample(sum, /8) (PixelData.hpp:916-967).  One thread per ds voxel.
+// ---------------------------------------------------------------------------
+template <typename IT>
+__device__ __forceinline__ float grad_mag(const IT *__restrict__ im, int y, int x, int z, int yn, int xn, int zn,
+                                          float hx2, float hy2, float hz2) {
+    if (yn < 2) return 0.0f;
+    const int xl = x > 0 ? x - 1 : 0, xr = x + 1 < xn - 1 ? x + 1 : xn - 1;
+    const int zu = z > 0 ? z - 1 : 0, zd = z + 1 < zn - 1 ? z + 1 : zn - 1;
+    const int ym = y > 0 ? y - 1 : 0, yp = y < yn - 1 ? y + 1 : yn - 1;
+    float gx = ((float)im[idx3(y, xr, z, yn, xn)] - (float)im[idx3(y, xl, z, yn, xn)]) / hx2;
+    float gz = ((float)im[idx3(y, x, zd, yn, xn)] - (float)im[idx3(y, x, zu, yn, xn)]) / hz2;
+    float gy = ((float)im[idx3(yp, x, z, yn, xn)] - (float)im[idx3(ym, x, z, yn, xn)]) / hy2;
+    double s = (double)gx * (double)gx + (double)gz * (double)gz;
+    s = s + (double)gy * (double)gy;
+    double r = sqrt(s);
+    return sizeof(IT) == 2 ? cvt_u16d(r) : (float)r;
+}
+
+template <typename IT>
+__global__ void grad_ds_kernel(const IT *__restrict__ im, int yn, int xn, int zn, IT *__restrict__ grad,
+                               float *__restrict__ ids, int yd, int xd, int zd, float hx, float hy, float hz) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t nd = (uint64_t)yd * xd * zd;
+    if (g >= nd) return;
+    const int k = (int)(g % yd);
+    const int xk = (int)((g / yd) % xd);
+    const int zk = (int)(g / ((uint64_t)yd * xd));
+    const float hx2 = 2 * hx, hy2 = 2 * hy, hz2 = 2 * hz;
+    float gmax = 0.0f;
+    const int ks = 2 * k + 1 < yn - 1 ? 2 * k + 1 : yn - 1;
+    for (int z = 2 * zk; z <= 2 * zk + 1 && z < zn; ++z)
+        for (int x = 2 * xk; x <= 2 * xk + 1 && x < xn; ++x) {
+            float a = grad_mag(im, 2 * k, x, z, yn, xn, zn, hx2, hy2, hz2);
+            float b = grad_mag(im, ks, x, z, yn, xn, zn, hx2, hy2, hz2);
+            float m = b > gmax ? b : gmax;
+            gmax = a > m ? a : m;
+        }
+    grad[g] = to_it<IT>(gmax);
+    const int shx = 2 * xk + 1 < xn - 1 ? 2 * xk + 1 : xn - 1;
+    const int shz = 2 * zk + 1 < zn - 1 ? 2 * zk + 1 : zn - 1;
+    const int y0 = 2 * k, x0 = 2 * xk, z0 = 2 * zk;
+    float r = (float)im[idx3(y0, x0, z0, yn, xn)];
+    r = r + (float)im[idx3(ks, x0, z0, yn, xn)];
+    r = r + (float)im[idx3(y0, shx, z0, yn, xn)];
+    r = r + (float)im[idx3(ks, shx, z0, yn, xn)];
+    r = r + (float)im[idx3(y0, x0, shz, yn, xn)];
+    r = r + (float)im[idx3(ks, x0, shz, yn, xn)];
+    r = r + (float)im[idx3(y0, shx, shz, yn, xn)];
+    r = r + (float)im[idx3(ks, shx, shz, yn, xn)];
+    ids[g] = r / 8.0f;
+}
+
+// ---------------------------------------------------------------------------
+// a5: calc_inv_bspline_y/x/z (ComputeGradient.hpp:785-964), the three
+// in-place passes fused: each output re-evaluates the y and x passes of its
+// 3x3x3 neighbourhood with identical float operations.
+// ---------------------------------------------------------------------------
+struct InvB {
+    float a1, a2, a3, a13;
+};
+
+__device__ __forceinline__ float inv_y(const float *__restrict__ I, int y, int x, int z, int yd, int xd, bool on,
+                                       InvB c) {
+    const float *L = I + idx3(0, x, z, yd, xd);
+    if (!on) return L[y];
+    if (y == 0) return c.a2 * L[0] + c.a13 * L[1];
+    if (y == yd - 1) return c.a13 * L[yd - 2] + c.a2 * L[yd - 1];
+    return c.a1 * L[y - 1] + c.a2 * L[y] + c.a3 * L[y + 1];
+}
+
+__device__ __forceinline__ float inv_x(const float *__restrict__ I, int y, int x, int z, int yd, int xd, bool ony,
+                                       bool onx, InvB c) {
+    if (!onx) return inv_y(I, y, x, z, yd, xd, ony, c);
+    if (x == xd - 1)
+        return c.a13 * inv_y(I, y, xd - 2, z, yd, xd, ony, c) + c.a2 * inv_y(I, y, xd - 1, z, yd, xd, ony, c);
+    const int xm = x == 0 ? 1 : x - 1;
+    return c.a1 * inv_y(I, y, xm, z, yd, xd, ony, c) + c.a2 * inv_y(I, y, x, z, yd, xd, ony, c) +
+           c.a3 * inv_y(I, y, x + 1, z, yd, xd, ony, c);
+}
+
+__global__ void inv_bspline_kernel(const float *__restrict__ I, float *__restrict__ O, int yd, int xd, int zd,
+                                   int ony, int onx, int onz, InvB c) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)yd * xd * zd) return;
+    const int y = (int)(g % yd), x = (int)((g / yd) % xd), z = (int)(g / ((uint64_t)yd * xd));
+    float r;
+    if (!onz) {
+        r = inv_x(I, y, x, z, yd, xd, ony, onx, c);
+    } else if (z == zd - 1) {
+        r = c.a13 * inv_x(I, y, x, zd - 2, yd, xd, ony, onx, c) + c.a2 * inv_x(I, y, x, zd - 1, yd, xd, ony, onx, c);
+    } else {
+        const int zm = z == 0 ? 1 : z - 1;
+        r = c.a1 * inv_x(I, y, x, zm, yd, xd, ony, onx, c) + c.a2 * inv_x(I, y, x, z, yd, xd, ony, onx, c) +
+            c.a3 * inv_x(I, y, x, z + 1, yd, xd, ony, onx, c);
+    }
+    O[g] = r;
+}
+
+// ---------------------------------------------------------------------------
+// a6: local intensity scale (LocalIntensityScale.hpp:26-150) on the
+// reflect-padded ds image (paddPixels, PixelData.hpp:1071-1178).
+// ---------------------------------------------------------------------------
+__global__ void pad_reflect_kernel(const float *__restrict__ in, int yn, int xn, int zn, float *__restrict__ out,
+                                   int sy, int sx, int sz, int py, int px, int pz) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)py * px * pz) return;
+    int y = (int)(g % py), x = (int)((g / py) % px), z = (int)(g / ((uint64_t)py * px));
+    int ry = y - sy, rx = x - sx, rz = z - sz;
+    ry = ry < 0 ? -ry : (ry > yn - 1 ? 2 * (yn - 1) - ry : ry);
+    rx = rx < 0 ? -rx : (rx > xn - 1 ? 2 * (xn - 1) - rx : rx);
+    rz = rz < 0 ? -rz : (rz > zn - 1 ? 2 * (zn - 1) - rz : rz);
+    out[g] = in[idx3(ry, rx, rz, yn, xn)];
+}
+
+// One output of calc_sat_mean_y (:311-362) given the line's cumulative sums.
+template <int OFF>
+__device__ __forceinline__ float sat_y_value(int i, int n, float d, float cm /*C[i-off-1]*/, float cp /*C[i+off]*/,
+                                             float clast /*C[n-1]*/) {
+    float v = (i <= OFF) ? 0.0f : -cm / d;
+    if (i < n - OFF) v = v + cp / d;
+    if (i >= n - OFF) {
+        float cnt = (float)(i - (n - OFF) + 1);
+        v = v * d;
+        v = v + clast;
+        v = (float)((double)v * (1.0 / (double)(d - cnt)));
+    }
+    if (i >= 1 && i <= OFF) v = (float)((double)v * ((double)d / ((double)i + (double)OFF + 1.0)));
+    if (i == 0) v = (float)((double)v * ((double)d / ((double)OFF + 1.0)));
+    return v;
+}
+
+// y box mean: one thread per y-line, cumulative sum carried in a register
+// shift window of 2*OFF+2 entries; tiles through shared memory as in the IIR.
+// absdiff_ref != nullptr makes the input |in - absdiff_ref| (calc_abs_diff,
+// :188-196) on the fly.
+template <int OFF>
+__global__ void __launch_bounds__(kYWarps * 32) sat_y_kernel(const float *__restrict__ in,
+                                                              const float *__restrict__ absdiff_ref,
+                                                              float *__restrict__ out, int n, uint64_t nlines) {
+    constexpr int W = 2 * OFF + 2;
+    __shared__ float tin[kYWarps][kTile][kTile + 1];
+    __shared__ float tout[kYWarps][kTile][kTile + 1];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t line0 = ((uint64_t)blockIdx.x * kYWarps + w) * kTile;
+    if (line0 >= nlines) return;
+    const bool valid = line0 + lane < nlines;
+    const float d = (float)(2 * OFF + 1);
+    float c[W];
+#pragma unroll
+    for (int q = 0; q < W; ++q) c[q] = 0.0f;
+    float C = 0.0f;
+    for (int y0 = 0; y0 < n; y0 += kTile) {
+        for (int j = 0; j < kTile; ++j) {
+            uint64_t ln = line0 + j;
+            if (ln < nlines && y0 + lane < n) {
+                uint64_t a = ln * (uint64_t)n + y0 + lane;
+                float v = in[a];
+                if (absdiff_ref) v = fabsf(v - absdiff_ref[a]);
+                tin[w][j][lane] = v;
+            }
+        }
+        __syncwarp();
+        if (valid) {
+            const int kend = min(kTile, n - y0);
+            for (int k = 0; k < kend; ++k) {
+                const int j = y0 + k;
+                C = C + tin[w][lane][k];
+#pragma unroll
+                for (int q = 0; q < W - 1; ++q) c[q] = c[q + 1];
+                c[W - 1] = C;
+                const int i = j - OFF;
+                if (i >= 0 && i < n - OFF) tout[w][lane][k] = sat_y_value<OFF>(i, n, d, c[0], C, 0.0f);
+            }
+        }
+        __syncwarp();
+        for (int j = 0; j < kTile; ++j) {
+            uint64_t ln = line0 + j;
+            int i = y0 + lane - OFF;
+            if (ln < nlines && y0 + lane < n && i >= 0 && i < n - OFF) out[ln * (uint64_t)n + i] = tout[w][j][lane];
+        }
+        __syncwarp();
+    }
+    if (valid) {
+        // right-hand tail: outputs n-OFF .. n-1 need C[n-1] (= c[W-1])
+        for (int i = n - OFF; i < n; ++i) {
+            if (i < 0) continue;
+            const int back = (n - 1) - (i - OFF - 1);  // distance from C[n-1] to C[i-off-1]
+            float cm = 0.0f;
+#pragma unroll
+            for (int q = 0; q < W; ++q)
+                if (q == W - 1 - back) cm = c[q];
+            out[(line0 + lane) * (uint64_t)n + i] = sat_y_value<OFF>(i, n, d, cm, 0.0f, C);
+        }
+    }
+}
+
+// x / z box mean (:364-494): one thread per strided line, coalesced over y.
+template <int OFF>
+__global__ void sat_strided_kernel(const float *__restrict__ in, const float *__restrict__ absdiff_ref,
+                                   float *__restrict__ out, int yn, int n, uint64_t stride, uint64_t outer_stride,
+                                   uint64_t nlines) {
+    constexpr int W = 2 * OFF + 2;
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= nlines) return;
+    const uint64_t y = g % (uint64_t)yn, o = g / (uint64_t)yn;
+    const uint64_t base = o * outer_stride + y;
+    float c[W];
+#pragma unroll
+    for (int q = 0; q < W; ++q) c[q] = 0.0f;
+    float C = 0.0f;
+    const float dd = (float)(2 * OFF + 1);
+    for (int j = 0; j < n; ++j) {
+        uint64_t a = base + (uint64_t)j * stride;
+        float v = in[a];
+        if (absdiff_ref) v = fabsf(v - absdiff_ref[a]);
+        C = (j == 0) ? v : v + C;
+#pragma unroll
+        for (int q = 0; q < W - 1; ++q) c[q] = c[q + 1];
+        c[W - 1] = C;
+        const int i = j - OFF;
+        if (i >= 0) {
+            if (i < OFF + 1)
+                out[base + (uint64_t)i * stride] = C / (float)(i + OFF + 1);
+            else if (i < n - OFF)
+                out[base + (uint64_t)i * stride] = (C - c[0]) / dd;
+        }
+    }
+    for (int i = n - OFF; i < n; ++i) {
+        if (i < 0) continue;
+        const int back = (n - 1) - (i - OFF - 1);
+        float cm = 0.0f;
+#pragma unroll
+        for (int q = 0; q < W; ++q)
+            if (q == W - 1 - back) cm = c[q];
+        out[base + (uint64_t)i * stride] = (C - cm) / (float)(n - i + OFF);
+    }
+}
+
+__global__ void unpad_rescale_kernel(const float *__restrict__ in, int py, int px, float *__restrict__ out, int yn,
+                                     int xn, int zn, int oy, int ox, int oz, float rescale) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)yn * xn * zn) return;
+    int y = (int)(g % yn), x = (int)((g / yn) % xn), z = (int)(g / ((uint64_t)yn * xn));
+    out[g] = in[idx3(y + oy, x + ox, z + oz, py, px)] * rescale;
+}
+
+// constant-scale fallback (:126-148): sum in double, min in float
+__global__ void sum_min_kernel(const float *__restrict__ in, uint64_t n, double *sum, unsigned *minbits) {
+    double s = 0;
+    float mn = 660000.0f;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        float t = in[i];
+        s += t;
+        mn = t < mn ? t : mn;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        s += __shfl_down_sync(0xffffffffu, s, o);
+        mn = fminf(mn, __shfl_down_sync(0xffffffffu, mn, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicAdd(sum, s);
+        // order-preserving float bits for non-negative and negative values
+        unsigned b = __float_as_uint(mn);
+        b = (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+        atomicMin(minbits, b);
+    }
+}
+
+__global__ void const_scale_fill_kernel(float *out, uint64_t n, const double *sum, const unsigned *minbits,
+                                        float numel) {
+    unsigned b = *minbits;
+    b = (b & 0x80000000u) ? (b & 0x7fffffffu) : ~b;
+    const float mn = __uint_as_float(b);
+    const float sv = (float)(*sum / (double)numel - (double)mn);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = sv;
+}
+
+// ---------------------------------------------------------------------------
+// a7 + a8 + first fill of a9: applyParameters (APRConverter.hpp:250-297),
+// computeLevels / compute_level_for_array (LocalParticleCellSet.hpp:129-171)
+// and PullingScheme::fill at the top pct level (PullingScheme.hpp:137-149).
+// ---------------------------------------------------------------------------
+template <typename IT>
+__global__ void levels_kernel(IT *__restrict__ grad, float *__restrict__ lis, const float *__restrict__ ids,
+                              uint64_t nd, const float *__restrict__ d_offset, float Ip_th, float sigma_th,
+                              float sigma_th_max, float grad_th, float mult, int top_level, uint8_t *__restrict__ level,
+                              uint8_t *__restrict__ status, int keep) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nd) return;
+    const float th = Ip_th + (d_offset ? *d_offset : 0.0f);
+    float g = (float)grad[i];
+    float s = lis[i];
+    if (ids[i] <= th) g = 0.0f;
+    if (s < sigma_th) s = (s < sigma_th_max) ? 60000.0f : sigma_th;
+    if (g < grad_th) g = 0.0f;
+    if (keep) {
+        grad[i] = to_it<IT>(g);
+        lis[i] = s;
+    }
+    const float q = g / s;
+    const uint32_t u = cvt_u32(q * mult);
+    const int lev = u == 0 ? 0 : 31 - __clz(u);
+    level[i] = (uint8_t)lev;
+    status[i] = ((float)lev >= (float)top_level) ? kSeed : kEmpty;
+}
+
+// ---------------------------------------------------------------------------
+// host drivers
+// ---------------------------------------------------------------------------
+void upload_bc(const IIRCoef &c, cudaStream_t s) {
+    if (c.minLen > kMaxK0) {
+        set_error("recursive filter support exceeds the supported maximum (lambda too large)");
+        throw Error{APRB_ERR_UNSUPPORTED};
+    }
+    float h[4][kMaxK0] = {};
+    for (int k = 0; k < c.minLen; ++k) {
+        h[0][k] = c.bc1[k];
+        h[1][k] = c.bc2[k];
+        h[2][k] = c.bc3[k];
+        h[3][k] = c.bc4[k];
+    }
+    APRB_CUDA(cudaMemcpyToSymbolAsync(c_bc, h, sizeof(h), 0, cudaMemcpyHostToDevice, s));
+}
+
+static IIRDev dev_coef(const IIRCoef &c) {
+    IIRDev d;
+    d.b1 = c.b1;
+    d.b2 = c.b2;
+    d.norm = c.norm;
+    d.minLen = c.minLen;
+    return d;
+}
+
+void launch_minmax_offset(const uint16_t *img, uint64_t n, unsigned *mm, float *offset, int apply, cudaStream_t s) {
+    APRB_PROF("offset", s);
+    if (apply) {
+        unsigned init[2] = {0xffffu, 0u};
+        APRB_CUDA(cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, s));
+        unsigned blocks = (unsigned)std::min<uint64_t>(blocks_for(n, 256), 148u * 16u);
+        minmax_u16_kernel<<<blocks, 256, 0, s>>>(img, n, mm);
+        count_launch();
+        APRB_CHECK_LAUNCH();
+    }
+    offset_kernel<<<1, 32, 0, s>>>(mm, offset, apply);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+}
+
+template <typename IT>
+void launch_smooth(const uint16_t *img, IT *work, int yn, int xn, int zn, float lambda, const float *d_offset,
+                   unsigned *d_err, cudaStream_t s) {
+    const uint64_t n = (uint64_t)yn * xn * zn;
+    bool copied = false;
+    if (lambda > 0 && yn > 2) {
+        APRB_PROF("bspline_y", s);
+        IIRCoef c = iir_coefficients(lambda, yn);
+        upload_bc(c, s);
+        const uint64_t nlines = (uint64_t)xn * zn;
+        const unsigned blocks = blocks_for(nlines, kYWarps * kTile);
+        iir_y_kernel<IT><<<blocks, kYWarps * 32, 0, s>>>(img, work, yn, nlines, dev_coef(c), d_offset, d_err);
+        count_launch();
+        APRB_CHECK_LAUNCH();
+        copied = true;
+    }
+    if (!copied) {
+        APRB_PROF("offset_copy", s);
+        unsigned blocks = (unsigned)std::min<uint64_t>(blocks_for(n, 256), 148u * 32u);
+        offset_copy_kernel<IT><<<blocks, 256, 0, s>>>(img, work, n, d_offset);
+        count_launch();
+        APRB_CHECK_LAUNCH();
+    }
+    if (lambda > 0 && xn > 2) {
+        APRB_PROF("bspline_x", s);
+        IIRCoef c = iir_coefficients(lambda, xn);
+        upload_bc(c, s);
+        const uint64_t nlines = (uint64_t)yn * zn;
+        iir_strided_kernel<IT><<<blocks_for(nlines, 128), 128, 0, s>>>(work, yn, xn, (uint64_t)yn,
+                                                                     (uint64_t)xn * yn, nlines, dev_coef(c), d_err);
+        count_launch();
+        APRB_CHECK_LAUNCH();
+    }
+    if (lambda > 0 && zn > 2) {
+        APRB_PROF("bspline_z", s);
+        IIRCoef c = iir_coefficients(lambda, zn);
+        upload_bc(c, s);
+        const uint64_t nlines = (uint64_t)yn * xn;
+        iir_strided_kernel<IT><<<blocks_for(nlines, 128), 128, 0, s>>>(work, yn, zn, (uint64_t)xn * yn, (uint64_t)yn,
+                                                                     nlines, dev_coef(c), d_err);
+        count_launch();
+        APRB_CHECK_LAUNCH();
+    }
+}
+
+template <typename IT>
+void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *ids_raw, float *ids, int yd, int xd,
+                     int zd, const aprb_params &p, cudaStream_t s) {
+    const uint64_t nd = (uint64_t)yd * xd * zd;
+    {
+    APRB_PROF("gradient_ds", s);
+    grad_ds_kernel<IT><<<blocks_for(nd, 256), 256, 0, s>>>(work, yn, xn, zn, grad, ids_raw, yd, xd, zd, p.dx, p.dy,
+                                                          p.dz);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+    }
+    APRB_PROF("inv_bspline", s);
+    const bool on = p.lambda > 0;
+    InvB c;
+    c.a1 = (float)(1.0 / 6.0);
+    c.a2 = (float)(4.0 / 6.0);
+    c.a3 = (float)(1.0 / 6.0);
+    c.a13 = c.a1 + c.a3;
+    inv_bspline_kernel<<<blocks_for(nd, 256), 256, 0, s>>>(ids_raw, ids, yd, xd, zd, on && yn > 2, on && xn > 2,
+                                                          on && zn > 2, c);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+}
+
+template <int OFF>
+static void sat_axis_t(const float *in, const float *absref, float *out, int py, int px, int pz, int axis,
+                       cudaStream_t s) {
+    if (axis == 0) {
+        const uint64_t nlines = (uint64_t)px * pz;
+        sat_y_kernel<OFF><<<blocks_for(nlines, kYWarps * kTile), kYWarps * 32, 0, s>>>(in, absref, out, py, nlines);
+    } else if (axis == 1) {
+        const uint64_t nlines = (uint64_t)py * pz;
+        sat_strided_kernel<OFF><<<blocks_for(nlines, 128), 128, 0, s>>>(in, absref, out, py, px, (uint64_t)py,
+                                                                       (uint64_t)px * py, nlines);
+    } else {
+        const uint64_t nlines = (uint64_t)py * px;
+        sat_strided_kernel<OFF><<<blocks_for(nlines, 128), 128, 0, s>>>(in, absref, out, py, pz, (uint64_t)px * py,
+                                                                       (uint64_t)py, nlines);
+    }
+    count_launch();
+    APRB_CHECK_LAUNCH();
+}
+
+static void sat_axis(const float *in, const float *absref, float *out, int py, int px, int pz, int axis, int off,
+                     cudaStream_t s) {
+    switch (off) {
+        case 1: sat_axis_t<1>(in, absref, out, py, px, pz, axis, s); break;
+        case 2: sat_axis_t<2>(in, absref, out, py, px, pz, axis, s); break;
+        case 3: sat_axis_t<3>(in, absref, out, py, px, pz, axis, s); break;
+        case 4: sat_axis_t<4>(in, absref, out, py, px, pz, axis, s); break;
+        case 5: sat_axis_t<5>(in, absref, out, py, px, pz, axis, s); break;
+        case 6: sat_axis_t<6>(in, absref, out, py, px, pz, axis, s); break;
+        default: set_error("unsupported local intensity scale window"); throw Error{APRB_ERR_UNSUPPORTED};
+    }
+}
+
+void launch_local_intensity_scale(const float *ids, float *lis, int yd, int xd, int zd, const aprb_params &p,
+                                  LisBuffers &b, cudaStream_t s) {
+    APRB_PROF("local_intensity_scale", s);
+    const LisWindow w = lis_window(p, yd, xd, zd);
+    const uint64_t nd = (uint64_t)yd * xd * zd;
+    if (p.constant_intensity_scale || w.n_active == 0) {
+        double *sum = b.scalars.as<double>(2);
+        unsigned *mb = (unsigned *)(sum + 1);
+        unsigned init_min = 0xffffffffu;
+        APRB_CUDA(cudaMemsetAsync(sum, 0, sizeof(double), s));
+        APRB_CUDA(cudaMemcpyAsync(mb, &init_min, sizeof(unsigned), cudaMemcpyHostToDevice, s));
+        unsigned blocks = (unsigned)std::min<uint64_t>(blocks_for(nd, 256), 148u * 8u);
+        sum_min_kernel<<<blocks, 256, 0, s>>>(ids, nd, sum, mb);
+        const_scale_fill_kernel<<<blocks, 256, 0, s>>>(lis, nd, sum, mb, (float)(yd * xd * zd));
+        count_launch(2);
+        APRB_CHECK_LAUNCH();
+        return;
+    }
+    int sy = std::max(w.win1[0], w.win2[0]), sx = std::max(w.win1[1], w.win2[1]), sz = std::max(w.win1[2], w.win2[2]);
+    if (p.reflect_bc_lis) {
+        sy = yd > 1 ? std::min(sy, yd - 1) : 0;
+        sx = xd > 1 ? std::min(sx, xd - 1) : 0;
+        sz = zd > 1 ? std::min(sz, zd - 1) : 0;
+    } else {
+        sy = sx = sz = 0;
+    }
+    const int py = yd + 2 * sy, px = xd + 2 * sx, pz = zd + 2 * sz;
+    const int pd[3] = {py, px, pz};
+    for (int a = 0; a < 3; ++a)
+        if (w.active[a] && pd[a] < 2 * std::max(w.win1[a], w.win2[a]) + 2) {
+            set_error("local intensity scale window longer than the (padded) image axis");
+            throw Error{APRB_ERR_UNSUPPORTED};
+        }
+    const uint64_t pn = (uint64_t)py * px * pz;
+    float *B = b.padded.as<float>(pn);
+    float *A = b.a.as<float>(pn);
+    float *C2 = b.c.as<float>(pn);
+    pad_reflect_kernel<<<blocks_for(pn, 256), 256, 0, s>>>(ids, yd, xd, zd, B, sy, sx, sz, py, px, pz);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+    const float *src = B;
+    float *bufs[2] = {A, C2};
+    int nb = 0;
+    for (int a = 0; a < 3; ++a)
+        if (w.active[a]) {
+            sat_axis(src, nullptr, bufs[nb], py, px, pz, a, w.win1[a], s);
+            src = bufs[nb];
+            nb ^= 1;
+        }
+    bool first = true;
+    for (int a = 0; a < 3; ++a)
+        if (w.active[a]) {
+            sat_axis(src, first ? B : nullptr, bufs[nb], py, px, pz, a, w.win2[a], s);
+            first = false;
+            src = bufs[nb];
+            nb ^= 1;
+        }
+    unpad_rescale_kernel<<<blocks_for(nd, 256), 256, 0, s>>>(src, py, px, lis, yd, xd, zd, (py - yd) / 2,
+                                                            (px - xd) / 2, (pz - zd) / 2, w.rescale);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+}
+
+template <typename IT>
+void launch_levels(IT *grad, float *lis, const float *ids, uint64_t nd, const float *d_offset, const aprb_params &p,
+                   int apr_l_max, int top_level, uint8_t *level, uint8_t *status, int keep, cudaStream_t s) {
+    APRB_PROF("levels", s);
+    const float mxz = p.dz < p.dx ? p.dz : p.dx;
+    const float min_dim = mxz < p.dy ? mxz : p.dy;
+    const float level_factor = (float)(std::pow(2.0, (double)apr_l_max) * (double)min_dim);
+    const float mult = level_factor / p.rel_error;
+    levels_kernel<IT><<<blocks_for(nd, 256), 256, 0, s>>>(grad, lis, ids, nd, d_offset, p.Ip_th, p.sigma_th,
+                                                         p.sigma_th_max, p.grad_th, mult, top_level, level, status,
+                                                         keep);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+}
+
+template void launch_smooth<uint16_t>(const uint16_t *, uint16_t *, int, int, int, float, const float *, unsigned *,
+                                      cudaStream_t);
+template void launch_smooth<float>(const uint16_t *, float *, int, int, int, float, const float *, unsigned *,
+                                   cudaStream_t);
+template void launch_gradient<uint16_t>(const uint16_t *, int, int, int, uint16_t *, float *, float *, int, int, int,
+                                        const aprb_params &, cudaStream_t);
+template void launch_gradient<float>(const float *, int, int, int, float *, float *, float *, int, int, int,
+                                     const aprb_params &, cudaStream_t);
+template void launch_levels<uint16_t>(uint16_t *, float *, const float *, uint64_t, const float *, const aprb_params &,
+                                      int, int, uint8_t *, uint8_t *, int, cudaStream_t);
+template void launch_levels<float>(float *, float *, const float *, uint64_t, const float *, const aprb_params &, int,
+                                   int, uint8_t *, uint8_t *, int, cudaStream_t);
+
+}  // namespace aprb

@@ -1,0 +1,567 @@
+// Particle-cell pyramid, Pulling Scheme, linear access structure, particle
+// sampling and the APR tree, on the GPU.
+//
+// The Pulling Scheme's per-level steps are "set-if-status" transitions whose
+// sources are never targets within the same step (PullingScheme.hpp:250-393),
+// so each step is written here as a gather over the target cells; the
+// equivalence optimisation runs levels in ascending order as the reference
+// does (LinearAccess.hpp:262-293).  Row counts are scanned on the device and
+// rows are filled by warp-ballot compaction, which keeps the reference's
+// level -> z -> x -> y particle order.
+#include "kernels.cuh"
+
+namespace aprb {
+
+namespace {
+
+struct LevelDims {
+    int yn, xn, zn;
+};
+
+__device__ __forceinline__ void cell_of(uint64_t g, int yn, int xn, int &y, int &x, int &z) {
+    y = (int)(g % (uint64_t)yn);
+    uint64_t r = g / (uint64_t)yn;
+    x = (int)(r % (uint64_t)xn);
+    z = (int)(r / (uint64_t)xn);
+}
+
+// PullingScheme::fill below the top level (PullingScheme.hpp:137-168) on the
+// max-downsampled level image (LocalParticleCellSet.hpp:74-88).
+__global__ void pyramid_fill_kernel(const uint8_t *__restrict__ lev_in, LevelDims di, uint8_t *__restrict__ lev_out,
+                                    uint8_t *__restrict__ status, LevelDims d, int level, int is_min) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)d.yn * d.xn * d.zn) return;
+    int y, x, z;
+    cell_of(g, d.yn, d.xn, y, x, z);
+    const int y1 = min(2 * y + 1, di.yn - 1), x1 = min(2 * x + 1, di.xn - 1), z1 = min(2 * z + 1, di.zn - 1);
+    uint8_t m = lev_in[idx3(2 * y, 2 * x, 2 * z, di.yn, di.xn)];
+    m = max(m, lev_in[idx3(y1, 2 * x, 2 * z, di.yn, di.xn)]);
+    m = max(m, lev_in[idx3(2 * y, x1, 2 * z, di.yn, di.xn)]);
+    m = max(m, lev_in[idx3(y1, x1, 2 * z, di.yn, di.xn)]);
+    m = max(m, lev_in[idx3(2 * y, 2 * x, z1, di.yn, di.xn)]);
+    m = max(m, lev_in[idx3(y1, 2 * x, z1, di.yn, di.xn)]);
+    m = max(m, lev_in[idx3(2 * y, x1, z1, di.yn, di.xn)]);
+    m = max(m, lev_in[idx3(y1, x1, z1, di.yn, di.xn)]);
+    lev_out[g] = m;
+    const bool seed = is_min ? (m <= level) : (m == level);
+    status[g] = seed ? kSeed : kEmpty;
+}
+
+// set_ascendant_neighbours (:250-289)
+__global__ void asc_neighbours_kernel(uint8_t *__restrict__ st, LevelDims d) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)d.yn * d.xn * d.zn) return;
+    const uint8_t s = st[g];
+    if (s != kEmpty && s != kSeed) return;
+    int y, x, z;
+    cell_of(g, d.yn, d.xn, y, x, z);
+    bool hit = false;
+    for (int dz = max(z - 1, 0); dz <= min(z + 1, d.zn - 1) && !hit; ++dz)
+        for (int dx = max(x - 1, 0); dx <= min(x + 1, d.xn - 1) && !hit; ++dx)
+            for (int dy = max(y - 1, 0); dy <= min(y + 1, d.yn - 1); ++dy)
+                if (st[idx3(dy, dx, dz, d.yn, d.xn)] == kAscendant) {
+                    hit = true;
+                    break;
+                }
+    if (hit) st[g] = (s == kEmpty) ? kAscendantNeighbour : kPropagate;
+}
+
+// set_filler (:291-343): children of ASCENDANTNEIGHBOUR / PROPOGATE cells
+__global__ void set_filler_kernel(const uint8_t *__restrict__ parent, LevelDims dp, uint8_t *__restrict__ child,
+                                  LevelDims dc) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)dc.yn * dc.xn * dc.zn) return;
+    if (child[g] != kEmpty) return;
+    int y, x, z;
+    cell_of(g, dc.yn, dc.xn, y, x, z);
+    const uint8_t s = parent[idx3(y / 2, x / 2, z / 2, dp.yn, dp.xn)];
+    if (s == kAscendantNeighbour || s == kPropagate) child[g] = kFiller;
+}
+
+// fill_neighbours (:345-381), boundary part
+__global__ void boundary_kernel(uint8_t *__restrict__ st, LevelDims d) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)d.yn * d.xn * d.zn) return;
+    if (st[g] != kEmpty) return;
+    int y, x, z;
+    cell_of(g, d.yn, d.xn, y, x, z);
+    for (int dz = max(z - 1, 0); dz <= min(z + 1, d.zn - 1); ++dz)
+        for (int dx = max(x - 1, 0); dx <= min(x + 1, d.xn - 1); ++dx)
+            for (int dy = max(y - 1, 0); dy <= min(y + 1, d.yn - 1); ++dy) {
+                const uint8_t q = st[idx3(dy, dx, dz, d.yn, d.xn)];
+                if (q == kSeed || q == kPropagate) {
+                    st[g] = kBoundary;
+                    return;
+                }
+            }
+}
+
+// fill_neighbours -> fill_parent (:372-393), as a gather over the parents
+__global__ void fill_parent_kernel(const uint8_t *__restrict__ child, LevelDims dc, uint8_t *__restrict__ parent,
+                                   LevelDims dp) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)dp.yn * dp.xn * dp.zn) return;
+    if (parent[g] == kSeed) return;
+    int y, x, z;
+    cell_of(g, dp.yn, dp.xn, y, x, z);
+    for (int cz = 2 * z; cz < min(2 * z + 2, dc.zn); ++cz)
+        for (int cx = 2 * x; cx < min(2 * x + 2, dc.xn); ++cx)
+            for (int cy = 2 * y; cy < min(2 * y + 2, dc.yn); ++cy) {
+                const uint8_t q = child[idx3(cy, cx, cz, dc.yn, dc.xn)];
+                if (q == kSeed || q == kPropagate || q == kAscendant) {
+                    parent[g] = kAscendant;
+                    return;
+                }
+            }
+}
+
+// equivalence optimisation (LinearAccess.hpp:262-293) for one level
+__global__ void eqopt_kernel(const uint8_t *__restrict__ parent, LevelDims dp, uint8_t *__restrict__ st, LevelDims d,
+                             int min_type) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)d.yn * d.xn * d.zn) return;
+    int y, x, z;
+    cell_of(g, d.yn, d.xn, y, x, z);
+    const uint8_t s = parent[idx3(y / 2, x / 2, z / 2, dp.yn, dp.xn)];
+    if (s > 0 && s <= min_type) st[g] = kUpsamplingSeed;
+}
+
+__device__ __forceinline__ bool is_particle(uint8_t s, int min_type) { return s > min_type && s <= kUpsamplingSeed; }
+__device__ __forceinline__ bool is_seed(uint8_t s, int min_type) { return s > 0 && s <= min_type; }
+
+// row counts (LinearAccess.hpp:297-407): one warp per (z, x) row
+__global__ void row_count_kernel(const uint8_t *__restrict__ st, LevelDims d, uint64_t *__restrict__ xz_end,
+                                 uint64_t row_base, int min_type) {
+    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= (uint64_t)d.xn * d.zn) return;
+    const uint8_t *R = st + row * (uint64_t)d.yn;
+    unsigned c = 0;
+    for (int y = lane; y < d.yn; y += 32) c += is_particle(R[y], min_type);
+    c = __reduce_add_sync(0xffffffffu, c);
+    if (lane == 0) xz_end[row_base + row] = c;
+}
+
+// top pct level: its own particles plus the l_max particles of its seeds,
+// copied to every l_max row the cell covers (:339-407)
+__global__ void row_count_top_kernel(const uint8_t *__restrict__ st, LevelDims d, uint64_t *__restrict__ xz_end,
+                                     uint64_t row_base, uint64_t row_base_m, int ylm, int xlm, int zlm,
+                                     int min_type) {
+    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= (uint64_t)d.xn * d.zn) return;
+    const uint8_t *R = st + row * (uint64_t)d.yn;
+    unsigned c = 0, cl = 0;
+    for (int y = lane; y < d.yn; y += 32) {
+        const uint8_t s = R[y];
+        if (is_particle(s, min_type))
+            c++;
+        else if (is_seed(s, min_type))
+            cl += 1 + (2 * y < ylm - 1);
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    cl = __reduce_add_sync(0xffffffffu, cl);
+    if (lane < 4) {
+        const int x = (int)(row % (uint64_t)d.xn), z = (int)(row / (uint64_t)d.xn);
+        const int zz = 2 * z + (lane >> 1), xx = 2 * x + (lane & 1);
+        if (zz < zlm && xx < xlm) xz_end[row_base_m + (uint64_t)zz * xlm + xx] = cl;
+        if (lane == 0) xz_end[row_base + row] = c;
+    }
+}
+
+// y fill by ordered warp compaction (:414-497)
+__global__ void row_fill_kernel(const uint8_t *__restrict__ st, LevelDims d, const uint64_t *__restrict__ xz_end,
+                                uint64_t row_base, uint16_t *__restrict__ y_vec, int min_type) {
+    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= (uint64_t)d.xn * d.zn) return;
+    const uint8_t *R = st + row * (uint64_t)d.yn;
+    uint64_t o = xz_end[row_base + row - 1];
+    const unsigned lt = (1u << lane) - 1u;
+    for (int y0 = 0; y0 < d.yn; y0 += 32) {
+        const int y = y0 + lane;
+        const bool f = y < d.yn && is_particle(R[y], min_type);
+        const unsigned m = __ballot_sync(0xffffffffu, f);
+        if (f) y_vec[o + __popc(m & lt)] = (uint16_t)y;
+        o += __popc(m);
+    }
+}
+
+__global__ void row_fill_top_kernel(const uint8_t *__restrict__ st, LevelDims d, const uint64_t *__restrict__ xz_end,
+                                    uint64_t row_base, uint64_t row_base_m, int ylm, int xlm, int zlm,
+                                    uint16_t *__restrict__ y_vec, int min_type) {
+    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= (uint64_t)d.xn * d.zn) return;
+    const int x = (int)(row % (uint64_t)d.xn), z = (int)(row / (uint64_t)d.xn);
+    const uint8_t *R = st + row * (uint64_t)d.yn;
+    uint64_t o = xz_end[row_base + row - 1];
+    uint64_t om[4];
+    bool have[4];
+    for (int q = 0; q < 4; ++q) {
+        const int zz = 2 * z + (q >> 1), xx = 2 * x + (q & 1);
+        have[q] = zz < zlm && xx < xlm;
+        om[q] = have[q] ? xz_end[row_base_m + (uint64_t)zz * xlm + xx - 1] : 0;
+    }
+    uint64_t cm = 0;
+    const unsigned lt = (1u << lane) - 1u;
+    for (int y0 = 0; y0 < d.yn; y0 += 32) {
+        const int y = y0 + lane;
+        const uint8_t s = y < d.yn ? R[y] : 0;
+        const bool f = y < d.yn && is_particle(s, min_type);
+        const unsigned m = __ballot_sync(0xffffffffu, f);
+        if (f) y_vec[o + __popc(m & lt)] = (uint16_t)y;
+        o += __popc(m);
+        const unsigned cnt = (y < d.yn && is_seed(s, min_type)) ? 1u + (2 * y < ylm - 1) : 0u;
+        unsigned incl = cnt;
+        for (int k = 1; k < 32; k <<= 1) {
+            unsigned t = __shfl_up_sync(0xffffffffu, incl, k);
+            if (lane >= k) incl += t;
+        }
+        const unsigned excl = incl - cnt;
+        for (int q = 0; q < 4; ++q) {
+            if (!have[q] || cnt == 0) continue;
+            y_vec[om[q] + cm + excl] = (uint16_t)(2 * y);
+            if (cnt == 2) y_vec[om[q] + cm + excl + 1] = (uint16_t)(2 * y + 1);
+        }
+        cm += __shfl_sync(0xffffffffu, incl, 31);
+    }
+}
+
+// l_max <= 2: every pixel is a particle (LinearAccess.hpp:226-259)
+__global__ void full_res_counts_kernel(uint64_t *xz_end, uint64_t base, int yn, uint64_t rows) {
+    const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (r < rows) xz_end[base + r] = (r + 1) * (uint64_t)yn;
+}
+__global__ void full_res_fill_kernel(uint16_t *y_vec, int yn, uint64_t n) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) y_vec[i] = (uint16_t)(i % (uint64_t)yn);
+}
+
+// ---------------------------------------------------------------------------
+// inclusive scan of uint64 (three phases: block sums, scan of sums, apply)
+// ---------------------------------------------------------------------------
+constexpr int kScanThreads = 256, kScanItems = 8, kScanBlock = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint64_t block_exclusive_scan(uint64_t v, uint64_t *sh, uint64_t &total) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    uint64_t x = v;
+    for (int k = 1; k < 32; k <<= 1) {
+        uint64_t t = __shfl_up_sync(0xffffffffu, x, k);
+        if (lane >= k) x += t;
+    }
+    if (lane == 31) sh[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        uint64_t s = lane < (int)(blockDim.x >> 5) ? sh[lane] : 0;
+        for (int k = 1; k < 32; k <<= 1) {
+            uint64_t t = __shfl_up_sync(0xffffffffu, s, k);
+            if (lane >= k) s += t;
+        }
+        if (lane < (int)(blockDim.x >> 5)) sh[lane] = s;
+    }
+    __syncthreads();
+    const uint64_t before = w > 0 ? sh[w - 1] : 0;
+    total = sh[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+__global__ void scan_sums_kernel(const uint64_t *__restrict__ d, uint64_t n, uint64_t *__restrict__ sums) {
+    __shared__ uint64_t sh[32];
+    const uint64_t base = (uint64_t)blockIdx.x * kScanBlock + (uint64_t)threadIdx.x * kScanItems;
+    uint64_t s = 0;
+    for (int k = 0; k < kScanItems; ++k)
+        if (base + k < n) s += d[base + k];
+    uint64_t total;
+    block_exclusive_scan(s, sh, total);
+    if (threadIdx.x == 0) sums[blockIdx.x] = total;
+}
+
+__global__ void scan_sums_serial_kernel(uint64_t *sums, uint64_t nb) {
+    __shared__ uint64_t sh[32];
+    uint64_t carry = 0;
+    for (uint64_t b0 = 0; b0 < nb; b0 += blockDim.x) {
+        const uint64_t i = b0 + threadIdx.x;
+        const uint64_t v = i < nb ? sums[i] : 0;
+        uint64_t total;
+        const uint64_t ex = block_exclusive_scan(v, sh, total);
+        if (i < nb) sums[i] = carry + ex;
+        carry += total;
+    }
+}
+
+__global__ void scan_apply_kernel(uint64_t *__restrict__ d, uint64_t n, const uint64_t *__restrict__ sums) {
+    __shared__ uint64_t sh[32];
+    const uint64_t base = (uint64_t)blockIdx.x * kScanBlock + (uint64_t)threadIdx.x * kScanItems;
+    uint64_t v[kScanItems];
+    uint64_t s = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < n ? d[base + k] : 0;
+        s += v[k];
+    }
+    uint64_t total;
+    uint64_t run = block_exclusive_scan(s, sh, total) + sums[blockIdx.x];
+    for (int k = 0; k < kScanItems; ++k) {
+        run += v[k];
+        if (base + k < n) d[base + k] = run;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// sampling
+// ---------------------------------------------------------------------------
+// downsample(sum, x/8.0f) into uint16 (PixelData.hpp:1037-1058): the 8-term
+// float sum is exact, so the stored value is floor(sum / 8).
+__global__ void pyr_mean_u16_kernel(const uint16_t *__restrict__ in, LevelDims di, uint16_t *__restrict__ out,
+                                    LevelDims d) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)d.yn * d.xn * d.zn) return;
+    int y, x, z;
+    cell_of(g, d.yn, d.xn, y, x, z);
+    const int y1 = min(2 * y + 1, di.yn - 1), x1 = min(2 * x + 1, di.xn - 1), z1 = min(2 * z + 1, di.zn - 1);
+    const int y0 = 2 * y, x0 = 2 * x, z0 = 2 * z;
+    unsigned s = in[idx3(y0, x0, z0, di.yn, di.xn)];
+    s += in[idx3(y1, x0, z0, di.yn, di.xn)];
+    s += in[idx3(y0, x1, z0, di.yn, di.xn)];
+    s += in[idx3(y1, x1, z0, di.yn, di.xn)];
+    s += in[idx3(y0, x0, z1, di.yn, di.xn)];
+    s += in[idx3(y1, x0, z1, di.yn, di.xn)];
+    s += in[idx3(y0, x1, z1, di.yn, di.xn)];
+    s += in[idx3(y1, x1, z1, di.yn, di.xn)];
+    out[g] = (uint16_t)(s >> 3);
+}
+
+__global__ void gather_kernel(const uint16_t *__restrict__ im, LevelDims d, const uint64_t *__restrict__ xz_end,
+                              uint64_t row_base, const uint16_t *__restrict__ y_vec, uint16_t *__restrict__ parts) {
+    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= (uint64_t)d.xn * d.zn) return;
+    const uint64_t b = xz_end[row_base + row - 1], e = xz_end[row_base + row];
+    const uint16_t *R = im + row * (uint64_t)d.yn;
+    for (uint64_t i = b + lane; i < e; i += 32) parts[i] = R[y_vec[i]];
+}
+
+// ---------------------------------------------------------------------------
+// APR tree (APR.hpp:633-689, LinearAccess.hpp:67-122)
+// ---------------------------------------------------------------------------
+__global__ void tree_mark_kernel(LevelDims d, const uint64_t *__restrict__ xz_end, uint64_t row_base,
+                                 const uint16_t *__restrict__ y_vec, uint8_t *__restrict__ flags, LevelDims dp) {
+    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= (uint64_t)d.xn * d.zn) return;
+    const int x = (int)(row % (uint64_t)d.xn), z = (int)(row / (uint64_t)d.xn);
+    const uint64_t b = xz_end[row_base + row - 1], e = xz_end[row_base + row];
+    uint8_t *P = flags + idx3(0, x / 2, z / 2, dp.yn, dp.xn);
+    for (uint64_t i = b + lane; i < e; i += 32) P[y_vec[i] / 2] = 1;
+}
+
+__global__ void tree_prop_kernel(uint8_t *__restrict__ p, LevelDims d, const uint8_t *__restrict__ c, LevelDims dc) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)d.yn * d.xn * d.zn) return;
+    int y, x, z;
+    cell_of(g, d.yn, d.xn, y, x, z);
+    p[g] = p[g] | c[idx3(2 * y, 2 * x, 2 * z, dc.yn, dc.xn)];
+}
+
+__global__ void flag_count_kernel(const uint8_t *__restrict__ f, LevelDims d, uint64_t *__restrict__ xz_end,
+                                  uint64_t row_base) {
+    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= (uint64_t)d.xn * d.zn) return;
+    const uint8_t *R = f + row * (uint64_t)d.yn;
+    unsigned c = 0;
+    for (int y = lane; y < d.yn; y += 32) c += R[y];
+    c = __reduce_add_sync(0xffffffffu, c);
+    if (lane == 0) xz_end[row_base + row] = c;
+}
+
+__global__ void flag_fill_kernel(const uint8_t *__restrict__ f, LevelDims d, const uint64_t *__restrict__ xz_end,
+                                 uint64_t row_base, uint16_t *__restrict__ y_vec) {
+    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= (uint64_t)d.xn * d.zn) return;
+    const uint8_t *R = f + row * (uint64_t)d.yn;
+    uint64_t o = xz_end[row_base + row - 1];
+    const unsigned lt = (1u << lane) - 1u;
+    for (int y0 = 0; y0 < d.yn; y0 += 32) {
+        const int y = y0 + lane;
+        const bool fl = y < d.yn && R[y] != 0;
+        const unsigned m = __ballot_sync(0xffffffffu, fl);
+        if (fl) y_vec[o + __popc(m & lt)] = (uint16_t)y;
+        o += __popc(m);
+    }
+}
+
+LevelDims dims(const Geom &g, int l) { return LevelDims{g.y_num[l], g.x_num[l], g.z_num[l]}; }
+uint64_t ncell(const Geom &g, int l) { return (uint64_t)g.y_num[l] * g.x_num[l] * g.z_num[l]; }
+uint64_t nrow(const Geom &g, int l) { return (uint64_t)g.x_num[l] * g.z_num[l]; }
+unsigned row_blocks(uint64_t rows) { return blocks_for(rows * 32, 256); }
+
+}  // namespace
+
+void inclusive_scan_u64(uint64_t *data, uint64_t n, DevBuf &tmp, cudaStream_t s) {
+    const uint64_t nb = (n + kScanBlock - 1) / kScanBlock;
+    uint64_t *sums = tmp.as<uint64_t>(nb + 1);
+    scan_sums_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(data, n, sums);
+    scan_sums_serial_kernel<<<1, 1024, 0, s>>>(sums, nb);
+    scan_apply_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(data, n, sums);
+    count_launch(3);
+    APRB_CHECK_LAUNCH();
+}
+
+void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s) {
+    const int top = g.l_max - 1, lmin = g.l_min;
+    if (top < lmin) return;
+    APRB_PROF("pulling_scheme", s);
+    for (int l = top - 1; l >= lmin; --l) {
+        pyramid_fill_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(pm.level[l + 1], dims(g, l + 1), pm.level[l],
+                                                                        pm.status[l], dims(g, l), l, l == lmin);
+        count_launch();
+    }
+    APRB_CHECK_LAUNCH();
+    for (int l = top; l >= lmin; --l) {
+        if (l != top) {
+            asc_neighbours_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(pm.status[l], dims(g, l));
+            set_filler_kernel<<<blocks_for(ncell(g, l + 1), 256), 256, 0, s>>>(pm.status[l], dims(g, l),
+                                                                              pm.status[l + 1], dims(g, l + 1));
+            count_launch(2);
+        }
+        boundary_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(pm.status[l], dims(g, l));
+        count_launch();
+        if (l - 1 >= lmin) {
+            fill_parent_kernel<<<blocks_for(ncell(g, l - 1), 256), 256, 0, s>>>(pm.status[l], dims(g, l),
+                                                                               pm.status[l - 1], dims(g, l - 1));
+            count_launch();
+        }
+    }
+    APRB_CHECK_LAUNCH();
+}
+
+uint64_t launch_linear_counts(const Geom &g, Pyramid &pm, uint64_t *xz_end, uint64_t n_xz, int min_type,
+                              DevBuf &scan_tmp, cudaStream_t s) {
+    APRB_PROF("linear_counts", s);
+    const int L = g.l_max, lmin = g.l_min;
+    APRB_CUDA(cudaMemsetAsync(xz_end, 0, n_xz * sizeof(uint64_t), s));
+    for (int l = lmin + 1; l < L; ++l) {
+        eqopt_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(pm.status[l - 1], dims(g, l - 1), pm.status[l],
+                                                                 dims(g, l), min_type);
+        count_launch();
+    }
+    for (int l = lmin; l < L - 1; ++l) {
+        row_count_kernel<<<row_blocks(nrow(g, l)), 256, 0, s>>>(pm.status[l], dims(g, l), xz_end, g.level_xz[l],
+                                                               min_type);
+        count_launch();
+    }
+    row_count_top_kernel<<<row_blocks(nrow(g, L - 1)), 256, 0, s>>>(pm.status[L - 1], dims(g, L - 1), xz_end,
+                                                                   g.level_xz[L - 1], g.level_xz[L], g.y_num[L],
+                                                                   g.x_num[L], g.z_num[L], min_type);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+    inclusive_scan_u64(xz_end, n_xz, scan_tmp, s);
+    uint64_t P = 0;
+    APRB_CUDA(cudaMemcpyAsync(&P, xz_end + n_xz - 1, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    APRB_CUDA(cudaStreamSynchronize(s));
+    return P;
+}
+
+void launch_linear_fill(const Geom &g, const Pyramid &pm, const uint64_t *xz_end, uint16_t *y_vec, int min_type,
+                        cudaStream_t s) {
+    APRB_PROF("linear_fill", s);
+    const int L = g.l_max, lmin = g.l_min;
+    for (int l = lmin; l < L - 1; ++l) {
+        row_fill_kernel<<<row_blocks(nrow(g, l)), 256, 0, s>>>(pm.status[l], dims(g, l), xz_end, g.level_xz[l], y_vec,
+                                                              min_type);
+        count_launch();
+    }
+    row_fill_top_kernel<<<row_blocks(nrow(g, L - 1)), 256, 0, s>>>(pm.status[L - 1], dims(g, L - 1), xz_end,
+                                                                  g.level_xz[L - 1], g.level_xz[L], g.y_num[L],
+                                                                  g.x_num[L], g.z_num[L], y_vec, min_type);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+}
+
+void launch_full_resolution_structure(const Geom &g, uint64_t *xz_end, uint16_t *y_vec, cudaStream_t s) {
+    const int L = g.l_max;
+    const uint64_t rows = nrow(g, L);
+    full_res_counts_kernel<<<blocks_for(rows, 256), 256, 0, s>>>(xz_end, g.level_xz[L], g.y_num[L], rows);
+    if (y_vec) full_res_fill_kernel<<<blocks_for(ncell(g, L), 256), 256, 0, s>>>(y_vec, g.y_num[L], ncell(g, L));
+    count_launch(y_vec ? 2 : 1);
+    APRB_CHECK_LAUNCH();
+}
+
+void launch_sample(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const uint16_t *img,
+                   uint16_t *parts, DevBuf &pyr, cudaStream_t s) {
+    APRB_PROF("sample_image", s);
+    const int L = g.l_max, lmin = g.l_min;
+    uint64_t total = 0;
+    uint64_t off[32] = {};
+    for (int l = lmin; l < L; ++l) {
+        off[l] = total;
+        total += (ncell(g, l) + 7) & ~uint64_t(7);
+    }
+    uint16_t *base = pyr.as<uint16_t>(total ? total : 8);
+    const uint16_t *lev[32] = {};
+    lev[L] = img;
+    for (int l = L - 1; l >= lmin; --l) {
+        uint16_t *o = base + off[l];
+        pyr_mean_u16_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(lev[l + 1], dims(g, l + 1), o, dims(g, l));
+        count_launch();
+        lev[l] = o;
+    }
+    for (int l = lmin; l <= L; ++l) {
+        gather_kernel<<<row_blocks(nrow(g, l)), 256, 0, s>>>(lev[l], dims(g, l), xz_end, g.level_xz[l], y_vec, parts);
+        count_launch();
+    }
+    APRB_CHECK_LAUNCH();
+}
+
+uint64_t launch_tree_build(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
+                           uint64_t *t_xz_end, uint64_t t_n_xz, DevBuf &flags, DevBuf &scan_tmp, cudaStream_t s) {
+    APRB_PROF("tree_build", s);
+    uint64_t total = 0;
+    uint64_t off[32] = {};
+    for (int t = tg.l_min; t <= tg.l_max; ++t) {
+        off[t] = total;
+        total += (ncell(tg, t) + 15) & ~uint64_t(15);
+    }
+    uint8_t *f = flags.as<uint8_t>(total ? total : 16);
+    APRB_CUDA(cudaMemsetAsync(f, 0, total ? total : 16, s));
+    for (int l = g.l_max; l >= g.l_min; --l) {
+        if (l - 1 < tg.l_min) continue;
+        tree_mark_kernel<<<row_blocks(nrow(g, l)), 256, 0, s>>>(dims(g, l), xz_end, g.level_xz[l], y_vec,
+                                                               f + off[l - 1], dims(tg, l - 1));
+        count_launch();
+    }
+    for (int t = tg.l_max - 1; t >= tg.l_min; --t) {
+        tree_prop_kernel<<<blocks_for(ncell(tg, t), 256), 256, 0, s>>>(f + off[t], dims(tg, t), f + off[t + 1],
+                                                                       dims(tg, t + 1));
+        count_launch();
+    }
+    APRB_CUDA(cudaMemsetAsync(t_xz_end, 0, t_n_xz * sizeof(uint64_t), s));
+    for (int t = tg.l_min; t <= tg.l_max; ++t) {
+        flag_count_kernel<<<row_blocks(nrow(tg, t)), 256, 0, s>>>(f + off[t], dims(tg, t), t_xz_end, tg.level_xz[t]);
+        count_launch();
+    }
+    APRB_CHECK_LAUNCH();
+    inclusive_scan_u64(t_xz_end, t_n_xz, scan_tmp, s);
+    uint64_t T = 0;
+    APRB_CUDA(cudaMemcpyAsync(&T, t_xz_end + t_n_xz - 1, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    APRB_CUDA(cudaStreamSynchronize(s));
+    return T;
+}
+
+void launch_tree_fill(const Geom &tg, const DevBuf &flags, const uint64_t *t_xz_end, uint16_t *t_y_vec,
+                      cudaStream_t s) {
+    uint64_t total = 0;
+    const uint8_t *f = (const uint8_t *)flags.p;
+    for (int t = tg.l_min; t <= tg.l_max; ++t) {
+        flag_fill_kernel<<<row_blocks(nrow(tg, t)), 256, 0, s>>>(f + total, dims(tg, t), t_xz_end, tg.level_xz[t],
+                                                                t_y_vec);
+        count_launch();
+        total += (ncell(tg, t) + 15) & ~uint64_t(15);
+    }
+    APRB_CHECK_LAUNCH();
+}
+
+}  // namespace aprb

@@ -1,0 +1,149 @@
+// Seeded synthetic benchmark volumes: background + isotropic Gaussian blobs +
+// Poisson noise, rounded and clipped to uint16.  Blob parameters come from a
+// host splitmix64 stream; each 16^3 brick of the volume sums the blobs whose
+// 4-sigma box meets it, in blob order, so the image is deterministic.  Poisson
+// deviates use a counter-based generator per voxel: multiplication of
+// uniforms for small means, Hoermann's transformed rejection (PTRS, 1993)
+// otherwise.
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace aprb {
+
+namespace {
+
+constexpr int kBrick = 16;
+
+struct Blob {
+    float cz, cx, cy, inv2s2, amp;
+};
+
+uint64_t splitmix64(uint64_t &s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+double unif(uint64_t &s) { return (double)(splitmix64(s) >> 11) * (1.0 / 9007199254740992.0); }
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z) {
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+struct Rng {
+    uint64_t s;
+    __device__ double next() {
+        s += 0x9E3779B97F4A7C15ull;
+        return (double)(mix64(s) >> 11) * (1.0 / 9007199254740992.0);
+    }
+};
+
+__device__ int poisson(double lam, Rng &r) {
+    if (lam <= 0) return 0;
+    if (lam < 10.0) {
+        const double L = exp(-lam);
+        double p = 1.0;
+        int k = 0;
+        do {
+            ++k;
+            p *= r.next();
+        } while (p > L && k < 1000);
+        return k - 1;
+    }
+    const double slam = sqrt(lam), loglam = log(lam);
+    const double b = 0.931 + 2.53 * slam, a = -0.059 + 0.02483 * b;
+    const double invalpha = 1.1239 + 1.1328 / (b - 3.4), vr = 0.9277 - 3.6224 / (b - 2);
+    for (int it = 0; it < 1000; ++it) {
+        const double U = r.next() - 0.5, V = r.next();
+        const double us = 0.5 - fabs(U);
+        const long long k = (long long)floor((2 * a / us + b) * U + lam + 0.43);
+        if (us >= 0.07 && V <= vr) return (int)k;
+        if (k < 0 || (us < 0.013 && V > us)) continue;
+        if (log(V) + log(invalpha) - log(a / (us * us) + b) <= -lam + k * loglam - lgamma((double)k + 1)) return (int)k;
+    }
+    return (int)lam;
+}
+
+__global__ void render_kernel(uint16_t *__restrict__ img, int yn, int xn, int zn, const Blob *__restrict__ blobs,
+                              const uint32_t *__restrict__ boff, const uint32_t *__restrict__ bidx, int bx, int by,
+                              float bg, uint64_t seed) {
+    const int brick = blockIdx.x;
+    const int bYi = brick % by, bXi = (brick / by) % bx, bZi = brick / (by * bx);
+    const uint32_t b0 = boff[brick], b1 = boff[brick + 1];
+    for (int t = threadIdx.x; t < kBrick * kBrick * kBrick; t += blockDim.x) {
+        const int y = bYi * kBrick + (t % kBrick), x = bXi * kBrick + ((t / kBrick) % kBrick),
+                  z = bZi * kBrick + t / (kBrick * kBrick);
+        if (y >= yn || x >= xn || z >= zn) continue;
+        float v = bg;
+        const float fy = y + 0.5f, fx = x + 0.5f, fz = z + 0.5f;
+        for (uint32_t k = b0; k < b1; ++k) {
+            const Blob B = blobs[bidx[k]];
+            const float dy = fy - B.cy, dx = fx - B.cx, dz = fz - B.cz;
+            v += B.amp * expf(-(dy * dy + dx * dx + dz * dz) * B.inv2s2);
+        }
+        const uint64_t vox = idx3(y, x, z, yn, xn);
+        Rng r{mix64(seed ^ mix64(vox + 0x1234567ull))};
+        int p = poisson((double)v, r);
+        p = p < 0 ? 0 : (p > 65535 ? 65535 : p);
+        img[vox] = (uint16_t)p;
+    }
+}
+
+}  // namespace
+
+void launch_synth_blobs(uint16_t *img, int yn, int xn, int zn, int n_blobs, float slo, float shi, float alo,
+                        float ahi, float bg, uint64_t seed, DevBuf &buf, cudaStream_t s) {
+    uint64_t st = seed * 0x2545F4914F6CDD1Dull + 0x632BE59BD9B4E019ull;
+    std::vector<Blob> blobs((size_t)n_blobs);
+    const int by = (yn + kBrick - 1) / kBrick, bx = (xn + kBrick - 1) / kBrick, bz = (zn + kBrick - 1) / kBrick;
+    const uint64_t nb = (uint64_t)by * bx * bz;
+    std::vector<uint32_t> count(nb + 1, 0);
+    std::vector<int> lo(6 * (size_t)n_blobs);
+    for (int i = 0; i < n_blobs; ++i) {
+        Blob &B = blobs[i];
+        B.cz = (float)(unif(st) * zn);
+        B.cx = (float)(unif(st) * xn);
+        B.cy = (float)(unif(st) * yn);
+        const float sg = (float)(slo + unif(st) * (shi - slo));
+        B.amp = (float)(alo + unif(st) * (ahi - alo));
+        B.inv2s2 = 1.0f / (2.0f * sg * sg);
+        const float r = 4.0f * sg;
+        int *q = &lo[6 * (size_t)i];
+        q[0] = std::max(0, (int)std::floor((B.cz - r) / kBrick));
+        q[1] = std::min(bz - 1, (int)std::floor((B.cz + r) / kBrick));
+        q[2] = std::max(0, (int)std::floor((B.cx - r) / kBrick));
+        q[3] = std::min(bx - 1, (int)std::floor((B.cx + r) / kBrick));
+        q[4] = std::max(0, (int)std::floor((B.cy - r) / kBrick));
+        q[5] = std::min(by - 1, (int)std::floor((B.cy + r) / kBrick));
+        for (int a = q[0]; a <= q[1]; ++a)
+            for (int b = q[2]; b <= q[3]; ++b)
+                for (int c = q[4]; c <= q[5]; ++c) count[((uint64_t)a * bx + b) * by + c + 1]++;
+    }
+    for (uint64_t i = 1; i <= nb; ++i) count[i] += count[i - 1];
+    std::vector<uint32_t> idx(count[nb]);
+    std::vector<uint32_t> fill(count.begin(), count.end() - 1);
+    for (int i = 0; i < n_blobs; ++i) {
+        const int *q = &lo[6 * (size_t)i];
+        for (int a = q[0]; a <= q[1]; ++a)
+            for (int b = q[2]; b <= q[3]; ++b)
+                for (int c = q[4]; c <= q[5]; ++c) idx[fill[((uint64_t)a * bx + b) * by + c]++] = (uint32_t)i;
+    }
+    const size_t bytes_blobs = sizeof(Blob) * blobs.size(), bytes_off = sizeof(uint32_t) * count.size(),
+                 bytes_idx = sizeof(uint32_t) * idx.size();
+    char *d = (char *)buf.get(bytes_blobs + bytes_off + bytes_idx + 64);
+    Blob *dB = (Blob *)d;
+    uint32_t *dO = (uint32_t *)(d + ((bytes_blobs + 15) & ~size_t(15)));
+    uint32_t *dI = dO + count.size();
+    APRB_CUDA(cudaMemcpyAsync(dB, blobs.data(), bytes_blobs, cudaMemcpyHostToDevice, s));
+    APRB_CUDA(cudaMemcpyAsync(dO, count.data(), bytes_off, cudaMemcpyHostToDevice, s));
+    if (bytes_idx) APRB_CUDA(cudaMemcpyAsync(dI, idx.data(), bytes_idx, cudaMemcpyHostToDevice, s));
+    render_kernel<<<(unsigned)nb, 256, 0, s>>>(img, yn, xn, zn, dB, dO, dI, bx, by, bg, seed);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+    APRB_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
+}
+
+}  // namespace aprb

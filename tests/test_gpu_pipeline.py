@@ -1,0 +1,112 @@
+"""GPU parity of get_apr and sample_image, through the C ABI, against the CPU
+oracle (bit-exact structure, intermediates and uint16 intensities) and against
+the reference's golden fixtures."""
+import os
+
+import numpy as np
+import pytest
+
+import libapr_b200 as A
+from oracle import bind as B
+from tests.helpers import bits_equal, lib_params, oracle_params, volume
+
+pytestmark = pytest.mark.gpu
+
+STAGE_SHAPE_DS = lambda s: ((s[0] + 1) // 2, (s[1] + 1) // 2, (s[2] + 1) // 2)
+
+SHAPES = [((40, 48, 56), 30, 1), ((17, 33, 70), 12, 2), ((5, 64, 9), 4, 3), ((33, 65, 31), 20, 6),
+          ((1, 63, 64), 6, 4), ((1, 1, 100), 2, 5), ((64, 64, 64), 60, 8)]
+
+
+def gpu_apr(img, image_type, **kw):
+    conv = A.APRConverter("uint16" if image_type == 1 else "float")
+    conv.par = lib_params(**kw)
+    conv.keep_intermediates(True)
+    apr = A.APR()
+    assert conv.get_apr(apr, img)
+    return conv, apr
+
+
+@pytest.mark.parametrize("image_type", [1, 0])
+@pytest.mark.parametrize("shape,blobs,seed", SHAPES)
+def test_get_apr_bit_exact(shape, blobs, seed, image_type):
+    img = volume(shape, blobs, seed)
+    e, acc, (off, inter) = B.orc_get_apr(img, oracle_params(), image_type)
+    assert e == 0
+    conv, apr = gpu_apr(img, image_type)
+    ds = STAGE_SHAPE_DS(shape)
+    assert apr.bspline_offset() == off
+    assert bits_equal(conv.intermediate(0, shape), inter[0]), "smoothed image"
+    for w in range(1, 7):
+        assert bits_equal(conv.intermediate(w, ds), inter[w]), "stage %d" % w
+    lx, xe, yv = apr.linear_access()
+    assert np.array_equal(lx, acc.level_xz)
+    assert np.array_equal(xe, acc.xz_end)
+    assert np.array_equal(yv, acc.y_vec)
+    parts = A.ParticleData().sample_image(apr, img).data
+    assert np.array_equal(parts, B.orc_sample(acc, img))
+
+
+@pytest.mark.parametrize("kw", [dict(lambda_=0.5), dict(lambda_=10.0), dict(sigma_th=0.0, grad_th=0.0),
+                                dict(neighborhood_optimization=False), dict(Ip_th=150.0, rel_error=0.05),
+                                dict(constant_intensity_scale=True), dict(lambda_=0.0)])
+def test_get_apr_parameter_variants(kw):
+    img = volume((24, 40, 36), 10, 11)
+    e, acc, (off, inter) = B.orc_get_apr(img, oracle_params(**kw), 1)
+    assert e == 0
+    conv, apr = gpu_apr(img, 1, **kw)
+    lx, xe, yv = apr.linear_access()
+    assert np.array_equal(xe, acc.xz_end) and np.array_equal(yv, acc.y_vec)
+    for w in range(1, 7):
+        assert bits_equal(conv.intermediate(w, STAGE_SHAPE_DS(img.shape)), inter[w]), w
+
+
+@pytest.mark.parametrize("case", ["sphere_diff_dims", "sphere_120", "sphere_2D", "sphere_1D"])
+def test_golden_spheres(golden_dir, case):
+    d = np.load(os.path.join(golden_dir, case + ".npz"))
+    lam, E, gth, sth, sthm = [float(v) for v in d["params"]]
+    img = d["original"]
+    conv, apr = gpu_apr(img, 1, lambda_=lam, rel_error=E, grad_th=gth, sigma_th=max(sth, 0.1),
+                        sigma_th_max=max(sthm, 0.1), Ip_th=0.0)
+    ds = STAGE_SHAPE_DS(img.shape)
+    assert np.abs(conv.intermediate(1, ds) - d["gradient_saved"].astype(np.float32)).max() <= 1
+    assert np.abs(conv.intermediate(3, ds) - d["scale_saved"]).max() <= 1
+    assert apr.total_number_particles() == int(d["total_number_particles"][0])
+
+
+def test_overflow_raises_value_error():
+    img = volume((20, 24, 28), 5, 7)
+    img[10, 12, 14] = 65535 - 100
+    img[0, 0, 0] = 0
+    conv = A.APRConverter("uint16")
+    conv.par = lib_params()
+    with pytest.raises(ValueError):
+        conv.get_apr(A.APR(), img)
+    # float ImageType has no overflow check
+    conv = A.APRConverter("float")
+    conv.par = lib_params()
+    assert conv.get_apr(A.APR(), img)
+
+
+def test_dimension_check():
+    conv = A.APRConverter("uint16")
+    conv.par = lib_params(check_input=True)
+    img = volume((40, 1, 1), 2, 3)  # data along z only: fails the check
+    assert conv.get_apr(A.APR(), img) is False
+    conv.par = lib_params(check_input=True, swap_dimensions=True)
+    assert conv.get_apr(A.APR(), img) is True
+
+
+def test_empty_and_flat_inputs():
+    conv = A.APRConverter("uint16")
+    conv.par = lib_params()
+    flat = np.full((16, 16, 16), 100, np.uint16)
+    apr = A.APR()
+    assert conv.get_apr(apr, flat)
+    e, acc, _ = B.orc_get_apr(flat, oracle_params(), 1)
+    lx, xe, yv = apr.linear_access()
+    assert np.array_equal(xe, acc.xz_end) and np.array_equal(yv, acc.y_vec)
+    tiny = np.array([[[7, 9, 200]]], np.uint16)
+    assert conv.get_apr(apr, tiny)
+    e, acc, _ = B.orc_get_apr(tiny, oracle_params(), 1)
+    assert np.array_equal(apr.linear_access()[2], acc.y_vec)
