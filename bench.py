@@ -6,7 +6,9 @@ then APR isotropic 3x3x3 and 5x5x5 convolution over its particles.
 One JSON line on rank 0.  A step is one get_apr + sample_image pass over one
 seeded synthetic volume (background 100, 60000 Gaussian blobs sigma U[2,8] px,
 amplitude U[500,6000], Poisson noise; APR parameters lambda=3, E=0.1,
-Ip_th=0, sigma_th=50, grad_th=10, ImageType uint16).  ``value`` is whole-job
+Ip_th=0, sigma_th=50, grad_th=10; ImageType float by default, because with
+ImageType uint16 the reference's B-spline overflow check throws on this
+volume).  ``value`` is whole-job
 GVox/s with the input resident in HBM; ``e2e`` is the same through the
 host-buffer C ABI (image host->device and particles device->host inside the
 timed region).  Under torchrun every rank converts its own volume (different
@@ -104,17 +106,18 @@ def lib_params():
     return p
 
 
-def algorithmic_bytes(stage, N, Nd, P, T):
-    """Minimum HBM bytes of one launch of a stage (uint16 ImageType)."""
+def algorithmic_bytes(stage, N, Nd, P, T, its=2):
+    """Minimum HBM bytes of one launch of a stage (its = bytes per ImageType
+    value: 2 for uint16, 4 for float)."""
     return {
-        "bspline_y": 2 * 2 * N, "bspline_x": 2 * 2 * N, "bspline_z": 2 * 2 * N,
-        "gradient_ds": 2 * N + 6 * Nd, "inv_bspline": 8 * Nd, "local_intensity_scale": 8 * Nd,
+        "bspline_y": (2 + its) * N, "bspline_x": 2 * its * N, "bspline_z": 2 * its * N,
+        "gradient_ds": its * N + (its + 8) * Nd, "inv_bspline": 8 * Nd, "local_intensity_scale": 8 * Nd,
         "levels": 14 * Nd, "offset": 2 * N, "sample_image": 2 * N + 4 * P,
         "convolve": 10 * P + 10 * T, "fill_tree_mean": 6 * P + 6 * T,
     }.get(stage)
 
 
-def cpu_baseline(host_img, steps=2):
+def cpu_baseline(host_img, image_type, steps=2):
     """The reference's own CPU get_apr + sample_image (oracle/_ref, Release
     flags) on a z-slab of the volume, all host threads."""
     from oracle import bind as B
@@ -125,7 +128,10 @@ def cpu_baseline(host_img, steps=2):
     ts = []
     for _ in range(steps):
         t0 = time.perf_counter()
-        e, r = B.ref_get_apr(slab, p, 1, staged=False, fast=True)
+        e, r = B.ref_get_apr(slab, p, image_type, staged=False, fast=True)
+        if e != 0:
+            return {"value": None, "unit": "GVox/s", "cores": os.cpu_count(), "kind": "reference",
+                    "sample": "reference get_apr failed with status %d on the slab" % e}
         r.sample(slab)
         ts.append(time.perf_counter() - t0)
         del r
@@ -164,7 +170,10 @@ def run_reference(args):
     times = []
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        e, r = B.ref_get_apr(img, p, 1, staged=False, fast=True)
+        e, r = B.ref_get_apr(img, p, 1 if args.image_type == "uint16" else 0, staged=False, fast=True)
+        if e != 0:
+            print(json.dumps({"impl": "reference", "unavailable": "reference get_apr failed with status %d" % e}))
+            return 0
         r.sample(img)
         dt = time.perf_counter() - t0
         del r
@@ -174,9 +183,10 @@ def run_reference(args):
     v = img.size / t / 1e9
     line = {"metric": METRIC, "value": v, "unit": "GVox/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f32" if args.image_type == "float" else "u16", "data": "synthetic",
             "config": {"workload": "get_apr + sample_image, uint16 2048x2048x512 blob volume (each step a "
-                                   "2048x2048x%d z-slab of it)" % CPU_SLAB_Z, "image_type": "uint16", **PARAMS},
+                                   "2048x2048x%d z-slab of it)" % CPU_SLAB_Z, "image_type": args.image_type,
+                       **PARAMS},
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "GVox/s", "cores": os.cpu_count(), "kind": "reference",
                              "sample": "z-slab %s per step, LibAPR CPU get_apr_cpu + sample_image at Release "
@@ -195,6 +205,8 @@ def main():
     ap.add_argument("--shape", default=None, help="z,x,y override (debugging only)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-conv", action="store_true")
+    ap.add_argument("--image-type", default="float", choices=["float", "uint16"],
+                    help="APRConverter ImageType; uint16 throws the reference's overflow error on this volume")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -222,8 +234,9 @@ def main():
     A.synth_blobs_device(img, int(BLOBS * N / (SHAPE[0] * SHAPE[1] * SHAPE[2])), SIGMA, AMP, BG,
                          seed=1000 + rank, stream=stream)
     torch.cuda.synchronize()
-    conv = A.APRConverter("uint16")
+    conv = A.APRConverter(args.image_type)
     par = lib_params().c()
+    it_code = 1 if args.image_type == "uint16" else 0
     iptr = C.c_void_p(img.data_ptr())
 
     def get_apr_dev():
@@ -296,13 +309,13 @@ def main():
         dom = max(stages.items(), key=lambda kv: kv[1][0])
         dname, (dms, dcnt) = dom
         per = dms / dcnt / 1e3
-        ab = algorithmic_bytes(dname, N, Nd, P, 0)
+        ab = algorithmic_bytes(dname, N, Nd, P, 0, 2 if it_code == 1 else 4)
         achieved = ab / per / 1e9 if ab else None
         out["roofline"] = {"bound": "hbm", "kernel": dname, "achieved": achieved, "peak": hbm, "unit": "GB/s",
                            "frac": achieved / hbm if achieved else None, "traffic": None,
                            "peak_source": peak_kind, "algorithmic_bytes_per_launch": ab,
                            "launch_ms": per * 1e3}
-        pipe_b = 10 * N + 4 * P
+        pipe_b = (10 if it_code == 1 else 14) * N + 4 * P
         out["pipeline_roofline"] = {"algorithmic_bytes": pipe_b, "achieved_gbs": pipe_b / (ms_all / 1e3) / 1e9,
                                     "frac": pipe_b / (ms_all / 1e3) / 1e9 / hbm}
         out["stages_ms_per_step"] = {k: v[0] / args.steps for k, v in stages.items()}
@@ -376,13 +389,14 @@ def main():
                "d2h_bytes_per_step": 2 * P, "ms_per_step": te * 1e3}
         cpu = None
         if not args.no_cpu:
-            cpu = cpu_baseline(host.numpy().view(np.uint16))
+            cpu = cpu_baseline(host.numpy().view(np.uint16), it_code)
         line = {"metric": METRIC, "value": N * world / (ms_all / 1e3) / 1e9, "unit": "GVox/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_all, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "u16", "data": "synthetic",
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32" if it_code == 0 else "u16",
+                "data": "synthetic",
                 "config": {"workload": "get_apr + sample_image, uint16 %dx%dx%d (y,x,z) blob volume, "
                                        "60000 blobs per 2048x2048x512, per GPU" % (y, x, z),
-                           "image_type": "uint16", **PARAMS, "particles": P,
+                           "image_type": args.image_type, **PARAMS, "particles": P,
                            "l2": "input 4 GiB > L2, no flush needed",
                            "parallelism": "independent volume per GPU" if world > 1 else "1 GPU"},
                 "gpu_launches": int(launches), "e2e": e2e, "cpu_baseline": cpu, **out, **conv_res}
