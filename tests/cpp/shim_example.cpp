@@ -1,0 +1,40 @@
+// Drop-in use of the C++ host layer (include/aprb200.hpp): the calls below
+// have the shape of LibAPR code (Example_get_apr.cpp / Example_apr_filter.cpp).
+// Prints "P=<particles> sum=<sum of intensities> conv=<sum of conv output>".
+#include <cstdio>
+#include <cstdlib>
+
+#include "aprb200.hpp"
+
+using namespace aprb200::compat;
+
+int main(int argc, char **argv) {
+    const char *path = argc > 1 ? argv[1] : nullptr;
+    int y = 48, x = 40, z = 24;
+    PixelData<uint16_t> img(y, x, z);
+    if (path) {
+        FILE *f = std::fopen(path, "rb");
+        if (!f || std::fread(img.mesh.data(), 2, img.mesh.size(), f) != img.mesh.size()) return 2;
+        std::fclose(f);
+    }
+    APRConverter<uint16_t> conv;
+    conv.par.lambda = 3;
+    conv.par.rel_error = 0.1f;
+    conv.par.sigma_th = 50;
+    conv.par.grad_th = 10;
+    APR apr;
+    if (!conv.get_apr(apr, img)) return 3;
+    ParticleData<uint16_t> parts;
+    parts.sample_image(apr, img);
+    unsigned long long sum = 0;
+    for (size_t i = 0; i < parts.size(); ++i) sum += parts[i];
+    PixelData<float> st(3, 3, 3);
+    for (auto &v : st.mesh) v = 1.0f / 27.0f;
+    ParticleData<float> in, out;
+    in.data.assign(parts.data.begin(), parts.data.end());
+    APRFilter::convolve_pencil(apr, st, in, out, true, true, false);
+    double cs = 0;
+    for (float v : out.data) cs += v;
+    std::printf("P=%llu sum=%llu conv=%.6f\n", (unsigned long long)apr.total_number_particles(), sum, cs);
+    return 0;
+}
