@@ -126,6 +126,23 @@ aprb_status aprb_apr_from_arrays(int y_num, int x_num, int z_num, const uint64_t
 aprb_status aprb_sample_image(const aprb_apr *a, const uint16_t *img, uint16_t *parts);
 aprb_status aprb_sample_image_device(const aprb_apr *a, const uint16_t *img_dev, uint16_t *parts_dev, void *stream);
 
+/* Particle sampling that allocates no device memory.  No counterpart in the
+ * reference.  For callers that cannot allocate GPU memory while they run:
+ * code replayed inside a captured CUDA graph, real-time acquisition loops and
+ * plugin hosts that own a fixed device-memory budget and forbid cudaMalloc
+ * and cudaFree after start-up.  It takes the APR's device arrays (xz_end,
+ * y_vec, e.g. from aprb_apr_device_arrays) and the image dimensions (y, x, z),
+ * and keeps its down-sampling pyramid in one 64 MiB buffer that the library
+ * reserves in device memory at load time (every GPU the library is loaded on
+ * holds it until the process exits).  Volumes whose pyramid below l_max needs
+ * more than 32 Mi uint16 values (about 2.2e8 voxels) are rejected with
+ * APRB_ERR_INVALID_ARGUMENT.  The first call on a device looks the buffer up
+ * for that device; make that first call before any stream capture.  All
+ * calls share the buffer: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller. */
+aprb_status aprb_sample_image_noalloc(const uint64_t *xz_end_dev, const uint16_t *y_vec_dev, int y_num, int x_num,
+                                      int z_num, const uint16_t *img_dev, uint16_t *parts_dev, void *stream);
+
 /* --- APR tree: APR::initialize_tree_dense (APR.hpp:633-689) ---------------------- */
 aprb_status aprb_apr_init_tree(aprb_apr *a);
 aprb_status aprb_apr_export_tree(aprb_apr *a, uint64_t *level_xz, uint64_t *xz_end, uint16_t *y_vec);

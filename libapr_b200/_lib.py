@@ -53,6 +53,7 @@ SIGNATURES = {
     "aprb_apr_from_arrays": ([_i, _i, _i, _vp, _u64, _vp, _u64, _vp, _u64, C.POINTER(_vp)], _i),
     "aprb_sample_image": ([_vp, _vp, _vp], _i),
     "aprb_sample_image_device": ([_vp, _vp, _vp, _vp], _i),
+    "aprb_sample_image_noalloc": ([_vp, _vp, _i, _i, _i, _vp, _vp, _vp], _i),
     "aprb_apr_init_tree": ([_vp], _i),
     "aprb_apr_export_tree": ([_vp, _vp, _vp, _vp], _i),
     "aprb_fill_tree_mean": ([_vp, _vp, _vp], _i),

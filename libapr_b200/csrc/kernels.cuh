@@ -60,6 +60,12 @@ void inclusive_scan_u64(uint64_t *data, uint64_t n, DevBuf &tmp, cudaStream_t s)
 void launch_sample(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const uint16_t *img,
                    uint16_t *parts, DevBuf &pyr, cudaStream_t s);
 
+// sampling into caller-provided scratch (no allocation): the pyramid levels
+// below l_max need sample_scratch_elems(g) uint16 elements
+uint64_t sample_scratch_elems(const Geom &g);
+void launch_sample_scratch(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const uint16_t *img,
+                           uint16_t *parts, uint16_t *scratch, cudaStream_t s);
+
 // tree (APR.hpp:633-689)
 uint64_t launch_tree_build(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
                            uint64_t *t_xz_end, uint64_t t_n_xz, DevBuf &flags, DevBuf &scan_tmp, cudaStream_t s);

@@ -516,6 +516,33 @@ void launch_sample(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec,
     APRB_CHECK_LAUNCH();
 }
 
+uint64_t sample_scratch_elems(const Geom &g) {
+    uint64_t total = 0;
+    for (int l = g.l_min; l < g.l_max; ++l) total += (ncell(g, l) + 7) & ~uint64_t(7);
+    return total;
+}
+
+void launch_sample_scratch(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const uint16_t *img,
+                           uint16_t *parts, uint16_t *scratch, cudaStream_t s) {
+    const int L = g.l_max, lmin = g.l_min;
+    uint64_t off = 0;
+    const uint16_t *lev[32] = {};
+    uint16_t *slot[32] = {};
+    for (int l = lmin; l < L; ++l) {
+        slot[l] = scratch + off;
+        off += (ncell(g, l) + 7) & ~uint64_t(7);
+    }
+    lev[L] = img;
+    for (int l = L - 1; l >= lmin; --l) {
+        pyr_mean_u16_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(lev[l + 1], dims(g, l + 1), slot[l],
+                                                                        dims(g, l));
+        lev[l] = slot[l];
+    }
+    for (int l = lmin; l <= L; ++l)
+        gather_kernel<<<row_blocks(nrow(g, l)), 256, 0, s>>>(lev[l], dims(g, l), xz_end, g.level_xz[l], y_vec, parts);
+    APRB_CHECK_LAUNCH();
+}
+
 uint64_t launch_tree_build(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
                            uint64_t *t_xz_end, uint64_t t_n_xz, DevBuf &flags, DevBuf &scan_tmp, cudaStream_t s) {
     APRB_PROF("tree_build", s);
