@@ -106,6 +106,7 @@ struct aprb_apr {
     // filter work
     DevBuf scan_tmp, tree_vals, pyr, parts_f, parts_u16, out_f, rb, stencils, stencils_f, io_in, io_out;
     FilterBuffers fb;
+    FilterIndex fi;
     uint64_t last_stale = 0;
 };
 
@@ -542,6 +543,7 @@ void ensure_tree(aprb_apr *a, cudaStream_t s) {
     launch_tree_fill(a->tg, a->t_flags, txz, ty, s);
     APRB_CUDA(cudaStreamSynchronize(s));
     a->t_flags.release();
+    build_filter_index(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg, txz, ty, a->fi, s);
     a->tree_built = true;
 }
 
@@ -575,7 +577,7 @@ void convolve_impl(aprb_apr *a, const float *stencil, int ks, const float *in, f
     APRB_CUDA(cudaMemcpyAsync(dst, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice, s));
     float *tree = a->tree_vals.as<float>(a->T ? a->T : 1);
     filter_apply(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
-                 (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, in, tree, &plan, dst, out, 0,
+                 (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, a->fi, in, tree, &plan, dst, out, 0,
                  nullptr, a->fb, s);
     a->last_stale = filter_stale_count(a->fb, s);
 }
@@ -611,8 +613,8 @@ void rl_impl(aprb_apr *a, const uint16_t *in, float *out, const float *psf, int 
     const uint16_t *tyv = (const uint16_t *)a->t_y_vec.p;
     for (int it = 0; it < niter; ++it) {
         // rb = in / conv(psf_flipped, out); out = out * conv(psf, rb)  (APRNumerics.hpp:565-570)
-        filter_apply(a->g, xz, yv, a->tg, txz, tyv, out, tree, &plan_f, df, rb, 1, in, a->fb, s);
-        filter_apply(a->g, xz, yv, a->tg, txz, tyv, rb, tree, &plan, dp, out, 2, nullptr, a->fb, s);
+        filter_apply(a->g, xz, yv, a->tg, txz, tyv, a->fi, out, tree, &plan_f, df, rb, 1, in, a->fb, s);
+        filter_apply(a->g, xz, yv, a->tg, txz, tyv, a->fi, rb, tree, &plan, dp, out, 2, nullptr, a->fb, s);
     }
 }
 
@@ -646,7 +648,7 @@ aprb_status aprb_fill_tree_mean_device(aprb_apr *a, const float *parts_dev, floa
         cudaStream_t s = (cudaStream_t)stream;
         ensure_tree(a, s);
         filter_apply(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
-                     (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, parts_dev, tree_dev, nullptr,
+                     (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, a->fi, parts_dev, tree_dev, nullptr,
                      nullptr, nullptr, 0, nullptr, a->fb, s);
     });
 }
@@ -661,7 +663,7 @@ aprb_status aprb_fill_tree_mean(aprb_apr *a, const float *parts, float *tree) {
         float *dt = a->out_f.as<float>(a->T ? a->T : 1);
         APRB_CUDA(cudaMemcpyAsync(dp, parts, a->P * sizeof(float), cudaMemcpyHostToDevice, s));
         filter_apply(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
-                     (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, dp, dt, nullptr, nullptr,
+                     (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, a->fi, dp, dt, nullptr, nullptr,
                      nullptr, 0, nullptr, a->fb, s);
         APRB_CUDA(cudaMemcpyAsync(tree, dt, a->T * sizeof(float), cudaMemcpyDeviceToHost, s));
         APRB_CUDA(cudaStreamSynchronize(s));

@@ -1,223 +1,449 @@
 // APR tree means and APR isotropic convolution on the GPU.
 //
-// Levels are processed from l_max down.  For level l a dense level image is
-// built in HBM from the particles of level l, the tree nodes of level l (the
-// means of finer particles) and, for the stencil's reach, the particles one
-// level coarser (piecewise constant) -- the isotropic neighbourhood that
-// APRFilter::update_dense_array builds per pencil (APRFilter.hpp:825-849).
-// The same image feeds (a) the tree means of level l-1, accumulated in the
-// exact child order of APRTreeNumerics::fill_tree_mean (APRTreeNumerics.hpp:
-// 63-203): particle children first, then tree children, each in z, x, y order,
-// and (b) the stencil sums of level-l particles in the order of
-// run_convolution_pencil (APRFilter.hpp:706-736), without FMA contraction.
+// Row chunk index: for every row of every level (particles and tree), the
+// offset of the first element at or after each multiple of 64 in y.  It is
+// built once per APR and lets a CTA find the part of a row inside its y
+// window with one load instead of a search.
+//
+// Tree means (APRTreeNumerics::fill_tree_mean, APRTreeNumerics.hpp:63-203):
+// one CTA per (parent row, 256-cell y chunk) stages its four child rows in
+// shared memory (value + kind: particle or tree node) and every parent sums
+// its children in the reference's order -- particle children first, then tree
+// children, z then x then y within each -- with the reference's boundary scale
+// factors (:97-110).  Levels run from fine to coarse.
+//
+// Convolution (APRFilter::convolve_pencil, APRFilter.hpp:1094-1216): one CTA
+// per (8 x-rows, 128-y chunk, 16-z range) of a level streams z through a ring
+// of 2R+1 shared-memory slices.  Each slice is the isotropic neighbourhood the
+// reference builds in its pencil buffer (update_dense_array, :825-849):
+// same-level particles, parents one level coarser (piecewise constant,
+// :766-793) and tree means of the same level (:802-818), with the reflective
+// or zero boundary (:287-504) folded into the slice contents.  Each particle
+// of the centre slice sums its 27 / 125 taps in the stencil's memory order
+// without contraction (run_convolution_pencil, :706-736).  A cell no particle
+// covers holds a sentinel; reading it is counted as a stale read (the
+// reference would read a stale pencil buffer there) and contributes 0.
 #include "kernels.cuh"
 
 namespace aprb {
 
 namespace {
 
+constexpr uint32_t kMissingBits = 0x7fbadbadu;  // NaN payload marking an uncovered cell
+constexpr int kYC = 64;                         // y chunk of the row index
+
 struct LD {
     int yn, xn, zn;
 };
 LD ld(const Geom &g, int l) { return LD{g.y_num[l], g.x_num[l], g.z_num[l]}; }
-uint64_t ncell(const Geom &g, int l) { return (uint64_t)g.y_num[l] * g.x_num[l] * g.z_num[l]; }
 uint64_t nrow(const Geom &g, int l) { return (uint64_t)g.x_num[l] * g.z_num[l]; }
-unsigned row_blocks(uint64_t rows) { return blocks_for(rows * 32, 256); }
+__host__ __device__ __forceinline__ int nchunk(int yn) { return (yn + kYC - 1) / kYC; }
 
-constexpr uint8_t kTypeParticle = 1, kTypeTree = 2, kTypeParent = 3;
-
-// scatter one level's values (particles or tree nodes) into the dense image
-__global__ void scatter_kernel(LD d, const uint64_t *__restrict__ xz_end, uint64_t row_base,
-                               const uint16_t *__restrict__ y_vec, const float *__restrict__ val,
-                               float *__restrict__ D, uint8_t *__restrict__ T, uint8_t type) {
-    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (row >= (uint64_t)d.xn * d.zn) return;
-    const uint64_t b = xz_end[row_base + row - 1], e = xz_end[row_base + row];
-    const uint64_t o = row * (uint64_t)d.yn;
-    for (uint64_t i = b + lane; i < e; i += 32) {
-        const uint64_t q = o + y_vec[i];
-        D[q] = val[i];
-        T[q] = type;
-    }
-}
-
-// parents one level coarser fill their 2x2x2 children (update_higher_level,
-// APRFilter.hpp:766-793), clipped to the level's dims
-__global__ void scatter_parent_kernel(LD dp, const uint64_t *__restrict__ xz_end, uint64_t row_base,
-                                      const uint16_t *__restrict__ y_vec, const float *__restrict__ val, LD d,
-                                      float *__restrict__ D, uint8_t *__restrict__ T) {
-    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (row >= (uint64_t)dp.xn * dp.zn) return;
-    const int xp = (int)(row % (uint64_t)dp.xn), zp = (int)(row / (uint64_t)dp.xn);
-    const uint64_t b = xz_end[row_base + row - 1], e = xz_end[row_base + row];
-    for (uint64_t i = b + lane; i < e; i += 32) {
-        const int yp = y_vec[i];
-        const float v = val[i];
-        for (int z = 2 * zp; z < min(2 * zp + 2, d.zn); ++z)
-            for (int x = 2 * xp; x < min(2 * xp + 2, d.xn); ++x)
-                for (int y = 2 * yp; y < min(2 * yp + 2, d.yn); ++y) {
-                    const uint64_t q = idx3(y, x, z, d.yn, d.xn);
-                    D[q] = v;
-                    T[q] = kTypeParent;
-                }
-    }
-}
-
-// tree means of level t from the dense image of level t+1
-__global__ void tree_gather_kernel(LD dt, const uint64_t *__restrict__ t_xz_end, uint64_t row_base,
-                                   const uint16_t *__restrict__ t_y_vec, LD d, const float *__restrict__ D,
-                                   const uint8_t *__restrict__ T, float *__restrict__ tree) {
-    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    if (row >= (uint64_t)dt.xn * dt.zn) return;
-    const int x = (int)(row % (uint64_t)dt.xn), z = (int)(row / (uint64_t)dt.xn);
-    const uint64_t b = t_xz_end[row_base + row - 1], e = t_xz_end[row_base + row];
-    float sxz = (float)((((2 * dt.xn != d.xn) && (x == dt.xn - 1)) + ((2 * dt.zn != d.zn) && (z == dt.zn - 1))) * 2);
-    if (sxz == 0) sxz = 1;
-    const float syxz = (2 * dt.yn != d.yn) ? sxz * 2 : sxz;
-    for (uint64_t i = b + lane; i < e; i += 32) {
-        const int y = t_y_vec[i];
-        const float s = (y == dt.yn - 1) ? syxz : sxz;
-        float acc = 0.0f;
-        for (int type = kTypeParticle; type <= kTypeTree; ++type)
-            for (int cz = 2 * z; cz < min(2 * z + 2, d.zn); ++cz)
-                for (int cx = 2 * x; cx < min(2 * x + 2, d.xn); ++cx)
-                    for (int cy = 2 * y; cy < min(2 * y + 2, d.yn); ++cy) {
-                        const uint64_t q = idx3(cy, cx, cz, d.yn, d.xn);
-                        if (T[q] == type) acc = (s * D[q]) / 8.0f + acc;
-                    }
-        tree[i] = acc;
-    }
-}
-
-__device__ __forceinline__ int bc_index(int i, int n, int reflect, int &state) {
+// Reflection about the edge sample (APRFilter.hpp:287-504), or the zero pad
+// (ok = false); a reflection that still leaves the level marks the cell stale.
+__device__ __forceinline__ int reflect_idx(int i, int n, int reflect, bool &ok) {
     if (i >= 0 && i < n) return i;
     if (!reflect) {
-        state = 1;  // zero pad
+        ok = false;
         return 0;
     }
     const int r = i < 0 ? -i : 2 * (n - 1) - i;
     if (r < 0 || r >= n) {
-        state = 2;  // reflection leaves the level: the reference reads stale data
+        ok = false;
         return 0;
     }
     return r;
 }
 
-template <int S>
-__global__ void conv_kernel(LD d, const uint64_t *__restrict__ xz_end, uint64_t row_base,
-                            const uint16_t *__restrict__ y_vec, const float *__restrict__ D,
-                            const uint8_t *__restrict__ T, const float *__restrict__ stencil, int reflect,
-                            float *__restrict__ out, int mode, const uint16_t *__restrict__ rl_in,
-                            unsigned long long *stale) {
-    constexpr int R = (S - 1) / 2;
-    __shared__ float st[S * S * S];
-    for (int k = threadIdx.x; k < S * S * S; k += blockDim.x) st[k] = stencil[k];
-    __syncthreads();
+// cidx[row * (nc + 1) + c] = offset (from the row start) of the first element
+// with y >= c * kYC; entry nc is the row length.
+__global__ void chunk_index_kernel(const uint64_t *__restrict__ xz_end, uint64_t row_base,
+                                   const uint16_t *__restrict__ y_vec, uint64_t rows, int nc,
+                                   uint16_t *__restrict__ cidx) {
     const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
-    if (row >= (uint64_t)d.xn * d.zn) return;
-    const int x = (int)(row % (uint64_t)d.xn), z = (int)(row / (uint64_t)d.xn);
+    if (row >= rows) return;
     const uint64_t b = xz_end[row_base + row - 1], e = xz_end[row_base + row];
-    unsigned nstale = 0;
+    uint16_t *C = cidx + row * (uint64_t)(nc + 1);
     for (uint64_t i = b + lane; i < e; i += 32) {
-        const int y = y_vec[i];
-        float val = 0.0f;
-        int cnt = 0;
-#pragma unroll
-        for (int iz = 0; iz < S; ++iz) {
-            int sz = 0;
-            const int zz = bc_index(z + iz - R, d.zn, reflect, sz);
-#pragma unroll
-            for (int ix = 0; ix < S; ++ix) {
-                int sx = 0;
-                const int xx = bc_index(x + ix - R, d.xn, reflect, sx);
-#pragma unroll
-                for (int iy = 0; iy < S; ++iy) {
-                    int sy = 0;
-                    const int yy = bc_index(y + iy - R, d.yn, reflect, sy);
-                    float v = 0.0f;
-                    const int worst = max(sz, max(sx, sy));
-                    if (worst == 0) {
-                        const uint64_t q = idx3(yy, xx, zz, d.yn, d.xn);
-                        if (T[q])
-                            v = D[q];
-                        else
-                            nstale++;
-                    } else if (worst == 2) {
-                        nstale++;
-                    }
-                    val = __fadd_rn(val, __fmul_rn(v, st[cnt]));
-                    cnt++;
+        const int c = y_vec[i] / kYC;
+        const int pc = (i == b) ? -1 : y_vec[i - 1] / kYC;
+        for (int q = pc + 1; q <= c; ++q) C[q] = (uint16_t)(i - b);
+    }
+    const int lastc = (e > b) ? y_vec[e - 1] / kYC : -1;
+    for (int q = lastc + 1 + lane; q <= nc; q += 32) C[q] = (uint16_t)(e - b);
+}
+
+// ---------------------------------------------------------------------------
+// tree means of tree level t (children at level t+1)
+// ---------------------------------------------------------------------------
+constexpr int kTW = 256;  // parent cells per CTA along y (a multiple of kYC)
+
+struct TreeLevelArgs {
+    LD dt;                  // tree level t dims (== APR level t dims)
+    LD dc;                  // child level dims
+    uint64_t t_row_base;    // tree level_xz[t]
+    uint64_t c_row_base;    // APR level_xz[t+1]
+    uint64_t ct_row_base;   // tree level_xz[t+1] (0 when t+1 has no tree level)
+    const uint16_t *t_cidx, *c_cidx, *ct_cidx;
+};
+
+__global__ void __launch_bounds__(128) tree_mean_kernel(TreeLevelArgs a, const uint64_t *__restrict__ xz_end,
+                                                        const uint16_t *__restrict__ y_vec,
+                                                        const float *__restrict__ parts,
+                                                        const uint64_t *__restrict__ t_xz_end,
+                                                        const uint16_t *__restrict__ t_y_vec,
+                                                        float *__restrict__ tree) {
+    __shared__ float sv[4][2 * kTW];
+    __shared__ uint8_t sk[4][2 * kTW];
+    const uint64_t prow = blockIdx.x;  // parent row z*xt + x
+    const int xp = (int)(prow % (uint64_t)a.dt.xn), zp = (int)(prow / (uint64_t)a.dt.xn);
+    const int y0 = blockIdx.y * kTW;
+    const int cy0 = 2 * y0, cy1 = min(2 * y0 + 2 * kTW, a.dc.yn);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int k = threadIdx.x; k < 4 * 2 * kTW; k += blockDim.x) (&sk[0][0])[k] = 0;
+    __syncthreads();
+    {
+        const int cz = 2 * zp + (w >> 1), cx = 2 * xp + (w & 1);
+        if (cz < a.dc.zn && cx < a.dc.xn && cy0 < cy1) {
+            const uint64_t row = (uint64_t)cz * a.dc.xn + cx;
+            const int ncc = nchunk(a.dc.yn);
+            {
+                const uint64_t b = xz_end[a.c_row_base + row - 1], e = xz_end[a.c_row_base + row];
+                const uint64_t s = b + a.c_cidx[row * (uint64_t)(ncc + 1) + cy0 / kYC];
+                for (uint64_t i = s + lane; i < e; i += 32) {
+                    const int y = y_vec[i];
+                    if (y >= cy1) break;
+                    sv[w][y - cy0] = parts[i];
+                    sk[w][y - cy0] = 1;
+                }
+            }
+            if (a.ct_row_base) {
+                const uint64_t b = t_xz_end[a.ct_row_base + row - 1], e = t_xz_end[a.ct_row_base + row];
+                const uint64_t s = b + a.ct_cidx[row * (uint64_t)(ncc + 1) + cy0 / kYC];
+                for (uint64_t i = s + lane; i < e; i += 32) {
+                    const int y = t_y_vec[i];
+                    if (y >= cy1) break;
+                    sv[w][y - cy0] = tree[i];
+                    sk[w][y - cy0] = 2;
                 }
             }
         }
-        if (mode == 0)
-            out[i] = val;
-        else if (mode == 1)
-            out[i] = (float)rl_in[i] / val;
-        else
-            out[i] = out[i] * val;
+    }
+    __syncthreads();
+    const int nct = nchunk(a.dt.yn);
+    const uint64_t pb = t_xz_end[a.t_row_base + prow - 1], pe = t_xz_end[a.t_row_base + prow];
+    const uint16_t *PC = a.t_cidx + prow * (uint64_t)(nct + 1);
+    const uint64_t ps = pb + PC[y0 / kYC];
+    const uint64_t pend = pb + PC[min(y0 / kYC + kTW / kYC, nct)];
+    float sxz = (float)((((2 * a.dt.xn != a.dc.xn) && (xp == a.dt.xn - 1)) +
+                         ((2 * a.dt.zn != a.dc.zn) && (zp == a.dt.zn - 1))) * 2);
+    if (sxz == 0) sxz = 1;
+    const float syxz = (2 * a.dt.yn != a.dc.yn) ? sxz * 2 : sxz;
+    (void)pe;
+    for (uint64_t i = ps + threadIdx.x; i < pend; i += blockDim.x) {
+        const int y = t_y_vec[i];
+        const float s = (y == a.dt.yn - 1) ? syxz : sxz;
+        const int o = 2 * (y - y0);
+        float acc = 0.0f;
+#pragma unroll
+        for (int kind = 1; kind <= 2; ++kind)
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int d = 0; d < 2; ++d)
+                    if (o + d < cy1 - cy0 && sk[q][o + d] == kind)
+                        acc = __fadd_rn(__fdiv_rn(__fmul_rn(s, sv[q][o + d]), 8.0f), acc);
+        tree[i] = acc;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// convolution of one level
+// ---------------------------------------------------------------------------
+constexpr int kBX = 8, kBY = 128, kBZ = 16;
+
+struct ConvLevelArgs {
+    LD d;                 // level dims
+    LD dp;                // parent level dims
+    uint64_t row_base;    // APR level_xz[l]
+    uint64_t prow_base;   // APR level_xz[l-1] (0: no parents used)
+    uint64_t trow_base;   // tree level_xz[l] (0: no tree level)
+    const uint16_t *cidx, *pcidx, *tcidx;
+    int reflect;
+    int mode;
+};
+
+template <int R>
+struct ConvSmem {
+    static constexpr int S = 2 * R + 1, RX = kBX + 2 * R, RY = kBY + 2 * R;
+    float ring[S][RX][RY];
+    float st[S * S * S];
+    uint64_t ob[kBX];
+    int ocnt[kBX + 1];
+};
+
+// Fills one slice row (level row (zr, xr) over the y window) of the ring.
+template <int R>
+__device__ void fill_slice_row(float *__restrict__ rowbuf, int zr, int xr, int y0, const ConvLevelArgs &a,
+                               const uint64_t *__restrict__ xz_end, const uint16_t *__restrict__ y_vec,
+                               const float *__restrict__ in, const uint64_t *__restrict__ t_xz_end,
+                               const uint16_t *__restrict__ t_y_vec, const float *__restrict__ tree, int lane) {
+    constexpr int RY = kBY + 2 * R;
+    const int ys = y0 - R;  // y of rowbuf[0]
+    const float miss = __uint_as_float(kMissingBits);
+    for (int k = lane; k < RY; k += 32) rowbuf[k] = miss;
+    __syncwarp();
+    const int ya = max(ys, 0), yb = min(ys + RY - 1, a.d.yn - 1);  // real y range needed
+    if (ya <= yb) {
+        const uint64_t row = (uint64_t)zr * a.d.xn + xr;
+        const int nc = nchunk(a.d.yn);
+        {  // same-level particles
+            const uint64_t b = xz_end[a.row_base + row - 1], e = xz_end[a.row_base + row];
+            const uint64_t s = b + a.cidx[row * (uint64_t)(nc + 1) + ya / kYC];
+            for (uint64_t i = s + lane; i < e; i += 32) {
+                const int y = y_vec[i];
+                if (y > yb) break;
+                if (y >= ya) rowbuf[y - ys] = in[i];
+            }
+        }
+        if (a.prow_base) {  // parents one level coarser fill their y pair
+            const uint64_t prow = (uint64_t)(zr / 2) * a.dp.xn + xr / 2;
+            const int npc = nchunk(a.dp.yn);
+            const uint64_t b = xz_end[a.prow_base + prow - 1], e = xz_end[a.prow_base + prow];
+            const uint64_t s = b + a.pcidx[prow * (uint64_t)(npc + 1) + (ya / 2) / kYC];
+            for (uint64_t i = s + lane; i < e; i += 32) {
+                const int yp = y_vec[i];
+                if (2 * yp > yb) break;
+                const float v = in[i];
+                const int c0 = 2 * yp, c1 = min(2 * yp + 1, a.d.yn - 1);
+                if (c0 >= ya) rowbuf[c0 - ys] = v;
+                if (c1 != c0 && c1 >= ya && c1 <= yb) rowbuf[c1 - ys] = v;
+            }
+        }
+        if (a.trow_base) {  // tree means of the same level
+            const uint64_t b = t_xz_end[a.trow_base + row - 1], e = t_xz_end[a.trow_base + row];
+            const uint64_t s = b + a.tcidx[row * (uint64_t)(nc + 1) + ya / kYC];
+            for (uint64_t i = s + lane; i < e; i += 32) {
+                const int y = t_y_vec[i];
+                if (y > yb) break;
+                if (y >= ya) rowbuf[y - ys] = tree[i];
+            }
+        }
+    }
+    __syncwarp();
+    // y boundary: reflection about the edge sample, or zero
+    for (int k = lane; k < RY; k += 32) {
+        const int y = ys + k;
+        if (y >= 0 && y < a.d.yn) continue;
+        if (!a.reflect) {
+            rowbuf[k] = 0.0f;
+        } else {
+            const int r = y < 0 ? -y : 2 * (a.d.yn - 1) - y;
+            rowbuf[k] = (r >= 0 && r < a.d.yn && r - ys >= 0 && r - ys < RY) ? rowbuf[r - ys] : miss;
+        }
+    }
+}
+
+template <int R>
+__global__ void __launch_bounds__(32 * (kBX + 2 * R)) conv_tile_kernel(
+    ConvLevelArgs a, const uint64_t *__restrict__ xz_end, const uint16_t *__restrict__ y_vec,
+    const float *__restrict__ in, const uint64_t *__restrict__ t_xz_end, const uint16_t *__restrict__ t_y_vec,
+    const float *__restrict__ tree, const float *__restrict__ stencil, float *__restrict__ out,
+    const uint16_t *__restrict__ rl_in, unsigned long long *stale) {
+    constexpr int S = 2 * R + 1, RX = kBX + 2 * R, RY = kBY + 2 * R, NT = 32 * RX;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    ConvSmem<R> &sm = *reinterpret_cast<ConvSmem<R> *>(smem_raw);
+    const int x0 = blockIdx.x * kBX, y0 = blockIdx.y * kBY, z0 = blockIdx.z * kBZ;
+    const int z1 = min(z0 + kBZ, a.d.zn);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int k = threadIdx.x; k < S * S * S; k += NT) sm.st[k] = stencil[k];
+    unsigned nstale = 0;
+    const uint32_t missb = kMissingBits;
+    const int nc = nchunk(a.d.yn);
+
+    // warp w fills ring row w of the slice at z (z may lie outside the level)
+    auto load_slice = [&](int zq) {
+        float(*slot)[RY] = sm.ring[(zq - (z0 - R)) % S];
+        bool ok = true;
+        const int zr = reflect_idx(zq, a.d.zn, a.reflect, ok);
+        const int xr = reflect_idx(x0 - R + w, a.d.xn, a.reflect, ok);
+        if (!ok) {
+            const float v = a.reflect ? __uint_as_float(missb) : 0.0f;
+            for (int k = lane; k < RY; k += 32) slot[w][k] = v;
+        } else {
+            fill_slice_row<R>(slot[w], zr, xr, y0, a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, lane);
+        }
+    };
+
+    for (int zq = z0 - R; zq < z0 + R; ++zq) load_slice(zq);
+    for (int z = z0; z < z1; ++z) {
+        load_slice(z + R);
+        if (threadIdx.x < kBX) {  // output particles of the centre rows
+            const int x = x0 + threadIdx.x;
+            uint64_t b = 0, e = 0;
+            if (x < a.d.xn) {
+                const uint64_t row = (uint64_t)z * a.d.xn + x;
+                const uint64_t rb = xz_end[a.row_base + row - 1];
+                const uint16_t *Cr = a.cidx + row * (uint64_t)(nc + 1);
+                b = rb + Cr[y0 / kYC];
+                e = rb + Cr[min(y0 / kYC + kBY / kYC, nc)];
+            }
+            sm.ob[threadIdx.x] = b;
+            sm.ocnt[threadIdx.x + 1] = (int)(e - b);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            sm.ocnt[0] = 0;
+            for (int q = 1; q <= kBX; ++q) sm.ocnt[q] += sm.ocnt[q - 1];
+        }
+        __syncthreads();
+        const int total = sm.ocnt[kBX];
+        for (int k = threadIdx.x; k < total; k += NT) {
+            int q = 0;
+            while (q + 1 < kBX && sm.ocnt[q + 1] <= k) ++q;
+            const uint64_t i = sm.ob[q] + (uint64_t)(k - sm.ocnt[q]);
+            const int yy = (int)y_vec[i] - (y0 - R);  // ring column of the particle
+            float val = 0.0f;
+            int cnt = 0;
+#pragma unroll
+            for (int iz = 0; iz < S; ++iz) {
+                const float(*slot)[RY] = sm.ring[(z + iz - R - (z0 - R)) % S];
+#pragma unroll
+                for (int ix = 0; ix < S; ++ix) {
+                    const float *rowp = slot[q + ix] + (yy - R);
+#pragma unroll
+                    for (int iy = 0; iy < S; ++iy) {
+                        float v = rowp[iy];
+                        if (__float_as_uint(v) == missb) {
+                            v = 0.0f;
+                            nstale++;
+                        }
+                        val = __fadd_rn(val, __fmul_rn(v, sm.st[cnt]));
+                        cnt++;
+                    }
+                }
+            }
+            if (a.mode == 0)
+                out[i] = val;
+            else if (a.mode == 1)
+                out[i] = (float)rl_in[i] / val;
+            else
+                out[i] = out[i] * val;
+        }
+        __syncthreads();
     }
     if (nstale) atomicAdd(stale, (unsigned long long)nstale);
 }
 
+template <int R>
+void launch_conv_level(const ConvLevelArgs &a, const uint64_t *xz_end, const uint16_t *y_vec, const float *in,
+                       const uint64_t *t_xz_end, const uint16_t *t_y_vec, const float *tree, const float *st,
+                       float *out, const uint16_t *rl_in, unsigned long long *stale, cudaStream_t s) {
+    const size_t smem = sizeof(ConvSmem<R>);
+    APRB_CUDA(cudaFuncSetAttribute(conv_tile_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((a.d.xn + kBX - 1) / kBX, (a.d.yn + kBY - 1) / kBY, (a.d.zn + kBZ - 1) / kBZ);
+    conv_tile_kernel<R><<<grid, 32 * (kBX + 2 * R), smem, s>>>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st, out,
+                                                               rl_in, stale);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+}
+
 }  // namespace
 
+void build_filter_index(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
+                        const uint64_t *t_xz_end, const uint16_t *t_y_vec, FilterIndex &fi, cudaStream_t s) {
+    APRB_PROF("filter_index", s);
+    uint64_t total = 0;
+    for (int l = g.l_min; l <= g.l_max; ++l) {
+        fi.apr_off[l] = total;
+        total += nrow(g, l) * (uint64_t)(nchunk(g.y_num[l]) + 1);
+    }
+    for (int t = tg.l_min; t <= tg.l_max; ++t) {
+        fi.tree_off[t] = total;
+        total += nrow(tg, t) * (uint64_t)(nchunk(tg.y_num[t]) + 1);
+    }
+    uint16_t *c = fi.buf.as<uint16_t>(total ? total : 1);
+    for (int l = 0; l < 32; ++l) fi.level_count[l] = 0;
+    for (int l = g.l_min; l <= g.l_max; ++l) {
+        uint64_t be[2] = {0, 0};
+        APRB_CUDA(cudaMemcpyAsync(&be[0], xz_end + g.level_xz[l] - 1, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaMemcpyAsync(&be[1], xz_end + g.level_xz[l + 1] - 1, sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaStreamSynchronize(s));
+        fi.level_count[l] = be[1] - be[0];
+    }
+    for (int l = g.l_min; l <= g.l_max; ++l) {
+        const uint64_t rows = nrow(g, l);
+        if (!rows) continue;
+        chunk_index_kernel<<<blocks_for(rows * 32, 256), 256, 0, s>>>(xz_end, g.level_xz[l], y_vec, rows,
+                                                                     nchunk(g.y_num[l]), c + fi.apr_off[l]);
+        count_launch();
+    }
+    for (int t = tg.l_min; t <= tg.l_max; ++t) {
+        const uint64_t rows = nrow(tg, t);
+        if (!rows) continue;
+        chunk_index_kernel<<<blocks_for(rows * 32, 256), 256, 0, s>>>(t_xz_end, tg.level_xz[t], t_y_vec, rows,
+                                                                     nchunk(tg.y_num[t]), c + fi.tree_off[t]);
+        count_launch();
+    }
+    APRB_CHECK_LAUNCH();
+    fi.built = true;
+}
+
 void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
-                  const uint64_t *t_xz_end, const uint16_t *t_y_vec, const float *in, float *tree,
-                  const ConvPlan *plan, const float *d_stencils, float *out, int mode, const uint16_t *rl_in,
-                  FilterBuffers &fb, cudaStream_t s) {
+                  const uint64_t *t_xz_end, const uint16_t *t_y_vec, const FilterIndex &fi, const float *in,
+                  float *tree, const ConvPlan *plan, const float *d_stencils, float *out, int mode,
+                  const uint16_t *rl_in, FilterBuffers &fb, cudaStream_t s) {
     APRB_PROF(plan ? "convolve" : "fill_tree_mean", s);
     const int L = g.l_max;
-    const uint64_t nmax = ncell(g, L);
-    float *D = fb.dense.as<float>(nmax);
-    uint8_t *T = fb.type.as<uint8_t>(nmax);
+    const uint16_t *cbase = (const uint16_t *)fi.buf.p;
     unsigned long long *stale = fb.stale.as<unsigned long long>(1);
     APRB_CUDA(cudaMemsetAsync(stale, 0, sizeof(unsigned long long), s));
-    for (int l = L; l >= g.l_min; --l) {
-        const LD d = ld(g, l);
-        APRB_CUDA(cudaMemsetAsync(T, 0, ncell(g, l), s));
-        scatter_kernel<<<row_blocks(nrow(g, l)), 256, 0, s>>>(d, xz_end, g.level_xz[l], y_vec, in, D, T,
-                                                             kTypeParticle);
+    // tree means, fine to coarse
+    for (int t = tg.l_max; t >= tg.l_min; --t) {
+        const int l = t + 1;  // child level
+        if (l > L || l < g.l_min) continue;
+        TreeLevelArgs ta;
+        ta.dt = ld(tg, t);
+        ta.dc = ld(g, l);
+        ta.t_row_base = tg.level_xz[t];
+        ta.c_row_base = g.level_xz[l];
+        ta.ct_row_base = (l <= tg.l_max) ? tg.level_xz[l] : 0;
+        ta.t_cidx = cbase + fi.tree_off[t];
+        ta.c_cidx = cbase + fi.apr_off[l];
+        ta.ct_cidx = (l <= tg.l_max) ? cbase + fi.tree_off[l] : nullptr;
+        const uint64_t rows = (uint64_t)ta.dt.xn * ta.dt.zn;
+        const unsigned ych = (unsigned)((ta.dt.yn + kTW - 1) / kTW);
+        if (rows == 0 || ych == 0) continue;
+        dim3 grid((unsigned)rows, ych);
+        tree_mean_kernel<<<grid, 128, 0, s>>>(ta, xz_end, y_vec, in, t_xz_end, t_y_vec, tree);
         count_launch();
-        if (l <= tg.l_max) {
-            scatter_kernel<<<row_blocks(nrow(tg, l)), 256, 0, s>>>(d, t_xz_end, tg.level_xz[l], t_y_vec, tree, D, T,
-                                                                  kTypeTree);
-            count_launch();
-        }
-        int side = 0;
-        if (plan) {
-            const int sn = std::min(plan->nstencils - 1, L - l);
-            side = plan->sides[sn];
-            const int r = (side - 1) / 2;
-            const int max_npl = (int)std::ceil(std::log2((double)(r + 2)) - 1);
-            const int npl = std::min(max_npl, l - g.l_min);
-            if (npl >= 1)
-                scatter_parent_kernel<<<row_blocks(nrow(g, l - 1)), 256, 0, s>>>(
-                    ld(g, l - 1), xz_end, g.level_xz[l - 1], y_vec, in, d, D, T);
-            if (npl >= 1) count_launch();
-        }
-        APRB_CHECK_LAUNCH();
-        if (l - 1 >= tg.l_min) {
-            tree_gather_kernel<<<row_blocks(nrow(tg, l - 1)), 256, 0, s>>>(ld(tg, l - 1), t_xz_end,
-                                                                          tg.level_xz[l - 1], t_y_vec, d, D, T, tree);
-            count_launch();
-        }
-        if (plan) {
-            const int sn = std::min(plan->nstencils - 1, L - l);
-            const float *st = d_stencils + plan->offsets[sn];
-            if (side == 3)
-                conv_kernel<3><<<row_blocks(nrow(g, l)), 256, 0, s>>>(d, xz_end, g.level_xz[l], y_vec, D, T, st,
-                                                                     plan->reflect, out, mode, rl_in, stale);
-            else
-                conv_kernel<5><<<row_blocks(nrow(g, l)), 256, 0, s>>>(d, xz_end, g.level_xz[l], y_vec, D, T, st,
-                                                                     plan->reflect, out, mode, rl_in, stale);
-            count_launch();
-        }
-        APRB_CHECK_LAUNCH();
+    }
+    APRB_CHECK_LAUNCH();
+    if (!plan) return;
+    for (int l = L; l >= g.l_min; --l) {
+        if (fi.level_count[l] == 0) continue;
+        const int sn = std::min(plan->nstencils - 1, L - l);
+        const int side = plan->sides[sn];
+        const int r = (side - 1) / 2;
+        const int max_npl = (int)std::ceil(std::log2((double)(r + 2)) - 1);
+        const int npl = std::min(max_npl, l - g.l_min);
+        ConvLevelArgs a;
+        a.d = ld(g, l);
+        a.dp = l > g.l_min ? ld(g, l - 1) : LD{1, 1, 1};
+        a.row_base = g.level_xz[l];
+        a.prow_base = npl >= 1 ? g.level_xz[l - 1] : 0;
+        a.trow_base = l <= tg.l_max ? tg.level_xz[l] : 0;
+        a.cidx = cbase + fi.apr_off[l];
+        a.pcidx = npl >= 1 ? cbase + fi.apr_off[l - 1] : nullptr;
+        a.tcidx = l <= tg.l_max ? cbase + fi.tree_off[l] : nullptr;
+        a.reflect = plan->reflect;
+        a.mode = mode;
+        const float *st = d_stencils + plan->offsets[sn];
+        if (side == 3)
+            launch_conv_level<1>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st, out, rl_in, stale, s);
+        else
+            launch_conv_level<2>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st, out, rl_in, stale, s);
     }
 }
 

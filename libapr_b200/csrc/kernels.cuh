@@ -85,10 +85,20 @@ struct ConvPlan {
     std::vector<int> offsets;
     int reflect = 1;
 };
+// Row chunk index of every APR and tree level (built once per APR) and the
+// particle count of every APR level.
+struct FilterIndex {
+    DevBuf buf;
+    uint64_t apr_off[32] = {}, tree_off[32] = {};
+    uint64_t level_count[32] = {};
+    bool built = false;
+};
+void build_filter_index(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
+                        const uint64_t *t_xz_end, const uint16_t *t_y_vec, FilterIndex &fi, cudaStream_t s);
 void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
-                  const uint64_t *t_xz_end, const uint16_t *t_y_vec, const float *in, float *tree,
-                  const ConvPlan *plan, const float *d_stencils, float *out, int mode, const uint16_t *rl_in,
-                  FilterBuffers &fb, cudaStream_t s);
+                  const uint64_t *t_xz_end, const uint16_t *t_y_vec, const FilterIndex &fi, const float *in,
+                  float *tree, const ConvPlan *plan, const float *d_stencils, float *out, int mode,
+                  const uint16_t *rl_in, FilterBuffers &fb, cudaStream_t s);
 uint64_t filter_stale_count(FilterBuffers &fb, cudaStream_t s);
 
 // ---- synth.cu

@@ -85,25 +85,33 @@ __device__ __forceinline__ IT to_it(float v) {
 // ---------------------------------------------------------------------------
 // a2 (y): bspline_filt_rec_y (ComputeGradient.hpp:249-413).
 // One thread owns one y-line (the recurrence is sequential); a warp owns 32
-// consecutive lines and moves them through shared memory in 32x32 tiles so
-// global loads and stores are coalesced.  The forward pass stores its values,
-// the backward pass reads them back through L2 (__ldcg).
+// consecutive lines and moves them through shared memory in 32 x 64 tiles
+// (coalesced loads/stores), prefetching the next tile into registers while
+// the current one runs.  The forward pass stores its values; the backward pass
+// reads them back (through L2, __ldcg).
 // ---------------------------------------------------------------------------
 constexpr int kTile = 32;
+constexpr int kYW = 64;  // y extent of a tile
 constexpr int kYWarps = 4;
+
+template <typename IT>
+__device__ __forceinline__ float ld_it(const IT *p) {
+    return (float)__ldcg(p);
+}
 
 template <typename IT>
 __global__ void __launch_bounds__(kYWarps * 32) iir_y_kernel(const uint16_t *__restrict__ src, IT *__restrict__ dst,
                                                               int yn, uint64_t nlines, IIRDev c,
                                                               const float *__restrict__ d_offset, unsigned *err_out) {
-    __shared__ float tile[kYWarps][kTile][kTile + 1];
+    __shared__ float tile[kYWarps][kTile][kYW + 1];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint64_t line0 = ((uint64_t)blockIdx.x * kYWarps + w) * kTile;
     if (line0 >= nlines) return;
     const uint64_t myline = line0 + lane;
     const bool valid = myline < nlines;
+    const int nl = (int)min((uint64_t)kTile, nlines - line0);  // lines of this warp
     const float off = d_offset ? *d_offset : 0.0f;
-    float(*T)[kTile + 1] = tile[w];
+    float(*T)[kYW + 1] = tile[w];
     unsigned err = 0;
 
     float t1 = 0, t2 = 0, t3 = 0, t4 = 0;
@@ -120,15 +128,33 @@ __global__ void __launch_bounds__(kYWarps * 32) iir_y_kernel(const uint16_t *__r
             t4 = t4 + c_bc[3][k] * v;
         }
     }
-    // forward (causal) pass
-    for (int y0 = 0; y0 < yn; y0 += kTile) {
+    const int ya = 2 * lane, yb = 2 * lane + 1;  // columns this lane moves
+    // ---- forward (causal) pass
+    uint16_t pa[kTile], pb[kTile];
+#pragma unroll
+    for (int j = 0; j < kTile; ++j) {
+        const uint16_t *L = src + (line0 + j) * (uint64_t)yn;
+        pa[j] = (j < nl && ya < yn) ? L[ya] : 0;
+        pb[j] = (j < nl && yb < yn) ? L[yb] : 0;
+    }
+    for (int y0 = 0; y0 < yn; y0 += kYW) {
+#pragma unroll
         for (int j = 0; j < kTile; ++j) {
-            uint64_t ln = line0 + j;
-            if (ln < nlines && y0 + lane < yn) T[j][lane] = raw_to_it<IT>(src[ln * (uint64_t)yn + y0 + lane], off);
+            T[j][ya] = raw_to_it<IT>(pa[j], off);
+            T[j][yb] = raw_to_it<IT>(pb[j], off);
         }
         __syncwarp();
+        const int n0 = y0 + kYW;
+        if (n0 < yn) {
+#pragma unroll
+            for (int j = 0; j < kTile; ++j) {
+                const uint16_t *L = src + (line0 + j) * (uint64_t)yn + n0;
+                pa[j] = (j < nl && n0 + ya < yn) ? L[ya] : 0;
+                pb[j] = (j < nl && n0 + yb < yn) ? L[yb] : 0;
+            }
+        }
         if (valid) {
-            const int kend = min(kTile, yn - y0);
+            const int kend = min(kYW, yn - y0);
             for (int k = 0; k < kend; ++k) {
                 const int y = y0 + k;
                 float out;
@@ -148,28 +174,47 @@ __global__ void __launch_bounds__(kYWarps * 32) iir_y_kernel(const uint16_t *__r
             }
         }
         __syncwarp();
-        for (int j = 0; j < kTile; ++j) {
-            uint64_t ln = line0 + j;
-            if (ln < nlines && y0 + lane < yn) dst[ln * (uint64_t)yn + y0 + lane] = to_it<IT>(T[j][lane]);
+#pragma unroll 4
+        for (int j = 0; j < nl; ++j) {
+            IT *L = dst + (line0 + j) * (uint64_t)yn + y0;
+            if (y0 + ya < yn) L[ya] = to_it<IT>(T[j][ya]);
+            if (y0 + yb < yn) L[yb] = to_it<IT>(T[j][yb]);
         }
         __syncwarp();
     }
-    // backward (anti-causal) pass
+    // ---- backward (anti-causal) pass
     float b2v = 0, b1v = 0;
     if (valid) {
         const IT *L = dst + myline * (uint64_t)yn;
-        b2v = (float)__ldcg(&L[yn - 1]) / c.norm;
-        b1v = (float)__ldcg(&L[yn - 2]) / c.norm;
+        b2v = ld_it(&L[yn - 1]) / c.norm;
+        b1v = ld_it(&L[yn - 2]) / c.norm;
     }
-    const int last0 = ((yn - 1) / kTile) * kTile;
-    for (int y0 = last0; y0 >= 0; y0 -= kTile) {
+    const int last0 = ((yn - 1) / kYW) * kYW;
+    float fa[kTile], fb[kTile];
+#pragma unroll
+    for (int j = 0; j < kTile; ++j) {
+        const IT *L = dst + (line0 + j) * (uint64_t)yn + last0;
+        fa[j] = (j < nl && last0 + ya < yn) ? ld_it(&L[ya]) : 0.0f;
+        fb[j] = (j < nl && last0 + yb < yn) ? ld_it(&L[yb]) : 0.0f;
+    }
+    for (int y0 = last0; y0 >= 0; y0 -= kYW) {
+#pragma unroll
         for (int j = 0; j < kTile; ++j) {
-            uint64_t ln = line0 + j;
-            if (ln < nlines && y0 + lane < yn) T[j][lane] = (float)__ldcg(&dst[ln * (uint64_t)yn + y0 + lane]);
+            T[j][ya] = fa[j];
+            T[j][yb] = fb[j];
         }
         __syncwarp();
+        const int p0 = y0 - kYW;
+        if (p0 >= 0) {
+#pragma unroll
+            for (int j = 0; j < kTile; ++j) {
+                const IT *L = dst + (line0 + j) * (uint64_t)yn + p0;
+                fa[j] = (j < nl) ? ld_it(&L[ya]) : 0.0f;
+                fb[j] = (j < nl) ? ld_it(&L[yb]) : 0.0f;
+            }
+        }
         if (valid) {
-            const int kend = min(kTile, yn - y0);
+            const int kend = min(kYW, yn - y0);
             for (int k = kend - 1; k >= 0; --k) {
                 const int y = y0 + k;
                 if (y > yn - 3) continue;
@@ -180,9 +225,11 @@ __global__ void __launch_bounds__(kYWarps * 32) iir_y_kernel(const uint16_t *__r
             }
         }
         __syncwarp();
-        for (int j = 0; j < kTile; ++j) {
-            uint64_t ln = line0 + j;
-            if (ln < nlines && y0 + lane < yn) dst[ln * (uint64_t)yn + y0 + lane] = to_it<IT>(T[j][lane]);
+#pragma unroll 4
+        for (int j = 0; j < nl; ++j) {
+            IT *L = dst + (line0 + j) * (uint64_t)yn + y0;
+            if (y0 + ya < yn) L[ya] = to_it<IT>(T[j][ya]);
+            if (y0 + yb < yn) L[yb] = to_it<IT>(T[j][yb]);
         }
         __syncwarp();
     }
@@ -273,102 +320,147 @@ __global__ void offset_copy_kernel(const uint16_t *__restrict__ src, IT *__restr
 
 // ---------------------------------------------------------------------------
 // a3 + a4: calc_bspline_fd_ds_mag (ComputeGradient.hpp:976-1051) fused with
-// downsample(sum, /8) (PixelData.hpp:916-967).  One thread per ds voxel.
+// downsample(sum, /8) (PixelData.hpp:916-967).  A CTA owns 8 x 64 ds cells in
+// (x, y) and streams 8 ds slices in z through a 4-slice shared-memory ring of
+// the full-resolution tile plus a one-sample halo, stored with the index
+// clamping both reference functions use (replicate boundary).
 // ---------------------------------------------------------------------------
-template <typename IT>
-__device__ __forceinline__ float grad_mag(const IT *__restrict__ im, int y, int x, int z, int yn, int xn, int zn,
-                                          float hx2, float hy2, float hz2) {
-    if (yn < 2) return 0.0f;
-    const int xl = x > 0 ? x - 1 : 0, xr = x + 1 < xn - 1 ? x + 1 : xn - 1;
-    const int zu = z > 0 ? z - 1 : 0, zd = z + 1 < zn - 1 ? z + 1 : zn - 1;
-    const int ym = y > 0 ? y - 1 : 0, yp = y < yn - 1 ? y + 1 : yn - 1;
-    float gx = ((float)im[idx3(y, xr, z, yn, xn)] - (float)im[idx3(y, xl, z, yn, xn)]) / hx2;
-    float gz = ((float)im[idx3(y, x, zd, yn, xn)] - (float)im[idx3(y, x, zu, yn, xn)]) / hz2;
-    float gy = ((float)im[idx3(yp, x, z, yn, xn)] - (float)im[idx3(ym, x, z, yn, xn)]) / hy2;
-    double s = (double)gx * (double)gx + (double)gz * (double)gz;
-    s = s + (double)gy * (double)gy;
-    double r = sqrt(s);
-    return sizeof(IT) == 2 ? cvt_u16d(r) : (float)r;
-}
+constexpr int kGX = 8, kGY = 64, kGZ = 8, kGThreads = 256;
+constexpr int kTX = 2 * kGX + 2, kTY = 2 * kGY + 2;
 
 template <typename IT>
-__global__ void grad_ds_kernel(const IT *__restrict__ im, int yn, int xn, int zn, IT *__restrict__ grad,
-                               float *__restrict__ ids, int yd, int xd, int zd, float hx, float hy, float hz) {
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const uint64_t nd = (uint64_t)yd * xd * zd;
-    if (g >= nd) return;
-    const int k = (int)(g % yd);
-    const int xk = (int)((g / yd) % xd);
-    const int zk = (int)(g / ((uint64_t)yd * xd));
+__global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict__ im, int yn, int xn, int zn,
+                                                            IT *__restrict__ grad, float *__restrict__ ids, int yd,
+                                                            int xd, int zd, float hx, float hy, float hz) {
+    __shared__ float ring[4][kTX][kTY];
+    const int yd0 = blockIdx.x * kGY, xd0 = blockIdx.y * kGX, zd0 = blockIdx.z * kGZ;
+    const int zd1 = min(zd0 + kGZ, zd);
+    const int xf0 = 2 * xd0 - 1, yf0 = 2 * yd0 - 1;
     const float hx2 = 2 * hx, hy2 = 2 * hy, hz2 = 2 * hz;
-    float gmax = 0.0f;
-    const int ks = 2 * k + 1 < yn - 1 ? 2 * k + 1 : yn - 1;
-    for (int z = 2 * zk; z <= 2 * zk + 1 && z < zn; ++z)
-        for (int x = 2 * xk; x <= 2 * xk + 1 && x < xn; ++x) {
-            float a = grad_mag(im, 2 * k, x, z, yn, xn, zn, hx2, hy2, hz2);
-            float b = grad_mag(im, ks, x, z, yn, xn, zn, hx2, hy2, hz2);
-            float m = b > gmax ? b : gmax;
-            gmax = a > m ? a : m;
+
+    auto load = [&](int zf) {  // zf >= -1
+        float(*S)[kTY] = ring[(zf + 4) & 3];
+        const int zc = min(max(zf, 0), zn - 1);
+        for (int t = threadIdx.x; t < kTX * kTY; t += kGThreads) {
+            const int r = t / kTY, cc = t % kTY;
+            const int xg = min(max(xf0 + r, 0), xn - 1), yg = min(max(yf0 + cc, 0), yn - 1);
+            S[r][cc] = (float)im[idx3(yg, xg, zc, yn, xn)];
         }
-    grad[g] = to_it<IT>(gmax);
-    const int shx = 2 * xk + 1 < xn - 1 ? 2 * xk + 1 : xn - 1;
-    const int shz = 2 * zk + 1 < zn - 1 ? 2 * zk + 1 : zn - 1;
-    const int y0 = 2 * k, x0 = 2 * xk, z0 = 2 * zk;
-    float r = (float)im[idx3(y0, x0, z0, yn, xn)];
-    r = r + (float)im[idx3(ks, x0, z0, yn, xn)];
-    r = r + (float)im[idx3(y0, shx, z0, yn, xn)];
-    r = r + (float)im[idx3(ks, shx, z0, yn, xn)];
-    r = r + (float)im[idx3(y0, x0, shz, yn, xn)];
-    r = r + (float)im[idx3(ks, x0, shz, yn, xn)];
-    r = r + (float)im[idx3(y0, shx, shz, yn, xn)];
-    r = r + (float)im[idx3(ks, shx, shz, yn, xn)];
-    ids[g] = r / 8.0f;
+    };
+    auto gmag = [&](int zf, int xf, int yf) -> float {  // full-res coordinates inside the volume
+        if (yn < 2) return 0.0f;
+        const int r = xf - xf0, cc = yf - yf0;
+        const float(*C)[kTY] = ring[(zf + 4) & 3];
+        const float(*U)[kTY] = ring[(zf + 3) & 3];
+        const float(*D)[kTY] = ring[(zf + 5) & 3];
+        float gx = (C[r + 1][cc] - C[r - 1][cc]) / hx2;
+        float gz = (D[r][cc] - U[r][cc]) / hz2;
+        float gy = (C[r][cc + 1] - C[r][cc - 1]) / hy2;
+        double s = (double)gx * (double)gx + (double)gz * (double)gz;
+        s = s + (double)gy * (double)gy;
+        const double q = sqrt(s);
+        return sizeof(IT) == 2 ? cvt_u16d(q) : (float)q;
+    };
+
+    load(2 * zd0 - 1);
+    load(2 * zd0);
+    for (int z = zd0; z < zd1; ++z) {
+        load(2 * z + 1);
+        load(2 * z + 2);
+        __syncthreads();
+        for (int t = threadIdx.x; t < kGX * kGY; t += kGThreads) {
+            const int xl = t / kGY, yl = t % kGY;
+            const int xk = xd0 + xl, k = yd0 + yl;
+            if (xk >= xd || k >= yd) continue;
+            const int y0 = 2 * k, ks = min(2 * k + 1, yn - 1), x0 = 2 * xk, z0 = 2 * z;
+            float gmax = 0.0f;
+            for (int zf = z0; zf <= z0 + 1 && zf < zn; ++zf)
+                for (int xf = x0; xf <= x0 + 1 && xf < xn; ++xf) {
+                    const float a = gmag(zf, xf, y0), b = gmag(zf, xf, ks);
+                    const float m = b > gmax ? b : gmax;
+                    gmax = a > m ? a : m;
+                }
+            const uint64_t o = idx3(k, xk, z, yd, xd);
+            grad[o] = to_it<IT>(gmax);
+            // mean with the clamped indices of downsample (held by the tile)
+            const float(*A)[kTY] = ring[(z0 + 4) & 3];
+            const float(*B)[kTY] = ring[(z0 + 5) & 3];
+            const int r0 = x0 - xf0, c0 = y0 - yf0;
+            float s = A[r0][c0];
+            s = s + A[r0][c0 + 1];
+            s = s + A[r0 + 1][c0];
+            s = s + A[r0 + 1][c0 + 1];
+            s = s + B[r0][c0];
+            s = s + B[r0][c0 + 1];
+            s = s + B[r0 + 1][c0];
+            s = s + B[r0 + 1][c0 + 1];
+            ids[o] = s / 8.0f;
+        }
+        __syncthreads();
+    }
 }
 
 // ---------------------------------------------------------------------------
 // a5: calc_inv_bspline_y/x/z (ComputeGradient.hpp:785-964), the three
 // in-place passes fused: each output re-evaluates the y and x passes of its
-// 3x3x3 neighbourhood with identical float operations.
+// 3x3x3 neighbourhood with the same float operations, reading a shared-memory
+// tile of the input (8 x 8 x 64 outputs plus a one-sample halo).
 // ---------------------------------------------------------------------------
 struct InvB {
     float a1, a2, a3, a13;
 };
 
-__device__ __forceinline__ float inv_y(const float *__restrict__ I, int y, int x, int z, int yd, int xd, bool on,
-                                       InvB c) {
-    const float *L = I + idx3(0, x, z, yd, xd);
-    if (!on) return L[y];
-    if (y == 0) return c.a2 * L[0] + c.a13 * L[1];
-    if (y == yd - 1) return c.a13 * L[yd - 2] + c.a2 * L[yd - 1];
-    return c.a1 * L[y - 1] + c.a2 * L[y] + c.a3 * L[y + 1];
-}
-
-__device__ __forceinline__ float inv_x(const float *__restrict__ I, int y, int x, int z, int yd, int xd, bool ony,
-                                       bool onx, InvB c) {
-    if (!onx) return inv_y(I, y, x, z, yd, xd, ony, c);
-    if (x == xd - 1)
-        return c.a13 * inv_y(I, y, xd - 2, z, yd, xd, ony, c) + c.a2 * inv_y(I, y, xd - 1, z, yd, xd, ony, c);
-    const int xm = x == 0 ? 1 : x - 1;
-    return c.a1 * inv_y(I, y, xm, z, yd, xd, ony, c) + c.a2 * inv_y(I, y, x, z, yd, xd, ony, c) +
-           c.a3 * inv_y(I, y, x + 1, z, yd, xd, ony, c);
-}
-
-__global__ void inv_bspline_kernel(const float *__restrict__ I, float *__restrict__ O, int yd, int xd, int zd,
-                                   int ony, int onx, int onz, InvB c) {
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= (uint64_t)yd * xd * zd) return;
-    const int y = (int)(g % yd), x = (int)((g / yd) % xd), z = (int)(g / ((uint64_t)yd * xd));
-    float r;
-    if (!onz) {
-        r = inv_x(I, y, x, z, yd, xd, ony, onx, c);
-    } else if (z == zd - 1) {
-        r = c.a13 * inv_x(I, y, x, zd - 2, yd, xd, ony, onx, c) + c.a2 * inv_x(I, y, x, zd - 1, yd, xd, ony, onx, c);
-    } else {
-        const int zm = z == 0 ? 1 : z - 1;
-        r = c.a1 * inv_x(I, y, x, zm, yd, xd, ony, onx, c) + c.a2 * inv_x(I, y, x, z, yd, xd, ony, onx, c) +
-            c.a3 * inv_x(I, y, x, z + 1, yd, xd, ony, onx, c);
+constexpr int kIX = 8, kIY = 64, kIZ = 8;
+struct InvTile {
+    const float *s;
+    int x0, y0, z0;  // global coordinates of the tile's first interior sample
+    __device__ __forceinline__ float at(int y, int x, int z) const {
+        return s[((z - z0 + 1) * (kIX + 2) + (x - x0 + 1)) * (kIY + 2) + (y - y0 + 1)];
     }
-    O[g] = r;
+};
+
+__device__ __forceinline__ float inv_y(const InvTile &I, int y, int x, int z, int yd, bool on, InvB c) {
+    if (!on) return I.at(y, x, z);
+    if (y == 0) return c.a2 * I.at(0, x, z) + c.a13 * I.at(1, x, z);
+    if (y == yd - 1) return c.a13 * I.at(yd - 2, x, z) + c.a2 * I.at(yd - 1, x, z);
+    return c.a1 * I.at(y - 1, x, z) + c.a2 * I.at(y, x, z) + c.a3 * I.at(y + 1, x, z);
+}
+
+__device__ __forceinline__ float inv_x(const InvTile &I, int y, int x, int z, int yd, int xd, bool ony, bool onx,
+                                       InvB c) {
+    if (!onx) return inv_y(I, y, x, z, yd, ony, c);
+    if (x == xd - 1) return c.a13 * inv_y(I, y, xd - 2, z, yd, ony, c) + c.a2 * inv_y(I, y, xd - 1, z, yd, ony, c);
+    const int xm = x == 0 ? 1 : x - 1;
+    return c.a1 * inv_y(I, y, xm, z, yd, ony, c) + c.a2 * inv_y(I, y, x, z, yd, ony, c) +
+           c.a3 * inv_y(I, y, x + 1, z, yd, ony, c);
+}
+
+__global__ void __launch_bounds__(256) inv_bspline_kernel(const float *__restrict__ in, float *__restrict__ O, int yd,
+                                                          int xd, int zd, int ony, int onx, int onz, InvB c) {
+    __shared__ float s[(kIZ + 2) * (kIX + 2) * (kIY + 2)];
+    const int y0 = blockIdx.x * kIY, x0 = blockIdx.y * kIX, z0 = blockIdx.z * kIZ;
+    for (int t = threadIdx.x; t < (kIZ + 2) * (kIX + 2) * (kIY + 2); t += blockDim.x) {
+        const int yy = t % (kIY + 2), xx = (t / (kIY + 2)) % (kIX + 2), zz = t / ((kIY + 2) * (kIX + 2));
+        const int yg = y0 - 1 + yy, xg = x0 - 1 + xx, zg = z0 - 1 + zz;
+        if (yg >= 0 && yg < yd && xg >= 0 && xg < xd && zg >= 0 && zg < zd) s[t] = in[idx3(yg, xg, zg, yd, xd)];
+    }
+    __syncthreads();
+    const InvTile I{s, x0, y0, z0};
+    for (int t = threadIdx.x; t < kIX * kIY * kIZ; t += blockDim.x) {
+        const int y = y0 + t % kIY, x = x0 + (t / kIY) % kIX, z = z0 + t / (kIY * kIX);
+        if (y >= yd || x >= xd || z >= zd) continue;
+        float r;
+        if (!onz) {
+            r = inv_x(I, y, x, z, yd, xd, ony, onx, c);
+        } else if (z == zd - 1) {
+            r = c.a13 * inv_x(I, y, x, zd - 2, yd, xd, ony, onx, c) + c.a2 * inv_x(I, y, x, zd - 1, yd, xd, ony, onx, c);
+        } else {
+            const int zm = z == 0 ? 1 : z - 1;
+            r = c.a1 * inv_x(I, y, x, zm, yd, xd, ony, onx, c) + c.a2 * inv_x(I, y, x, z, yd, xd, ony, onx, c) +
+                c.a3 * inv_x(I, y, x, z + 1, yd, xd, ony, onx, c);
+        }
+        O[idx3(y, x, z, yd, xd)] = r;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -670,13 +762,12 @@ void launch_smooth(const uint16_t *img, IT *work, int yn, int xn, int zn, float 
 template <typename IT>
 void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *ids_raw, float *ids, int yd, int xd,
                      int zd, const aprb_params &p, cudaStream_t s) {
-    const uint64_t nd = (uint64_t)yd * xd * zd;
     {
-    APRB_PROF("gradient_ds", s);
-    grad_ds_kernel<IT><<<blocks_for(nd, 256), 256, 0, s>>>(work, yn, xn, zn, grad, ids_raw, yd, xd, zd, p.dx, p.dy,
-                                                          p.dz);
-    count_launch();
-    APRB_CHECK_LAUNCH();
+        APRB_PROF("gradient_ds", s);
+        dim3 grid((yd + kGY - 1) / kGY, (xd + kGX - 1) / kGX, (zd + kGZ - 1) / kGZ);
+        grad_ds_kernel<IT><<<grid, kGThreads, 0, s>>>(work, yn, xn, zn, grad, ids_raw, yd, xd, zd, p.dx, p.dy, p.dz);
+        count_launch();
+        APRB_CHECK_LAUNCH();
     }
     APRB_PROF("inv_bspline", s);
     const bool on = p.lambda > 0;
@@ -685,8 +776,8 @@ void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *id
     c.a2 = (float)(4.0 / 6.0);
     c.a3 = (float)(1.0 / 6.0);
     c.a13 = c.a1 + c.a3;
-    inv_bspline_kernel<<<blocks_for(nd, 256), 256, 0, s>>>(ids_raw, ids, yd, xd, zd, on && yn > 2, on && xn > 2,
-                                                          on && zn > 2, c);
+    dim3 grid((yd + kIY - 1) / kIY, (xd + kIX - 1) / kIX, (zd + kIZ - 1) / kIZ);
+    inv_bspline_kernel<<<grid, 256, 0, s>>>(ids_raw, ids, yd, xd, zd, on && yn > 2, on && xn > 2, on && zn > 2, c);
     count_launch();
     APRB_CHECK_LAUNCH();
 }
