@@ -254,8 +254,11 @@ def main():
     L.aprb_apr_free(h0)
 
     def step(keep):
+        # one APR alive at a time, as a converter loop over a stream of volumes
         h = get_apr_dev()
         _lib.check(L.aprb_sample_image_device(h, iptr, pptr, sptr))
+        while keep:
+            L.aprb_apr_free(keep.pop())
         keep.append(h)
 
     hs = []

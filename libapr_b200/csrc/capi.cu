@@ -5,7 +5,9 @@
 #include <cuda_runtime.h>
 
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -42,6 +44,44 @@ void prof_record(const char *name, cudaStream_t s, bool begin) {
         g_prof_open.pop_back();
         cudaEventRecord(g_prof[i].b, s);
     }
+}
+
+void *pool_alloc(size_t bytes, cudaStream_t s) {
+    int dev = 0;
+    APRB_CUDA(cudaGetDevice(&dev));
+    static std::mutex mu;
+    static uint64_t configured = 0;  // bit per device
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (dev < 64 && !(configured >> dev & 1)) {
+            cudaMemPool_t pool;
+            APRB_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+            uint64_t keep_all = UINT64_MAX;
+            APRB_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep_all));
+            configured |= uint64_t(1) << dev;
+        }
+    }
+    void *p = nullptr;
+    APRB_CUDA(cudaMallocAsync(&p, bytes, s));
+    return p;
+}
+
+// Work buffers of the filter and sampling calls, shared by every APR that the
+// calling thread uses on one device (they only live for the duration of one
+// call).  Calls issued by one thread on different streams that overlap on the
+// GPU share these buffers; use one thread per concurrent stream.
+struct ThreadScratch {
+    DevBuf scan_tmp, tree_vals, pyr, parts_f, parts_u16, out_f, rb, stencils, stencils_f, io_in, t_flags;
+    FilterBuffers fb;
+};
+
+static ThreadScratch &scratch() {
+    thread_local std::map<int, std::unique_ptr<ThreadScratch>> per_device;
+    int dev = 0;
+    APRB_CUDA(cudaGetDevice(&dev));
+    auto &p = per_device[dev];
+    if (!p) p.reset(new ThreadScratch());
+    return *p;
 }
 
 static void require_device() {
@@ -97,15 +137,12 @@ struct aprb_apr {
     int org[3] = {0, 0, 0};
     uint64_t n_xz = 0, P = 0;
     float offset = 0;
-    DevBuf xz_end, y_vec, level_xz;
+    DevBuf xz_end, y_vec;  // pooled
     // tree
     bool tree_built = false;
     Geom tg{};
     uint64_t t_n_xz = 0, T = 0;
-    DevBuf t_xz_end, t_y_vec, t_flags;
-    // filter work
-    DevBuf scan_tmp, tree_vals, pyr, parts_f, parts_u16, out_f, rb, stencils, stencils_f, io_in, io_out;
-    FilterBuffers fb;
+    DevBuf t_xz_end, t_y_vec;  // pooled
     FilterIndex fi;
     uint64_t last_stale = 0;
 };
@@ -303,7 +340,7 @@ void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, i
         launch_levels<IT>(grad, lis, ids, nd, d_off, p, L, top, lvl, sts, c->keep, s);
     }
 
-    uint64_t *xz_end = a->xz_end.as<uint64_t>(a->n_xz);
+    uint64_t *xz_end = a->xz_end.as_pooled<uint64_t>(a->n_xz, s);
     const int min_type = p.neighborhood_optimization ? 1 : 2;
     unsigned h_err = 0;
     if (L <= 2) {
@@ -316,7 +353,7 @@ void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, i
             set_error("integer under-/overflow encountered in the B-spline smoothing");
             throw Error{APRB_ERR_INTEGER_OVERFLOW};
         }
-        uint16_t *yv = a->y_vec.as<uint16_t>(a->P);
+        uint16_t *yv = a->y_vec.as_pooled<uint16_t>(a->P, s);
         launch_full_resolution_structure(g, xz_end, yv, s);
     } else {
         launch_pulling_scheme(g, pm, s);
@@ -326,7 +363,7 @@ void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, i
             set_error("integer under-/overflow encountered in the B-spline smoothing");
             throw Error{APRB_ERR_INTEGER_OVERFLOW};
         }
-        uint16_t *yv = a->y_vec.as<uint16_t>(a->P ? a->P : 1);
+        uint16_t *yv = a->y_vec.as_pooled<uint16_t>(a->P ? a->P : 1, s);
         launch_linear_fill(g, pm, xz_end, yv, min_type, s);
     }
     APRB_CUDA(cudaMemcpyAsync(&a->offset, d_off, sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -493,8 +530,8 @@ aprb_status aprb_apr_from_arrays(int y_num, int x_num, int z_num, const uint64_t
         a->org[1] = x_num;
         a->org[2] = z_num;
         a->P = n_particles;
-        APRB_CUDA(cudaMemcpy(a->xz_end.as<uint64_t>(n_xz), xz_end, n_xz * sizeof(uint64_t), cudaMemcpyHostToDevice));
-        uint16_t *yv = a->y_vec.as<uint16_t>(n_particles ? n_particles : 1);
+        APRB_CUDA(cudaMemcpy(a->xz_end.as_pooled<uint64_t>(n_xz, 0), xz_end, n_xz * sizeof(uint64_t), cudaMemcpyHostToDevice));
+        uint16_t *yv = a->y_vec.as_pooled<uint16_t>(n_particles ? n_particles : 1, 0);
         if (n_particles) {
             ARG_CHECK(y_vec, "null y_vec");
             APRB_CUDA(cudaMemcpy(yv, y_vec, n_particles * sizeof(uint16_t), cudaMemcpyHostToDevice));
@@ -507,8 +544,7 @@ aprb_status aprb_sample_image_device(const aprb_apr *a, const uint16_t *img_dev,
     return guarded([&] {
         require_device();
         ARG_CHECK(a && img_dev && parts_dev, "null argument");
-        aprb_apr *m = const_cast<aprb_apr *>(a);
-        launch_sample(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, img_dev, parts_dev, m->pyr,
+        launch_sample(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, img_dev, parts_dev, scratch().pyr,
                       (cudaStream_t)stream);
     });
 }
@@ -517,13 +553,12 @@ aprb_status aprb_sample_image(const aprb_apr *a, const uint16_t *img, uint16_t *
     return guarded([&] {
         require_device();
         ARG_CHECK(a && img && parts, "null argument");
-        aprb_apr *m = const_cast<aprb_apr *>(a);
         cudaStream_t s = cudaStreamPerThread;
         const uint64_t n = (uint64_t)a->org[0] * a->org[1] * a->org[2];
-        uint16_t *di = m->io_in.as<uint16_t>(n);
-        uint16_t *dp = m->parts_u16.as<uint16_t>(a->P ? a->P : 1);
+        uint16_t *di = scratch().io_in.as<uint16_t>(n);
+        uint16_t *dp = scratch().parts_u16.as<uint16_t>(a->P ? a->P : 1);
         APRB_CUDA(cudaMemcpyAsync(di, img, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
-        launch_sample(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, di, dp, m->pyr, s);
+        launch_sample(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, di, dp, scratch().pyr, s);
         if (a->P) APRB_CUDA(cudaMemcpyAsync(parts, dp, a->P * sizeof(uint16_t), cudaMemcpyDeviceToHost, s));
         APRB_CUDA(cudaStreamSynchronize(s));
     });
@@ -536,13 +571,12 @@ namespace {
 void ensure_tree(aprb_apr *a, cudaStream_t s) {
     if (a->tree_built) return;
     a->t_n_xz = tree_geometry(a->org[0], a->org[1], a->org[2], a->tg);
-    uint64_t *txz = a->t_xz_end.as<uint64_t>(a->t_n_xz);
+    uint64_t *txz = a->t_xz_end.as_pooled<uint64_t>(a->t_n_xz, s);
     a->T = launch_tree_build(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg, txz,
-                             a->t_n_xz, a->t_flags, a->scan_tmp, s);
-    uint16_t *ty = a->t_y_vec.as<uint16_t>(a->T ? a->T : 1);
-    launch_tree_fill(a->tg, a->t_flags, txz, ty, s);
+                             a->t_n_xz, scratch().t_flags, scratch().scan_tmp, s);
+    uint16_t *ty = a->t_y_vec.as_pooled<uint16_t>(a->T ? a->T : 1, s);
+    launch_tree_fill(a->tg, scratch().t_flags, txz, ty, s);
     APRB_CUDA(cudaStreamSynchronize(s));
-    a->t_flags.release();
     build_filter_index(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg, txz, ty, a->fi, s);
     a->tree_built = true;
 }
@@ -573,13 +607,13 @@ void convolve_impl(aprb_apr *a, const float *stencil, int ks, const float *in, f
     ensure_tree(a, s);
     std::vector<float> host;
     ConvPlan plan = make_plan(a, stencil, ks, ds, normalize, reflect, host);
-    float *dst = a->stencils.as<float>(host.size());
+    float *dst = scratch().stencils.as<float>(host.size());
     APRB_CUDA(cudaMemcpyAsync(dst, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice, s));
-    float *tree = a->tree_vals.as<float>(a->T ? a->T : 1);
+    float *tree = scratch().tree_vals.as<float>(a->T ? a->T : 1);
     filter_apply(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
                  (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, a->fi, in, tree, &plan, dst, out, 0,
-                 nullptr, a->fb, s);
-    a->last_stale = filter_stale_count(a->fb, s);
+                 nullptr, scratch().fb, s);
+    a->last_stale = filter_stale_count(scratch().fb, s);
 }
 
 __global__ void fill_kernel(float *p, uint64_t n, float v) {
@@ -596,8 +630,8 @@ void rl_impl(aprb_apr *a, const uint16_t *in, float *out, const float *psf, int 
     std::vector<float> hp, hf;
     ConvPlan plan = make_plan(a, psf, ks, ds, normalize, 1, hp);
     ConvPlan plan_f = make_plan(a, flipped.data(), ks, ds, normalize, 1, hf);
-    float *dp = a->stencils.as<float>(hp.size());
-    float *df = a->stencils_f.as<float>(hf.size());
+    float *dp = scratch().stencils.as<float>(hp.size());
+    float *df = scratch().stencils_f.as<float>(hf.size());
     APRB_CUDA(cudaMemcpyAsync(dp, hp.data(), hp.size() * sizeof(float), cudaMemcpyHostToDevice, s));
     APRB_CUDA(cudaMemcpyAsync(df, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice, s));
     if (!resume && a->P) {
@@ -605,16 +639,16 @@ void rl_impl(aprb_apr *a, const uint16_t *in, float *out, const float *psf, int 
         count_launch();
         APRB_CHECK_LAUNCH();
     }
-    float *tree = a->tree_vals.as<float>(a->T ? a->T : 1);
-    float *rb = a->rb.as<float>(a->P ? a->P : 1);
+    float *tree = scratch().tree_vals.as<float>(a->T ? a->T : 1);
+    float *rb = scratch().rb.as<float>(a->P ? a->P : 1);
     const uint64_t *xz = (const uint64_t *)a->xz_end.p;
     const uint16_t *yv = (const uint16_t *)a->y_vec.p;
     const uint64_t *txz = (const uint64_t *)a->t_xz_end.p;
     const uint16_t *tyv = (const uint16_t *)a->t_y_vec.p;
     for (int it = 0; it < niter; ++it) {
         // rb = in / conv(psf_flipped, out); out = out * conv(psf, rb)  (APRNumerics.hpp:565-570)
-        filter_apply(a->g, xz, yv, a->tg, txz, tyv, a->fi, out, tree, &plan_f, df, rb, 1, in, a->fb, s);
-        filter_apply(a->g, xz, yv, a->tg, txz, tyv, a->fi, rb, tree, &plan, dp, out, 2, nullptr, a->fb, s);
+        filter_apply(a->g, xz, yv, a->tg, txz, tyv, a->fi, out, tree, &plan_f, df, rb, 1, in, scratch().fb, s);
+        filter_apply(a->g, xz, yv, a->tg, txz, tyv, a->fi, rb, tree, &plan, dp, out, 2, nullptr, scratch().fb, s);
     }
 }
 
@@ -649,7 +683,7 @@ aprb_status aprb_fill_tree_mean_device(aprb_apr *a, const float *parts_dev, floa
         ensure_tree(a, s);
         filter_apply(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
                      (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, a->fi, parts_dev, tree_dev, nullptr,
-                     nullptr, nullptr, 0, nullptr, a->fb, s);
+                     nullptr, nullptr, 0, nullptr, scratch().fb, s);
     });
 }
 
@@ -659,12 +693,12 @@ aprb_status aprb_fill_tree_mean(aprb_apr *a, const float *parts, float *tree) {
         ARG_CHECK(a && parts && tree, "null argument");
         cudaStream_t s = cudaStreamPerThread;
         ensure_tree(a, s);
-        float *dp = a->parts_f.as<float>(a->P ? a->P : 1);
-        float *dt = a->out_f.as<float>(a->T ? a->T : 1);
+        float *dp = scratch().parts_f.as<float>(a->P ? a->P : 1);
+        float *dt = scratch().out_f.as<float>(a->T ? a->T : 1);
         APRB_CUDA(cudaMemcpyAsync(dp, parts, a->P * sizeof(float), cudaMemcpyHostToDevice, s));
         filter_apply(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
                      (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, a->fi, dp, dt, nullptr, nullptr,
-                     nullptr, 0, nullptr, a->fb, s);
+                     nullptr, 0, nullptr, scratch().fb, s);
         APRB_CUDA(cudaMemcpyAsync(tree, dt, a->T * sizeof(float), cudaMemcpyDeviceToHost, s));
         APRB_CUDA(cudaStreamSynchronize(s));
     });
@@ -686,8 +720,8 @@ aprb_status aprb_convolve(aprb_apr *a, const float *stencil, int ksize, const fl
         require_device();
         ARG_CHECK(a && stencil && in && out, "null argument");
         cudaStream_t s = cudaStreamPerThread;
-        float *di = a->parts_f.as<float>(a->P ? a->P : 1);
-        float *dout = a->out_f.as<float>(a->P ? a->P : 1);
+        float *di = scratch().parts_f.as<float>(a->P ? a->P : 1);
+        float *dout = scratch().out_f.as<float>(a->P ? a->P : 1);
         APRB_CUDA(cudaMemcpyAsync(di, in, a->P * sizeof(float), cudaMemcpyHostToDevice, s));
         convolve_impl(a, stencil, ksize, di, dout, reflect, use_stencil_downsample, normalize, s);
         APRB_CUDA(cudaMemcpyAsync(out, dout, a->P * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -712,8 +746,8 @@ aprb_status aprb_richardson_lucy(aprb_apr *a, const uint16_t *in, float *out, co
         require_device();
         ARG_CHECK(a && in && out && psf && niter >= 0, "invalid argument");
         cudaStream_t s = cudaStreamPerThread;
-        uint16_t *di = a->parts_u16.as<uint16_t>(a->P ? a->P : 1);
-        float *dout = a->out_f.as<float>(a->P ? a->P : 1);
+        uint16_t *di = scratch().parts_u16.as<uint16_t>(a->P ? a->P : 1);
+        float *dout = scratch().out_f.as<float>(a->P ? a->P : 1);
         APRB_CUDA(cudaMemcpyAsync(di, in, a->P * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
         if (resume) APRB_CUDA(cudaMemcpyAsync(dout, out, a->P * sizeof(float), cudaMemcpyHostToDevice, s));
         rl_impl(a, di, dout, psf, ksize, niter, use_stencil_downsample, normalize, resume, s);

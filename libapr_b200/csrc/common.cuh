@@ -52,19 +52,36 @@ inline unsigned blocks_for(uint64_t n, unsigned threads) {
 }
 
 // ------------------------------------------------------------------ device buffers
+// Stream-ordered allocation from the device's default memory pool, whose
+// release threshold is raised so that freed blocks stay reserved for the next
+// APR instead of going back to the driver (cudaMalloc/cudaFree synchronise
+// the device and cost milliseconds at these sizes).
+void *pool_alloc(size_t bytes, cudaStream_t s);
+
 // A device allocation that grows on demand and is reused across calls, as the
-// reference converter keeps its scratch images as members.
+// reference converter keeps its scratch images as members.  Pooled buffers
+// (get_pooled) come from pool_alloc; release() waits for the device before it
+// hands them back, as cudaFree would.
 struct DevBuf {
     void *p = nullptr;
     size_t cap = 0;
+    bool pooled = false;
     void *get(size_t bytes) {
         if (bytes > cap) {
-            if (p) cudaFree(p);
-            p = nullptr;
-            cap = 0;
+            release();
             size_t want = bytes ? bytes : 16;
             APRB_CUDA(cudaMalloc(&p, want));
             cap = want;
+        }
+        return p;
+    }
+    void *get_pooled(size_t bytes, cudaStream_t s) {
+        if (bytes > cap) {
+            release();
+            size_t want = bytes ? bytes : 16;
+            p = pool_alloc(want, s);
+            cap = want;
+            pooled = true;
         }
         return p;
     }
@@ -72,10 +89,22 @@ struct DevBuf {
     T *as(size_t n) {
         return (T *)get(n * sizeof(T));
     }
+    template <typename T>
+    T *as_pooled(size_t n, cudaStream_t s) {
+        return (T *)get_pooled(n * sizeof(T), s);
+    }
     void release() {
-        if (p) cudaFree(p);
+        if (p) {
+            if (pooled) {
+                cudaDeviceSynchronize();
+                cudaFreeAsync(p, 0);
+            } else {
+                cudaFree(p);
+            }
+        }
         p = nullptr;
         cap = 0;
+        pooled = false;
     }
     ~DevBuf() { release(); }
     DevBuf() = default;

@@ -328,7 +328,9 @@ __global__ void offset_copy_kernel(const uint16_t *__restrict__ src, IT *__restr
 constexpr int kGX = 8, kGY = 64, kGZ = 8, kGThreads = 256;
 constexpr int kTX = 2 * kGX + 2, kTY = 2 * kGY + 2;
 
-template <typename IT>
+// PW2: every 2h is a power of two, so dividing by it is the exact multiply by
+// its reciprocal (both round the same real number once).
+template <typename IT, bool PW2>
 __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict__ im, int yn, int xn, int zn,
                                                             IT *__restrict__ grad, float *__restrict__ ids, int yd,
                                                             int xd, int zd, float hx, float hy, float hz) {
@@ -337,6 +339,7 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
     const int zd1 = min(zd0 + kGZ, zd);
     const int xf0 = 2 * xd0 - 1, yf0 = 2 * yd0 - 1;
     const float hx2 = 2 * hx, hy2 = 2 * hy, hz2 = 2 * hz;
+    const float ihx2 = 1.0f / hx2, ihy2 = 1.0f / hy2, ihz2 = 1.0f / hz2;
 
     auto load = [&](int zf) {  // zf >= -1
         float(*S)[kTY] = ring[(zf + 4) & 3];
@@ -353,9 +356,16 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
         const float(*C)[kTY] = ring[(zf + 4) & 3];
         const float(*U)[kTY] = ring[(zf + 3) & 3];
         const float(*D)[kTY] = ring[(zf + 5) & 3];
-        float gx = (C[r + 1][cc] - C[r - 1][cc]) / hx2;
-        float gz = (D[r][cc] - U[r][cc]) / hz2;
-        float gy = (C[r][cc + 1] - C[r][cc - 1]) / hy2;
+        float gx, gz, gy;
+        if (PW2) {
+            gx = (C[r + 1][cc] - C[r - 1][cc]) * ihx2;
+            gz = (D[r][cc] - U[r][cc]) * ihz2;
+            gy = (C[r][cc + 1] - C[r][cc - 1]) * ihy2;
+        } else {
+            gx = (C[r + 1][cc] - C[r - 1][cc]) / hx2;
+            gz = (D[r][cc] - U[r][cc]) / hz2;
+            gy = (C[r][cc + 1] - C[r][cc - 1]) / hy2;
+        }
         double s = (double)gx * (double)gx + (double)gz * (double)gz;
         s = s + (double)gy * (double)gy;
         const double q = sqrt(s);
@@ -394,7 +404,7 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
             s = s + B[r0][c0 + 1];
             s = s + B[r0 + 1][c0];
             s = s + B[r0 + 1][c0 + 1];
-            ids[o] = s / 8.0f;
+            ids[o] = s * 0.125f;  // == s / 8 exactly
         }
         __syncthreads();
     }
@@ -765,7 +775,17 @@ void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *id
     {
         APRB_PROF("gradient_ds", s);
         dim3 grid((yd + kGY - 1) / kGY, (xd + kGX - 1) / kGX, (zd + kGZ - 1) / kGZ);
-        grad_ds_kernel<IT><<<grid, kGThreads, 0, s>>>(work, yn, xn, zn, grad, ids_raw, yd, xd, zd, p.dx, p.dy, p.dz);
+        auto pow2 = [](float h) {
+            int e = 0;
+            const float m = std::frexp(2.0f * h, &e);
+            return m == 0.5f && e > -120 && e < 120;
+        };
+        if (pow2(p.dx) && pow2(p.dy) && pow2(p.dz))
+            grad_ds_kernel<IT, true><<<grid, kGThreads, 0, s>>>(work, yn, xn, zn, grad, ids_raw, yd, xd, zd, p.dx, p.dy,
+                                                                p.dz);
+        else
+            grad_ds_kernel<IT, false><<<grid, kGThreads, 0, s>>>(work, yn, xn, zn, grad, ids_raw, yd, xd, zd, p.dx,
+                                                                 p.dy, p.dz);
         count_launch();
         APRB_CHECK_LAUNCH();
     }

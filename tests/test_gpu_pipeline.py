@@ -49,7 +49,8 @@ def test_get_apr_bit_exact(shape, blobs, seed, image_type):
 
 @pytest.mark.parametrize("kw", [dict(lambda_=0.5), dict(lambda_=10.0), dict(sigma_th=0.0, grad_th=0.0),
                                 dict(neighborhood_optimization=False), dict(Ip_th=150.0, rel_error=0.05),
-                                dict(constant_intensity_scale=True), dict(lambda_=0.0)])
+                                dict(constant_intensity_scale=True), dict(lambda_=0.0),
+                                dict(dx=0.5, dy=0.25, dz=2.0), dict(dx=0.7, dy=1.3, dz=1.0)])
 def test_get_apr_parameter_variants(kw):
     img = volume((24, 40, 36), 10, 11)
     e, acc, (off, inter) = B.orc_get_apr(img, oracle_params(**kw), 1)
