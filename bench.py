@@ -196,6 +196,80 @@ def run_reference(args):
     return 0
 
 
+BATCH_AXES = (64, 96, 128, 192, 256, 384, 512)
+
+
+def batch_shapes(n=96, seed=2024):
+    """Seeded uneven volumes: every axis from BATCH_AXES, z <= 256, blob
+    density uniform in [1e-5, 5e-4] per voxel."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        z = int(rng.choice([a for a in BATCH_AXES if a <= 256]))
+        x = int(rng.choice(BATCH_AXES))
+        y = int(rng.choice(BATCH_AXES))
+        dens = float(rng.uniform(1e-5, 5e-4))
+        out.append(((z, x, y), max(1, int(round(dens * z * x * y)))))
+    return out
+
+
+def bench_batch(A, L, _lib, torch, stream, sptr, args):
+    """96 volumes through the blocked converter (z tiles of 128 planes, 16 ghost
+    planes) in one batch call, beside one whole-volume get_apr per volume."""
+    shapes = batch_shapes()
+    vols = []
+    for i, (shp, nb) in enumerate(shapes):
+        t = torch.empty(shp, dtype=torch.int16, device="cuda")
+        A.synth_blobs_device(t, nb, SIGMA, AMP, BG, seed=5000 + i, stream=stream)
+        vols.append(t)
+    torch.cuda.synchronize()
+    conv = A.APRConverterBatch("float", z_block_size=128, ghost_z=16)
+    conv.par = lib_params()
+    plain = A.APRConverter("float")
+    plain.par = lib_params()
+    nvox = sum(int(v.numel()) for v in vols)
+    par = plain.par.c()
+
+    def run_batch():
+        aprs = conv.get_apr_batch(vols, stream=stream)
+        return sum(a.total_number_particles() for a in aprs)
+
+    def run_plain():
+        P = 0
+        for v in vols:
+            h = C.c_void_p()
+            z, x, y = v.shape
+            _lib.check(L.aprb_get_apr_device(plain._h, C.byref(par), C.c_void_p(v.data_ptr()), y, x, z, sptr,
+                                             C.byref(h)))
+            info = _lib.aprb_apr_info()
+            L.aprb_apr_get_info(h, C.byref(info))
+            P += int(info.total_number_particles)
+            L.aprb_apr_free(h)
+        return P
+
+    res = {}
+    for name, fn in (("batch", run_batch), ("per_volume", run_plain)):
+        for _ in range(max(1, args.warmup - 1)):
+            fn()
+        torch.cuda.synchronize()
+        reps = 2
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            P = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        res[name] = {"ms": ms, "value": nvox / (ms / 1e3) / 1e9, "unit": "GVox/s", "particles": P}
+    res["volumes"] = len(vols)
+    res["voxels"] = nvox
+    res["workload"] = ("96 seeded uint16 blob volumes, axes from %s with z <= 256, blob density U[1e-5, 5e-4]; "
+                       "batch: blocked converter, z tiles 128 + ghost 16; per_volume: whole-volume get_apr, "
+                       "one call per volume; ImageType float" % (BATCH_AXES,))
+    del vols
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -205,6 +279,7 @@ def main():
     ap.add_argument("--shape", default=None, help="z,x,y override (debugging only)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-conv", action="store_true")
+    ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--image-type", default="float", choices=["float", "uint16"],
                     help="APRConverter ImageType; uint16 throws the reference's overflow error on this volume")
     args = ap.parse_args()
@@ -366,6 +441,10 @@ def main():
         del pf, outp
     L.aprb_apr_free(last)
 
+    batch_res = None
+    if not args.no_batch and rank == 0:
+        batch_res = bench_batch(A, L, _lib, torch, stream, sptr, args)
+
     # --- end to end through the host-buffer C ABI
     e2e = None
     if rank == 0:
@@ -403,6 +482,8 @@ def main():
                            "l2": "input 4 GiB > L2, no flush needed",
                            "parallelism": "independent volume per GPU" if world > 1 else "1 GPU"},
                 "gpu_launches": int(launches), "e2e": e2e, "cpu_baseline": cpu, **out, **conv_res}
+        if batch_res:
+            line["batch_by_block"] = batch_res
         if ck:
             line["clocks"] = ck
         print(json.dumps(line))

@@ -106,6 +106,30 @@ aprb_status aprb_get_apr(aprb_converter *c, const aprb_params *p, const uint16_t
 /* same, image already on the device; enqueued on stream, returns after the particle count is known */
 aprb_status aprb_get_apr_device(aprb_converter *c, const aprb_params *p, const uint16_t *img_dev, int y_num,
                                 int x_num, int z_num, void *stream, aprb_apr **out);
+/* Blocked construction, APRConverterBatch<IT> (APRConverterBatch.hpp:114-175): the pixel
+ * pipeline runs per z-tile of z_block_size planes (the last tile takes the remainder) with
+ * up to ghost_z planes of overlap on each side (get_apr_method_patch :190-271), every tile
+ * fills the global particle-cell tree (fill_global_particle_cell_tree :282-314), then one
+ * pulling scheme and one linear structure are built.  The reference reads the tiles from a
+ * TIFF file (get_apr(APR&) :48-64); here the caller passes the volume.  Reference defaults:
+ * z_block_size 128, ghost_z 32.  Where the reference's integer ghost cropping maps the last
+ * tile one plane past a coarse level, the reference writes outside that level's array; here
+ * those planes are skipped. */
+aprb_status aprb_get_apr_by_block(aprb_converter *c, const aprb_params *p, const uint16_t *img, int y_num,
+                                  int x_num, int z_num, int z_block_size, int ghost_z, aprb_apr **out);
+aprb_status aprb_get_apr_by_block_device(aprb_converter *c, const aprb_params *p, const uint16_t *img_dev, int y_num,
+                                         int x_num, int z_num, int z_block_size, int ghost_z, void *stream,
+                                         aprb_apr **out);
+/* many volumes of uneven sizes through the blocked converter, in order, on one stream
+ * (the reference converts one file per call); outs[i] receives volume i's APR, and on an
+ * error no APR is returned */
+typedef struct {
+    const uint16_t *img_dev;
+    int y_num, x_num, z_num;
+} aprb_volume;
+aprb_status aprb_get_apr_batch_device(aprb_converter *c, const aprb_params *p, int n_volumes,
+                                      const aprb_volume *volumes, int z_block_size, int ghost_z, void *stream,
+                                      aprb_apr **outs);
 /* copy one APRB_STAGE_* intermediate of the last get_apr to the host (n = element count) */
 aprb_status aprb_converter_intermediate(const aprb_converter *c, int stage, float *dst, size_t n);
 
@@ -125,6 +149,13 @@ aprb_status aprb_apr_from_arrays(int y_num, int x_num, int z_num, const uint64_t
 /* --- particle sampling: ParticleData::sample_image (ParticleData.hpp:123-127) --- */
 aprb_status aprb_sample_image(const aprb_apr *a, const uint16_t *img, uint16_t *parts);
 aprb_status aprb_sample_image_device(const aprb_apr *a, const uint16_t *img_dev, uint16_t *parts_dev, void *stream);
+/* blocked sampling, sample_parts_from_img_blocked (ParticleData.hpp:140-142, 288-372): every
+ * z-tile builds its own mean pyramid and writes the particles of its rows (reference
+ * defaults z_block_size 256, ghost_z 32; tiles from memory instead of a TIFF file) */
+aprb_status aprb_sample_image_by_block(const aprb_apr *a, const uint16_t *img, int z_block_size, int ghost_z,
+                                       uint16_t *parts);
+aprb_status aprb_sample_image_by_block_device(const aprb_apr *a, const uint16_t *img_dev, int z_block_size,
+                                              int ghost_z, uint16_t *parts_dev, void *stream);
 
 /* Particle sampling that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot allocate GPU memory while they run:

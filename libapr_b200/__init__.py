@@ -234,6 +234,54 @@ class APRConverter:
         return out
 
 
+class APRConverterBatch(APRConverter):
+    """APRConverterBatch<ImageType> (src/algorithm/APRConverterBatch.hpp:32-98):
+    the pipeline per z-tile of ``z_block_size`` planes with ``ghost_z`` planes
+    of overlap, then one pulling scheme for the volume.  The reference reads
+    the tiles from ``par.input_dir + par.input_image_name`` (a TIFF file);
+    here ``get_apr(apr, img)`` takes the volume (numpy (z, x, y) uint16 array or
+    a CUDA tensor)."""
+
+    def __init__(self, image_type="uint16", z_block_size=128, ghost_z=32):
+        super().__init__(image_type)
+        self.z_block_size = z_block_size
+        self.ghost_z = ghost_z
+
+    def get_apr(self, apr, img):
+        p = self.par.c()
+        h = C.c_void_p()
+        if hasattr(img, "data_ptr"):
+            z, x, y = img.shape
+            st = lib().aprb_get_apr_by_block_device(self._h, C.byref(p), _dptr(img), y, x, z, self.z_block_size,
+                                                    self.ghost_z, None, C.byref(h))
+        else:
+            a = np.ascontiguousarray(img, np.uint16)
+            z, x, y = a.shape
+            st = lib().aprb_get_apr_by_block(self._h, C.byref(p), _ptr(a), y, x, z, self.z_block_size, self.ghost_z,
+                                             C.byref(h))
+        return self._finish(st, h, apr)
+
+    def get_apr_batch(self, imgs, stream=None):
+        """Blocked get_apr of many device volumes (CUDA tensors (z, x, y)) in one
+        call; returns the list of APRs."""
+        p = self.par.c()
+        n = len(imgs)
+        vols = (_lib.aprb_volume * max(n, 1))()
+        for i, t in enumerate(imgs):
+            z, x, y = t.shape
+            vols[i] = _lib.aprb_volume(_dptr(t), y, x, z)
+        outs = (C.c_void_p * max(n, 1))()
+        sp = None if stream is None else C.c_void_p(stream.cuda_stream)
+        check(lib().aprb_get_apr_batch_device(self._h, C.byref(p), n, vols, self.z_block_size, self.ghost_z, sp,
+                                              outs))
+        res = []
+        for i in range(n):
+            a = APR()
+            a._set(C.c_void_p(outs[i]))
+            res.append(a)
+        return res
+
+
 class ParticleData:
     """ParticleData<T> (ParticleData.hpp:26-218): ``data`` is a numpy array."""
 
@@ -242,6 +290,15 @@ class ParticleData:
 
     def __len__(self):
         return 0 if self.data is None else len(self.data)
+
+    def sample_parts_from_img_blocked(self, apr, img, z_block_size=256, ghost_z=32):
+        """sample_parts_from_img_blocked (ParticleData.hpp:140-142): tiles of the
+        in-memory volume instead of a TIFF file."""
+        a = np.ascontiguousarray(img, np.uint16)
+        out = np.zeros(max(apr.total_number_particles(), 1), np.uint16)
+        check(lib().aprb_sample_image_by_block(apr._h, _ptr(a), z_block_size, ghost_z, _ptr(out)))
+        self.data = out[: apr.total_number_particles()]
+        return self
 
     def sample_image(self, apr, img):
         a = np.ascontiguousarray(img, np.uint16)

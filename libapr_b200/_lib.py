@@ -34,6 +34,10 @@ class aprb_apr_info(C.Structure):
                 ("tree_n_level_xz", C.c_uint64), ("tree_n_xz", C.c_uint64)]
 
 
+class aprb_volume(C.Structure):
+    _fields_ = [("img_dev", C.c_void_p), ("y_num", C.c_int), ("x_num", C.c_int), ("z_num", C.c_int)]
+
+
 # Every exported entry point and its C signature (include/aprb200.h).
 _vp, _u64, _i, _f = C.c_void_p, C.c_uint64, C.c_int, C.c_float
 SIGNATURES = {
@@ -45,6 +49,11 @@ SIGNATURES = {
     "aprb_converter_keep_intermediates": ([_vp, _i], _i),
     "aprb_get_apr": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, C.POINTER(_vp)], _i),
     "aprb_get_apr_device": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, _vp, C.POINTER(_vp)], _i),
+    "aprb_get_apr_by_block": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, _i, _i, C.POINTER(_vp)], _i),
+    "aprb_get_apr_by_block_device": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, _i, _i, _vp, C.POINTER(_vp)],
+                                     _i),
+    "aprb_get_apr_batch_device": ([_vp, C.POINTER(aprb_params), _i, C.POINTER(aprb_volume), _i, _i, _vp,
+                                   C.POINTER(_vp)], _i),
     "aprb_converter_intermediate": ([_vp, _i, _vp, C.c_size_t], _i),
     "aprb_apr_free": ([_vp], _i),
     "aprb_apr_get_info": ([_vp, C.POINTER(aprb_apr_info)], _i),
@@ -53,6 +62,8 @@ SIGNATURES = {
     "aprb_apr_from_arrays": ([_i, _i, _i, _vp, _u64, _vp, _u64, _vp, _u64, C.POINTER(_vp)], _i),
     "aprb_sample_image": ([_vp, _vp, _vp], _i),
     "aprb_sample_image_device": ([_vp, _vp, _vp, _vp], _i),
+    "aprb_sample_image_by_block": ([_vp, _vp, _i, _i, _vp], _i),
+    "aprb_sample_image_by_block_device": ([_vp, _vp, _i, _i, _vp, _vp], _i),
     "aprb_sample_image_noalloc": ([_vp, _vp, _i, _i, _i, _vp, _vp, _vp], _i),
     "aprb_apr_init_tree": ([_vp], _i),
     "aprb_apr_export_tree": ([_vp, _vp, _vp, _vp], _i),

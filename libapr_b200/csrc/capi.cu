@@ -152,7 +152,7 @@ struct aprb_converter {
     int keep = 0;
     int dims[3] = {0, 0, 0};  // y, x, z of the last call
     DevBuf img, work, grad, grad_keep, ids_raw, ids, lis, lis_keep, pyr_status, pyr_level, mm, offset, err;
-    DevBuf scan_tmp;
+    DevBuf scan_tmp, tile_pyr;
     LisBuffers lisb;
     bool have = false;
 };
@@ -283,6 +283,74 @@ bool check_dims(const aprb_params &p, int &y, int &x, int &z) {
     return false;
 }
 
+// Pixel stages of one image -- the whole volume, or one z-tile of the blocked
+// converter (APRConverterBatch.hpp:190-271): offset, smoothing, gradient +
+// ds image, inverse B-spline, local intensity scale.  Overflow is accumulated
+// in the converter's error flag, which the caller clears and reads.
+template <typename IT>
+struct PixelOut {
+    IT *grad;
+    float *lis, *ids;
+    const float *d_off;
+    uint64_t nd;
+};
+
+template <typename IT>
+PixelOut<IT> pixel_stages(aprb_converter *c, const aprb_params &p, const uint16_t *img, int yn, int xn, int zn,
+                          cudaStream_t s) {
+    const int yd = (yn + 1) / 2, xd = (xn + 1) / 2, zd = (zn + 1) / 2;
+    const uint64_t n = (uint64_t)yn * xn * zn, nd = (uint64_t)yd * xd * zd;
+    const bool is_u16 = sizeof(IT) == 2;
+    unsigned *mm = c->mm.as<unsigned>(2);
+    float *d_off = c->offset.as<float>(1);
+    unsigned *d_err = c->err.as<unsigned>(1);
+    launch_minmax_offset(img, n, mm, d_off, is_u16 && p.lambda > 0, s);
+    IT *work = c->work.as<IT>(n);
+    launch_smooth<IT>(img, work, yn, xn, zn, p.lambda, d_off, d_err, s);
+    IT *grad = c->grad.as<IT>(nd);
+    float *ids_raw = c->ids_raw.as<float>(nd);
+    float *ids = c->ids.as<float>(nd);
+    launch_gradient<IT>(work, yn, xn, zn, grad, ids_raw, ids, yd, xd, zd, p, s);
+    float *lis = c->lis.as<float>(nd);
+    launch_local_intensity_scale(ids, lis, yd, xd, zd, p, c->lisb, s);
+    return PixelOut<IT>{grad, lis, ids, d_off, nd};
+}
+
+void throw_if_overflow(aprb_converter *c, cudaStream_t s) {
+    unsigned h_err = 0;
+    APRB_CUDA(cudaMemcpyAsync(&h_err, c->err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    APRB_CUDA(cudaStreamSynchronize(s));
+    if (h_err) {
+        set_error("integer under-/overflow encountered in the B-spline smoothing");
+        throw Error{APRB_ERR_INTEGER_OVERFLOW};
+    }
+}
+
+// Linear access structure from the solved particle-cell pyramid
+// (generateDatastructures, APRConverter.hpp:339-363); reads the overflow
+// flag before the particle count is trusted.
+void build_structure(aprb_converter *c, const aprb_params &p, Pyramid &pm, aprb_apr *a, cudaStream_t s) {
+    const Geom &g = a->g;
+    const int L = g.l_max;
+    uint64_t *xz_end = a->xz_end.as_pooled<uint64_t>(a->n_xz, s);
+    const int min_type = p.neighborhood_optimization ? 1 : 2;
+    if (L <= 2) {
+        APRB_CUDA(cudaMemsetAsync(xz_end, 0, a->n_xz * sizeof(uint64_t), s));
+        launch_full_resolution_structure(g, xz_end, nullptr, s);
+        a->P = (uint64_t)g.y_num[L] * g.x_num[L] * g.z_num[L];
+        throw_if_overflow(c, s);
+        uint16_t *yv = a->y_vec.as_pooled<uint16_t>(a->P, s);
+        launch_full_resolution_structure(g, xz_end, yv, s);
+    } else {
+        a->P = launch_linear_counts(g, pm, xz_end, a->n_xz, min_type, c->scan_tmp, s);
+        throw_if_overflow(c, s);
+        uint16_t *yv = a->y_vec.as_pooled<uint16_t>(a->P ? a->P : 1, s);
+        launch_linear_fill(g, pm, xz_end, yv, min_type, s);
+    }
+    APRB_CUDA(cudaMemcpyAsync(&a->offset, c->offset.p, sizeof(float), cudaMemcpyDeviceToHost, s));
+    APRB_CUDA(cudaStreamSynchronize(s));
+}
+
 template <typename IT>
 void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, int yn, int xn, int zn,
                  cudaStream_t s, aprb_apr *a) {
@@ -292,26 +360,12 @@ void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, i
     a->org[1] = xn;
     a->org[2] = zn;
     const int L = g.l_max;
-    const int yd = (yn + 1) / 2, xd = (xn + 1) / 2, zd = (zn + 1) / 2;
-    const uint64_t n = (uint64_t)yn * xn * zn, nd = (uint64_t)yd * xd * zd;
-    const bool is_u16 = sizeof(IT) == 2;
-
-    unsigned *mm = c->mm.as<unsigned>(2);
-    float *d_off = c->offset.as<float>(1);
-    unsigned *d_err = c->err.as<unsigned>(1);
-    APRB_CUDA(cudaMemsetAsync(d_err, 0, sizeof(unsigned), s));
-    launch_minmax_offset(img, n, mm, d_off, is_u16 && p.lambda > 0, s);
-
-    IT *work = c->work.as<IT>(n);
-    launch_smooth<IT>(img, work, yn, xn, zn, p.lambda, d_off, d_err, s);
-
-    IT *grad = c->grad.as<IT>(nd);
-    float *ids_raw = c->ids_raw.as<float>(nd);
-    float *ids = c->ids.as<float>(nd);
-    launch_gradient<IT>(work, yn, xn, zn, grad, ids_raw, ids, yd, xd, zd, p, s);
-
-    float *lis = c->lis.as<float>(nd);
-    launch_local_intensity_scale(ids, lis, yd, xd, zd, p, c->lisb, s);
+    const uint64_t nd = (uint64_t)((yn + 1) / 2) * ((xn + 1) / 2) * ((zn + 1) / 2);
+    APRB_CUDA(cudaMemsetAsync(c->err.as<unsigned>(1), 0, sizeof(unsigned), s));
+    PixelOut<IT> po = pixel_stages<IT>(c, p, img, yn, xn, zn, s);
+    IT *grad = po.grad;
+    float *lis = po.lis, *ids = po.ids;
+    const float *d_off = po.d_off;
     if (c->keep) {
         APRB_CUDA(cudaMemcpyAsync(c->grad_keep.as<IT>(nd), grad, nd * sizeof(IT), cudaMemcpyDeviceToDevice, s));
         APRB_CUDA(cudaMemcpyAsync(c->lis_keep.as<float>(nd), lis, nd * sizeof(float), cudaMemcpyDeviceToDevice, s));
@@ -331,47 +385,54 @@ void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, i
         pm.status[l] = st + off[l];
         pm.level[l] = lv + off[l];
     }
-    uint8_t scratch_status_dummy = 0;
-    (void)scratch_status_dummy;
     if (top >= g.l_min) {
         launch_levels<IT>(grad, lis, ids, nd, d_off, p, L, top, pm.level[top], pm.status[top], c->keep, s);
     } else {
         uint8_t *lvl = c->pyr_level.as<uint8_t>(nd), *sts = c->pyr_status.as<uint8_t>(nd);
         launch_levels<IT>(grad, lis, ids, nd, d_off, p, L, top, lvl, sts, c->keep, s);
     }
-
-    uint64_t *xz_end = a->xz_end.as_pooled<uint64_t>(a->n_xz, s);
-    const int min_type = p.neighborhood_optimization ? 1 : 2;
-    unsigned h_err = 0;
-    if (L <= 2) {
-        APRB_CUDA(cudaMemsetAsync(xz_end, 0, a->n_xz * sizeof(uint64_t), s));
-        launch_full_resolution_structure(g, xz_end, nullptr, s);
-        a->P = (uint64_t)g.y_num[L] * g.x_num[L] * g.z_num[L];
-        APRB_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-        APRB_CUDA(cudaStreamSynchronize(s));
-        if (h_err) {
-            set_error("integer under-/overflow encountered in the B-spline smoothing");
-            throw Error{APRB_ERR_INTEGER_OVERFLOW};
-        }
-        uint16_t *yv = a->y_vec.as_pooled<uint16_t>(a->P, s);
-        launch_full_resolution_structure(g, xz_end, yv, s);
-    } else {
-        launch_pulling_scheme(g, pm, s);
-        APRB_CUDA(cudaMemcpyAsync(&h_err, d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
-        a->P = launch_linear_counts(g, pm, xz_end, a->n_xz, min_type, c->scan_tmp, s);
-        if (h_err) {
-            set_error("integer under-/overflow encountered in the B-spline smoothing");
-            throw Error{APRB_ERR_INTEGER_OVERFLOW};
-        }
-        uint16_t *yv = a->y_vec.as_pooled<uint16_t>(a->P ? a->P : 1, s);
-        launch_linear_fill(g, pm, xz_end, yv, min_type, s);
-    }
-    APRB_CUDA(cudaMemcpyAsync(&a->offset, d_off, sizeof(float), cudaMemcpyDeviceToHost, s));
-    APRB_CUDA(cudaStreamSynchronize(s));
+    if (L > 2) launch_pulling_scheme(g, pm, s);
+    build_structure(c, p, pm, a, s);
     c->dims[0] = yn;
     c->dims[1] = xn;
     c->dims[2] = zn;
     c->have = true;
+}
+
+// APRConverterBatch<IT> (APRConverterBatch.hpp:114-175): the pixel stages and
+// levels per z-tile with ghost planes, each tile filling the global
+// particle-cell pyramid (fill_global_particle_cell_tree, :282-314), then one
+// pulling scheme and one linear structure for the volume.
+template <typename IT>
+void run_get_apr_by_block(aprb_converter *c, const aprb_params &p, const uint16_t *img, int yn, int xn, int zn,
+                          int zblock, int ghost, cudaStream_t s, aprb_apr *a) {
+    Geom &g = a->g;
+    a->n_xz = apr_geometry(yn, xn, zn, g);
+    a->org[0] = yn;
+    a->org[1] = xn;
+    a->org[2] = zn;
+    const int L = g.l_max, top = L - 1;
+    APRB_CUDA(cudaMemsetAsync(c->err.as<unsigned>(1), 0, sizeof(unsigned), s));
+    Pyramid pm;
+    uint64_t tot = 0, off[32] = {};
+    for (int l = g.l_min; l <= top; ++l) {
+        off[l] = tot;
+        tot += ((uint64_t)g.y_num[l] * g.x_num[l] * g.z_num[l] + 15) & ~uint64_t(15);
+    }
+    uint8_t *st = c->pyr_status.as<uint8_t>(tot ? tot : 16);
+    APRB_CUDA(cudaMemsetAsync(st, 0, tot ? tot : 16, s));
+    for (int l = g.l_min; l <= top; ++l) pm.status[l] = st + off[l];
+    const int nb = std::max(zn / zblock, 1);
+    for (int b = 0; b < nb; ++b) {
+        const ZTile t = z_tile(b, nb, zn, zblock, ghost);
+        PixelOut<IT> po = pixel_stages<IT>(c, p, img + (uint64_t)(t.z0 - t.gl) * xn * yn, yn, xn, t.pz, s);
+        uint8_t *lev = c->pyr_level.as<uint8_t>(po.nd);
+        launch_levels<IT>(po.grad, po.lis, po.ids, po.nd, po.d_off, p, L, top, lev, nullptr, 0, s);
+        launch_fill_patch(g, pm, lev, t, c->tile_pyr, s);
+    }
+    if (L > 2) launch_pulling_scheme(g, pm, s, false);
+    build_structure(c, p, pm, a, s);
+    c->have = false;  // intermediates are per tile
 }
 
 void get_apr_impl(aprb_converter *c, const aprb_params *p, const uint16_t *img_dev, int y, int x, int z,
@@ -394,9 +455,66 @@ void get_apr_impl(aprb_converter *c, const aprb_params *p, const uint16_t *img_d
     *out = a.release();
 }
 
+void get_apr_by_block_impl(aprb_converter *c, const aprb_params *p, const uint16_t *img_dev, int y, int x, int z,
+                           int zblock, int ghost, cudaStream_t s, aprb_apr **out) {
+    require_device();
+    ARG_CHECK(c && p && img_dev && out, "null argument");
+    ARG_CHECK(y >= 1 && x >= 1 && z >= 1, "dimensions must be positive");
+    ARG_CHECK(y <= 65535 && x <= 65535 && z <= 65535, "each dimension must fit the uint16 coordinates");
+    ARG_CHECK(zblock >= 1 && ghost >= 0, "z_block_size must be positive and ghost_z non-negative");
+    ARG_CHECK(p->rel_error > 0, "rel_error must be positive");
+    std::unique_ptr<aprb_apr> a(new aprb_apr());
+    if (c->image_type == APRB_IMAGE_U16)
+        run_get_apr_by_block<uint16_t>(c, *p, img_dev, y, x, z, zblock, ghost, s, a.get());
+    else
+        run_get_apr_by_block<float>(c, *p, img_dev, y, x, z, zblock, ghost, s, a.get());
+    *out = a.release();
+}
+
 }  // namespace
 
 extern "C" {
+
+aprb_status aprb_get_apr_by_block_device(aprb_converter *c, const aprb_params *p, const uint16_t *img_dev, int y_num,
+                                         int x_num, int z_num, int z_block_size, int ghost_z, void *stream,
+                                         aprb_apr **out) {
+    return guarded([&] {
+        get_apr_by_block_impl(c, p, img_dev, y_num, x_num, z_num, z_block_size, ghost_z, (cudaStream_t)stream, out);
+    });
+}
+
+aprb_status aprb_get_apr_by_block(aprb_converter *c, const aprb_params *p, const uint16_t *img, int y_num, int x_num,
+                                  int z_num, int z_block_size, int ghost_z, aprb_apr **out) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(c && img, "null argument");
+        const uint64_t n = (uint64_t)y_num * x_num * z_num;
+        cudaStream_t s = cudaStreamPerThread;
+        uint16_t *d = c->img.as<uint16_t>(n);
+        APRB_CUDA(cudaMemcpyAsync(d, img, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+        get_apr_by_block_impl(c, p, d, y_num, x_num, z_num, z_block_size, ghost_z, s, out);
+    });
+}
+
+aprb_status aprb_get_apr_batch_device(aprb_converter *c, const aprb_params *p, int n_volumes,
+                                      const aprb_volume *volumes, int z_block_size, int ghost_z, void *stream,
+                                      aprb_apr **outs) {
+    return guarded([&] {
+        ARG_CHECK(n_volumes >= 0 && (n_volumes == 0 || (volumes && outs)), "invalid volume list");
+        for (int i = 0; i < n_volumes; ++i) outs[i] = nullptr;
+        try {
+            for (int i = 0; i < n_volumes; ++i)
+                get_apr_by_block_impl(c, p, volumes[i].img_dev, volumes[i].y_num, volumes[i].x_num,
+                                      volumes[i].z_num, z_block_size, ghost_z, (cudaStream_t)stream, &outs[i]);
+        } catch (...) {
+            for (int i = 0; i < n_volumes; ++i) {
+                delete outs[i];
+                outs[i] = nullptr;
+            }
+            throw;
+        }
+    });
+}
 
 aprb_status aprb_get_apr_device(aprb_converter *c, const aprb_params *p, const uint16_t *img_dev, int y_num,
                                 int x_num, int z_num, void *stream, aprb_apr **out) {
@@ -546,6 +664,35 @@ aprb_status aprb_sample_image_device(const aprb_apr *a, const uint16_t *img_dev,
         ARG_CHECK(a && img_dev && parts_dev, "null argument");
         launch_sample(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, img_dev, parts_dev, scratch().pyr,
                       (cudaStream_t)stream);
+    });
+}
+
+aprb_status aprb_sample_image_by_block_device(const aprb_apr *a, const uint16_t *img_dev, int z_block_size,
+                                              int ghost_z, uint16_t *parts_dev, void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && img_dev && parts_dev, "null argument");
+        ARG_CHECK(z_block_size >= 1 && ghost_z >= 0, "z_block_size must be positive and ghost_z non-negative");
+        launch_sample_by_block(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, img_dev, parts_dev,
+                               z_block_size, ghost_z, scratch().pyr, (cudaStream_t)stream);
+    });
+}
+
+aprb_status aprb_sample_image_by_block(const aprb_apr *a, const uint16_t *img, int z_block_size, int ghost_z,
+                                       uint16_t *parts) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && img && parts, "null argument");
+        ARG_CHECK(z_block_size >= 1 && ghost_z >= 0, "z_block_size must be positive and ghost_z non-negative");
+        cudaStream_t s = cudaStreamPerThread;
+        const uint64_t n = (uint64_t)a->org[0] * a->org[1] * a->org[2];
+        uint16_t *di = scratch().io_in.as<uint16_t>(n);
+        uint16_t *dp = scratch().parts_u16.as<uint16_t>(a->P ? a->P : 1);
+        APRB_CUDA(cudaMemcpyAsync(di, img, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+        launch_sample_by_block(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, di, dp,
+                               z_block_size, ghost_z, scratch().pyr, s);
+        if (a->P) APRB_CUDA(cudaMemcpyAsync(parts, dp, a->P * sizeof(uint16_t), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaStreamSynchronize(s));
     });
 }
 

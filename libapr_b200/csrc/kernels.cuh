@@ -46,7 +46,18 @@ struct Pyramid {
     uint8_t *status[32] = {};
     uint8_t *level[32] = {};
 };
-void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s);
+void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s, bool fill_pyramid = true);
+
+// z-tiles of the blocked converter (APRConverterBatch.hpp:125-160): planes
+// [z0 - gl, zf + gr) of which [z0, zf) belong to the tile.
+struct ZTile {
+    int z0, zf, gl, gr, pz;
+};
+ZTile z_tile(int b, int nb, int zn, int zblock, int ghost);
+void launch_fill_patch(const Geom &g, Pyramid &pm, const uint8_t *lev_top, const ZTile &t, DevBuf &tmp,
+                       cudaStream_t s);
+void launch_sample_by_block(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const uint16_t *img,
+                            uint16_t *parts, int zblock, int ghost, DevBuf &pyr, cudaStream_t s);
 // Linear access structure: writes row counts into xz_end (n_xz entries) and
 // scans them; returns the particle count (synchronises the stream once).
 uint64_t launch_linear_counts(const Geom &g, Pyramid &pm, uint64_t *xz_end, uint64_t n_xz, int min_type,

@@ -43,8 +43,28 @@ __global__ void pyramid_fill_kernel(const uint8_t *__restrict__ lev_in, LevelDim
     m = max(m, lev_in[idx3(2 * y, x1, z1, di.yn, di.xn)]);
     m = max(m, lev_in[idx3(y1, x1, z1, di.yn, di.xn)]);
     lev_out[g] = m;
+    if (!status) return;  // level pyramid of a z-tile only
     const bool seed = is_min ? (m <= level) : (m == level);
     status[g] = seed ? kSeed : kEmpty;
+}
+
+// PullingScheme::fill_patch (PullingScheme.hpp:175-247) for a z-tile: the
+// tile's level image at one pct level (tile-local planes zlo..zhi-1) marks
+// SEED cells of the global level at plane z + offz.  mode 0: level >= k (top),
+// 1: level <= k (l_min), 2: level == k.  Planes past the global level are
+// skipped (the reference writes beyond the level's array there).
+__global__ void fill_patch_kernel(const uint8_t *__restrict__ lev, LevelDims dp, uint8_t *__restrict__ status,
+                                  LevelDims d, int zlo, int zhi, int offz, int level, int mode) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= (uint64_t)(zhi - zlo) * dp.xn * dp.yn) return;
+    int y, x, z;
+    cell_of(g, dp.yn, dp.xn, y, x, z);
+    z += zlo;
+    const int zg = z + offz;
+    if (zg < 0 || zg >= d.zn) return;
+    const int v = lev[idx3(y, x, z, dp.yn, dp.xn)];
+    const bool sd = mode == 0 ? v >= level : (mode == 1 ? v <= level : v == level);
+    if (sd) status[idx3(y, x, zg, d.yn, d.xn)] = kSeed;
 }
 
 // set_ascendant_neighbours (:250-289)
@@ -332,6 +352,24 @@ __global__ void pyr_mean_u16_kernel(const uint16_t *__restrict__ in, LevelDims d
     out[g] = (uint16_t)(s >> 3);
 }
 
+// sample_parts_from_img_downsampled_patch (ParticleData.hpp:330-372): the
+// particles of global rows (zlo + offz .. zhi - 1 + offz, x) of one level take
+// the tile's pyramid value at tile-local plane z.
+__global__ void gather_patch_kernel(const uint16_t *__restrict__ im, LevelDims dp, int zlo, int zhi, int offz,
+                                    int gzn, const uint64_t *__restrict__ xz_end, uint64_t row_base,
+                                    const uint16_t *__restrict__ y_vec, uint16_t *__restrict__ parts) {
+    const uint64_t r = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (r >= (uint64_t)(zhi - zlo) * dp.xn) return;
+    const int x = (int)(r % (uint64_t)dp.xn), z = zlo + (int)(r / (uint64_t)dp.xn);
+    const int zg = z + offz;
+    if (zg < 0 || zg >= gzn) return;
+    const uint64_t row = (uint64_t)zg * dp.xn + x;
+    const uint64_t b = xz_end[row_base + row - 1], e = xz_end[row_base + row];
+    const uint16_t *R = im + ((uint64_t)z * dp.xn + x) * (uint64_t)dp.yn;
+    for (uint64_t i = b + lane; i < e; i += 32) parts[i] = R[y_vec[i]];
+}
+
 __global__ void gather_kernel(const uint16_t *__restrict__ im, LevelDims d, const uint64_t *__restrict__ xz_end,
                               uint64_t row_base, const uint16_t *__restrict__ y_vec, uint16_t *__restrict__ parts) {
     const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -410,11 +448,11 @@ void inclusive_scan_u64(uint64_t *data, uint64_t n, DevBuf &tmp, cudaStream_t s)
     APRB_CHECK_LAUNCH();
 }
 
-void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s) {
+void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s, bool fill_pyramid) {
     const int top = g.l_max - 1, lmin = g.l_min;
     if (top < lmin) return;
     APRB_PROF("pulling_scheme", s);
-    for (int l = top - 1; l >= lmin; --l) {
+    for (int l = top - 1; l >= lmin && fill_pyramid; --l) {
         pyramid_fill_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(pm.level[l + 1], dims(g, l + 1), pm.level[l],
                                                                         pm.status[l], dims(g, l), l, l == lmin);
         count_launch();
@@ -541,6 +579,94 @@ void launch_sample_scratch(const Geom &g, const uint64_t *xz_end, const uint16_t
     for (int l = lmin; l <= L; ++l)
         gather_kernel<<<row_blocks(nrow(g, l)), 256, 0, s>>>(lev[l], dims(g, l), xz_end, g.level_xz[l], y_vec, parts);
     APRB_CHECK_LAUNCH();
+}
+
+// z-tiling of APRConverterBatch (APRConverterBatch.hpp:125-160)
+ZTile z_tile(int b, int nb, int zn, int zblock, int ghost) {
+    ZTile t;
+    t.z0 = b * zblock;
+    t.zf = (b == nb - 1) ? zn : (b + 1) * zblock;
+    t.gl = std::min(t.z0, ghost);
+    t.gr = std::min(zn - t.zf, ghost);
+    t.pz = t.zf + t.gr - (t.z0 - t.gl);
+    return t;
+}
+
+// fill_global_particle_cell_tree (APRConverterBatch.hpp:282-314): the tile's
+// levels at pct l_max (lev_top, ds tile dims) and their max pyramid fill the
+// global particle-cell pyramid.  tmp holds the tile pyramid.
+void launch_fill_patch(const Geom &g, Pyramid &pm, const uint8_t *lev_top, const ZTile &t, DevBuf &tmp,
+                       cudaStream_t s) {
+    const int top = g.l_max - 1, lmin = g.l_min;
+    if (top < lmin) return;
+    APRB_PROF("fill_patch", s);
+    LevelDims pd[32];
+    pd[top] = LevelDims{g.y_num[top], g.x_num[top], (t.pz + 1) / 2};
+    uint64_t off[32] = {}, total = 0;
+    for (int l = top - 1; l >= lmin; --l) {
+        pd[l] = LevelDims{g.y_num[l], g.x_num[l], (pd[l + 1].zn + 1) / 2};
+        off[l] = total;
+        total += ((uint64_t)pd[l].yn * pd[l].xn * pd[l].zn + 15) & ~uint64_t(15);
+    }
+    uint8_t *base = tmp.as<uint8_t>(total ? total : 16);
+    const uint8_t *lev = lev_top;
+    for (int l = top; l >= lmin; --l) {
+        uint8_t *cur = nullptr;
+        if (l != top) {
+            cur = base + off[l];
+            pyramid_fill_kernel<<<blocks_for((uint64_t)pd[l].yn * pd[l].xn * pd[l].zn, 256), 256, 0, s>>>(
+                lev, pd[l + 1], cur, nullptr, pd[l], l, 0);
+            count_launch();
+            lev = cur;
+        }
+        const int lf = 1 << (top + 1 - l);
+        const int zlo = t.gl / lf, zhi = pd[l].zn - t.gr / lf, offz = t.z0 / lf - t.gl / lf;
+        const int mode = l == top ? 0 : (l == lmin ? 1 : 2);
+        if (zhi > zlo) {
+            fill_patch_kernel<<<blocks_for((uint64_t)(zhi - zlo) * pd[l].xn * pd[l].yn, 256), 256, 0, s>>>(
+                lev, pd[l], pm.status[l], dims(g, l), zlo, zhi, offz, l, mode);
+            count_launch();
+        }
+    }
+    APRB_CHECK_LAUNCH();
+}
+
+void launch_sample_by_block(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const uint16_t *img,
+                            uint16_t *parts, int zblock, int ghost, DevBuf &pyr, cudaStream_t s) {
+    APRB_PROF("sample_image_by_block", s);
+    const int L = g.l_max, lmin = g.l_min;
+    const int zn = g.z_num[L];
+    const int nb = std::max(zn / zblock, 1);
+    for (int b = 0; b < nb; ++b) {
+        const ZTile t = z_tile(b, nb, zn, zblock, ghost);
+        LevelDims pd[32];
+        pd[L] = LevelDims{g.y_num[L], g.x_num[L], t.pz};
+        uint64_t off[32] = {}, total = 0;
+        for (int l = L - 1; l >= lmin; --l) {
+            pd[l] = LevelDims{g.y_num[l], g.x_num[l], (pd[l + 1].zn + 1) / 2};
+            off[l] = total;
+            total += ((uint64_t)pd[l].yn * pd[l].xn * pd[l].zn + 7) & ~uint64_t(7);
+        }
+        uint16_t *base = pyr.as<uint16_t>(total ? total : 8);
+        const uint16_t *lev[32] = {};
+        lev[L] = img + (uint64_t)(t.z0 - t.gl) * g.x_num[L] * g.y_num[L];
+        for (int l = L - 1; l >= lmin; --l) {
+            uint16_t *o = base + off[l];
+            pyr_mean_u16_kernel<<<blocks_for((uint64_t)pd[l].yn * pd[l].xn * pd[l].zn, 256), 256, 0, s>>>(
+                lev[l + 1], pd[l + 1], o, pd[l]);
+            count_launch();
+            lev[l] = o;
+        }
+        for (int l = lmin; l <= L; ++l) {
+            const int lf = 1 << (L - l);
+            const int zlo = t.gl / lf, zhi = pd[l].zn - t.gr / lf, offz = t.z0 / lf - t.gl / lf;
+            if (zhi <= zlo) continue;
+            gather_patch_kernel<<<row_blocks((uint64_t)(zhi - zlo) * pd[l].xn), 256, 0, s>>>(
+                lev[l], pd[l], zlo, zhi, offz, g.z_num[l], xz_end, g.level_xz[l], y_vec, parts);
+            count_launch();
+        }
+        APRB_CHECK_LAUNCH();
+    }
 }
 
 uint64_t launch_tree_build(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,

@@ -855,10 +855,13 @@ static float *dup_f(const float *s, size_t n) {
     return d;
 }
 
-/* applyParameters (:250-297), solveForAPR (:301-336), generateDatastructures (:339-363) */
-static int finish_apr(orc_apr *r, float *grad, float *lis, const float *ids, const orc_params *p, int keep) {
-    size_t nd = (size_t)r->yd * r->xd * r->zd;
-    float th = p->Ip_th + r->offset;
+/* applyParameters (src/algorithm/APRConverter.hpp:250-297) and computeLevels
+ * (src/algorithm/LocalParticleCellSet.hpp:129-171): grad and lis (ds) are
+ * thresholded in place and lis receives the level image.  ids may be NULL
+ * (custom gradient entry point: no intensity threshold). */
+static void apply_and_levels(orc_apr *keep_r, float *grad, float *lis, const float *ids, size_t nd, float offset,
+                             const orc_params *p, int apr_l_max) {
+    float th = p->Ip_th + offset;
     if (ids)
         for (size_t i = 0; i < nd; ++i)
             if (ids[i] <= th) grad[i] = 0;
@@ -868,18 +871,24 @@ static int finish_apr(orc_apr *r, float *grad, float *lis, const float *ids, con
     }
     for (size_t i = 0; i < nd; ++i)
         if (grad[i] < p->grad_th) grad[i] = 0;
-    if (keep) { r->inter[4] = dup_f(grad, nd); r->inter[5] = dup_f(lis, nd); }
-    /* computeLevels (src/algorithm/LocalParticleCellSet.hpp:129-171) */
+    if (keep_r) { keep_r->inter[4] = dup_f(grad, nd); keep_r->inter[5] = dup_f(lis, nd); }
     float mxz = p->dz < p->dx ? p->dz : p->dx;          /* std::min(dx, dz) */
     float min_dim = mxz < p->dy ? mxz : p->dy;            /* std::min(dy, .) */
-    float level_factor = (float)(pow(2.0, (double)r->acc.l_max) * (double)min_dim);
+    float level_factor = (float)(pow(2.0, (double)apr_l_max) * (double)min_dim);
     float mult = level_factor / p->rel_error;
     for (size_t i = 0; i < nd; ++i) {
         float q = grad[i] / lis[i];
         uint32_t u = cvt_u32(q * mult);
         lis[i] = (float)(u == 0 ? 0u : (uint32_t)(31 - __builtin_clz(u)));
     }
-    if (keep) r->inter[6] = dup_f(lis, nd);
+    if (keep_r) keep_r->inter[6] = dup_f(lis, nd);
+}
+
+/* solveForAPR (APRConverter.hpp:301-336) after the levels, and
+ * generateDatastructures (:339-363) */
+static int finish_apr(orc_apr *r, float *grad, float *lis, const float *ids, const orc_params *p, int keep) {
+    size_t nd = (size_t)r->yd * r->xd * r->zd;
+    apply_and_levels(keep ? r : NULL, grad, lis, ids, nd, r->offset, p, r->acc.l_max);
     pct_t t;
     pct_init(&t, &r->acc);
     if (t.l_max >= t.l_min) {
@@ -891,29 +900,28 @@ static int finish_apr(orc_apr *r, float *grad, float *lis, const float *ids, con
     return e;
 }
 
-int orc_get_apr(const uint16_t *img, int yn, int xn, int zn, const orc_params *p, int image_type, orc_apr **out) {
-    *out = NULL;
-    if (yn < 1 || xn < 1 || zn < 1) return ORC_ERR_DIMS;
-    int nd3 = (yn > 1) + (xn > 1) + (zn > 1);
-    if (nd3 == 0) return ORC_ERR_DIMS;
-    orc_apr *r = (orc_apr *)calloc(1, sizeof(orc_apr));
-    geninfo_init(&r->acc, yn, xn, zn);
-    r->yn = yn; r->xn = xn; r->zn = zn;
-    r->yd = (int)ceil(yn / 2.0); r->xd = (int)ceil(xn / 2.0); r->zd = (int)ceil(zn / 2.0);
-    size_t n = (size_t)yn * xn * zn, nd = (size_t)r->yd * r->xd * r->zd;
-    int is_u16 = image_type == 1;
+/* The pixel stages of one image (the whole volume, or one z-tile of the
+ * blocked converter, APRConverterBatch.hpp:190-271): offset, smoothing,
+ * gradient + ds image, inverse B-spline, local intensity scale.  Returns
+ * ORC_ERR_OVERFLOW on a uint16 smoothing overflow.  On success *grad, *ids and
+ * *lis hold ds images the caller frees; keep_r (optional) receives the
+ * smoothed image and the stage intermediates. */
+static int pixel_stages(const uint16_t *img, int yn, int xn, int zn, const orc_params *p, int is_u16,
+                        float *offset, float **grad_out, float **ids_out, float **lis_out, orc_apr *keep_r) {
+    int yd = (int)ceil(yn / 2.0), xd = (int)ceil(xn / 2.0), zd = (int)ceil(zn / 2.0);
+    size_t n = (size_t)yn * xn * zn, nd = (size_t)yd * xd * zd;
     float *im = (float *)malloc(sizeof(float) * n);
     /* offset (:216-223) and compute_bspline_offset (src/algorithm/AutoParameters.hpp:186-197) */
-    r->offset = 0;
+    *offset = 0;
     if (is_u16) {
         if (p->lambda > 0) {
             uint16_t mn = 65535, mx = 0;
             for (size_t i = 0; i < n; ++i) { if (img[i] > mx) mx = img[i]; if (img[i] < mn) mn = img[i]; }
             float off = (float)((65535 - (mx - mn)) / 2 - mn);
             off = off < 100.f ? off : 100.f;
-            r->offset = off > -100.f ? off : -100.f;
+            *offset = off > -100.f ? off : -100.f;
         }
-        for (size_t i = 0; i < n; ++i) im[i] = cvt_u16((float)img[i] + r->offset);
+        for (size_t i = 0; i < n; ++i) im[i] = cvt_u16((float)img[i] + *offset);
     } else {
         for (size_t i = 0; i < n; ++i) im[i] = (float)img[i];
     }
@@ -923,31 +931,131 @@ int orc_get_apr(const uint16_t *img, int yn, int xn, int zn, const orc_params *p
         if (yn > 2) err += orc_bspline_axis(im, yn, xn, zn, 0, p->lambda, is_u16);
         if (xn > 2) err += orc_bspline_axis(im, yn, xn, zn, 1, p->lambda, is_u16);
         if (zn > 2) err += orc_bspline_axis(im, yn, xn, zn, 2, p->lambda, is_u16);
-        if (err) { free(im); orc_free(r); return ORC_ERR_OVERFLOW; }
+        if (err) { free(im); return ORC_ERR_OVERFLOW; }
     }
-    r->inter[0] = dup_f(im, n);
+    if (keep_r) keep_r->inter[0] = dup_f(im, n);
     float *grad = (float *)malloc(sizeof(float) * nd);
-    gradient_ds(im, yn, xn, zn, grad, r->yd, r->xd, r->zd, p->dx, p->dy, p->dz, is_u16);
+    gradient_ds(im, yn, xn, zn, grad, yd, xd, zd, p->dx, p->dy, p->dz, is_u16);
     float *ids = (float *)malloc(sizeof(float) * nd);
     downsample2(im, yn, xn, zn, ids, DS_MEAN_D8);
     free(im);
     if (p->lambda > 0) {
-        if (yn > 2) inv_bspline_y(ids, r->yd, r->xd, r->zd);
+        if (yn > 2) inv_bspline_y(ids, yd, xd, zd);
         if (xn > 2)
-            for (int z = 0; z < r->zd; ++z)
-                for (int y = 0; y < r->yd; ++y) inv_bspline_strided(ids + IDX(y, 0, z, r->yd, r->xd), (size_t)r->yd, r->xd);
+            for (int z = 0; z < zd; ++z)
+                for (int y = 0; y < yd; ++y) inv_bspline_strided(ids + IDX(y, 0, z, yd, xd), (size_t)yd, xd);
         if (zn > 2)
-            for (int x = 0; x < r->xd; ++x)
-                for (int y = 0; y < r->yd; ++y)
-                    inv_bspline_strided(ids + IDX(y, x, 0, r->yd, r->xd), (size_t)r->yd * r->xd, r->zd);
+            for (int x = 0; x < xd; ++x)
+                for (int y = 0; y < yd; ++y)
+                    inv_bspline_strided(ids + IDX(y, x, 0, yd, xd), (size_t)yd * xd, zd);
     }
-    r->inter[1] = dup_f(grad, nd);
-    r->inter[2] = dup_f(ids, nd);
+    if (keep_r) { keep_r->inter[1] = dup_f(grad, nd); keep_r->inter[2] = dup_f(ids, nd); }
     float *lis = (float *)malloc(sizeof(float) * nd);
-    local_intensity_scale(ids, r->yd, r->xd, r->zd, p, lis);
-    r->inter[3] = dup_f(lis, nd);
-    int e = finish_apr(r, grad, lis, ids, p, 1);
+    local_intensity_scale(ids, yd, xd, zd, p, lis);
+    if (keep_r) keep_r->inter[3] = dup_f(lis, nd);
+    *grad_out = grad; *ids_out = ids; *lis_out = lis;
+    return ORC_OK;
+}
+
+int orc_get_apr(const uint16_t *img, int yn, int xn, int zn, const orc_params *p, int image_type, orc_apr **out) {
+    *out = NULL;
+    if (yn < 1 || xn < 1 || zn < 1) return ORC_ERR_DIMS;
+    int nd3 = (yn > 1) + (xn > 1) + (zn > 1);
+    if (nd3 == 0) return ORC_ERR_DIMS;
+    orc_apr *r = (orc_apr *)calloc(1, sizeof(orc_apr));
+    geninfo_init(&r->acc, yn, xn, zn);
+    r->yn = yn; r->xn = xn; r->zn = zn;
+    r->yd = (int)ceil(yn / 2.0); r->xd = (int)ceil(xn / 2.0); r->zd = (int)ceil(zn / 2.0);
+    float *grad, *ids, *lis;
+    int e = pixel_stages(img, yn, xn, zn, p, image_type == 1, &r->offset, &grad, &ids, &lis, r);
+    if (e != ORC_OK) { orc_free(r); return e; }
+    e = finish_apr(r, grad, lis, ids, p, 1);
     free(grad); free(lis); free(ids);
+    if (e != ORC_OK) { orc_free(r); return e; }
+    *out = r;
+    return ORC_OK;
+}
+
+/* PullingScheme::fill_patch (src/algorithm/PullingScheme.hpp:175-247) for a
+ * z-tile (no x/y ghost): level image lv of the tile at pct level k, tile dims
+ * (py, px, pz) at that level; the ghost is cropped by integer division. */
+static int pct_fill_patch(pct_t *t, int k, const float *lv, int py, int px, int pz, int ghost_l, int ghost_r,
+                          int z0) {
+    int lf = (int)powr(2, t->l_max + 1 - k);
+    int zgl = ghost_l / lf, zgr = ghost_r / lf;
+    int offz = z0 / lf - zgl;  /* (z_offset + z_ghost_l) / lf - z_ghost_l / lf */
+    float kf = (float)k;
+    for (int z = zgl; z < pz - zgr; ++z) {
+        /* planes past the level: the reference writes beyond its array there */
+        if (z + offz < 0 || z + offz >= t->z_num[k]) continue;
+        for (int x = 0; x < px; ++x)
+            for (int y = 0; y < py; ++y) {
+                float v = lv[IDX(y, x, z, py, px)];
+                int sd;
+                if (k == t->l_max) sd = v >= kf;
+                else if (k == t->l_min) sd = v <= kf;
+                else sd = v == kf;
+                if (sd) t->m[k][IDX(y, x, z + offz, t->y_num[k], t->x_num[k])] = PS_SEED;
+            }
+    }
+    return ORC_OK;
+}
+
+/* z-tiling of APRConverterBatch::get_apr_batch_method_from_file
+ * (src/algorithm/APRConverterBatch.hpp:125-160) */
+static void z_block(int b, int nb, int zn, int zblock, int ghost, int *z0, int *zf, int *gl, int *gr) {
+    *z0 = b * zblock;
+    *zf = (b == nb - 1) ? zn : (b + 1) * zblock;
+    *gl = *z0 < ghost ? *z0 : ghost;
+    *gr = (zn - *zf) < ghost ? (zn - *zf) : ghost;
+}
+
+/* APRConverterBatch<IT>: get_apr_method_patch per z-tile
+ * (APRConverterBatch.hpp:190-271), fill_global_particle_cell_tree (:282-314),
+ * then one pulling scheme and linear structure for the whole volume. */
+int orc_get_apr_by_block(const uint16_t *img, int yn, int xn, int zn, const orc_params *p, int image_type,
+                         int zblock, int ghost, orc_apr **out) {
+    *out = NULL;
+    if (yn < 1 || xn < 1 || zn < 1 || zblock < 1 || ghost < 0) return ORC_ERR_ARG;
+    orc_apr *r = (orc_apr *)calloc(1, sizeof(orc_apr));
+    geninfo_init(&r->acc, yn, xn, zn);
+    r->yn = yn; r->xn = xn; r->zn = zn;
+    r->yd = (int)ceil(yn / 2.0); r->xd = (int)ceil(xn / 2.0); r->zd = (int)ceil(zn / 2.0);
+    pct_t t;
+    pct_init(&t, &r->acc);
+    int nb = zn / zblock > 1 ? zn / zblock : 1;
+    int e = ORC_OK;
+    for (int b = 0; b < nb && e == ORC_OK; ++b) {
+        int z0, zf, gl, gr;
+        z_block(b, nb, zn, zblock, ghost, &z0, &zf, &gl, &gr);
+        int pz = zf + gr - (z0 - gl);
+        float *grad, *ids, *lis;
+        e = pixel_stages(img + (size_t)(z0 - gl) * xn * yn, yn, xn, pz, p, image_type == 1, &r->offset, &grad, &ids,
+                         &lis, NULL);
+        if (e != ORC_OK) break;
+        int cy = (int)ceil(yn / 2.0), cx = (int)ceil(xn / 2.0), cz = (int)ceil(pz / 2.0);
+        apply_and_levels(NULL, grad, lis, ids, (size_t)cy * cx * cz, r->offset, p, r->acc.l_max);
+        free(grad); free(ids);
+        float *cur = lis;
+        if (t.l_max >= t.l_min) {
+            e = pct_fill_patch(&t, t.l_max, cur, cy, cx, cz, gl, gr, z0);
+            for (int l = t.l_max - 1; l >= t.l_min && e == ORC_OK; --l) {
+                int ny = (int)ceil(cy / 2.0), nx = (int)ceil(cx / 2.0), nz = (int)ceil(cz / 2.0);
+                float *nxt = (float *)malloc(sizeof(float) * (size_t)ny * nx * nz);
+                downsample2(cur, cy, cx, cz, nxt, DS_MAX);
+                free(cur);
+                cur = nxt;
+                cy = ny; cx = nx; cz = nz;
+                e = pct_fill_patch(&t, l, cur, cy, cx, cz, gl, gr, z0);
+            }
+        }
+        free(cur);
+    }
+    if (e == ORC_OK) {
+        if (t.l_max >= t.l_min) pulling_scheme(&t);
+        e = linear_structure(&r->acc, &t, p->neighborhood_optimization);
+    }
+    pct_free(&t);
     if (e != ORC_OK) { orc_free(r); return e; }
     *out = r;
     return ORC_OK;
@@ -992,6 +1100,49 @@ int orc_sample_image(const orc_access *a, const uint16_t *img, uint16_t *parts) 
                 for (uint64_t i = row_begin(a, l, z, x); i < row_end(a, l, z, x); ++i)
                     parts[i] = (uint16_t)lev[l][IDX(a->y_vec[i], x, z, a->y_num[l], a->x_num[l])];
     for (int l = 0; l < ORC_MAX_LEVELS; ++l) free(lev[l]);
+    return ORC_OK;
+}
+
+/* sample_parts_from_img_downsampled_patch
+ * (src/data_structures/APR/particles/ParticleData.hpp:330-372) over the
+ * z-tiles of sample_parts_from_img_blocked_gen (:288-322): every tile builds
+ * its own uint16 mean pyramid and writes the particles of its rows; a later
+ * tile overwrites an earlier one where their cropped rows overlap. */
+int orc_sample_image_by_block(const orc_access *a, const uint16_t *img, int zblock, int ghost, uint16_t *parts) {
+    int L = a->l_max, yn = a->org[0], xn = a->org[1], zn = a->org[2];
+    if (zblock < 1 || ghost < 0) return ORC_ERR_ARG;
+    int nb = zn / zblock > 1 ? zn / zblock : 1;
+    for (int b = 0; b < nb; ++b) {
+        int z0, zf, gl, gr;
+        z_block(b, nb, zn, zblock, ghost, &z0, &zf, &gl, &gr);
+        int pz = zf + gr - (z0 - gl);
+        float *lev[ORC_MAX_LEVELS] = {0};
+        int ly[ORC_MAX_LEVELS], lx[ORC_MAX_LEVELS], lz[ORC_MAX_LEVELS];
+        size_t n = (size_t)yn * xn * pz;
+        lev[L] = (float *)malloc(sizeof(float) * n);
+        const uint16_t *src = img + (size_t)(z0 - gl) * xn * yn;
+        for (size_t i = 0; i < n; ++i) lev[L][i] = (float)src[i];
+        ly[L] = yn; lx[L] = xn; lz[L] = pz;
+        for (int l = L; l > a->l_min; --l) {
+            ly[l - 1] = (int)ceil(ly[l] / 2.0); lx[l - 1] = (int)ceil(lx[l] / 2.0); lz[l - 1] = (int)ceil(lz[l] / 2.0);
+            lev[l - 1] = (float *)malloc(sizeof(float) * (size_t)ly[l - 1] * lx[l - 1] * lz[l - 1]);
+            downsample2(lev[l], ly[l], lx[l], lz[l], lev[l - 1], DS_MEAN_U16);
+        }
+        int err = 0;
+        for (int l = a->l_min; l <= L && !err; ++l) {
+            int lf = (int)powr(2, L - l);
+            int zgl = gl / lf, zgr = gr / lf, offz = z0 / lf - zgl;
+            for (int z = zgl; z < lz[l] - zgr && !err; ++z) {
+                /* rows past the level: the reference reads beyond its row index there */
+                if (z + offz < 0 || z + offz >= a->z_num[l]) continue;
+                for (int x = 0; x < lx[l]; ++x)
+                    for (uint64_t i = row_begin(a, l, z + offz, x); i < row_end(a, l, z + offz, x); ++i)
+                        parts[i] = (uint16_t)lev[l][IDX(a->y_vec[i], x, z, ly[l], lx[l])];
+            }
+        }
+        for (int l = 0; l < ORC_MAX_LEVELS; ++l) free(lev[l]);
+        if (err) return ORC_ERR_ARG;
+    }
     return ORC_OK;
 }
 

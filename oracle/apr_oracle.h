@@ -67,6 +67,13 @@ int orc_get_apr(const uint16_t *img, int y, int x, int z, const orc_params *p,
 int orc_get_apr_custom(const float *grad_ds, const float *lis_ds, int y, int x, int z,
                        const orc_params *p, orc_apr **out);
 
+/* Blocked construction, APRConverterBatch<IT> (src/algorithm/APRConverterBatch.hpp:114-175,
+ * 190-271, 282-314) with the z-tiles cut from the in-memory volume instead of
+ * read from a TIFF file: z tiles of zblock planes (the last one takes the
+ * remainder) with up to ghost planes of overlap on each side. */
+int orc_get_apr_by_block(const uint16_t *img, int y, int x, int z, const orc_params *p, int image_type,
+                         int zblock, int ghost, orc_apr **out);
+
 void orc_free(orc_apr *a);
 const orc_access *orc_get_access(const orc_apr *a);
 /* Intermediates kept by orc_get_apr (ds = ceil(dim/2) per axis):
@@ -81,6 +88,10 @@ float orc_bspline_offset(const orc_apr *a);
 /* Particle sampling: ParticleData::sample_image with the default mean
  * pyramid (src/data_structures/APR/particles/ParticleData.hpp:123-127). */
 int orc_sample_image(const orc_access *acc, const uint16_t *img, uint16_t *parts);
+
+/* Blocked sampling, sample_parts_from_img_blocked
+ * (src/data_structures/APR/particles/ParticleData.hpp:288-372), tiles from memory. */
+int orc_sample_image_by_block(const orc_access *acc, const uint16_t *img, int zblock, int ghost, uint16_t *parts);
 
 /* APR tree of an access structure (APR::initialize_tree_dense,
  * src/data_structures/APR/APR.hpp:633-689); the caller frees with

@@ -10,6 +10,7 @@ this module.  Images are numpy arrays of shape (z, x, y) in C order, i.e. the
 reference's PixelData memory order (y fastest).
 """
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -75,6 +76,10 @@ def lib():
                                           C.c_int, C.c_int]
         L.orc_bspline_axis.argtypes = [C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int]
         L.orc_bspline_axis.restype = C.c_uint64
+        L.orc_get_apr_by_block.argtypes = [C.POINTER(C.c_uint16), C.c_int, C.c_int, C.c_int, C.POINTER(OrcParams),
+                                           C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+        L.orc_sample_image_by_block.argtypes = [C.POINTER(OrcAccess), C.POINTER(C.c_uint16), C.c_int, C.c_int,
+                                                C.POINTER(C.c_uint16)]
         _lib = L
     return _lib
 
@@ -108,6 +113,9 @@ def ref(fast=False):
                                           C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int]
         R.ref_richardson_lucy.argtypes = [vp, C.POINTER(C.c_uint16), vp, C.POINTER(C.c_float), C.c_int, C.c_int,
                                           C.c_int, C.c_int, C.c_int, C.c_int]
+        R.ref_get_apr_by_block.argtypes = [C.POINTER(C.c_uint16), C.c_int, C.c_int, C.c_int, C.POINTER(OrcParams),
+                                           C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
+        R.ref_sample_image_by_block.argtypes = [vp, C.POINTER(C.c_uint16), C.c_int, C.c_int, C.POINTER(C.c_uint16)]
         R.ref_smooth.argtypes = [C.POINTER(C.c_uint16), C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, C.c_float,
                                  C.POINTER(C.c_float)]
         _ref[fast] = R
@@ -217,6 +225,29 @@ def orc_get_apr_custom(grad, lis, shape_zxy, params):
     return acc
 
 
+def orc_get_apr_by_block(img, params, image_type, z_block, ghost):
+    """Blocked construction (APRConverterBatch) from the C restatement."""
+    L = lib()
+    img = np.ascontiguousarray(img, dtype=np.uint16)
+    z, x, y = img.shape
+    h = C.c_void_p()
+    e = L.orc_get_apr_by_block(_ptr(img, C.c_uint16), y, x, z, C.byref(params), image_type, z_block, ghost,
+                               C.byref(h))
+    if e != 0:
+        return e, None
+    acc = Access.from_c(L.orc_get_access(h).contents)
+    L.orc_free(h)
+    return 0, acc
+
+
+def orc_sample_by_block(acc, img, z_block, ghost):
+    out = np.zeros(max(acc.P, 1), np.uint16)
+    img = np.ascontiguousarray(img, dtype=np.uint16)
+    assert lib().orc_sample_image_by_block(C.byref(acc.c()), _ptr(img, C.c_uint16), z_block, ghost,
+                                           _ptr(out, C.c_uint16)) == 0
+    return out[:acc.P]
+
+
 def orc_sample(acc, img):
     out = np.zeros(acc.P, np.uint16)
     img = np.ascontiguousarray(img, dtype=np.uint16)
@@ -324,6 +355,12 @@ class RefAPR:
         self.R.ref_sample_image(self.h, _ptr(img, C.c_uint16), _ptr(out, C.c_uint16))
         return out
 
+    def sample_by_block(self, img, z_block, ghost):
+        out = np.zeros(max(self.access().P, 1), np.uint16)
+        img = np.ascontiguousarray(img, dtype=np.uint16)
+        self.R.ref_sample_image_by_block(self.h, _ptr(img, C.c_uint16), z_block, ghost, _ptr(out, C.c_uint16))
+        return out
+
     def tree(self):
         nl, nx, P = C.c_uint64(), C.c_uint64(), C.c_uint64()
         self.R.ref_tree_info(self.h, C.byref(nl), C.byref(nx), C.byref(P))
@@ -395,6 +432,18 @@ def ref_get_apr(img, params, image_type=1, staged=True, fast=False):
     return 0, RefAPR(h.value, img.shape, fast)
 
 
+def ref_get_apr_by_block(img, params, image_type, z_block, ghost, fast=False):
+    R = ref(fast)
+    img = np.ascontiguousarray(img, dtype=np.uint16)
+    z, x, y = img.shape
+    h = C.c_void_p()
+    e = R.ref_get_apr_by_block(_ptr(img, C.c_uint16), y, x, z, C.byref(params), image_type, z_block, ghost,
+                               C.byref(h))
+    if e != 0:
+        return e, None
+    return 0, RefAPR(h.value, img.shape, fast)
+
+
 def ref_get_apr_custom(grad, lis, shape_zxy, params):
     R = ref()
     z, x, y = shape_zxy
@@ -421,3 +470,26 @@ def ref_smooth(img, lambda_, image_type, offset):
     out = np.zeros(img.shape, np.float32)
     e = R.ref_smooth(_ptr(img, C.c_uint16), y, x, z, lambda_, image_type, offset, _ptr(out, C.c_float))
     return e, out
+
+
+def block_tiling_in_bounds(shape_zxy, z_block, ghost):
+    """True when every z-tile of the blocked converter writes inside every
+    level of the particle-cell pyramid and of the APR.  At coarse levels the
+    reference maps a tile's planes by integer division of the ghost width, so
+    the last tile can reach one plane past the level's end; the reference then
+    writes (and its blocked sampling reads) outside the level's arrays."""
+    z, x, y = shape_zxy
+    L = max(int(math.ceil(math.log2(max(z, x, y)))), 0)
+    nb = max(z // z_block, 1)
+    for b in range(nb):
+        z0 = b * z_block
+        zf = z if b == nb - 1 else (b + 1) * z_block
+        gl, gr = min(z0, ghost), min(z - zf, ghost)
+        pz = zf + gr - (z0 - gl)
+        for lf_exp in range(0, L + 1):
+            lf = 2 ** lf_exp
+            nzp = -(-pz // lf)
+            hi = z0 // lf - gl // lf + nzp - gr // lf
+            if hi > -(-z // lf):
+                return False
+    return True

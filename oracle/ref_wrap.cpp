@@ -9,6 +9,7 @@
  * call goes through the reference's own classes.
  */
 #include "algorithm/APRConverter.hpp"
+#include "algorithm/APRConverterBatch.hpp"
 #include "numerics/APRFilter.hpp"
 #include "numerics/APRNumerics.hpp"
 #include "numerics/APRStencil.hpp"
@@ -74,6 +75,42 @@ struct StagedConverter : public APRConverter<IT> {
     }
 };
 
+/* APRConverterBatch<IT> driven from memory: the steps of
+ * get_apr_batch_method_from_file (src/algorithm/APRConverterBatch.hpp:114-175)
+ * with each z-tile cut from the in-memory volume where the reference reads it
+ * from a TIFF file (TiffUtils::getMesh); the per-tile work is the reference's
+ * own public get_apr_method_patch. */
+template <typename IT>
+struct BlockConverter : public APRConverterBatch<IT> {
+    bool run(APR &apr, const PixelData<uint16_t> &img, int zblock, int ghost) {
+        this->z_block_size = zblock;
+        this->ghost_z = ghost;
+        apr.parameters = this->par;
+        apr.aprInfo.init(img.y_num, img.x_num, img.z_num);
+        apr.linearAccess.genInfo = &apr.aprInfo;
+        apr.apr_access.genInfo = &apr.aprInfo;
+        const int y_num = img.y_num, x_num = img.x_num, z_num = img.z_num;
+        const int nb = std::max(z_num / zblock, 1);
+        std::vector<ImagePatch> patches(nb);
+        this->iPullingScheme.initialize_particle_cell_tree(apr.aprInfo);
+        for (int b = 0; b < nb; ++b) {
+            const int z0 = b * zblock, zf = (b == nb - 1) ? z_num : (b + 1) * zblock;
+            const int gl = std::min(z0, ghost), gr = std::min(z_num - zf, ghost);
+            initPatchGlobal(patches[b], z0 - gl, zf + gr, 0, x_num, 0, y_num);
+            patches[b].z_ghost_l = gl;
+            patches[b].z_ghost_r = gr;
+            patches[b].z_offset = z0 - gl;
+            PixelData<uint16_t> tile(y_num, x_num, zf + gr - (z0 - gl));
+            std::memcpy(tile.mesh.begin(), img.mesh.begin() + (size_t)(z0 - gl) * x_num * y_num,
+                        tile.mesh.size() * sizeof(uint16_t));
+            this->get_apr_method_patch(apr, tile, patches[b]);
+        }
+        this->iPullingScheme.pulling_scheme_main();
+        this->generateDatastructures(apr);
+        return true;
+    }
+};
+
 struct RefHandle {
     APR apr;
     float offset = 0;
@@ -119,6 +156,56 @@ int ref_get_apr(const uint16_t *img, int y, int x, int z, const orc_params *p, i
         return 2;
     }
     *out = h;
+    return 0;
+}
+
+/* Blocked get_apr (APRConverterBatch) on an in-memory volume. */
+int ref_get_apr_by_block(const uint16_t *img, int y, int x, int z, const orc_params *p, int image_type, int zblock,
+                         int ghost, void **out) {
+    *out = nullptr;
+    PixelData<uint16_t> in(y, x, z);
+    std::memcpy(in.mesh.begin(), img, sizeof(uint16_t) * (size_t)y * x * z);
+    RefHandle *h = new RefHandle();
+    try {
+        if (image_type == 1) {
+            BlockConverter<uint16_t> c;
+            set_params(c.par, p);
+            c.run(h->apr, in, zblock, ghost);
+        } else {
+            BlockConverter<float> c;
+            set_params(c.par, p);
+            c.run(h->apr, in, zblock, ghost);
+        }
+    } catch (std::invalid_argument &) {
+        delete h;
+        return 2;
+    }
+    *out = h;
+    return 0;
+}
+
+/* sample_parts_from_img_downsampled_patch (ParticleData.hpp:330-372) over the
+ * z-tiles of sample_parts_from_img_blocked_gen (:288-322), tiles from memory. */
+int ref_sample_image_by_block(void *hv, const uint16_t *img, int zblock, int ghost, uint16_t *parts) {
+    RefHandle *h = (RefHandle *)hv;
+    APR &apr = h->apr;
+    const int y_num = apr.org_dims(0), x_num = apr.org_dims(1), z_num = apr.org_dims(2);
+    ParticleData<uint16_t> pd;
+    pd.init(apr);
+    const int nb = std::max(z_num / zblock, 1);
+    for (int b = 0; b < nb; ++b) {
+        const int z0 = b * zblock, zf = (b == nb - 1) ? z_num : (b + 1) * zblock;
+        const int gl = std::min(z0, ghost), gr = std::min(z_num - zf, ghost);
+        ImagePatch patch;
+        initPatchGlobal(patch, z0 - gl, zf + gr, 0, x_num, 0, y_num);
+        patch.z_ghost_l = gl;
+        patch.z_ghost_r = gr;
+        patch.z_offset = z0 - gl;
+        PixelData<uint16_t> tile(y_num, x_num, zf + gr - (z0 - gl));
+        std::memcpy(tile.mesh.begin(), img + (size_t)(z0 - gl) * x_num * y_num, tile.mesh.size() * sizeof(uint16_t));
+        sample_parts_from_img_downsampled_patch(apr, pd, tile, patch);
+    }
+    std::memcpy(parts, pd.data.begin(), pd.size() * sizeof(uint16_t));
     return 0;
 }
 

@@ -107,3 +107,35 @@ def test_overflow_detected_like_reference():
     e, _, _ = B.orc_get_apr(img, oracle_params(), 1)
     e2, _ = B.ref_get_apr(img, oracle_params(), 1)
     assert e == 2 and e2 == 2
+
+
+# z-tilings of the blocked converter, all inside every level (the reference
+# writes outside a level's array for tilings that fail block_tiling_in_bounds)
+BLOCK_CASES = [((100, 40, 48), 32, 8), ((96, 30, 40), 20, 8), ((65, 37, 29), 16, 4), ((200, 32, 32), 128, 16),
+               ((80, 24, 70), 16, 16), ((64, 40, 30), 128, 32)]
+
+
+@pytest.mark.parametrize("shape,zb,ghost", BLOCK_CASES)
+def test_block_cases_stay_in_bounds(shape, zb, ghost):
+    assert B.block_tiling_in_bounds(shape, zb, ghost)
+
+
+def test_block_bounds_predicate_flags_overrun():
+    # 70 planes in tiles of 16 with ghost 4: the last tile reaches plane 9 of
+    # a 9-plane level at 1/8 resolution
+    assert not B.block_tiling_in_bounds((70, 33, 50), 16, 4)
+
+
+@ref_missing
+@pytest.mark.parametrize("image_type", [1, 0])
+@pytest.mark.parametrize("shape,zb,ghost", BLOCK_CASES[:4])
+def test_block_oracle_matches_reference_build(shape, zb, ghost, image_type):
+    img = volume(shape, 30, 3)
+    p = oracle_params()
+    e, acc = B.orc_get_apr_by_block(img, p, image_type, zb, ghost)
+    e2, r = B.ref_get_apr_by_block(img, p, image_type, zb, ghost)
+    assert e == e2 == 0
+    ra = r.access()
+    assert np.array_equal(acc.level_xz, ra.level_xz)
+    assert np.array_equal(acc.xz_end, ra.xz_end) and np.array_equal(acc.y_vec, ra.y_vec)
+    assert np.array_equal(B.orc_sample_by_block(acc, img, zb, ghost), r.sample_by_block(img, zb, ghost)[:ra.P])
