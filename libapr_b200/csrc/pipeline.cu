@@ -679,7 +679,7 @@ __global__ void levels_kernel(IT *__restrict__ grad, float *__restrict__ lis, co
     const uint32_t u = cvt_u32(q * mult);
     const int lev = u == 0 ? 0 : 31 - __clz(u);
     level[i] = (uint8_t)lev;
-    status[i] = ((float)lev >= (float)top_level) ? kSeed : kEmpty;
+    if (status) status[i] = ((float)lev >= (float)top_level) ? kSeed : kEmpty;
 }
 
 // ---------------------------------------------------------------------------
