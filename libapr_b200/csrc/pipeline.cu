@@ -411,63 +411,86 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
 }
 
 // ---------------------------------------------------------------------------
-// a5: calc_inv_bspline_y/x/z (ComputeGradient.hpp:785-964), the three
-// in-place passes fused: each output re-evaluates the y and x passes of its
-// 3x3x3 neighbourhood with the same float operations, reading a shared-memory
-// tile of the input (8 x 8 x 64 outputs plus a one-sample halo).
+// a5: calc_inv_bspline_y/x/z (ComputeGradient.hpp:785-964): the three in-place
+// passes run one after the other on a shared-memory tile of 8 x 8 x 64 outputs
+// plus a one-sample halo in x and z: the y pass over the tile and its halo,
+// the x pass over the tile's x range and the z halo, then the z pass.  Each
+// value is the reference's expression with its operand order, so the tile
+// reproduces the whole-volume passes exactly.
 // ---------------------------------------------------------------------------
 struct InvB {
     float a1, a2, a3, a13;
 };
 
 constexpr int kIX = 8, kIY = 64, kIZ = 8;
-struct InvTile {
-    const float *s;
-    int x0, y0, z0;  // global coordinates of the tile's first interior sample
-    __device__ __forceinline__ float at(int y, int x, int z) const {
-        return s[((z - z0 + 1) * (kIX + 2) + (x - x0 + 1)) * (kIY + 2) + (y - y0 + 1)];
-    }
-};
+constexpr int kIXH = kIX + 2, kIZH = kIZ + 2, kIYH = kIY + 2;
 
-__device__ __forceinline__ float inv_y(const InvTile &I, int y, int x, int z, int yd, bool on, InvB c) {
-    if (!on) return I.at(y, x, z);
-    if (y == 0) return c.a2 * I.at(0, x, z) + c.a13 * I.at(1, x, z);
-    if (y == yd - 1) return c.a13 * I.at(yd - 2, x, z) + c.a2 * I.at(yd - 1, x, z);
-    return c.a1 * I.at(y - 1, x, z) + c.a2 * I.at(y, x, z) + c.a3 * I.at(y + 1, x, z);
-}
-
-__device__ __forceinline__ float inv_x(const InvTile &I, int y, int x, int z, int yd, int xd, bool ony, bool onx,
-                                       InvB c) {
-    if (!onx) return inv_y(I, y, x, z, yd, ony, c);
-    if (x == xd - 1) return c.a13 * inv_y(I, y, xd - 2, z, yd, ony, c) + c.a2 * inv_y(I, y, xd - 1, z, yd, ony, c);
-    const int xm = x == 0 ? 1 : x - 1;
-    return c.a1 * inv_y(I, y, xm, z, yd, ony, c) + c.a2 * inv_y(I, y, x, z, yd, ony, c) +
-           c.a3 * inv_y(I, y, x + 1, z, yd, ony, c);
-}
+constexpr size_t kInvSmem = sizeof(float) * (kIZH * kIXH * kIYH + kIZH * kIXH * kIY);
 
 __global__ void __launch_bounds__(256) inv_bspline_kernel(const float *__restrict__ in, float *__restrict__ O, int yd,
                                                           int xd, int zd, int ony, int onx, int onz, InvB c) {
-    __shared__ float s[(kIZ + 2) * (kIX + 2) * (kIY + 2)];
+    extern __shared__ float inv_smem[];
+    float *S = inv_smem;                         // input tile with halo [zz][xx][yy], later the x pass
+    float *Yb = inv_smem + kIZH * kIXH * kIYH;  // y pass over the tile's y range [zz][xx][yy]
     const int y0 = blockIdx.x * kIY, x0 = blockIdx.y * kIX, z0 = blockIdx.z * kIZ;
-    for (int t = threadIdx.x; t < (kIZ + 2) * (kIX + 2) * (kIY + 2); t += blockDim.x) {
-        const int yy = t % (kIY + 2), xx = (t / (kIY + 2)) % (kIX + 2), zz = t / ((kIY + 2) * (kIX + 2));
+    for (int t = threadIdx.x; t < kIZH * kIXH * kIYH; t += blockDim.x) {
+        const int yy = t % kIYH, xx = (t / kIYH) % kIXH, zz = t / (kIYH * kIXH);
         const int yg = y0 - 1 + yy, xg = x0 - 1 + xx, zg = z0 - 1 + zz;
-        if (yg >= 0 && yg < yd && xg >= 0 && xg < xd && zg >= 0 && zg < zd) s[t] = in[idx3(yg, xg, zg, yd, xd)];
+        if (yg >= 0 && yg < yd && xg >= 0 && xg < xd && zg >= 0 && zg < zd) S[t] = in[idx3(yg, xg, zg, yd, xd)];
     }
     __syncthreads();
-    const InvTile I{s, x0, y0, z0};
-    for (int t = threadIdx.x; t < kIX * kIY * kIZ; t += blockDim.x) {
-        const int y = y0 + t % kIY, x = x0 + (t / kIY) % kIX, z = z0 + t / (kIY * kIX);
+    // y pass: (z, x) over the tile and its halo, y over the tile
+    for (int t = threadIdx.x; t < kIZH * kIXH * kIY; t += blockDim.x) {
+        const int yy = t % kIY, xx = (t / kIY) % kIXH, zz = t / (kIY * kIXH);
+        const int y = y0 + yy, xg = x0 - 1 + xx, zg = z0 - 1 + zz;
+        if (y >= yd || xg < 0 || xg >= xd || zg < 0 || zg >= zd) continue;
+        const int base = (zz * kIXH + xx) * kIYH + 1 - y0;  // + global y
+        float v;
+        if (!ony)
+            v = S[base + y];
+        else if (y == 0)
+            v = c.a2 * S[base + 0] + c.a13 * S[base + 1];
+        else if (y == yd - 1)
+            v = c.a13 * S[base + yd - 2] + c.a2 * S[base + yd - 1];
+        else
+            v = c.a1 * S[base + y - 1] + c.a2 * S[base + y] + c.a3 * S[base + y + 1];
+        Yb[t] = v;
+    }
+    __syncthreads();
+    // x pass into S, laid out [zz][xx][yy] with x over the tile only
+    for (int t = threadIdx.x; t < kIZH * kIX * kIY; t += blockDim.x) {
+        const int yy = t % kIY, xx = (t / kIY) % kIX, zz = t / (kIY * kIX);
+        const int y = y0 + yy, x = x0 + xx, zg = z0 - 1 + zz;
+        if (y >= yd || x >= xd || zg < 0 || zg >= zd) continue;
+        const int base = zz * kIXH * kIY + yy;  // + (global x - x0 + 1) * kIY
+        auto Y = [&](int xg) { return Yb[base + (xg - x0 + 1) * kIY]; };
+        float v;
+        if (!onx) {
+            v = Y(x);
+        } else if (x == xd - 1) {
+            v = c.a13 * Y(xd - 2) + c.a2 * Y(xd - 1);
+        } else {
+            const int xm = x == 0 ? 1 : x - 1;
+            v = c.a1 * Y(xm) + c.a2 * Y(x) + c.a3 * Y(x + 1);
+        }
+        S[t] = v;
+    }
+    __syncthreads();
+    // z pass and store
+    for (int t = threadIdx.x; t < kIZ * kIX * kIY; t += blockDim.x) {
+        const int yy = t % kIY, xx = (t / kIY) % kIX, zz = t / (kIY * kIX);
+        const int y = y0 + yy, x = x0 + xx, z = z0 + zz;
         if (y >= yd || x >= xd || z >= zd) continue;
+        const int base = xx * kIY + yy;  // + (global z - z0 + 1) * kIX * kIY
+        auto X = [&](int zg) { return S[base + (zg - z0 + 1) * (kIX * kIY)]; };
         float r;
         if (!onz) {
-            r = inv_x(I, y, x, z, yd, xd, ony, onx, c);
+            r = X(z);
         } else if (z == zd - 1) {
-            r = c.a13 * inv_x(I, y, x, zd - 2, yd, xd, ony, onx, c) + c.a2 * inv_x(I, y, x, zd - 1, yd, xd, ony, onx, c);
+            r = c.a13 * X(zd - 2) + c.a2 * X(zd - 1);
         } else {
             const int zm = z == 0 ? 1 : z - 1;
-            r = c.a1 * inv_x(I, y, x, zm, yd, xd, ony, onx, c) + c.a2 * inv_x(I, y, x, z, yd, xd, ony, onx, c) +
-                c.a3 * inv_x(I, y, x, z + 1, yd, xd, ony, onx, c);
+            r = c.a1 * X(zm) + c.a2 * X(z) + c.a3 * X(z + 1);
         }
         O[idx3(y, x, z, yd, xd)] = r;
     }
@@ -797,7 +820,9 @@ void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *id
     c.a3 = (float)(1.0 / 6.0);
     c.a13 = c.a1 + c.a3;
     dim3 grid((yd + kIY - 1) / kIY, (xd + kIX - 1) / kIX, (zd + kIZ - 1) / kIZ);
-    inv_bspline_kernel<<<grid, 256, 0, s>>>(ids_raw, ids, yd, xd, zd, on && yn > 2, on && xn > 2, on && zn > 2, c);
+    APRB_CUDA(cudaFuncSetAttribute(inv_bspline_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
+    inv_bspline_kernel<<<grid, 256, kInvSmem, s>>>(ids_raw, ids, yd, xd, zd, on && yn > 2, on && xn > 2, on && zn > 2,
+                                                   c);
     count_launch();
     APRB_CHECK_LAUNCH();
 }

@@ -67,25 +67,6 @@ __global__ void fill_patch_kernel(const uint8_t *__restrict__ lev, LevelDims dp,
     if (sd) status[idx3(y, x, zg, d.yn, d.xn)] = kSeed;
 }
 
-// set_ascendant_neighbours (:250-289)
-__global__ void asc_neighbours_kernel(uint8_t *__restrict__ st, LevelDims d) {
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= (uint64_t)d.yn * d.xn * d.zn) return;
-    const uint8_t s = st[g];
-    if (s != kEmpty && s != kSeed) return;
-    int y, x, z;
-    cell_of(g, d.yn, d.xn, y, x, z);
-    bool hit = false;
-    for (int dz = max(z - 1, 0); dz <= min(z + 1, d.zn - 1) && !hit; ++dz)
-        for (int dx = max(x - 1, 0); dx <= min(x + 1, d.xn - 1) && !hit; ++dx)
-            for (int dy = max(y - 1, 0); dy <= min(y + 1, d.yn - 1); ++dy)
-                if (st[idx3(dy, dx, dz, d.yn, d.xn)] == kAscendant) {
-                    hit = true;
-                    break;
-                }
-    if (hit) st[g] = (s == kEmpty) ? kAscendantNeighbour : kPropagate;
-}
-
 // set_filler (:291-343): children of ASCENDANTNEIGHBOUR / PROPOGATE cells
 __global__ void set_filler_kernel(const uint8_t *__restrict__ parent, LevelDims dp, uint8_t *__restrict__ child,
                                   LevelDims dc) {
@@ -98,22 +79,64 @@ __global__ void set_filler_kernel(const uint8_t *__restrict__ parent, LevelDims 
     if (s == kAscendantNeighbour || s == kPropagate) child[g] = kFiller;
 }
 
-// fill_neighbours (:345-381), boundary part
-__global__ void boundary_kernel(uint8_t *__restrict__ st, LevelDims d) {
-    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= (uint64_t)d.yn * d.xn * d.zn) return;
-    if (st[g] != kEmpty) return;
-    int y, x, z;
-    cell_of(g, d.yn, d.xn, y, x, z);
-    for (int dz = max(z - 1, 0); dz <= min(z + 1, d.zn - 1); ++dz)
-        for (int dx = max(x - 1, 0); dx <= min(x + 1, d.xn - 1); ++dx)
-            for (int dy = max(y - 1, 0); dy <= min(y + 1, d.yn - 1); ++dy) {
-                const uint8_t q = st[idx3(dy, dx, dz, d.yn, d.xn)];
-                if (q == kSeed || q == kPropagate) {
-                    st[g] = kBoundary;
-                    return;
-                }
-            }
+// 3x3x3 neighbourhood marking as a tiled OR-dilation, for the two
+// neighbour steps of the pulling scheme:
+//   MODE 0, set_ascendant_neighbours (:250-289): source ASCENDANT; an EMPTY
+//           cell next to one becomes ASCENDANTNEIGHBOUR, a SEED cell PROPOGATE;
+//   MODE 1, fill_neighbours (:345-381): source SEED or PROPOGATE; an EMPTY cell
+//           next to one becomes BOUNDARY.
+// A CTA owns 128 (y) x 8 (x) x 8 (z) cells.  Each warp turns one row of the
+// tile plus its one-cell halo into four 32-bit words of the y-dilated source
+// mask (warp ballots, neighbours by shuffles), the words are ORed over the
+// 3 x 3 (x, z) neighbourhood from shared memory, and the targets are written.
+// Writes never create a source value, so concurrent CTAs reading their halo
+// see the same sources in any order.
+constexpr int kDY = 128, kDX = 8, kDZ = 8, kDRows = (kDX + 2) * (kDZ + 2), kDWords = kDY / 32;
+
+template <int MODE>
+__device__ __forceinline__ bool dil_source(uint8_t s) {
+    return MODE == 0 ? s == kAscendant : (s == kSeed || s == kPropagate);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(256) dilate_kernel(uint8_t *__restrict__ st, LevelDims d) {
+    __shared__ uint32_t W[kDRows][kDWords];
+    const int y0 = blockIdx.x * kDY, x0 = blockIdx.y * kDX, z0 = blockIdx.z * kDZ;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int r = w; r < kDRows; r += 8) {
+        const int x = x0 - 1 + r % (kDX + 2), z = z0 - 1 + r / (kDX + 2);
+        const bool row_in = x >= 0 && x < d.xn && z >= 0 && z < d.zn;
+        const uint8_t *R = st + ((uint64_t)(row_in ? z : 0) * d.xn + (row_in ? x : 0)) * (uint64_t)d.yn;
+        for (int k = 0; k < kDWords; ++k) {
+            const int y = y0 + 32 * k + lane;
+            const bool p = row_in && y < d.yn && dil_source<MODE>(R[y]);
+            bool pl = __shfl_up_sync(0xffffffffu, p, 1), pr = __shfl_down_sync(0xffffffffu, p, 1);
+            if (lane == 0) pl = row_in && y >= 1 && y - 1 < d.yn && dil_source<MODE>(R[y - 1]);
+            if (lane == 31) pr = row_in && y + 1 < d.yn && dil_source<MODE>(R[y + 1]);
+            const uint32_t word = __ballot_sync(0xffffffffu, p || pl || pr);
+            if (lane == 0) W[r][k] = word;
+        }
+    }
+    __syncthreads();
+    for (int task = w; task < kDX * kDZ * kDWords; task += 8) {
+        const int k = task % kDWords, xx = (task / kDWords) % kDX, zz = task / (kDWords * kDX);
+        const int x = x0 + xx, z = z0 + zz, y = y0 + 32 * k + lane;
+        if (x >= d.xn || z >= d.zn) continue;
+        uint32_t m = 0;
+#pragma unroll
+        for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx) m |= W[(zz + dz) * (kDX + 2) + xx + dx][k];
+        if (y >= d.yn || !((m >> lane) & 1u)) continue;
+        uint8_t *c = st + ((uint64_t)z * d.xn + x) * (uint64_t)d.yn + y;
+        const uint8_t s = *c;
+        if (MODE == 0) {
+            if (s == kEmpty) *c = kAscendantNeighbour;
+            else if (s == kSeed) *c = kPropagate;
+        } else {
+            if (s == kEmpty) *c = kBoundary;
+        }
+    }
 }
 
 // fill_neighbours -> fill_parent (:372-393), as a gather over the parents
@@ -459,13 +482,14 @@ void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s, bool fill
     }
     APRB_CHECK_LAUNCH();
     for (int l = top; l >= lmin; --l) {
+        const dim3 dgrid((g.y_num[l] + kDY - 1) / kDY, (g.x_num[l] + kDX - 1) / kDX, (g.z_num[l] + kDZ - 1) / kDZ);
         if (l != top) {
-            asc_neighbours_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(pm.status[l], dims(g, l));
+            dilate_kernel<0><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
             set_filler_kernel<<<blocks_for(ncell(g, l + 1), 256), 256, 0, s>>>(pm.status[l], dims(g, l),
                                                                               pm.status[l + 1], dims(g, l + 1));
             count_launch(2);
         }
-        boundary_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(pm.status[l], dims(g, l));
+        dilate_kernel<1><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
         count_launch();
         if (l - 1 >= lmin) {
             fill_parent_kernel<<<blocks_for(ncell(g, l - 1), 256), 256, 0, s>>>(pm.status[l], dims(g, l),
