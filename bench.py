@@ -98,6 +98,23 @@ class Clocks:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(value, world, device):
+    """The slowest rank's time: every rank of a weak-scaling run converts its
+    own volume, and the job is as fast as its slowest rank."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def volume_seed(rank):
+    """Each rank converts a different seeded volume of the same model."""
+    return 1000 + rank
+
+
 def lib_params():
     import libapr_b200 as A
     p = A.APRParameters()
@@ -270,6 +287,121 @@ def bench_batch(A, L, _lib, torch, stream, sptr, args):
     return res
 
 
+RL_BLOBS = 20000  # per 256 x 1024 x 1024
+
+
+def gaussian_psf(sigma=1.2, ks=5):
+    g = np.exp(-((np.arange(ks) - ks // 2) ** 2) / (2 * sigma * sigma)).astype(np.float32)
+    p = (g[:, None, None] * g[None, :, None] * g[None, None, :]).astype(np.float32)
+    return (p / p.sum()).astype(np.float32)
+
+
+def bench_rl(A, L, _lib, torch, stream, sptr, args):
+    """Plain APR Richardson-Lucy on the deconvolution workload: float ground
+    truth (background 50, Gaussian blobs sigma U[1,4], amplitude U[500,5000]),
+    blurred by the normalised 5x5x5 Gaussian PSF (sigma 1.2), Poisson noise,
+    uint16; APR with lambda=3, E=0.1, Ip_th=0, sigma_th=50, grad_th=10.  FP32 RL
+    time per iteration, and its relative L2 error after 20/100/500 iterations
+    against the FP64 RL (the reference's double instantiation on the GPU, which
+    the tests pin bit-exact to the FP64 oracle) after 500 iterations."""
+    import torch.nn.functional as F
+    shape = tuple(int(v) for v in args.rl_shape.split(","))
+    n = shape[0] * shape[1] * shape[2]
+    gt = torch.empty(shape, dtype=torch.float32, device="cuda")
+    A.synth_ground_truth_device(gt, max(1, int(RL_BLOBS * n / (256 * 1024 * 1024))), (1.0, 4.0), (500.0, 5000.0),
+                                50.0, seed=3000, stream=stream)
+    psf = gaussian_psf()
+    k = torch.from_numpy(psf).cuda().view(1, 1, 5, 5, 5)
+    blurred = F.conv3d(F.pad(gt[None, None], (2, 2, 2, 2, 2, 2), mode="replicate"), k)[0, 0]
+    del gt
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(3001)
+    noisy = torch.poisson(blurred, generator=gen).clamp_(0, 65535)
+    img = noisy.to(torch.int32).to(torch.int16).contiguous()  # low 16 bits: the uint16 value
+    del blurred, noisy
+    conv = A.APRConverter("float")
+    conv.par = lib_params()
+    apr = A.APR()
+    assert conv.get_apr(apr, img)
+    P = apr.total_number_particles()
+    parts = torch.empty(max(P, 1), dtype=torch.int16, device="cuda")
+    _lib.check(L.aprb_sample_image_device(apr._h, C.c_void_p(img.data_ptr()), C.c_void_p(parts.data_ptr()), sptr))
+    del img
+    apr.init_tree()
+    T = apr.total_number_tree_particles()
+    pp = C.c_void_p(parts.data_ptr())
+    st = C.c_void_p(psf.ctypes.data)
+    o32 = torch.empty(max(P, 1), dtype=torch.float32, device="cuda")
+    o64 = torch.empty(max(P, 1), dtype=torch.float64, device="cuda")
+
+    def rl32(iters, resume):
+        _lib.check(L.aprb_richardson_lucy_device(apr._h, pp, C.c_void_p(o32.data_ptr()), st, 5, iters, 1, 1,
+                                                 int(resume), sptr))
+
+    def rl64(iters, resume):
+        _lib.check(L.aprb_richardson_lucy_fp64_device(apr._h, pp, C.c_void_p(o64.data_ptr()), st, 5, iters, 1, 1,
+                                                      int(resume), sptr))
+
+    def timed(fn, *a):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn(*a)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    rl32(2, False)
+    torch.cuda.synchronize()
+    L.aprb_profile_reset()
+    L.aprb_profile_enable(1)
+    ms32 = timed(rl32, 20, False) / 20
+    L.aprb_profile_enable(0)
+    L.aprb_profile_reset()
+    f64 = {}
+    ms64 = 0.0
+    done = 0
+    for kk in (20, 100, 500):
+        ms64 += timed(rl64, kk - done, done > 0)
+        done = kk
+        f64[kk] = o64[:P].clone()
+    ref = f64[500]
+    rnorm = float(torch.linalg.norm(ref))
+    errs, errs_same, k_hit = {}, {}, None
+    done = 0
+    while done < 500:
+        step = 10
+        rl32(step, done > 0)
+        done += step
+        e = float(torch.linalg.norm(o32[:P].double() - ref)) / rnorm
+        if k_hit is None and e < 1e-3:
+            k_hit = done
+        if done in (20, 100, 500):
+            errs[done] = e
+            errs_same[done] = float(torch.linalg.norm(o32[:P].double() - f64[done])) / float(
+                torch.linalg.norm(f64[done]))
+    bytes_it = 2 * (10 * P + 10 * T) + 2 * P
+    hbm, kind = peaks()
+    res = {
+        "workload": "deconvolution: %dx%dx%d (z,x,y) blob ground truth (bg 50, %d blobs sigma U[1,4], amp "
+                    "U[500,5000]) * normalised 5^3 Gaussian PSF sigma 1.2, Poisson, uint16; APR lambda=3 E=0.1 "
+                    "Ip_th=0 sigma_th=50 grad_th=10; PSF as APR stencil, downsampled + normalised"
+                    % (shape + (max(1, int(RL_BLOBS * n / (256 * 1024 * 1024))),)),
+        "particles": P, "tree_nodes": T,
+        "fp32_ms_per_iteration": ms32, "fp32_gpart_per_s": P / (ms32 / 1e3) / 1e9,
+        "fp64_ms_per_iteration": ms64 / 500,
+        "roofline": {"bound": "hbm", "algorithmic_bytes_per_iteration": bytes_it,
+                     "achieved": bytes_it / (ms32 / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                     "frac": bytes_it / (ms32 / 1e3) / 1e9 / hbm, "peak_source": kind},
+        "rel_l2_vs_fp64_500": {str(kk): v for kk, v in errs.items()},
+        "rel_l2_fp32_vs_fp64_same_iterations": {str(kk): v for kk, v in errs_same.items()},
+        "iterations_to_1e-3_of_fp64_500": k_hit,
+        "time_to_1e-3_ms": None if k_hit is None else k_hit * ms32,
+    }
+    del o32, o64, parts, f64, ref
+    apr._free()
+    return res
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -280,6 +412,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-conv", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
+    ap.add_argument("--no-rl", action="store_true")
+    ap.add_argument("--rl-shape", default="256,1024,1024", help="z,x,y of the deconvolution workload")
     ap.add_argument("--image-type", default="float", choices=["float", "uint16"],
                     help="APRConverter ImageType; uint16 throws the reference's overflow error on this volume")
     args = ap.parse_args()
@@ -307,7 +441,7 @@ def main():
 
     img = torch.empty(shape, dtype=torch.int16, device="cuda")
     A.synth_blobs_device(img, int(BLOBS * N / (SHAPE[0] * SHAPE[1] * SHAPE[2])), SIGMA, AMP, BG,
-                         seed=1000 + rank, stream=stream)
+                         seed=volume_seed(rank), stream=stream)
     torch.cuda.synchronize()
     conv = A.APRConverter(args.image_type)
     par = lib_params().c()
@@ -371,10 +505,7 @@ def main():
     ns = L.aprb_profile_read(names, tms, cnts, 64)
     stages = {names[i].decode(): (tms[i], int(cnts[i])) for i in range(ns)}
     L.aprb_profile_reset()
-    t_max = torch.tensor([ms], device="cuda", dtype=torch.float64)
-    if world > 1:
-        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
-    ms_all = float(t_max.item())
+    ms_all = max_over_ranks(ms, world, "cuda")
     last = hs[-1]
     for h in hs[:-1]:
         L.aprb_apr_free(h)
@@ -441,37 +572,41 @@ def main():
         del pf, outp
     L.aprb_apr_free(last)
 
+    # the batch and deconvolution workloads are single-GPU measurements
     batch_res = None
-    if not args.no_batch and rank == 0:
+    if not args.no_batch and world == 1:
         batch_res = bench_batch(A, L, _lib, torch, stream, sptr, args)
+    rl_res = None
+    if not args.no_rl and world == 1:
+        rl_res = bench_rl(A, L, _lib, torch, stream, sptr, args)
 
-    # --- end to end through the host-buffer C ABI
+    # --- end to end through the host-buffer C ABI, on every rank
     e2e = None
-    if rank == 0:
-        host = torch.empty(shape, dtype=torch.int16, pin_memory=True)
-        host.copy_(img)
-        hparts = torch.empty(max(P, 1), dtype=torch.int16, pin_memory=True)
-        hp = C.c_void_p(host.data_ptr())
-        hpp = C.c_void_p(hparts.data_ptr())
+    host = torch.empty(shape, dtype=torch.int16, pin_memory=True)
+    host.copy_(img)
+    hparts = torch.empty(max(P, 1), dtype=torch.int16, pin_memory=True)
+    hp = C.c_void_p(host.data_ptr())
+    hpp = C.c_void_p(hparts.data_ptr())
 
-        def e2e_step():
-            h = C.c_void_p()
-            _lib.check(L.aprb_get_apr(conv._h, C.byref(par), hp, y, x, z, C.byref(h)))
-            _lib.check(L.aprb_sample_image(h, hp, hpp))
-            L.aprb_apr_free(h)
+    def e2e_step():
+        h = C.c_void_p()
+        _lib.check(L.aprb_get_apr(conv._h, C.byref(par), hp, y, x, z, C.byref(h)))
+        _lib.check(L.aprb_sample_image(h, hp, hpp))
+        L.aprb_apr_free(h)
 
+    e2e_step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
         e2e_step()
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        for _ in range(args.steps):
-            e2e_step()
-        torch.cuda.synchronize()
-        te = (time.perf_counter() - t0) / args.steps
-        e2e = {"value": N * world / te / 1e9, "unit": "GVox/s", "h2d_bytes_per_step": 4 * N,
-               "d2h_bytes_per_step": 2 * P, "ms_per_step": te * 1e3}
-        cpu = None
-        if not args.no_cpu:
-            cpu = cpu_baseline(host.numpy().view(np.uint16), it_code)
+    torch.cuda.synchronize()
+    te = max_over_ranks((time.perf_counter() - t0) / args.steps, world, "cuda")
+    e2e = {"value": N * world / te / 1e9, "unit": "GVox/s", "h2d_bytes_per_step": 4 * N,
+           "d2h_bytes_per_step": 2 * P, "ms_per_step": te * 1e3}
+    cpu = None
+    if not args.no_cpu and world == 1:
+        cpu = cpu_baseline(host.numpy().view(np.uint16), it_code)
+    if rank == 0:
         line = {"metric": METRIC, "value": N * world / (ms_all / 1e3) / 1e9, "unit": "GVox/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_all, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32" if it_code == 0 else "u16",
@@ -484,6 +619,8 @@ def main():
                 "gpu_launches": int(launches), "e2e": e2e, "cpu_baseline": cpu, **out, **conv_res}
         if batch_res:
             line["batch_by_block"] = batch_res
+        if rl_res:
+            line["rl_deconvolution"] = rl_res
         if ck:
             line["clocks"] = ck
         print(json.dumps(line))

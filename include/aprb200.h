@@ -201,6 +201,14 @@ aprb_status aprb_richardson_lucy(aprb_apr *a, const uint16_t *in, float *out, co
 aprb_status aprb_richardson_lucy_device(aprb_apr *a, const uint16_t *in_dev, float *out_dev, const float *psf,
                                         int ksize, int niter, int use_stencil_downsample, int normalize, int resume,
                                         void *stream);
+/* the reference's FP64 instantiation, APRNumerics::richardson_lucy<uint16_t, double, double>
+ * (APRNumerics.hpp:551-593): stencils, tree means, intermediates and output in double; psf is
+ * given as float and converted to double before it is flipped and down-sampled */
+aprb_status aprb_richardson_lucy_fp64(aprb_apr *a, const uint16_t *in, double *out, const float *psf, int ksize,
+                                      int niter, int use_stencil_downsample, int normalize, int resume);
+aprb_status aprb_richardson_lucy_fp64_device(aprb_apr *a, const uint16_t *in_dev, double *out_dev, const float *psf,
+                                             int ksize, int niter, int use_stencil_downsample, int normalize,
+                                             int resume, void *stream);
 
 /* --- synthetic data (benchmark inputs; no reference counterpart) ----------------
  * Background + n_blobs isotropic Gaussians (centre uniform, sigma and peak
@@ -208,6 +216,10 @@ aprb_status aprb_richardson_lucy_device(aprb_apr *a, const uint16_t *in_dev, flo
  * uint16, written to a device buffer of y*x*z elements. Deterministic for a
  * seed. */
 aprb_status aprb_synth_blobs_u16(uint16_t *img_dev, int y_num, int x_num, int z_num, int n_blobs, float sigma_lo,
+                                 float sigma_hi, float amp_lo, float amp_hi, float background, uint64_t seed,
+                                 void *stream);
+/* the same blobs without noise, as float intensities (ground truth of the deconvolution workload) */
+aprb_status aprb_synth_blobs_f32(float *img_dev, int y_num, int x_num, int z_num, int n_blobs, float sigma_lo,
                                  float sigma_hi, float amp_lo, float amp_hi, float background, uint64_t seed,
                                  void *stream);
 

@@ -365,20 +365,29 @@ def isotropic_convolve_555(apr, particle_input, stencil, reflective_bc=True, use
 class APRNumerics:
     @staticmethod
     def richardson_lucy(apr, particle_input, particle_output, psf, number_iterations, use_stencil_downsample=True,
-                        normalize=False, resume=False):
+                        normalize=False, resume=False, dtype=np.float32):
+        """APRNumerics::richardson_lucy (APRNumerics.hpp:132-134, 551-593).
+        dtype float64 runs the reference's double instantiation (double
+        stencils, tree and output), as a particle_output holding float64 data
+        also selects."""
         st = np.ascontiguousarray(psf, np.float32).ravel()
         ks = int(round(st.size ** (1.0 / 3.0)))
         if ks ** 3 != st.size or ks not in (3, 5):
             raise RuntimeError("APR RL: stencil side must be 3 or 5")
         parts = np.ascontiguousarray(getattr(particle_input, "data", particle_input), np.uint16)
         n = len(parts)
-        if resume and getattr(particle_output, "data", None) is not None:
-            out = np.ascontiguousarray(particle_output.data, np.float32).copy()
+        prev = getattr(particle_output, "data", None)
+        if prev is not None and np.asarray(prev).dtype == np.float64:
+            dtype = np.float64
+        dtype = np.dtype(dtype)
+        if resume and prev is not None:
+            out = np.ascontiguousarray(prev, dtype).copy()
         else:
-            out = np.zeros(max(n, 1), np.float32)
-        out = np.resize(out, max(n, 1)).astype(np.float32)
-        check(lib().aprb_richardson_lucy(apr._h, _ptr(parts), _ptr(out), _ptr(st), ks, int(number_iterations),
-                                         int(use_stencil_downsample), int(normalize), int(resume)))
+            out = np.zeros(max(n, 1), dtype)
+        out = np.resize(out, max(n, 1)).astype(dtype)
+        fn = lib().aprb_richardson_lucy_fp64 if dtype == np.float64 else lib().aprb_richardson_lucy
+        check(fn(apr._h, _ptr(parts), _ptr(out), _ptr(st), ks, int(number_iterations), int(use_stencil_downsample),
+                 int(normalize), int(resume)))
         res = out[:n]
         if particle_output is not None:
             particle_output.data = res
@@ -423,4 +432,12 @@ def synth_blobs_device(out_tensor, n_blobs, sigma=(2.0, 6.0), amp=(800.0, 4000.0
     """Fills a (z, x, y) uint16 CUDA tensor with the seeded blob + Poisson model."""
     z, x, y = out_tensor.shape
     check(lib().aprb_synth_blobs_u16(_dptr(out_tensor), y, x, z, int(n_blobs), sigma[0], sigma[1], amp[0], amp[1],
+                                     background, int(seed), _stream(stream)))
+
+
+def synth_ground_truth_device(out_tensor, n_blobs, sigma=(1.0, 4.0), amp=(500.0, 5000.0), background=50.0, seed=0,
+                              stream=None):
+    """Fills a (z, x, y) float32 CUDA tensor with the noise-free blob intensities."""
+    z, x, y = out_tensor.shape
+    check(lib().aprb_synth_blobs_f32(_dptr(out_tensor), y, x, z, int(n_blobs), sigma[0], sigma[1], amp[0], amp[1],
                                      background, int(seed), _stream(stream)))

@@ -73,7 +73,10 @@ SIGNATURES = {
     "aprb_convolve_device": ([_vp, _vp, _i, _vp, _vp, _i, _i, _i, _vp], _i),
     "aprb_richardson_lucy": ([_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i], _i),
     "aprb_richardson_lucy_device": ([_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp], _i),
+    "aprb_richardson_lucy_fp64": ([_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i], _i),
+    "aprb_richardson_lucy_fp64_device": ([_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp], _i),
     "aprb_synth_blobs_u16": ([_vp, _i, _i, _i, _i, _f, _f, _f, _f, _f, _u64, _vp], _i),
+    "aprb_synth_blobs_f32": ([_vp, _i, _i, _i, _i, _f, _f, _f, _f, _f, _u64, _vp], _i),
     "aprb_kernel_launch_count": ([], _u64),
     "aprb_profile_enable": ([_i], _i),
     "aprb_profile_reset": ([], _i),

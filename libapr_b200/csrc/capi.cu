@@ -730,15 +730,16 @@ void ensure_tree(aprb_apr *a, cudaStream_t s) {
 
 // stencil set of APRFilter::convolve_pencil(apr, stencil, ..., use_stencil_downsample, normalize)
 // (APRFilter.hpp:139-149): one stencil per level below l_max when downsampling
-ConvPlan make_plan(const aprb_apr *a, const float *stencil, int ks, int ds, int normalize, int reflect,
-                   std::vector<float> &host) {
+template <typename T>
+ConvPlan make_plan(const aprb_apr *a, const T *stencil, int ks, int ds, int normalize, int reflect,
+                   std::vector<T> &host) {
     if (ks != 3 && ks != 5) {
         set_error("stencil side must be 3 or 5");
         throw Error{APRB_ERR_UNSUPPORTED};
     }
     ConvPlan plan;
     const int nlev = ds ? std::max(a->g.l_max - a->g.l_min, 1) : 1;
-    host = downsampled_stencils(stencil, ks, nlev, normalize != 0, plan.sides);
+    host = downsampled_stencils<T>(stencil, ks, nlev, normalize != 0, plan.sides);
     plan.nstencils = (int)plan.sides.size();
     int o = 0;
     for (int sd : plan.sides) {
@@ -757,45 +758,51 @@ void convolve_impl(aprb_apr *a, const float *stencil, int ks, const float *in, f
     float *dst = scratch().stencils.as<float>(host.size());
     APRB_CUDA(cudaMemcpyAsync(dst, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice, s));
     float *tree = scratch().tree_vals.as<float>(a->T ? a->T : 1);
-    filter_apply(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
+    filter_apply<float>(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
                  (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, a->fi, in, tree, &plan, dst, out, 0,
                  nullptr, scratch().fb, s);
     a->last_stale = filter_stale_count(scratch().fb, s);
 }
 
-__global__ void fill_kernel(float *p, uint64_t n, float v) {
+template <typename T>
+__global__ void fill_kernel(T *p, uint64_t n, T v) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) p[i] = v;
 }
 
-void rl_impl(aprb_apr *a, const uint16_t *in, float *out, const float *psf, int ks, int niter, int ds, int normalize,
+// APRNumerics::richardson_lucy (APRNumerics.hpp:551-593) with value type T:
+// float, or double as the reference's FP64 instantiation.  The PSF is given
+// as float and converted to T before it is flipped and down-sampled.
+template <typename T>
+void rl_impl(aprb_apr *a, const uint16_t *in, T *out, const float *psf, int ks, int niter, int ds, int normalize,
              int resume, cudaStream_t s) {
     ensure_tree(a, s);
     const int n0 = ks * ks * ks;
-    std::vector<float> flipped(n0);
-    for (int i = 0; i < n0; ++i) flipped[i] = psf[n0 - 1 - i];
-    std::vector<float> hp, hf;
-    ConvPlan plan = make_plan(a, psf, ks, ds, normalize, 1, hp);
-    ConvPlan plan_f = make_plan(a, flipped.data(), ks, ds, normalize, 1, hf);
-    float *dp = scratch().stencils.as<float>(hp.size());
-    float *df = scratch().stencils_f.as<float>(hf.size());
-    APRB_CUDA(cudaMemcpyAsync(dp, hp.data(), hp.size() * sizeof(float), cudaMemcpyHostToDevice, s));
-    APRB_CUDA(cudaMemcpyAsync(df, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    std::vector<T> pt(n0), flipped(n0);
+    for (int i = 0; i < n0; ++i) pt[i] = (T)psf[i];
+    for (int i = 0; i < n0; ++i) flipped[i] = pt[n0 - 1 - i];
+    std::vector<T> hp, hf;
+    ConvPlan plan = make_plan<T>(a, pt.data(), ks, ds, normalize, 1, hp);
+    ConvPlan plan_f = make_plan<T>(a, flipped.data(), ks, ds, normalize, 1, hf);
+    T *dp = (T *)scratch().stencils.get(hp.size() * sizeof(T));
+    T *df = (T *)scratch().stencils_f.get(hf.size() * sizeof(T));
+    APRB_CUDA(cudaMemcpyAsync(dp, hp.data(), hp.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+    APRB_CUDA(cudaMemcpyAsync(df, hf.data(), hf.size() * sizeof(T), cudaMemcpyHostToDevice, s));
     if (!resume && a->P) {
-        fill_kernel<<<blocks_for(a->P, 256), 256, 0, s>>>(out, a->P, 1.0f);
+        fill_kernel<T><<<blocks_for(a->P, 256), 256, 0, s>>>(out, a->P, T(1));
         count_launch();
         APRB_CHECK_LAUNCH();
     }
-    float *tree = scratch().tree_vals.as<float>(a->T ? a->T : 1);
-    float *rb = scratch().rb.as<float>(a->P ? a->P : 1);
+    T *tree = (T *)scratch().tree_vals.get((a->T ? a->T : 1) * sizeof(T));
+    T *rb = (T *)scratch().rb.get((a->P ? a->P : 1) * sizeof(T));
     const uint64_t *xz = (const uint64_t *)a->xz_end.p;
     const uint16_t *yv = (const uint16_t *)a->y_vec.p;
     const uint64_t *txz = (const uint64_t *)a->t_xz_end.p;
     const uint16_t *tyv = (const uint16_t *)a->t_y_vec.p;
     for (int it = 0; it < niter; ++it) {
         // rb = in / conv(psf_flipped, out); out = out * conv(psf, rb)  (APRNumerics.hpp:565-570)
-        filter_apply(a->g, xz, yv, a->tg, txz, tyv, a->fi, out, tree, &plan_f, df, rb, 1, in, scratch().fb, s);
-        filter_apply(a->g, xz, yv, a->tg, txz, tyv, a->fi, rb, tree, &plan, dp, out, 2, nullptr, scratch().fb, s);
+        filter_apply<T>(a->g, xz, yv, a->tg, txz, tyv, a->fi, out, tree, &plan_f, df, rb, 1, in, scratch().fb, s);
+        filter_apply<T>(a->g, xz, yv, a->tg, txz, tyv, a->fi, rb, tree, &plan, dp, out, 2, nullptr, scratch().fb, s);
     }
 }
 
@@ -828,7 +835,7 @@ aprb_status aprb_fill_tree_mean_device(aprb_apr *a, const float *parts_dev, floa
         ARG_CHECK(a && parts_dev && tree_dev, "null argument");
         cudaStream_t s = (cudaStream_t)stream;
         ensure_tree(a, s);
-        filter_apply(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
+        filter_apply<float>(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
                      (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, a->fi, parts_dev, tree_dev, nullptr,
                      nullptr, nullptr, 0, nullptr, scratch().fb, s);
     });
@@ -843,7 +850,7 @@ aprb_status aprb_fill_tree_mean(aprb_apr *a, const float *parts, float *tree) {
         float *dp = scratch().parts_f.as<float>(a->P ? a->P : 1);
         float *dt = scratch().out_f.as<float>(a->T ? a->T : 1);
         APRB_CUDA(cudaMemcpyAsync(dp, parts, a->P * sizeof(float), cudaMemcpyHostToDevice, s));
-        filter_apply(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
+        filter_apply<float>(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
                      (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, a->fi, dp, dt, nullptr, nullptr,
                      nullptr, 0, nullptr, scratch().fb, s);
         APRB_CUDA(cudaMemcpyAsync(tree, dt, a->T * sizeof(float), cudaMemcpyDeviceToHost, s));
@@ -882,7 +889,7 @@ aprb_status aprb_richardson_lucy_device(aprb_apr *a, const uint16_t *in_dev, flo
     return guarded([&] {
         require_device();
         ARG_CHECK(a && in_dev && out_dev && psf && niter >= 0, "invalid argument");
-        rl_impl(a, in_dev, out_dev, psf, ksize, niter, use_stencil_downsample, normalize, resume,
+        rl_impl<float>(a, in_dev, out_dev, psf, ksize, niter, use_stencil_downsample, normalize, resume,
                 (cudaStream_t)stream);
     });
 }
@@ -897,8 +904,35 @@ aprb_status aprb_richardson_lucy(aprb_apr *a, const uint16_t *in, float *out, co
         float *dout = scratch().out_f.as<float>(a->P ? a->P : 1);
         APRB_CUDA(cudaMemcpyAsync(di, in, a->P * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
         if (resume) APRB_CUDA(cudaMemcpyAsync(dout, out, a->P * sizeof(float), cudaMemcpyHostToDevice, s));
-        rl_impl(a, di, dout, psf, ksize, niter, use_stencil_downsample, normalize, resume, s);
+        rl_impl<float>(a, di, dout, psf, ksize, niter, use_stencil_downsample, normalize, resume, s);
         APRB_CUDA(cudaMemcpyAsync(out, dout, a->P * sizeof(float), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+aprb_status aprb_richardson_lucy_fp64_device(aprb_apr *a, const uint16_t *in_dev, double *out_dev, const float *psf,
+                                             int ksize, int niter, int use_stencil_downsample, int normalize,
+                                             int resume, void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && in_dev && out_dev && psf && niter >= 0, "invalid argument");
+        rl_impl<double>(a, in_dev, out_dev, psf, ksize, niter, use_stencil_downsample, normalize, resume,
+                        (cudaStream_t)stream);
+    });
+}
+
+aprb_status aprb_richardson_lucy_fp64(aprb_apr *a, const uint16_t *in, double *out, const float *psf, int ksize,
+                                      int niter, int use_stencil_downsample, int normalize, int resume) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && in && out && psf && niter >= 0, "invalid argument");
+        cudaStream_t s = cudaStreamPerThread;
+        uint16_t *di = scratch().parts_u16.as<uint16_t>(a->P ? a->P : 1);
+        double *dout = (double *)scratch().out_f.get((a->P ? a->P : 1) * sizeof(double));
+        APRB_CUDA(cudaMemcpyAsync(di, in, a->P * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+        if (resume) APRB_CUDA(cudaMemcpyAsync(dout, out, a->P * sizeof(double), cudaMemcpyHostToDevice, s));
+        rl_impl<double>(a, di, dout, psf, ksize, niter, use_stencil_downsample, normalize, resume, s);
+        APRB_CUDA(cudaMemcpyAsync(out, dout, a->P * sizeof(double), cudaMemcpyDeviceToHost, s));
         APRB_CUDA(cudaStreamSynchronize(s));
     });
 }
@@ -912,6 +946,18 @@ aprb_status aprb_synth_blobs_u16(uint16_t *img_dev, int y_num, int x_num, int z_
         static thread_local DevBuf buf;
         launch_synth_blobs(img_dev, y_num, x_num, z_num, n_blobs, sigma_lo, sigma_hi, amp_lo, amp_hi, background,
                            seed, buf, (cudaStream_t)stream);
+    });
+}
+
+aprb_status aprb_synth_blobs_f32(float *img_dev, int y_num, int x_num, int z_num, int n_blobs, float sigma_lo,
+                                 float sigma_hi, float amp_lo, float amp_hi, float background, uint64_t seed,
+                                 void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(img_dev && y_num > 0 && x_num > 0 && z_num > 0 && n_blobs >= 0, "invalid argument");
+        static thread_local DevBuf buf;
+        launch_synth_blobs(img_dev, y_num, x_num, z_num, n_blobs, sigma_lo, sigma_hi, amp_lo, amp_hi, background, seed,
+                           buf, (cudaStream_t)stream);
     });
 }
 

@@ -29,8 +29,33 @@ namespace aprb {
 
 namespace {
 
-constexpr uint32_t kMissingBits = 0x7fbadbadu;  // NaN payload marking an uncovered cell
-constexpr int kYC = 64;                         // y chunk of the row index
+constexpr uint32_t kMissingBits = 0x7fbadbadu;               // NaN payload marking an uncovered cell
+constexpr uint64_t kMissingBits64 = 0x7ff7badbadbadbadull;  // the same for double values
+constexpr int kYC = 64;                                      // y chunk of the row index
+
+// Value type of the filter: float, or double for the FP64 instantiation of
+// richardson_lucy.  Arithmetic goes through the round-to-nearest intrinsics
+// so no contraction can change a result.
+template <typename T>
+struct VT;
+template <>
+struct VT<float> {
+    static __device__ __forceinline__ float miss() { return __uint_as_float(kMissingBits); }
+    static __device__ __forceinline__ bool is_miss(float v) { return __float_as_uint(v) == kMissingBits; }
+    static __device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+    static __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+    static __device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+};
+template <>
+struct VT<double> {
+    static __device__ __forceinline__ double miss() { return __longlong_as_double((long long)kMissingBits64); }
+    static __device__ __forceinline__ bool is_miss(double v) {
+        return (uint64_t)__double_as_longlong(v) == kMissingBits64;
+    }
+    static __device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+    static __device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+    static __device__ __forceinline__ double div(double a, double b) { return __ddiv_rn(a, b); }
+};
 
 struct LD {
     int yn, xn, zn;
@@ -88,13 +113,14 @@ struct TreeLevelArgs {
     const uint16_t *t_cidx, *c_cidx, *ct_cidx;
 };
 
+template <typename T>
 __global__ void __launch_bounds__(128) tree_mean_kernel(TreeLevelArgs a, const uint64_t *__restrict__ xz_end,
                                                         const uint16_t *__restrict__ y_vec,
-                                                        const float *__restrict__ parts,
+                                                        const T *__restrict__ parts,
                                                         const uint64_t *__restrict__ t_xz_end,
                                                         const uint16_t *__restrict__ t_y_vec,
-                                                        float *__restrict__ tree) {
-    __shared__ float sv[4][2 * kTW];
+                                                        T *__restrict__ tree) {
+    __shared__ T sv[4][2 * kTW];
     __shared__ uint8_t sk[4][2 * kTW];
     const uint64_t prow = blockIdx.x;  // parent row z*xt + x
     const int xp = (int)(prow % (uint64_t)a.dt.xn), zp = (int)(prow / (uint64_t)a.dt.xn);
@@ -145,7 +171,7 @@ __global__ void __launch_bounds__(128) tree_mean_kernel(TreeLevelArgs a, const u
         const int y = t_y_vec[i];
         const float s = (y == a.dt.yn - 1) ? syxz : sxz;
         const int o = 2 * (y - y0);
-        float acc = 0.0f;
+        T acc = T(0);
 #pragma unroll
         for (int kind = 1; kind <= 2; ++kind)
 #pragma unroll
@@ -153,7 +179,7 @@ __global__ void __launch_bounds__(128) tree_mean_kernel(TreeLevelArgs a, const u
 #pragma unroll
                 for (int d = 0; d < 2; ++d)
                     if (o + d < cy1 - cy0 && sk[q][o + d] == kind)
-                        acc = __fadd_rn(__fdiv_rn(__fmul_rn(s, sv[q][o + d]), 8.0f), acc);
+                        acc = VT<T>::add(VT<T>::div(VT<T>::mul(T(s), sv[q][o + d]), T(8)), acc);
         tree[i] = acc;
     }
 }
@@ -174,24 +200,24 @@ struct ConvLevelArgs {
     int mode;
 };
 
-template <int R>
+template <int R, typename T>
 struct ConvSmem {
     static constexpr int S = 2 * R + 1, RX = kBX + 2 * R, RY = kBY + 2 * R;
-    float ring[S][RX][RY];
-    float st[S * S * S];
+    T ring[S][RX][RY];
+    T st[S * S * S];
     uint64_t ob[kBX];
     int ocnt[kBX + 1];
 };
 
 // Fills one slice row (level row (zr, xr) over the y window) of the ring.
-template <int R>
-__device__ void fill_slice_row(float *__restrict__ rowbuf, int zr, int xr, int y0, const ConvLevelArgs &a,
+template <int R, typename T>
+__device__ void fill_slice_row(T *__restrict__ rowbuf, int zr, int xr, int y0, const ConvLevelArgs &a,
                                const uint64_t *__restrict__ xz_end, const uint16_t *__restrict__ y_vec,
-                               const float *__restrict__ in, const uint64_t *__restrict__ t_xz_end,
-                               const uint16_t *__restrict__ t_y_vec, const float *__restrict__ tree, int lane) {
+                               const T *__restrict__ in, const uint64_t *__restrict__ t_xz_end,
+                               const uint16_t *__restrict__ t_y_vec, const T *__restrict__ tree, int lane) {
     constexpr int RY = kBY + 2 * R;
     const int ys = y0 - R;  // y of rowbuf[0]
-    const float miss = __uint_as_float(kMissingBits);
+    const T miss = VT<T>::miss();
     for (int k = lane; k < RY; k += 32) rowbuf[k] = miss;
     __syncwarp();
     const int ya = max(ys, 0), yb = min(ys + RY - 1, a.d.yn - 1);  // real y range needed
@@ -215,7 +241,7 @@ __device__ void fill_slice_row(float *__restrict__ rowbuf, int zr, int xr, int y
             for (uint64_t i = s + lane; i < e; i += 32) {
                 const int yp = y_vec[i];
                 if (2 * yp > yb) break;
-                const float v = in[i];
+                const T v = in[i];
                 const int c0 = 2 * yp, c1 = min(2 * yp + 1, a.d.yn - 1);
                 if (c0 >= ya) rowbuf[c0 - ys] = v;
                 if (c1 != c0 && c1 >= ya && c1 <= yb) rowbuf[c1 - ys] = v;
@@ -237,7 +263,7 @@ __device__ void fill_slice_row(float *__restrict__ rowbuf, int zr, int xr, int y
         const int y = ys + k;
         if (y >= 0 && y < a.d.yn) continue;
         if (!a.reflect) {
-            rowbuf[k] = 0.0f;
+            rowbuf[k] = T(0);
         } else {
             const int r = y < 0 ? -y : 2 * (a.d.yn - 1) - y;
             rowbuf[k] = (r >= 0 && r < a.d.yn && r - ys >= 0 && r - ys < RY) ? rowbuf[r - ys] : miss;
@@ -245,34 +271,33 @@ __device__ void fill_slice_row(float *__restrict__ rowbuf, int zr, int xr, int y
     }
 }
 
-template <int R>
+template <int R, typename T>
 __global__ void __launch_bounds__(32 * (kBX + 2 * R)) conv_tile_kernel(
     ConvLevelArgs a, const uint64_t *__restrict__ xz_end, const uint16_t *__restrict__ y_vec,
-    const float *__restrict__ in, const uint64_t *__restrict__ t_xz_end, const uint16_t *__restrict__ t_y_vec,
-    const float *__restrict__ tree, const float *__restrict__ stencil, float *__restrict__ out,
+    const T *__restrict__ in, const uint64_t *__restrict__ t_xz_end, const uint16_t *__restrict__ t_y_vec,
+    const T *__restrict__ tree, const T *__restrict__ stencil, T *__restrict__ out,
     const uint16_t *__restrict__ rl_in, unsigned long long *stale) {
     constexpr int S = 2 * R + 1, RX = kBX + 2 * R, RY = kBY + 2 * R, NT = 32 * RX;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    ConvSmem<R> &sm = *reinterpret_cast<ConvSmem<R> *>(smem_raw);
+    ConvSmem<R, T> &sm = *reinterpret_cast<ConvSmem<R, T> *>(smem_raw);
     const int x0 = blockIdx.x * kBX, y0 = blockIdx.y * kBY, z0 = blockIdx.z * kBZ;
     const int z1 = min(z0 + kBZ, a.d.zn);
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int k = threadIdx.x; k < S * S * S; k += NT) sm.st[k] = stencil[k];
     unsigned nstale = 0;
-    const uint32_t missb = kMissingBits;
     const int nc = nchunk(a.d.yn);
 
     // warp w fills ring row w of the slice at z (z may lie outside the level)
     auto load_slice = [&](int zq) {
-        float(*slot)[RY] = sm.ring[(zq - (z0 - R)) % S];
+        T(*slot)[RY] = sm.ring[(zq - (z0 - R)) % S];
         bool ok = true;
         const int zr = reflect_idx(zq, a.d.zn, a.reflect, ok);
         const int xr = reflect_idx(x0 - R + w, a.d.xn, a.reflect, ok);
         if (!ok) {
-            const float v = a.reflect ? __uint_as_float(missb) : 0.0f;
+            const T v = a.reflect ? VT<T>::miss() : T(0);
             for (int k = lane; k < RY; k += 32) slot[w][k] = v;
         } else {
-            fill_slice_row<R>(slot[w], zr, xr, y0, a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, lane);
+            fill_slice_row<R, T>(slot[w], zr, xr, y0, a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, lane);
         }
     };
 
@@ -304,22 +329,22 @@ __global__ void __launch_bounds__(32 * (kBX + 2 * R)) conv_tile_kernel(
             while (q + 1 < kBX && sm.ocnt[q + 1] <= k) ++q;
             const uint64_t i = sm.ob[q] + (uint64_t)(k - sm.ocnt[q]);
             const int yy = (int)y_vec[i] - (y0 - R);  // ring column of the particle
-            float val = 0.0f;
+            T val = T(0);
             int cnt = 0;
 #pragma unroll
             for (int iz = 0; iz < S; ++iz) {
-                const float(*slot)[RY] = sm.ring[(z + iz - R - (z0 - R)) % S];
+                const T(*slot)[RY] = sm.ring[(z + iz - R - (z0 - R)) % S];
 #pragma unroll
                 for (int ix = 0; ix < S; ++ix) {
-                    const float *rowp = slot[q + ix] + (yy - R);
+                    const T *rowp = slot[q + ix] + (yy - R);
 #pragma unroll
                     for (int iy = 0; iy < S; ++iy) {
-                        float v = rowp[iy];
-                        if (__float_as_uint(v) == missb) {
-                            v = 0.0f;
+                        T v = rowp[iy];
+                        if (VT<T>::is_miss(v)) {
+                            v = T(0);
                             nstale++;
                         }
-                        val = __fadd_rn(val, __fmul_rn(v, sm.st[cnt]));
+                        val = VT<T>::add(val, VT<T>::mul(v, sm.st[cnt]));
                         cnt++;
                     }
                 }
@@ -327,24 +352,24 @@ __global__ void __launch_bounds__(32 * (kBX + 2 * R)) conv_tile_kernel(
             if (a.mode == 0)
                 out[i] = val;
             else if (a.mode == 1)
-                out[i] = (float)rl_in[i] / val;
+                out[i] = VT<T>::div((T)rl_in[i], val);
             else
-                out[i] = out[i] * val;
+                out[i] = VT<T>::mul(out[i], val);
         }
         __syncthreads();
     }
     if (nstale) atomicAdd(stale, (unsigned long long)nstale);
 }
 
-template <int R>
-void launch_conv_level(const ConvLevelArgs &a, const uint64_t *xz_end, const uint16_t *y_vec, const float *in,
-                       const uint64_t *t_xz_end, const uint16_t *t_y_vec, const float *tree, const float *st,
-                       float *out, const uint16_t *rl_in, unsigned long long *stale, cudaStream_t s) {
-    const size_t smem = sizeof(ConvSmem<R>);
-    APRB_CUDA(cudaFuncSetAttribute(conv_tile_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+template <int R, typename T>
+void launch_conv_level(const ConvLevelArgs &a, const uint64_t *xz_end, const uint16_t *y_vec, const T *in,
+                       const uint64_t *t_xz_end, const uint16_t *t_y_vec, const T *tree, const T *st, T *out,
+                       const uint16_t *rl_in, unsigned long long *stale, cudaStream_t s) {
+    const size_t smem = sizeof(ConvSmem<R, T>);
+    APRB_CUDA(cudaFuncSetAttribute(conv_tile_kernel<R, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((a.d.xn + kBX - 1) / kBX, (a.d.yn + kBY - 1) / kBY, (a.d.zn + kBZ - 1) / kBZ);
-    conv_tile_kernel<R><<<grid, 32 * (kBX + 2 * R), smem, s>>>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st, out,
-                                                               rl_in, stale);
+    conv_tile_kernel<R, T><<<grid, 32 * (kBX + 2 * R), smem, s>>>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st,
+                                                                  out, rl_in, stale);
     count_launch();
     APRB_CHECK_LAUNCH();
 }
@@ -390,10 +415,11 @@ void build_filter_index(const Geom &g, const uint64_t *xz_end, const uint16_t *y
     fi.built = true;
 }
 
+template <typename T>
 void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
-                  const uint64_t *t_xz_end, const uint16_t *t_y_vec, const FilterIndex &fi, const float *in,
-                  float *tree, const ConvPlan *plan, const float *d_stencils, float *out, int mode,
-                  const uint16_t *rl_in, FilterBuffers &fb, cudaStream_t s) {
+                  const uint64_t *t_xz_end, const uint16_t *t_y_vec, const FilterIndex &fi, const T *in, T *tree,
+                  const ConvPlan *plan, const T *d_stencils, T *out, int mode, const uint16_t *rl_in,
+                  FilterBuffers &fb, cudaStream_t s) {
     APRB_PROF(plan ? "convolve" : "fill_tree_mean", s);
     const int L = g.l_max;
     const uint16_t *cbase = (const uint16_t *)fi.buf.p;
@@ -416,7 +442,7 @@ void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, 
         const unsigned ych = (unsigned)((ta.dt.yn + kTW - 1) / kTW);
         if (rows == 0 || ych == 0) continue;
         dim3 grid((unsigned)rows, ych);
-        tree_mean_kernel<<<grid, 128, 0, s>>>(ta, xz_end, y_vec, in, t_xz_end, t_y_vec, tree);
+        tree_mean_kernel<T><<<grid, 128, 0, s>>>(ta, xz_end, y_vec, in, t_xz_end, t_y_vec, tree);
         count_launch();
     }
     APRB_CHECK_LAUNCH();
@@ -439,13 +465,20 @@ void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, 
         a.tcidx = l <= tg.l_max ? cbase + fi.tree_off[l] : nullptr;
         a.reflect = plan->reflect;
         a.mode = mode;
-        const float *st = d_stencils + plan->offsets[sn];
+        const T *st = d_stencils + plan->offsets[sn];
         if (side == 3)
-            launch_conv_level<1>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st, out, rl_in, stale, s);
+            launch_conv_level<1, T>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st, out, rl_in, stale, s);
         else
-            launch_conv_level<2>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st, out, rl_in, stale, s);
+            launch_conv_level<2, T>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st, out, rl_in, stale, s);
     }
 }
+
+template void filter_apply<float>(const Geom &, const uint64_t *, const uint16_t *, const Geom &, const uint64_t *,
+                                  const uint16_t *, const FilterIndex &, const float *, float *, const ConvPlan *,
+                                  const float *, float *, int, const uint16_t *, FilterBuffers &, cudaStream_t);
+template void filter_apply<double>(const Geom &, const uint64_t *, const uint16_t *, const Geom &, const uint64_t *,
+                                   const uint16_t *, const FilterIndex &, const double *, double *, const ConvPlan *,
+                                   const double *, double *, int, const uint16_t *, FilterBuffers &, cudaStream_t);
 
 uint64_t filter_stale_count(FilterBuffers &fb, cudaStream_t s) {
     unsigned long long v = 0;

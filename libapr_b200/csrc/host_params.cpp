@@ -136,13 +136,14 @@ uint64_t tree_geometry(int y, int x, int z, Geom &g) {
     return xz_linear(g);
 }
 
-std::vector<float> downsampled_stencils(const float *in, int ks, int nlevels, bool normalize, std::vector<int> &sides) {
+template <typename T>
+std::vector<T> downsampled_stencils(const T *in, int ks, int nlevels, bool normalize, std::vector<int> &sides) {
     if (nlevels < 1) nlevels = 1;
     const int n0 = ks * ks * ks;
-    std::vector<float> out(in, in + n0);
-    if (normalize) {  // PixelData::normalize (PixelData.hpp:771-778)
+    std::vector<T> out(in, in + n0);
+    if (normalize) {  // PixelData::normalize (PixelData.hpp:771-778): the sum is a float
         float s = 0.0f;
-        for (int i = 0; i < n0; ++i) s = s + out[i];
+        for (int i = 0; i < n0; ++i) s = (float)(s + out[i]);
         if (std::fabs(s) > 1e-6 && s != 1.0f)
             for (int i = 0; i < n0; ++i) out[i] = out[i] / s;
     }
@@ -152,7 +153,7 @@ std::vector<float> downsampled_stencils(const float *in, int ks, int nlevels, bo
         const int factor = (int)std::pow((float)step, 3.0f);
         int nd = 2 * (((ks - 1) / 2 + step - 1) / step) + 1;
         if (nd < 3) nd = 3;
-        std::vector<float> o((size_t)nd * nd * nd, 0.0f);
+        std::vector<T> o((size_t)nd * nd * nd, T(0));
         const int off = (nd / 2) * step - ks / 2;
         for (int iz = 0; iz < ks; ++iz)
             for (int ix = 0; ix < ks; ++ix)
@@ -171,10 +172,10 @@ std::vector<float> downsampled_stencils(const float *in, int ks, int nlevels, bo
                             }
                         }
                     }
-        float sum = 0;
+        float sum = 0;  // a float in the reference for every stencil type
         for (auto &v : o) {
             v /= factor;
-            sum += v;
+            sum = (float)(sum + v);
         }
         if (normalize) {
             float nf = 1.0f / sum;
@@ -185,5 +186,8 @@ std::vector<float> downsampled_stencils(const float *in, int ks, int nlevels, bo
     }
     return out;
 }
+
+template std::vector<float> downsampled_stencils<float>(const float *, int, int, bool, std::vector<int> &);
+template std::vector<double> downsampled_stencils<double>(const double *, int, int, bool, std::vector<int> &);
 
 }  // namespace aprb

@@ -41,7 +41,8 @@ uint64_t tree_geometry(int y, int x, int z, Geom &g);
 
 // APRStencil::get_downsampled_stencils (APRStencil.hpp:13-95) for a cubic
 // stencil of side ks: nlevels stencils packed back to back; sides[i] their side.
-std::vector<float> downsampled_stencils(const float *stencil, int ks, int nlevels, bool normalize,
-                                        std::vector<int> &sides);
+// T = float, or double for the FP64 instantiation of richardson_lucy.
+template <typename T>
+std::vector<T> downsampled_stencils(const T *stencil, int ks, int nlevels, bool normalize, std::vector<int> &sides);
 
 }  // namespace aprb

@@ -106,14 +106,18 @@ struct FilterIndex {
 };
 void build_filter_index(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
                         const uint64_t *t_xz_end, const uint16_t *t_y_vec, FilterIndex &fi, cudaStream_t s);
+// T = float, or double for the FP64 instantiation of richardson_lucy
+template <typename T>
 void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
-                  const uint64_t *t_xz_end, const uint16_t *t_y_vec, const FilterIndex &fi, const float *in,
-                  float *tree, const ConvPlan *plan, const float *d_stencils, float *out, int mode,
-                  const uint16_t *rl_in, FilterBuffers &fb, cudaStream_t s);
+                  const uint64_t *t_xz_end, const uint16_t *t_y_vec, const FilterIndex &fi, const T *in, T *tree,
+                  const ConvPlan *plan, const T *d_stencils, T *out, int mode, const uint16_t *rl_in,
+                  FilterBuffers &fb, cudaStream_t s);
 uint64_t filter_stale_count(FilterBuffers &fb, cudaStream_t s);
 
 // ---- synth.cu
-void launch_synth_blobs(uint16_t *img, int yn, int xn, int zn, int n_blobs, float slo, float shi, float alo,
-                        float ahi, float bg, uint64_t seed, DevBuf &blobs, cudaStream_t s);
+// OutT uint16_t: blobs + Poisson noise; OutT float: the noise-free intensity
+template <typename OutT>
+void launch_synth_blobs(OutT *img, int yn, int xn, int zn, int n_blobs, float slo, float shi, float alo, float ahi,
+                        float bg, uint64_t seed, DevBuf &blobs, cudaStream_t s);
 
 }  // namespace aprb

@@ -533,10 +533,21 @@ __device__ __forceinline__ float sat_y_value(int i, int n, float d, float cm /*C
 // shift window of 2*OFF+2 entries; tiles through shared memory as in the IIR.
 // absdiff_ref != nullptr makes the input |in - absdiff_ref| (calc_abs_diff,
 // :188-196) on the fly.
+// Reads of the padded image folded into the first y pass: padded (y, x, z)
+// maps to the unpadded image by reflection about the edge sample (paddPixels,
+// PixelData.hpp:1071-1178).  on_in maps the input, on_ref the |in - ref| operand.
+struct PadMap {
+    int on_in, on_ref;
+    int sy, sx, sz, yd, xd, zd, px;
+};
+
+__device__ __forceinline__ int reflect101(int i, int n) { return i < 0 ? -i : (i > n - 1 ? 2 * (n - 1) - i : i); }
+
 template <int OFF>
 __global__ void __launch_bounds__(kYWarps * 32) sat_y_kernel(const float *__restrict__ in,
                                                               const float *__restrict__ absdiff_ref,
-                                                              float *__restrict__ out, int n, uint64_t nlines) {
+                                                              float *__restrict__ out, int n, uint64_t nlines,
+                                                              PadMap pm) {
     constexpr int W = 2 * OFF + 2;
     __shared__ float tin[kYWarps][kTile][kTile + 1];
     __shared__ float tout[kYWarps][kTile][kTile + 1];
@@ -549,13 +560,23 @@ __global__ void __launch_bounds__(kYWarps * 32) sat_y_kernel(const float *__rest
 #pragma unroll
     for (int q = 0; q < W; ++q) c[q] = 0.0f;
     float C = 0.0f;
+    // unpadded row start of line line0 + lane when the reads are reflected
+    uint64_t mbase = 0;
+    if ((pm.on_in | pm.on_ref) && valid) {
+        const uint64_t ln = line0 + lane;
+        const int xp = (int)(ln % (uint64_t)pm.px), zp = (int)(ln / (uint64_t)pm.px);
+        mbase = idx3(0, reflect101(xp - pm.sx, pm.xd), reflect101(zp - pm.sz, pm.zd), pm.yd, pm.xd);
+    }
     for (int y0 = 0; y0 < n; y0 += kTile) {
+        const int my = (pm.on_in | pm.on_ref) ? reflect101(y0 + lane - pm.sy, pm.yd) : 0;
         for (int j = 0; j < kTile; ++j) {
-            uint64_t ln = line0 + j;
+            const uint64_t ln = line0 + j;
+            const uint64_t bj = __shfl_sync(0xffffffffu, mbase, j);
             if (ln < nlines && y0 + lane < n) {
-                uint64_t a = ln * (uint64_t)n + y0 + lane;
-                float v = in[a];
-                if (absdiff_ref) v = fabsf(v - absdiff_ref[a]);
+                const uint64_t a = ln * (uint64_t)n + y0 + lane;
+                const uint64_t am = bj + (uint64_t)my;
+                float v = in[pm.on_in ? am : a];
+                if (absdiff_ref) v = fabsf(v - absdiff_ref[pm.on_ref ? am : a]);
                 tin[w][j][lane] = v;
             }
         }
@@ -594,35 +615,73 @@ __global__ void __launch_bounds__(kYWarps * 32) sat_y_kernel(const float *__rest
     }
 }
 
-// x / z box mean (:364-494): one thread per strided line, coalesced over y.
-template <int OFF>
-__global__ void sat_strided_kernel(const float *__restrict__ in, const float *__restrict__ absdiff_ref,
-                                   float *__restrict__ out, int yn, int n, uint64_t stride, uint64_t outer_stride,
-                                   uint64_t nlines) {
-    constexpr int W = 2 * OFF + 2;
+#ifndef APRB_SAT_PREFETCH
+#define APRB_SAT_PREFETCH 8
+#endif
+
+// Final pass writing the unpadded window times the rescale factor
+// (unpaddPixels + rescale_var, LocalIntensityScale.hpp:174-184) directly.
+struct LisOut {
+    float *out;
+    int sy, sx, sz, yd, xd, zd, axis;
+    float rescale;
+};
+
+// x / z box mean (:364-494): one thread per strided line, coalesced over y,
+// with the next U samples of the line in flight.
+template <int OFF, bool FINAL>
+__global__ void __launch_bounds__(128) sat_strided_kernel(const float *__restrict__ in,
+                                                          const float *__restrict__ absdiff_ref,
+                                                          float *__restrict__ out, int yn, int n, uint64_t stride,
+                                                          uint64_t outer_stride, uint64_t nlines, LisOut fo) {
+    constexpr int W = 2 * OFF + 2, U = APRB_SAT_PREFETCH;
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= nlines) return;
     const uint64_t y = g % (uint64_t)yn, o = g / (uint64_t)yn;
     const uint64_t base = o * outer_stride + y;
+    auto ld = [&](int j) {
+        const uint64_t a = base + (uint64_t)j * stride;
+        float v = in[a];
+        if (absdiff_ref) v = fabsf(v - absdiff_ref[a]);
+        return v;
+    };
+    auto emit = [&](int i, float v) {
+        if (!FINAL) {
+            out[base + (uint64_t)i * stride] = v;
+            return;
+        }
+        const int xpad = fo.axis == 1 ? i : (int)o, zpad = fo.axis == 1 ? (int)o : i;
+        const int uy = (int)y - fo.sy, ux = xpad - fo.sx, uz = zpad - fo.sz;
+        if (uy >= 0 && uy < fo.yd && ux >= 0 && ux < fo.xd && uz >= 0 && uz < fo.zd)
+            fo.out[idx3(uy, ux, uz, fo.yd, fo.xd)] = v * fo.rescale;
+    };
     float c[W];
 #pragma unroll
     for (int q = 0; q < W; ++q) c[q] = 0.0f;
+    float pre[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) pre[u] = u < n ? ld(u) : 0.0f;
     float C = 0.0f;
     const float dd = (float)(2 * OFF + 1);
-    for (int j = 0; j < n; ++j) {
-        uint64_t a = base + (uint64_t)j * stride;
-        float v = in[a];
-        if (absdiff_ref) v = fabsf(v - absdiff_ref[a]);
-        C = (j == 0) ? v : v + C;
+    for (int j0 = 0; j0 < n; j0 += U) {
 #pragma unroll
-        for (int q = 0; q < W - 1; ++q) c[q] = c[q + 1];
-        c[W - 1] = C;
-        const int i = j - OFF;
-        if (i >= 0) {
-            if (i < OFF + 1)
-                out[base + (uint64_t)i * stride] = C / (float)(i + OFF + 1);
-            else if (i < n - OFF)
-                out[base + (uint64_t)i * stride] = (C - c[0]) / dd;
+        for (int u = 0; u < U; ++u) {
+            const int j = j0 + u;
+            if (j < n) {
+                const float v = pre[u];
+                if (j + U < n) pre[u] = ld(j + U);
+                C = (j == 0) ? v : v + C;
+#pragma unroll
+                for (int q = 0; q < W - 1; ++q) c[q] = c[q + 1];
+                c[W - 1] = C;
+                const int i = j - OFF;
+                if (i >= 0) {
+                    if (i < OFF + 1)
+                        emit(i, C / (float)(i + OFF + 1));
+                    else if (i < n - OFF)
+                        emit(i, (C - c[0]) / dd);
+                }
+            }
         }
     }
     for (int i = n - OFF; i < n; ++i) {
@@ -632,7 +691,7 @@ __global__ void sat_strided_kernel(const float *__restrict__ in, const float *__
 #pragma unroll
         for (int q = 0; q < W; ++q)
             if (q == W - 1 - back) cm = c[q];
-        out[base + (uint64_t)i * stride] = (C - cm) / (float)(n - i + OFF);
+        emit(i, (C - cm) / (float)(n - i + OFF));
     }
 }
 
@@ -829,32 +888,36 @@ void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *id
 
 template <int OFF>
 static void sat_axis_t(const float *in, const float *absref, float *out, int py, int px, int pz, int axis,
-                       cudaStream_t s) {
+                       const PadMap &pm, const LisOut *fo, cudaStream_t s) {
     if (axis == 0) {
         const uint64_t nlines = (uint64_t)px * pz;
-        sat_y_kernel<OFF><<<blocks_for(nlines, kYWarps * kTile), kYWarps * 32, 0, s>>>(in, absref, out, py, nlines);
-    } else if (axis == 1) {
-        const uint64_t nlines = (uint64_t)py * pz;
-        sat_strided_kernel<OFF><<<blocks_for(nlines, 128), 128, 0, s>>>(in, absref, out, py, px, (uint64_t)py,
-                                                                       (uint64_t)px * py, nlines);
+        sat_y_kernel<OFF><<<blocks_for(nlines, kYWarps * kTile), kYWarps * 32, 0, s>>>(in, absref, out, py, nlines,
+                                                                                    pm);
     } else {
-        const uint64_t nlines = (uint64_t)py * px;
-        sat_strided_kernel<OFF><<<blocks_for(nlines, 128), 128, 0, s>>>(in, absref, out, py, pz, (uint64_t)px * py,
-                                                                       (uint64_t)py, nlines);
+        const uint64_t nlines = axis == 1 ? (uint64_t)py * pz : (uint64_t)py * px;
+        const int n = axis == 1 ? px : pz;
+        const uint64_t stride = axis == 1 ? (uint64_t)py : (uint64_t)px * py;
+        const uint64_t outer = axis == 1 ? (uint64_t)px * py : (uint64_t)py;
+        if (fo)
+            sat_strided_kernel<OFF, true><<<blocks_for(nlines, 128), 128, 0, s>>>(in, absref, nullptr, py, n, stride,
+                                                                                  outer, nlines, *fo);
+        else
+            sat_strided_kernel<OFF, false><<<blocks_for(nlines, 128), 128, 0, s>>>(in, absref, out, py, n, stride,
+                                                                                   outer, nlines, LisOut{});
     }
     count_launch();
     APRB_CHECK_LAUNCH();
 }
 
 static void sat_axis(const float *in, const float *absref, float *out, int py, int px, int pz, int axis, int off,
-                     cudaStream_t s) {
+                     const PadMap &pm, const LisOut *fo, cudaStream_t s) {
     switch (off) {
-        case 1: sat_axis_t<1>(in, absref, out, py, px, pz, axis, s); break;
-        case 2: sat_axis_t<2>(in, absref, out, py, px, pz, axis, s); break;
-        case 3: sat_axis_t<3>(in, absref, out, py, px, pz, axis, s); break;
-        case 4: sat_axis_t<4>(in, absref, out, py, px, pz, axis, s); break;
-        case 5: sat_axis_t<5>(in, absref, out, py, px, pz, axis, s); break;
-        case 6: sat_axis_t<6>(in, absref, out, py, px, pz, axis, s); break;
+        case 1: sat_axis_t<1>(in, absref, out, py, px, pz, axis, pm, fo, s); break;
+        case 2: sat_axis_t<2>(in, absref, out, py, px, pz, axis, pm, fo, s); break;
+        case 3: sat_axis_t<3>(in, absref, out, py, px, pz, axis, pm, fo, s); break;
+        case 4: sat_axis_t<4>(in, absref, out, py, px, pz, axis, pm, fo, s); break;
+        case 5: sat_axis_t<5>(in, absref, out, py, px, pz, axis, pm, fo, s); break;
+        case 6: sat_axis_t<6>(in, absref, out, py, px, pz, axis, pm, fo, s); break;
         default: set_error("unsupported local intensity scale window"); throw Error{APRB_ERR_UNSUPPORTED};
     }
 }
@@ -887,39 +950,61 @@ void launch_local_intensity_scale(const float *ids, float *lis, int yd, int xd, 
     }
     const int py = yd + 2 * sy, px = xd + 2 * sx, pz = zd + 2 * sz;
     const int pd[3] = {py, px, pz};
-    for (int a = 0; a < 3; ++a)
+    int last = -1;
+    for (int a = 0; a < 3; ++a) {
         if (w.active[a] && pd[a] < 2 * std::max(w.win1[a], w.win2[a]) + 2) {
             set_error("local intensity scale window longer than the (padded) image axis");
             throw Error{APRB_ERR_UNSUPPORTED};
         }
+        if (w.active[a]) last = a;
+    }
+    // The padded copy is read only by the first pass of each window; when y is
+    // active that pass is a y pass, which reads the unpadded image through the
+    // reflection instead.  A final x or z pass writes the unpadded, rescaled
+    // window itself.
+    const bool fold_pad = w.active[0], fold_unpad = last >= 1;
     const uint64_t pn = (uint64_t)py * px * pz;
-    float *B = b.padded.as<float>(pn);
     float *A = b.a.as<float>(pn);
     float *C2 = b.c.as<float>(pn);
-    pad_reflect_kernel<<<blocks_for(pn, 256), 256, 0, s>>>(ids, yd, xd, zd, B, sy, sx, sz, py, px, pz);
-    count_launch();
-    APRB_CHECK_LAUNCH();
-    const float *src = B;
+    const float *padded = ids;
+    if (!fold_pad) {
+        float *B = b.padded.as<float>(pn);
+        pad_reflect_kernel<<<blocks_for(pn, 256), 256, 0, s>>>(ids, yd, xd, zd, B, sy, sx, sz, py, px, pz);
+        count_launch();
+        APRB_CHECK_LAUNCH();
+        padded = B;
+    }
+    const PadMap none{0, 0, 0, 0, 0, 1, 1, 1, 1};
+    const PadMap map_in{1, 0, sy, sx, sz, yd, xd, zd, px}, map_ref{0, 1, sy, sx, sz, yd, xd, zd, px};
+    const LisOut fo{lis, sy, sx, sz, yd, xd, zd, last, w.rescale};
+    const float *src = padded;
     float *bufs[2] = {A, C2};
     int nb = 0;
-    for (int a = 0; a < 3; ++a)
-        if (w.active[a]) {
-            sat_axis(src, nullptr, bufs[nb], py, px, pz, a, w.win1[a], s);
-            src = bufs[nb];
-            nb ^= 1;
-        }
     bool first = true;
     for (int a = 0; a < 3; ++a)
         if (w.active[a]) {
-            sat_axis(src, first ? B : nullptr, bufs[nb], py, px, pz, a, w.win2[a], s);
+            sat_axis(src, nullptr, bufs[nb], py, px, pz, a, w.win1[a], (first && fold_pad) ? map_in : none, nullptr,
+                     s);
             first = false;
             src = bufs[nb];
             nb ^= 1;
         }
-    unpad_rescale_kernel<<<blocks_for(nd, 256), 256, 0, s>>>(src, py, px, lis, yd, xd, zd, (py - yd) / 2,
-                                                            (px - xd) / 2, (pz - zd) / 2, w.rescale);
-    count_launch();
-    APRB_CHECK_LAUNCH();
+    first = true;
+    for (int a = 0; a < 3; ++a)
+        if (w.active[a]) {
+            const bool fin = fold_unpad && a == last;
+            sat_axis(src, first ? padded : nullptr, fin ? nullptr : bufs[nb], py, px, pz, a, w.win2[a],
+                     (first && fold_pad) ? map_ref : none, fin ? &fo : nullptr, s);
+            first = false;
+            src = bufs[nb];
+            nb ^= 1;
+        }
+    if (!fold_unpad) {
+        unpad_rescale_kernel<<<blocks_for(nd, 256), 256, 0, s>>>(src, py, px, lis, yd, xd, zd, (py - yd) / 2,
+                                                                (px - xd) / 2, (pz - zd) / 2, w.rescale);
+        count_launch();
+        APRB_CHECK_LAUNCH();
+    }
 }
 
 template <typename IT>

@@ -5,6 +5,7 @@
 // deviates use a counter-based generator per voxel: multiplication of
 // uniforms for small means, Hoermann's transformed rejection (PTRS, 1993)
 // otherwise.
+#include <type_traits>
 #include <vector>
 
 #include "kernels.cuh"
@@ -67,7 +68,11 @@ __device__ int poisson(double lam, Rng &r) {
     return (int)lam;
 }
 
-__global__ void render_kernel(uint16_t *__restrict__ img, int yn, int xn, int zn, const Blob *__restrict__ blobs,
+// NOISE: Poisson deviate clipped to uint16 (OutT uint16_t); otherwise the
+// noise-free intensity (OutT float), the ground truth of the deconvolution
+// workload.
+template <bool NOISE, typename OutT>
+__global__ void render_kernel(OutT *__restrict__ img, int yn, int xn, int zn, const Blob *__restrict__ blobs,
                               const uint32_t *__restrict__ boff, const uint32_t *__restrict__ bidx, int bx, int by,
                               float bg, uint64_t seed) {
     const int brick = blockIdx.x;
@@ -85,17 +90,22 @@ __global__ void render_kernel(uint16_t *__restrict__ img, int yn, int xn, int zn
             v += B.amp * expf(-(dy * dy + dx * dx + dz * dz) * B.inv2s2);
         }
         const uint64_t vox = idx3(y, x, z, yn, xn);
-        Rng r{mix64(seed ^ mix64(vox + 0x1234567ull))};
-        int p = poisson((double)v, r);
-        p = p < 0 ? 0 : (p > 65535 ? 65535 : p);
-        img[vox] = (uint16_t)p;
+        if (NOISE) {
+            Rng r{mix64(seed ^ mix64(vox + 0x1234567ull))};
+            int p = poisson((double)v, r);
+            p = p < 0 ? 0 : (p > 65535 ? 65535 : p);
+            img[vox] = (OutT)p;
+        } else {
+            img[vox] = (OutT)v;
+        }
     }
 }
 
 }  // namespace
 
-void launch_synth_blobs(uint16_t *img, int yn, int xn, int zn, int n_blobs, float slo, float shi, float alo,
-                        float ahi, float bg, uint64_t seed, DevBuf &buf, cudaStream_t s) {
+template <typename OutT>
+void launch_synth_blobs(OutT *img, int yn, int xn, int zn, int n_blobs, float slo, float shi, float alo, float ahi,
+                        float bg, uint64_t seed, DevBuf &buf, cudaStream_t s) {
     uint64_t st = seed * 0x2545F4914F6CDD1Dull + 0x632BE59BD9B4E019ull;
     std::vector<Blob> blobs((size_t)n_blobs);
     const int by = (yn + kBrick - 1) / kBrick, bx = (xn + kBrick - 1) / kBrick, bz = (zn + kBrick - 1) / kBrick;
@@ -140,10 +150,16 @@ void launch_synth_blobs(uint16_t *img, int yn, int xn, int zn, int n_blobs, floa
     APRB_CUDA(cudaMemcpyAsync(dB, blobs.data(), bytes_blobs, cudaMemcpyHostToDevice, s));
     APRB_CUDA(cudaMemcpyAsync(dO, count.data(), bytes_off, cudaMemcpyHostToDevice, s));
     if (bytes_idx) APRB_CUDA(cudaMemcpyAsync(dI, idx.data(), bytes_idx, cudaMemcpyHostToDevice, s));
-    render_kernel<<<(unsigned)nb, 256, 0, s>>>(img, yn, xn, zn, dB, dO, dI, bx, by, bg, seed);
+    render_kernel<std::is_same<OutT, uint16_t>::value, OutT>
+        <<<(unsigned)nb, 256, 0, s>>>(img, yn, xn, zn, dB, dO, dI, bx, by, bg, seed);
     count_launch();
     APRB_CHECK_LAUNCH();
     APRB_CUDA(cudaStreamSynchronize(s));  // host vectors go out of scope
 }
+
+template void launch_synth_blobs<uint16_t>(uint16_t *, int, int, int, int, float, float, float, float, float, uint64_t,
+                                           DevBuf &, cudaStream_t);
+template void launch_synth_blobs<float>(float *, int, int, int, int, float, float, float, float, float, uint64_t,
+                                        DevBuf &, cudaStream_t);
 
 }  // namespace aprb

@@ -67,3 +67,17 @@ def test_unsupported_psf_size(pair):
     img, acc, tr, apr, parts = pair
     with pytest.raises(RuntimeError):
         A.APRNumerics.richardson_lucy(apr, parts, None, np.ones(49, np.float32) / 49, 1)
+
+
+def test_richardson_lucy_fp64_bit_exact(pair):
+    """The reference's double instantiation on the GPU against the FP64 oracle."""
+    img, acc, tr, apr, parts = pair
+    psf = gaussian_psf()
+    ref = B.orc_richardson_lucy(acc, tr, parts, psf, 3, normalize=True, use_double=True)
+    out = A.APRNumerics.richardson_lucy(apr, parts, None, psf, 3, normalize=True, dtype=np.float64)
+    assert out.dtype == np.float64
+    assert np.array_equal(out.view(np.uint64), ref.view(np.uint64))
+    po = A.ParticleData(out.copy())
+    out2 = A.APRNumerics.richardson_lucy(apr, parts, po, psf, 2, normalize=True, resume=True)
+    ref2 = B.orc_richardson_lucy(acc, tr, parts, psf, 2, normalize=True, use_double=True, init=ref)
+    assert np.array_equal(out2.view(np.uint64), ref2.view(np.uint64))
