@@ -188,6 +188,7 @@ __global__ void __launch_bounds__(128) tree_mean_kernel(TreeLevelArgs a, const u
 // convolution of one level
 // ---------------------------------------------------------------------------
 constexpr int kBX = 8, kBY = 128, kBZ = 16;
+constexpr int kConvK = 4;  // output particles per thread and pass
 
 struct ConvLevelArgs {
     LD d;                 // level dims
@@ -219,42 +220,53 @@ __device__ void fill_slice_row(T *__restrict__ rowbuf, int zr, int xr, int y0, c
     const int ys = y0 - R;  // y of rowbuf[0]
     const T miss = VT<T>::miss();
     for (int k = lane; k < RY; k += 32) rowbuf[k] = miss;
-    __syncwarp();
     const int ya = max(ys, 0), yb = min(ys + RY - 1, a.d.yn - 1);  // real y range needed
     if (ya <= yb) {
+        // Bounds of the three sources inside the y window: same-level
+        // particles, parents one level coarser (each fills its y pair) and
+        // tree means of the same level.  They cover disjoint cells, so one
+        // merged pass writes them in any order.  Lanes 0-2 fetch the bounds.
         const uint64_t row = (uint64_t)zr * a.d.xn + xr;
         const int nc = nchunk(a.d.yn);
-        {  // same-level particles
-            const uint64_t b = xz_end[a.row_base + row - 1], e = xz_end[a.row_base + row];
-            const uint64_t s = b + a.cidx[row * (uint64_t)(nc + 1) + ya / kYC];
-            for (uint64_t i = s + lane; i < e; i += 32) {
-                const int y = y_vec[i];
-                if (y > yb) break;
-                if (y >= ya) rowbuf[y - ys] = in[i];
-            }
-        }
-        if (a.prow_base) {  // parents one level coarser fill their y pair
+        uint64_t lo = 0, hi = 0;
+        if (lane == 0) {
+            const uint64_t b = xz_end[a.row_base + row - 1];
+            hi = xz_end[a.row_base + row];
+            lo = b + a.cidx[row * (uint64_t)(nc + 1) + ya / kYC];
+        } else if (lane == 1 && a.prow_base) {
             const uint64_t prow = (uint64_t)(zr / 2) * a.dp.xn + xr / 2;
             const int npc = nchunk(a.dp.yn);
-            const uint64_t b = xz_end[a.prow_base + prow - 1], e = xz_end[a.prow_base + prow];
-            const uint64_t s = b + a.pcidx[prow * (uint64_t)(npc + 1) + (ya / 2) / kYC];
-            for (uint64_t i = s + lane; i < e; i += 32) {
-                const int yp = y_vec[i];
-                if (2 * yp > yb) break;
-                const T v = in[i];
-                const int c0 = 2 * yp, c1 = min(2 * yp + 1, a.d.yn - 1);
-                if (c0 >= ya) rowbuf[c0 - ys] = v;
-                if (c1 != c0 && c1 >= ya && c1 <= yb) rowbuf[c1 - ys] = v;
-            }
+            const uint64_t b = xz_end[a.prow_base + prow - 1];
+            hi = xz_end[a.prow_base + prow];
+            lo = b + a.pcidx[prow * (uint64_t)(npc + 1) + (ya / 2) / kYC];
+        } else if (lane == 2 && a.trow_base) {
+            const uint64_t b = t_xz_end[a.trow_base + row - 1];
+            hi = t_xz_end[a.trow_base + row];
+            lo = b + a.tcidx[row * (uint64_t)(nc + 1) + ya / kYC];
         }
-        if (a.trow_base) {  // tree means of the same level
-            const uint64_t b = t_xz_end[a.trow_base + row - 1], e = t_xz_end[a.trow_base + row];
-            const uint64_t s = b + a.tcidx[row * (uint64_t)(nc + 1) + ya / kYC];
-            for (uint64_t i = s + lane; i < e; i += 32) {
-                const int y = t_y_vec[i];
-                if (y > yb) break;
-                if (y >= ya) rowbuf[y - ys] = tree[i];
+        const uint64_t s0 = __shfl_sync(0xffffffffu, lo, 0), e0 = __shfl_sync(0xffffffffu, hi, 0);
+        const uint64_t s1 = __shfl_sync(0xffffffffu, lo, 1), e1 = __shfl_sync(0xffffffffu, hi, 1);
+        const uint64_t s2 = __shfl_sync(0xffffffffu, lo, 2), e2 = __shfl_sync(0xffffffffu, hi, 2);
+        __syncwarp();
+        bool go0 = true, go1 = true, go2 = true;
+        for (uint64_t t = lane; go0 || go1 || go2; t += 32) {
+            const uint64_t i0 = s0 + t, i1 = s1 + t, i2 = s2 + t;
+            const bool h0 = go0 && i0 < e0, h1 = go1 && i1 < e1, h2 = go2 && i2 < e2;
+            const int y0v = h0 ? (int)y_vec[i0] : 0x7fffffff;
+            const int y1v = h1 ? 2 * (int)y_vec[i1] : 0x7fffffff;
+            const int y2v = h2 ? (int)t_y_vec[i2] : 0x7fffffff;
+            if (y0v <= yb && y0v >= ya) rowbuf[y0v - ys] = in[i0];
+            if (y1v <= yb) {
+                const T v = in[i1];
+                const int c1 = min(y1v + 1, a.d.yn - 1);
+                if (y1v >= ya) rowbuf[y1v - ys] = v;
+                if (c1 != y1v && c1 >= ya && c1 <= yb) rowbuf[c1 - ys] = v;
             }
+            if (y2v <= yb && y2v >= ya) rowbuf[y2v - ys] = tree[i2];
+            // a source ends for the warp once any lane passes its window
+            go0 = __all_sync(0xffffffffu, h0 && y0v <= yb);
+            go1 = __all_sync(0xffffffffu, h1 && y1v <= yb);
+            go2 = __all_sync(0xffffffffu, h2 && y2v <= yb);
         }
     }
     __syncwarp();
@@ -324,37 +336,73 @@ __global__ void __launch_bounds__(32 * (kBX + 2 * R)) conv_tile_kernel(
         }
         __syncthreads();
         const int total = sm.ocnt[kBX];
-        for (int k = threadIdx.x; k < total; k += NT) {
-            int q = 0;
-            while (q + 1 < kBX && sm.ocnt[q + 1] <= k) ++q;
-            const uint64_t i = sm.ob[q] + (uint64_t)(k - sm.ocnt[q]);
-            const int yy = (int)y_vec[i] - (y0 - R);  // ring column of the particle
-            T val = T(0);
-            int cnt = 0;
+        const T *ring0 = &sm.ring[0][0][0];
+        auto slot_of = [&](int iz) { return ring0 + ((z + iz - R - (z0 - R)) % S) * (RX * RY); };
+        // Each thread takes kConvK particles; one z-slice of the stencil sits in
+        // registers while it is applied to all of them, in the stencil's order.
+        for (int base = 0; base < total; base += kConvK * NT) {
+            uint64_t ii[kConvK];
+            int roff[kConvK];
+            bool has[kConvK];
 #pragma unroll
-            for (int iz = 0; iz < S; ++iz) {
-                const T(*slot)[RY] = sm.ring[(z + iz - R - (z0 - R)) % S];
-#pragma unroll
-                for (int ix = 0; ix < S; ++ix) {
-                    const T *rowp = slot[q + ix] + (yy - R);
-#pragma unroll
-                    for (int iy = 0; iy < S; ++iy) {
-                        T v = rowp[iy];
-                        if (VT<T>::is_miss(v)) {
-                            v = T(0);
-                            nstale++;
-                        }
-                        val = VT<T>::add(val, VT<T>::mul(v, sm.st[cnt]));
-                        cnt++;
-                    }
+            for (int j = 0; j < kConvK; ++j) {
+                const int k = base + j * NT + threadIdx.x;
+                has[j] = k < total;
+                ii[j] = 0;
+                roff[j] = 0;
+                if (has[j]) {
+                    int q = 0;
+                    while (q + 1 < kBX && sm.ocnt[q + 1] <= k) ++q;
+                    ii[j] = sm.ob[q] + (uint64_t)(k - sm.ocnt[q]);
+                    roff[j] = q * RY + ((int)y_vec[ii[j]] - (y0 - R)) - R;  // ring offset of tap (ix, iy) = (0, 0)
                 }
             }
-            if (a.mode == 0)
-                out[i] = val;
-            else if (a.mode == 1)
-                out[i] = VT<T>::div((T)rl_in[i], val);
-            else
-                out[i] = VT<T>::mul(out[i], val);
+            T acc[kConvK];
+#pragma unroll
+            for (int j = 0; j < kConvK; ++j) acc[j] = T(0);
+#pragma unroll 1
+            for (int iz = 0; iz < S; ++iz) {
+                const T *sl = slot_of(iz);
+                T stv[S * S];
+#pragma unroll
+                for (int t = 0; t < S * S; ++t) stv[t] = sm.st[iz * S * S + t];
+#pragma unroll
+                for (int ix = 0; ix < S; ++ix)
+#pragma unroll
+                    for (int iy = 0; iy < S; ++iy)
+#pragma unroll
+                        for (int j = 0; j < kConvK; ++j)
+                            acc[j] = VT<T>::add(acc[j], VT<T>::mul(sl[roff[j] + ix * RY + iy], stv[ix * S + iy]));
+            }
+#pragma unroll
+            for (int j = 0; j < kConvK; ++j) {
+                if (!has[j]) continue;
+                T val = acc[j];
+                if (val != val) {  // NaN: a sentinel (or a NaN input) was read; redo with stale counting
+                    val = T(0);
+                    int cnt = 0;
+                    for (int iz = 0; iz < S; ++iz) {
+                        const T *sl = slot_of(iz);
+                        for (int ix = 0; ix < S; ++ix)
+                            for (int iy = 0; iy < S; ++iy) {
+                                T v = sl[roff[j] + ix * RY + iy];
+                                if (VT<T>::is_miss(v)) {
+                                    v = T(0);
+                                    nstale++;
+                                }
+                                val = VT<T>::add(val, VT<T>::mul(v, sm.st[cnt]));
+                                cnt++;
+                            }
+                    }
+                }
+                const uint64_t i = ii[j];
+                if (a.mode == 0)
+                    out[i] = val;
+                else if (a.mode == 1)
+                    out[i] = VT<T>::div((T)rl_in[i], val);
+                else
+                    out[i] = VT<T>::mul(out[i], val);
+            }
         }
         __syncthreads();
     }

@@ -615,10 +615,6 @@ __global__ void __launch_bounds__(kYWarps * 32) sat_y_kernel(const float *__rest
     }
 }
 
-#ifndef APRB_SAT_PREFETCH
-#define APRB_SAT_PREFETCH 8
-#endif
-
 // Final pass writing the unpadded window times the rescale factor
 // (unpaddPixels + rescale_var, LocalIntensityScale.hpp:174-184) directly.
 struct LisOut {
@@ -628,13 +624,13 @@ struct LisOut {
 };
 
 // x / z box mean (:364-494): one thread per strided line, coalesced over y,
-// with the next U samples of the line in flight.
+// with the next sample of the line in flight.
 template <int OFF, bool FINAL>
 __global__ void __launch_bounds__(128) sat_strided_kernel(const float *__restrict__ in,
                                                           const float *__restrict__ absdiff_ref,
                                                           float *__restrict__ out, int yn, int n, uint64_t stride,
                                                           uint64_t outer_stride, uint64_t nlines, LisOut fo) {
-    constexpr int W = 2 * OFF + 2, U = APRB_SAT_PREFETCH;
+    constexpr int W = 2 * OFF + 2, U = 1;  // deeper prefetch measured slower
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= nlines) return;
     const uint64_t y = g % (uint64_t)yn, o = g / (uint64_t)yn;
