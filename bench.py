@@ -560,6 +560,11 @@ def main():
             e1.record(stream)
             torch.cuda.synchronize()
             L.aprb_profile_enable(0)
+            cn = (C.c_char_p * 64)()
+            ct = (C.c_double * 64)()
+            cc = (C.c_uint64 * 64)()
+            nst = L.aprb_profile_read(cn, ct, cc, 64)
+            cstages = {cn[i].decode(): ct[i] / reps for i in range(nst)}
             L.aprb_profile_reset()
             cms = e0.elapsed_time(e1) / reps
             ab = 10 * P + 10 * T
@@ -568,7 +573,7 @@ def main():
                 "value": P / (cms / 1e3) / 1e9, "unit": "Gpart/s", "ms": cms, "particles": P, "tree_nodes": T,
                 "roofline": {"bound": "hbm", "achieved": ab / (cms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
                              "frac": ab / (cms / 1e3) / 1e9 / hbm, "algorithmic_bytes": ab},
-                "gflops": flops / (cms / 1e3) / 1e9}
+                "gflops": flops / (cms / 1e3) / 1e9, "stages_ms": cstages}
         del pf, outp
     L.aprb_apr_free(last)
 

@@ -12,17 +12,19 @@
 // children, z then x then y within each -- with the reference's boundary scale
 // factors (:97-110).  Levels run from fine to coarse.
 //
-// Convolution (APRFilter::convolve_pencil, APRFilter.hpp:1094-1216): one CTA
-// per (8 x-rows, 128-y chunk, 16-z range) of a level streams z through a ring
-// of 2R+1 shared-memory slices.  Each slice is the isotropic neighbourhood the
-// reference builds in its pencil buffer (update_dense_array, :825-849):
-// same-level particles, parents one level coarser (piecewise constant,
-// :766-793) and tree means of the same level (:802-818), with the reflective
-// or zero boundary (:287-504) folded into the slice contents.  Each particle
-// of the centre slice sums its 27 / 125 taps in the stencil's memory order
-// without contraction (run_convolution_pencil, :706-736).  A cell no particle
-// covers holds a sentinel; reading it is counted as a stale read (the
-// reference would read a stale pencil buffer there) and contributes 0.
+// Convolution (APRFilter::convolve_pencil, APRFilter.hpp:1094-1216), per level
+// from fine to coarse, in two kernels.  densify writes the level's isotropic
+// neighbourhood image -- the values the reference gathers into its pencil
+// buffer (update_dense_array, :825-849): same-level particles, parents one
+// level coarser (piecewise constant, :766-793) and tree means of the same
+// level (:802-818) -- to HBM once, one warp per row.  conv_gather then lets
+// every particle of the level sum its 27 / 125 taps from that image in the
+// stencil's memory order without contraction (run_convolution_pencil,
+// :706-736), reading through L1/L2 (neighbouring rows are shared by the warps
+// of a block), with the reflective or zero boundary (:287-504) applied to the
+// indices.  A cell no particle covers holds a sentinel; reading it is counted
+// as a stale read (the reference would read a stale pencil buffer there) and
+// contributes 0.
 #include "kernels.cuh"
 
 namespace aprb {
@@ -62,6 +64,7 @@ struct LD {
 };
 LD ld(const Geom &g, int l) { return LD{g.y_num[l], g.x_num[l], g.z_num[l]}; }
 uint64_t nrow(const Geom &g, int l) { return (uint64_t)g.x_num[l] * g.z_num[l]; }
+uint64_t ncell_of(const LD &d) { return (uint64_t)d.yn * d.xn * d.zn; }
 __host__ __device__ __forceinline__ int nchunk(int yn) { return (yn + kYC - 1) / kYC; }
 
 // Reflection about the edge sample (APRFilter.hpp:287-504), or the zero pad
@@ -187,8 +190,7 @@ __global__ void __launch_bounds__(128) tree_mean_kernel(TreeLevelArgs a, const u
 // ---------------------------------------------------------------------------
 // convolution of one level
 // ---------------------------------------------------------------------------
-constexpr int kBX = 8, kBY = 128, kBZ = 16;
-constexpr int kConvK = 4;  // output particles per thread and pass
+constexpr int kConvK = 4;  // output particles per lane and pass
 
 struct ConvLevelArgs {
     LD d;                 // level dims
@@ -201,223 +203,170 @@ struct ConvLevelArgs {
     int mode;
 };
 
-template <int R, typename T>
-struct ConvSmem {
-    static constexpr int S = 2 * R + 1, RX = kBX + 2 * R, RY = kBY + 2 * R;
-    T ring[S][RX][RY];
-    T st[S * S * S];
-    uint64_t ob[kBX];
-    int ocnt[kBX + 1];
-};
+// ---------------------------------------------------------------------------
+// convolution of one level in two kernels: the level's isotropic
+// neighbourhood image is written to HBM once (densify), then every particle
+// of the level gathers its taps from it (conv_gather)
+// ---------------------------------------------------------------------------
 
-// Fills one slice row (level row (zr, xr) over the y window) of the ring.
-template <int R, typename T>
-__device__ void fill_slice_row(T *__restrict__ rowbuf, int zr, int xr, int y0, const ConvLevelArgs &a,
-                               const uint64_t *__restrict__ xz_end, const uint16_t *__restrict__ y_vec,
-                               const T *__restrict__ in, const uint64_t *__restrict__ t_xz_end,
-                               const uint16_t *__restrict__ t_y_vec, const T *__restrict__ tree, int lane) {
-    constexpr int RY = kBY + 2 * R;
-    const int ys = y0 - R;  // y of rowbuf[0]
+// densify: one warp per row (z, x) of level l.  Cells start as the sentinel;
+// same-level particles, the parents one level coarser (each covering its y
+// pair) and the tree means of the level write their cells.  The three sources
+// cover disjoint cells (APR particle cells partition the volume).
+template <typename T>
+__global__ void __launch_bounds__(256) densify_kernel(ConvLevelArgs a, const uint64_t *__restrict__ xz_end,
+                                                      const uint16_t *__restrict__ y_vec, const T *__restrict__ in,
+                                                      const uint64_t *__restrict__ t_xz_end,
+                                                      const uint16_t *__restrict__ t_y_vec,
+                                                      const T *__restrict__ tree, T *__restrict__ D) {
+    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= (uint64_t)a.d.xn * a.d.zn) return;
+    const int yn = a.d.yn;
+    T *Rw = D + row * (uint64_t)yn;
     const T miss = VT<T>::miss();
-    for (int k = lane; k < RY; k += 32) rowbuf[k] = miss;
-    const int ya = max(ys, 0), yb = min(ys + RY - 1, a.d.yn - 1);  // real y range needed
-    if (ya <= yb) {
-        // Bounds of the three sources inside the y window: same-level
-        // particles, parents one level coarser (each fills its y pair) and
-        // tree means of the same level.  They cover disjoint cells, so one
-        // merged pass writes them in any order.  Lanes 0-2 fetch the bounds.
-        const uint64_t row = (uint64_t)zr * a.d.xn + xr;
-        const int nc = nchunk(a.d.yn);
-        uint64_t lo = 0, hi = 0;
-        if (lane == 0) {
-            const uint64_t b = xz_end[a.row_base + row - 1];
-            hi = xz_end[a.row_base + row];
-            lo = b + a.cidx[row * (uint64_t)(nc + 1) + ya / kYC];
-        } else if (lane == 1 && a.prow_base) {
-            const uint64_t prow = (uint64_t)(zr / 2) * a.dp.xn + xr / 2;
-            const int npc = nchunk(a.dp.yn);
-            const uint64_t b = xz_end[a.prow_base + prow - 1];
-            hi = xz_end[a.prow_base + prow];
-            lo = b + a.pcidx[prow * (uint64_t)(npc + 1) + (ya / 2) / kYC];
-        } else if (lane == 2 && a.trow_base) {
-            const uint64_t b = t_xz_end[a.trow_base + row - 1];
-            hi = t_xz_end[a.trow_base + row];
-            lo = b + a.tcidx[row * (uint64_t)(nc + 1) + ya / kYC];
-        }
-        const uint64_t s0 = __shfl_sync(0xffffffffu, lo, 0), e0 = __shfl_sync(0xffffffffu, hi, 0);
-        const uint64_t s1 = __shfl_sync(0xffffffffu, lo, 1), e1 = __shfl_sync(0xffffffffu, hi, 1);
-        const uint64_t s2 = __shfl_sync(0xffffffffu, lo, 2), e2 = __shfl_sync(0xffffffffu, hi, 2);
-        __syncwarp();
-        bool go0 = true, go1 = true, go2 = true;
-        for (uint64_t t = lane; go0 || go1 || go2; t += 32) {
-            const uint64_t i0 = s0 + t, i1 = s1 + t, i2 = s2 + t;
-            const bool h0 = go0 && i0 < e0, h1 = go1 && i1 < e1, h2 = go2 && i2 < e2;
-            const int y0v = h0 ? (int)y_vec[i0] : 0x7fffffff;
-            const int y1v = h1 ? 2 * (int)y_vec[i1] : 0x7fffffff;
-            const int y2v = h2 ? (int)t_y_vec[i2] : 0x7fffffff;
-            if (y0v <= yb && y0v >= ya) rowbuf[y0v - ys] = in[i0];
-            if (y1v <= yb) {
-                const T v = in[i1];
-                const int c1 = min(y1v + 1, a.d.yn - 1);
-                if (y1v >= ya) rowbuf[y1v - ys] = v;
-                if (c1 != y1v && c1 >= ya && c1 <= yb) rowbuf[c1 - ys] = v;
-            }
-            if (y2v <= yb && y2v >= ya) rowbuf[y2v - ys] = tree[i2];
-            // a source ends for the warp once any lane passes its window
-            go0 = __all_sync(0xffffffffu, h0 && y0v <= yb);
-            go1 = __all_sync(0xffffffffu, h1 && y1v <= yb);
-            go2 = __all_sync(0xffffffffu, h2 && y2v <= yb);
+    for (int y = lane; y < yn; y += 32) Rw[y] = miss;
+    __syncwarp();
+    {
+        const uint64_t b = xz_end[a.row_base + row - 1], e = xz_end[a.row_base + row];
+        for (uint64_t i = b + lane; i < e; i += 32) Rw[y_vec[i]] = in[i];
+    }
+    if (a.prow_base) {
+        const int zr = (int)(row / (uint64_t)a.d.xn), xr = (int)(row % (uint64_t)a.d.xn);
+        const uint64_t prow = (uint64_t)(zr / 2) * a.dp.xn + xr / 2;
+        const uint64_t b = xz_end[a.prow_base + prow - 1], e = xz_end[a.prow_base + prow];
+        for (uint64_t i = b + lane; i < e; i += 32) {
+            const int c0 = 2 * (int)y_vec[i], c1 = min(c0 + 1, yn - 1);
+            const T v = in[i];
+            Rw[c0] = v;
+            if (c1 != c0) Rw[c1] = v;
         }
     }
-    __syncwarp();
-    // y boundary: reflection about the edge sample, or zero
-    for (int k = lane; k < RY; k += 32) {
-        const int y = ys + k;
-        if (y >= 0 && y < a.d.yn) continue;
-        if (!a.reflect) {
-            rowbuf[k] = T(0);
-        } else {
-            const int r = y < 0 ? -y : 2 * (a.d.yn - 1) - y;
-            rowbuf[k] = (r >= 0 && r < a.d.yn && r - ys >= 0 && r - ys < RY) ? rowbuf[r - ys] : miss;
-        }
+    if (a.trow_base) {
+        const uint64_t b = t_xz_end[a.trow_base + row - 1], e = t_xz_end[a.trow_base + row];
+        for (uint64_t i = b + lane; i < e; i += 32) Rw[t_y_vec[i]] = tree[i];
     }
 }
 
+// One tap outside the fast path: reflection about the edge sample (or the
+// zero pad), and the sentinel of an uncovered cell counted as a stale read.
+template <typename T>
+__device__ __forceinline__ T gather_tap(const T *__restrict__ D, const ConvLevelArgs &a, int zz, int xx, int yy,
+                                        unsigned &nstale) {
+    bool ok = true;
+    const int zr = reflect_idx(zz, a.d.zn, a.reflect, ok);
+    const int xr = reflect_idx(xx, a.d.xn, a.reflect, ok);
+    const int yr = reflect_idx(yy, a.d.yn, a.reflect, ok);
+    if (!ok) {
+        if (a.reflect) nstale++;
+        return T(0);
+    }
+    const T v = D[((uint64_t)zr * a.d.xn + xr) * (uint64_t)a.d.yn + yr];
+    if (VT<T>::is_miss(v)) {
+        nstale++;
+        return T(0);
+    }
+    return v;
+}
+
+// conv_gather: one warp per row of level l; each lane takes kConvK particles
+// of the row.  A z-slice of the stencil sits in registers; the taps are
+// summed in the stencil's memory order without contraction
+// (run_convolution_pencil, APRFilter.hpp:706-736).  Particles whose window
+// stays inside the level read D directly; a NaN sum (a sentinel was read) is
+// redone through gather_tap, which counts stale reads.
 template <int R, typename T>
-__global__ void __launch_bounds__(32 * (kBX + 2 * R)) conv_tile_kernel(
-    ConvLevelArgs a, const uint64_t *__restrict__ xz_end, const uint16_t *__restrict__ y_vec,
-    const T *__restrict__ in, const uint64_t *__restrict__ t_xz_end, const uint16_t *__restrict__ t_y_vec,
-    const T *__restrict__ tree, const T *__restrict__ stencil, T *__restrict__ out,
-    const uint16_t *__restrict__ rl_in, unsigned long long *stale) {
-    constexpr int S = 2 * R + 1, RX = kBX + 2 * R, RY = kBY + 2 * R, NT = 32 * RX;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    ConvSmem<R, T> &sm = *reinterpret_cast<ConvSmem<R, T> *>(smem_raw);
-    const int x0 = blockIdx.x * kBX, y0 = blockIdx.y * kBY, z0 = blockIdx.z * kBZ;
-    const int z1 = min(z0 + kBZ, a.d.zn);
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int k = threadIdx.x; k < S * S * S; k += NT) sm.st[k] = stencil[k];
+__global__ void __launch_bounds__(256) conv_gather_kernel(ConvLevelArgs a, const uint64_t *__restrict__ xz_end,
+                                                          const uint16_t *__restrict__ y_vec, const T *__restrict__ D,
+                                                          const T *__restrict__ stencil, T *__restrict__ out,
+                                                          const uint16_t *__restrict__ rl_in,
+                                                          unsigned long long *stale) {
+    constexpr int S = 2 * R + 1, S3 = S * S * S;
+    __shared__ T st[S3];
+    for (int k = threadIdx.x; k < S3; k += blockDim.x) st[k] = stencil[k];
+    __syncthreads();
+    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= (uint64_t)a.d.xn * a.d.zn) return;
+    const uint64_t b = xz_end[a.row_base + row - 1], e = xz_end[a.row_base + row];
+    if (b == e) return;
+    const int z = (int)(row / (uint64_t)a.d.xn), x = (int)(row % (uint64_t)a.d.xn);
+    const int yn = a.d.yn;
+    // the S x S neighbour rows lie inside the level (warp-uniform)
+    const bool rows_in = z - R >= 0 && z + R < a.d.zn && x - R >= 0 && x + R < a.d.xn;
     unsigned nstale = 0;
-    const int nc = nchunk(a.d.yn);
-
-    // warp w fills ring row w of the slice at z (z may lie outside the level)
-    auto load_slice = [&](int zq) {
-        T(*slot)[RY] = sm.ring[(zq - (z0 - R)) % S];
-        bool ok = true;
-        const int zr = reflect_idx(zq, a.d.zn, a.reflect, ok);
-        const int xr = reflect_idx(x0 - R + w, a.d.xn, a.reflect, ok);
-        if (!ok) {
-            const T v = a.reflect ? VT<T>::miss() : T(0);
-            for (int k = lane; k < RY; k += 32) slot[w][k] = v;
-        } else {
-            fill_slice_row<R, T>(slot[w], zr, xr, y0, a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, lane);
-        }
-    };
-
-    for (int zq = z0 - R; zq < z0 + R; ++zq) load_slice(zq);
-    for (int z = z0; z < z1; ++z) {
-        load_slice(z + R);
-        if (threadIdx.x < kBX) {  // output particles of the centre rows
-            const int x = x0 + threadIdx.x;
-            uint64_t b = 0, e = 0;
-            if (x < a.d.xn) {
-                const uint64_t row = (uint64_t)z * a.d.xn + x;
-                const uint64_t rb = xz_end[a.row_base + row - 1];
-                const uint16_t *Cr = a.cidx + row * (uint64_t)(nc + 1);
-                b = rb + Cr[y0 / kYC];
-                e = rb + Cr[min(y0 / kYC + kBY / kYC, nc)];
-            }
-            sm.ob[threadIdx.x] = b;
-            sm.ocnt[threadIdx.x + 1] = (int)(e - b);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            sm.ocnt[0] = 0;
-            for (int q = 1; q <= kBX; ++q) sm.ocnt[q] += sm.ocnt[q - 1];
-        }
-        __syncthreads();
-        const int total = sm.ocnt[kBX];
-        const T *ring0 = &sm.ring[0][0][0];
-        auto slot_of = [&](int iz) { return ring0 + ((z + iz - R - (z0 - R)) % S) * (RX * RY); };
-        // Each thread takes kConvK particles; one z-slice of the stencil sits in
-        // registers while it is applied to all of them, in the stencil's order.
-        for (int base = 0; base < total; base += kConvK * NT) {
-            uint64_t ii[kConvK];
-            int roff[kConvK];
-            bool has[kConvK];
+    for (uint64_t base = b; base < e; base += 32 * kConvK) {
+        uint64_t ii[kConvK];
+        int yv[kConvK];
+        bool has[kConvK];
+        bool inner = rows_in;
 #pragma unroll
-            for (int j = 0; j < kConvK; ++j) {
-                const int k = base + j * NT + threadIdx.x;
-                has[j] = k < total;
-                ii[j] = 0;
-                roff[j] = 0;
-                if (has[j]) {
-                    int q = 0;
-                    while (q + 1 < kBX && sm.ocnt[q + 1] <= k) ++q;
-                    ii[j] = sm.ob[q] + (uint64_t)(k - sm.ocnt[q]);
-                    roff[j] = q * RY + ((int)y_vec[ii[j]] - (y0 - R)) - R;  // ring offset of tap (ix, iy) = (0, 0)
-                }
-            }
-            T acc[kConvK];
+        for (int j = 0; j < kConvK; ++j) {
+            ii[j] = base + (uint64_t)(j * 32 + lane);
+            has[j] = ii[j] < e;
+            yv[j] = has[j] ? (int)y_vec[ii[j]] : R;
+            inner = inner && yv[j] - R >= 0 && yv[j] + R < yn;
+        }
+        T acc[kConvK];
 #pragma unroll
-            for (int j = 0; j < kConvK; ++j) acc[j] = T(0);
+        for (int j = 0; j < kConvK; ++j) acc[j] = T(0);
+        if (inner) {
 #pragma unroll 1
             for (int iz = 0; iz < S; ++iz) {
-                const T *sl = slot_of(iz);
                 T stv[S * S];
 #pragma unroll
-                for (int t = 0; t < S * S; ++t) stv[t] = sm.st[iz * S * S + t];
+                for (int t = 0; t < S * S; ++t) stv[t] = st[iz * S * S + t];
+                const T *plane = D + (uint64_t)(z + iz - R) * a.d.xn * (uint64_t)yn;
 #pragma unroll
-                for (int ix = 0; ix < S; ++ix)
+                for (int ix = 0; ix < S; ++ix) {
+                    const T *rp = plane + (uint64_t)(x + ix - R) * yn - R;
 #pragma unroll
                     for (int iy = 0; iy < S; ++iy)
 #pragma unroll
                         for (int j = 0; j < kConvK; ++j)
-                            acc[j] = VT<T>::add(acc[j], VT<T>::mul(sl[roff[j] + ix * RY + iy], stv[ix * S + iy]));
-            }
-#pragma unroll
-            for (int j = 0; j < kConvK; ++j) {
-                if (!has[j]) continue;
-                T val = acc[j];
-                if (val != val) {  // NaN: a sentinel (or a NaN input) was read; redo with stale counting
-                    val = T(0);
-                    int cnt = 0;
-                    for (int iz = 0; iz < S; ++iz) {
-                        const T *sl = slot_of(iz);
-                        for (int ix = 0; ix < S; ++ix)
-                            for (int iy = 0; iy < S; ++iy) {
-                                T v = sl[roff[j] + ix * RY + iy];
-                                if (VT<T>::is_miss(v)) {
-                                    v = T(0);
-                                    nstale++;
-                                }
-                                val = VT<T>::add(val, VT<T>::mul(v, sm.st[cnt]));
-                                cnt++;
-                            }
-                    }
+                            acc[j] = VT<T>::add(acc[j], VT<T>::mul(__ldg(rp + yv[j] + iy), stv[ix * S + iy]));
                 }
-                const uint64_t i = ii[j];
-                if (a.mode == 0)
-                    out[i] = val;
-                else if (a.mode == 1)
-                    out[i] = VT<T>::div((T)rl_in[i], val);
-                else
-                    out[i] = VT<T>::mul(out[i], val);
             }
         }
-        __syncthreads();
+#pragma unroll
+        for (int j = 0; j < kConvK; ++j) {
+            if (!has[j]) continue;
+            T val = acc[j];
+            if (!inner || val != val) {
+                val = T(0);
+                int cnt = 0;
+                for (int iz = 0; iz < S; ++iz)
+                    for (int ix = 0; ix < S; ++ix)
+                        for (int iy = 0; iy < S; ++iy) {
+                            const T v = gather_tap(D, a, z + iz - R, x + ix - R, yv[j] + iy - R, nstale);
+                            val = VT<T>::add(val, VT<T>::mul(v, st[cnt++]));
+                        }
+            }
+            const uint64_t i = ii[j];
+            if (a.mode == 0)
+                out[i] = val;
+            else if (a.mode == 1)
+                out[i] = VT<T>::div((T)rl_in[i], val);
+            else
+                out[i] = VT<T>::mul(out[i], val);
+        }
     }
     if (nstale) atomicAdd(stale, (unsigned long long)nstale);
 }
 
 template <int R, typename T>
-void launch_conv_level(const ConvLevelArgs &a, const uint64_t *xz_end, const uint16_t *y_vec, const T *in,
-                       const uint64_t *t_xz_end, const uint16_t *t_y_vec, const T *tree, const T *st, T *out,
-                       const uint16_t *rl_in, unsigned long long *stale, cudaStream_t s) {
-    const size_t smem = sizeof(ConvSmem<R, T>);
-    APRB_CUDA(cudaFuncSetAttribute(conv_tile_kernel<R, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((a.d.xn + kBX - 1) / kBX, (a.d.yn + kBY - 1) / kBY, (a.d.zn + kBZ - 1) / kBZ);
-    conv_tile_kernel<R, T><<<grid, 32 * (kBX + 2 * R), smem, s>>>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st,
-                                                                  out, rl_in, stale);
+void launch_conv_level_dense(const ConvLevelArgs &a, const uint64_t *xz_end, const uint16_t *y_vec, const T *in,
+                             const uint64_t *t_xz_end, const uint16_t *t_y_vec, const T *tree, const T *st, T *out,
+                             const uint16_t *rl_in, unsigned long long *stale, T *D, cudaStream_t s) {
+    const uint64_t rows = (uint64_t)a.d.xn * a.d.zn;
+    {
+        APRB_PROF("densify", s);
+        densify_kernel<T><<<blocks_for(rows * 32, 256), 256, 0, s>>>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, D);
+        count_launch();
+        APRB_CHECK_LAUNCH();
+    }
+    APRB_PROF("conv_gather", s);
+    conv_gather_kernel<R, T><<<blocks_for(rows * 32, 256), 256, 0, s>>>(a, xz_end, y_vec, D, st, out, rl_in, stale);
     count_launch();
     APRB_CHECK_LAUNCH();
 }
@@ -514,10 +463,11 @@ void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, 
         a.reflect = plan->reflect;
         a.mode = mode;
         const T *st = d_stencils + plan->offsets[sn];
+        T *D = (T *)fb.dense.get(ncell_of(a.d) * sizeof(T));
         if (side == 3)
-            launch_conv_level<1, T>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st, out, rl_in, stale, s);
+            launch_conv_level_dense<1, T>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st, out, rl_in, stale, D, s);
         else
-            launch_conv_level<2, T>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st, out, rl_in, stale, s);
+            launch_conv_level_dense<2, T>(a, xz_end, y_vec, in, t_xz_end, t_y_vec, tree, st, out, rl_in, stale, D, s);
     }
 }
 
