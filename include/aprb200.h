@@ -210,6 +210,39 @@ aprb_status aprb_richardson_lucy_fp64_device(aprb_apr *a, const uint16_t *in_dev
                                              int ksize, int niter, int use_stencil_downsample, int normalize,
                                              int resume, void *stream);
 
+
+/* --- learned Richardson-Lucy proposal (no counterpart in the reference) -----------------
+ * A sparse CNN on the APR: every layer applies one 3x3x3 stencil of 16 x 16 channels on
+ * every level, over the neighbourhood convolve_pencil uses (same-level particles, parents,
+ * tree means; zero boundary).  Activations are P x 16 float, channels-last; W is
+ * [27 taps][16 out][16 in] float (taps in convolve_pencil's z, x, y memory order), rounded
+ * to bfloat16 for the tensor cores with float accumulation.  The network predicts
+ * log(u_{i+10} / u_i) from (log(u / (1 + d)), log(ratio), log(1 + d) / 8). */
+aprb_status aprb_cnn_layer_forward_device(aprb_apr *a, const float *in, const float *W, const float *bias, int relu,
+                                          float *out, void *stream);
+/* g_in = dL/d in (overwritten); dW, db accumulate */
+aprb_status aprb_cnn_layer_backward_device(aprb_apr *a, const float *in, const float *W, const float *out,
+                                           const float *g_out, int relu, float *g_in, float *dW, float *db,
+                                           void *stream);
+aprb_status aprb_cnn_features_device(const aprb_apr *a, const float *u, const float *ratio, const uint16_t *raw,
+                                     float *features, void *stream);
+/* loss_dev += mean (pred[:,0] - log(u1 / u0))^2 (zeroed first); g_pred = dloss/dpred */
+aprb_status aprb_cnn_loss_device(const aprb_apr *a, const float *pred, const float *u0, const float *u1, float *g_pred,
+                                 double *loss_dev, void *stream);
+/* the proposal: u <- u * exp(clamp(pred[:,0], -2, 2)) */
+aprb_status aprb_cnn_apply_device(const aprb_apr *a, const float *pred, float *u, void *stream);
+/* Adam step on n parameters (mask, when not NULL, multiplies the gradient) */
+aprb_status aprb_cnn_adam_device(float *params, const float *grads, float *m, float *v, const float *mask, uint64_t n,
+                                 float lr, float beta1, float beta2, float eps, int step, void *stream);
+/* the RL ratio d / conv(psf_flipped, u) of APRNumerics.hpp:565-566 */
+aprb_status aprb_rl_ratio_device(aprb_apr *a, const uint16_t *in_dev, const float *u_dev, float *ratio_dev,
+                                 const float *psf, int ksize, int use_stencil_downsample, int normalize,
+                                 void *stream);
+/* RL's Poisson data-fit objective sum(k - d log k), k = conv(psf_flipped, u); blocking */
+aprb_status aprb_rl_objective_device(aprb_apr *a, const uint16_t *in_dev, const float *u_dev, const float *psf,
+                                     int ksize, int use_stencil_downsample, int normalize, double *objective,
+                                     void *stream);
+
 /* --- synthetic data (benchmark inputs; no reference counterpart) ----------------
  * Background + n_blobs isotropic Gaussians (centre uniform, sigma and peak
  * uniform in the given ranges) + Poisson noise, rounded and clipped to

@@ -441,3 +441,5 @@ def synth_ground_truth_device(out_tensor, n_blobs, sigma=(1.0, 4.0), amp=(500.0,
     z, x, y = out_tensor.shape
     check(lib().aprb_synth_blobs_f32(_dptr(out_tensor), y, x, z, int(n_blobs), sigma[0], sigma[1], amp[0], amp[1],
                                      background, int(seed), _stream(stream)))
+
+from . import learned  # noqa: E402,F401  (the learned RL proposal)

@@ -75,6 +75,14 @@ SIGNATURES = {
     "aprb_richardson_lucy_device": ([_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp], _i),
     "aprb_richardson_lucy_fp64": ([_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i], _i),
     "aprb_richardson_lucy_fp64_device": ([_vp, _vp, _vp, _vp, _i, _i, _i, _i, _i, _vp], _i),
+    "aprb_cnn_layer_forward_device": ([_vp, _vp, _vp, _vp, _i, _vp, _vp], _i),
+    "aprb_cnn_layer_backward_device": ([_vp, _vp, _vp, _vp, _vp, _i, _vp, _vp, _vp, _vp], _i),
+    "aprb_cnn_features_device": ([_vp, _vp, _vp, _vp, _vp, _vp], _i),
+    "aprb_cnn_loss_device": ([_vp, _vp, _vp, _vp, _vp, _vp, _vp], _i),
+    "aprb_cnn_apply_device": ([_vp, _vp, _vp, _vp], _i),
+    "aprb_cnn_adam_device": ([_vp, _vp, _vp, _vp, _vp, _u64, _f, _f, _f, _f, _i, _vp], _i),
+    "aprb_rl_ratio_device": ([_vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp], _i),
+    "aprb_rl_objective_device": ([_vp, _vp, _vp, _vp, _i, _i, _i, C.POINTER(C.c_double), _vp], _i),
     "aprb_synth_blobs_u16": ([_vp, _i, _i, _i, _i, _f, _f, _f, _f, _f, _u64, _vp], _i),
     "aprb_synth_blobs_f32": ([_vp, _i, _i, _i, _i, _f, _f, _f, _f, _f, _u64, _vp], _i),
     "aprb_kernel_launch_count": ([], _u64),

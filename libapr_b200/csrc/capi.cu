@@ -71,8 +71,9 @@ void *pool_alloc(size_t bytes, cudaStream_t s) {
 // call).  Calls issued by one thread on different streams that overlap on the
 // GPU share these buffers; use one thread per concurrent stream.
 struct ThreadScratch {
-    DevBuf scan_tmp, tree_vals, pyr, parts_f, parts_u16, out_f, rb, stencils, stencils_f, io_in, t_flags;
+    DevBuf scan_tmp, tree_vals, pyr, parts_f, parts_u16, out_f, rb, stencils, stencils_f, io_in, t_flags, obj;
     FilterBuffers fb;
+    CnnScratch cnn;
 };
 
 static ThreadScratch &scratch() {
@@ -145,6 +146,9 @@ struct aprb_apr {
     DevBuf t_xz_end, t_y_vec;  // pooled
     FilterIndex fi;
     uint64_t last_stale = 0;
+    // learned proposal: level row of every particle (pooled), built on first use
+    DevBuf cnn_rows;
+    bool cnn_ready = false;
 };
 
 struct aprb_converter {
@@ -933,6 +937,149 @@ aprb_status aprb_richardson_lucy_fp64(aprb_apr *a, const uint16_t *in, double *o
         if (resume) APRB_CUDA(cudaMemcpyAsync(dout, out, a->P * sizeof(double), cudaMemcpyHostToDevice, s));
         rl_impl<double>(a, di, dout, psf, ksize, niter, use_stencil_downsample, normalize, resume, s);
         APRB_CUDA(cudaMemcpyAsync(out, dout, a->P * sizeof(double), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+}  // extern "C"
+
+namespace {
+
+CnnGeom cnn_geom(aprb_apr *a, cudaStream_t s) {
+    ensure_tree(a, s);
+    if (!a->cnn_ready) {
+        ARG_CHECK(a->P < 0xffffffffull, "too many particles for the learned proposal");
+        uint32_t *rows = a->cnn_rows.as_pooled<uint32_t>(a->P ? a->P : 1, s);
+        cnn_build_rows(a->g, (const uint64_t *)a->xz_end.p, rows, s);
+        a->cnn_ready = true;
+    }
+    CnnGeom cg;
+    cg.g = &a->g;
+    cg.tg = &a->tg;
+    cg.xz_end = (const uint64_t *)a->xz_end.p;
+    cg.y_vec = (const uint16_t *)a->y_vec.p;
+    cg.t_xz_end = (const uint64_t *)a->t_xz_end.p;
+    cg.t_y_vec = (const uint16_t *)a->t_y_vec.p;
+    cg.fi = &a->fi;
+    cg.prow = (const uint32_t *)a->cnn_rows.p;
+    for (int l = 0; l < 34; ++l) cg.level_begin[l] = 0;
+    uint64_t acc = 0;
+    for (int l = a->g.l_min; l <= a->g.l_max; ++l) {
+        cg.level_begin[l] = acc;
+        acc += a->fi.level_count[l];
+    }
+    cg.level_begin[a->g.l_max + 1] = acc;
+    cg.T = a->T;
+    return cg;
+}
+
+}  // namespace
+
+extern "C" {
+
+aprb_status aprb_cnn_layer_forward_device(aprb_apr *a, const float *in, const float *W, const float *bias, int relu,
+                                          float *out, void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && in && W && bias && out, "null argument");
+        cudaStream_t s = (cudaStream_t)stream;
+        const CnnGeom cg = cnn_geom(a, s);
+        cnn_layer_forward(cg, in, W, bias, relu, out, scratch().cnn, s);
+    });
+}
+
+aprb_status aprb_cnn_layer_backward_device(aprb_apr *a, const float *in, const float *W, const float *out,
+                                           const float *g_out, int relu, float *g_in, float *dW, float *db,
+                                           void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && in && W && out && g_out && g_in && dW && db, "null argument");
+        cudaStream_t s = (cudaStream_t)stream;
+        const CnnGeom cg = cnn_geom(a, s);
+        cnn_layer_backward(cg, in, W, out, g_out, relu, g_in, dW, db, scratch().cnn, s);
+    });
+}
+
+aprb_status aprb_cnn_features_device(const aprb_apr *a, const float *u, const float *ratio, const uint16_t *raw,
+                                     float *features, void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && u && ratio && raw && features, "null argument");
+        cnn_features(u, ratio, raw, features, a->P, (cudaStream_t)stream);
+    });
+}
+
+aprb_status aprb_cnn_loss_device(const aprb_apr *a, const float *pred, const float *u0, const float *u1, float *g_pred,
+                                 double *loss_dev, void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && pred && u0 && u1 && g_pred && loss_dev, "null argument");
+        cnn_loss(pred, u0, u1, g_pred, a->P, loss_dev, (cudaStream_t)stream);
+    });
+}
+
+aprb_status aprb_cnn_apply_device(const aprb_apr *a, const float *pred, float *u, void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && pred && u, "null argument");
+        cnn_apply(pred, u, a->P, (cudaStream_t)stream);
+    });
+}
+
+aprb_status aprb_cnn_adam_device(float *params, const float *grads, float *m, float *v, const float *mask, uint64_t n,
+                                 float lr, float beta1, float beta2, float eps, int step, void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(params && grads && m && v && step >= 1, "invalid argument");
+        cnn_adam(params, grads, m, v, mask, n, lr, beta1, beta2, eps, step, (cudaStream_t)stream);
+    });
+}
+
+aprb_status aprb_rl_ratio_device(aprb_apr *a, const uint16_t *in_dev, const float *u_dev, float *ratio_dev,
+                                 const float *psf, int ksize, int use_stencil_downsample, int normalize,
+                                 void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && in_dev && u_dev && ratio_dev && psf, "null argument");
+        cudaStream_t s = (cudaStream_t)stream;
+        ensure_tree(a, s);
+        const int n0 = ksize * ksize * ksize;
+        std::vector<float> flipped(n0);
+        for (int i = 0; i < n0; ++i) flipped[i] = psf[n0 - 1 - i];
+        std::vector<float> hf;
+        ConvPlan plan_f = make_plan<float>(a, flipped.data(), ksize, use_stencil_downsample, normalize, 1, hf);
+        float *df = (float *)scratch().stencils_f.get(hf.size() * sizeof(float));
+        APRB_CUDA(cudaMemcpyAsync(df, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+        float *tree = (float *)scratch().tree_vals.get((a->T ? a->T : 1) * sizeof(float));
+        filter_apply<float>(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
+                            (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, a->fi, u_dev, tree,
+                            &plan_f, df, ratio_dev, 1, in_dev, scratch().fb, s);
+    });
+}
+
+aprb_status aprb_rl_objective_device(aprb_apr *a, const uint16_t *in_dev, const float *u_dev, const float *psf,
+                                     int ksize, int use_stencil_downsample, int normalize, double *objective,
+                                     void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && in_dev && u_dev && psf && objective, "null argument");
+        cudaStream_t s = (cudaStream_t)stream;
+        ensure_tree(a, s);
+        const int n0 = ksize * ksize * ksize;
+        std::vector<float> flipped(n0);
+        for (int i = 0; i < n0; ++i) flipped[i] = psf[n0 - 1 - i];
+        std::vector<float> hf;
+        ConvPlan plan_f = make_plan<float>(a, flipped.data(), ksize, use_stencil_downsample, normalize, 1, hf);
+        float *df = (float *)scratch().stencils_f.get(hf.size() * sizeof(float));
+        APRB_CUDA(cudaMemcpyAsync(df, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+        float *tree = (float *)scratch().tree_vals.get((a->T ? a->T : 1) * sizeof(float));
+        float *k = (float *)scratch().rb.get((a->P ? a->P : 1) * sizeof(float));
+        filter_apply<float>(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
+                            (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, a->fi, u_dev, tree,
+                            &plan_f, df, k, 0, nullptr, scratch().fb, s);
+        double *d = (double *)scratch().obj.get(sizeof(double));
+        rl_objective_sum(k, in_dev, a->P, d, s);
+        APRB_CUDA(cudaMemcpyAsync(objective, d, sizeof(double), cudaMemcpyDeviceToHost, s));
         APRB_CUDA(cudaStreamSynchronize(s));
     });
 }

@@ -114,6 +114,33 @@ void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, 
                   FilterBuffers &fb, cudaStream_t s);
 uint64_t filter_stale_count(FilterBuffers &fb, cudaStream_t s);
 
+// ---- learned.cu: the learned RL proposal (a sparse APR CNN, 16 channels)
+struct CnnGeom {
+    const Geom *g, *tg;
+    const uint64_t *xz_end, *t_xz_end;
+    const uint16_t *y_vec, *t_y_vec;
+    const FilterIndex *fi;
+    const uint32_t *prow;        // row (z * x_num + x) of every particle within its level
+    uint64_t level_begin[34];    // first particle of each level (level_begin[l_max + 1] = P)
+    uint64_t T;                  // tree nodes
+};
+struct CnnScratch {
+    DevBuf tree, gtree, dense, gdense, gp, wt;
+};
+void cnn_build_rows(const Geom &g, const uint64_t *xz_end, uint32_t *prow, cudaStream_t s);
+// one layer: out = act(conv3x3x3(in) + b), W[27][16 co][16 ci] fp32 (bf16 on the tensor cores)
+void cnn_layer_forward(const CnnGeom &cg, const float *in, const float *W, const float *b, int relu, float *out,
+                       CnnScratch &sc, cudaStream_t s);
+// g_in = d/d in; dW, db accumulated
+void cnn_layer_backward(const CnnGeom &cg, const float *in, const float *W, const float *out, const float *g_out,
+                        int relu, float *g_in, float *dW, float *db, CnnScratch &sc, cudaStream_t s);
+void cnn_adam(float *p, const float *g, float *m, float *v, const float *mask, uint64_t n, float lr, float b1,
+              float b2, float eps, int step, cudaStream_t s);
+void cnn_features(const float *u, const float *ratio, const uint16_t *raw, float *f, uint64_t P, cudaStream_t s);
+void cnn_loss(const float *pred, const float *u0, const float *u1, float *g, uint64_t P, double *loss, cudaStream_t s);
+void cnn_apply(const float *pred, float *u, uint64_t P, cudaStream_t s);
+void rl_objective_sum(const float *k, const uint16_t *raw, uint64_t P, double *out, cudaStream_t s);
+
 // ---- synth.cu
 // OutT uint16_t: blobs + Poisson noise; OutT float: the noise-free intensity
 template <typename OutT>

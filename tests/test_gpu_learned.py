@@ -1,0 +1,91 @@
+"""The learned Richardson-Lucy proposal on the GPU: one layer's forward and
+backward kernels against the FP64 oracle (operands rounded to bfloat16 as the
+tensor cores see them, sums in FP64), and Adam training on RL trajectory
+pairs lowering the loss."""
+import numpy as np
+import pytest
+
+import libapr_b200 as A
+from oracle import bind as B
+from oracle import cnn_oracle as O
+from tests.helpers import gaussian_psf, lib_params, oracle_params, volume
+
+pytestmark = pytest.mark.gpu
+
+# bfloat16 operands, float accumulation on the GPU vs FP64 sums: relative to
+# the output's RMS (the tree means feeding the operands are float sums, so an
+# operand can round to the neighbouring bfloat16 value)
+REL_TOL = 2e-2
+
+
+@pytest.fixture(scope="module")
+def setup():
+    img = volume((24, 40, 36), 12, 5)
+    e, acc, _ = B.orc_get_apr(img, oracle_params(), 1)
+    assert e == 0
+    geo = O.Geometry(acc, B.orc_tree(acc))
+    conv = A.APRConverter("uint16")
+    conv.par = lib_params()
+    apr = A.APR()
+    assert conv.get_apr(apr, img)
+    assert np.array_equal(apr.linear_access()[2], acc.y_vec)
+    apr.init_tree()
+    return img, acc, geo, apr
+
+
+def rel_rms(a, b):
+    return float(np.sqrt(np.mean((a - b) ** 2)) / max(np.sqrt(np.mean(b ** 2)), 1e-30))
+
+
+@pytest.mark.parametrize("relu", [True, False])
+def test_layer_forward_and_backward_match_oracle(setup, relu):
+    import torch
+    img, acc, geo, apr = setup
+    rng = np.random.default_rng(3)
+    H = rng.normal(size=(geo.P, 16)).astype(np.float32)
+    W = (rng.normal(size=(27, 16, 16)) * 0.2).astype(np.float32)
+    b = (rng.normal(size=16) * 0.1).astype(np.float32)
+    G = rng.normal(size=(geo.P, 16)).astype(np.float32)
+    ref = O.layer_forward(geo, H.astype(np.float64), W, b, relu, round_bf16=True)
+    dev = lambda a: torch.from_numpy(a).cuda().contiguous()
+    h, w, bb, g = dev(H), dev(W), dev(b), dev(G)
+    out = torch.empty_like(h)
+    L = A._lib.lib()
+    p = lambda t: A.learned._p(t)
+    A._lib.check(L.aprb_cnn_layer_forward_device(apr._h, p(h), p(w), p(bb), int(relu), p(out), None))
+    got = out.cpu().numpy()
+    assert rel_rms(got, ref) < REL_TOL
+    ref_gin, ref_dW, ref_db = O.layer_backward(geo, H.astype(np.float64), W, ref, G, relu, round_bf16=True)
+    g_in = torch.empty_like(h)
+    dW = torch.zeros_like(w)
+    db = torch.zeros_like(bb)
+    A._lib.check(L.aprb_cnn_layer_backward_device(apr._h, p(h), p(w), p(out), p(g), int(relu), p(g_in), p(dW),
+                                                  p(db), None))
+    torch.cuda.synchronize()
+    assert rel_rms(db.cpu().numpy(), ref_db) < REL_TOL
+    assert rel_rms(dW.cpu().numpy(), ref_dW) < REL_TOL
+    assert rel_rms(g_in.cpu().numpy(), ref_gin) < REL_TOL
+
+
+def test_training_on_rl_pairs_lowers_the_loss(setup):
+    import torch
+    from libapr_b200 import learned as Lr
+    img, acc, geo, apr = setup
+    psf = gaussian_psf(1.2, 5)
+    raw = torch.from_numpy(A.ParticleData().sample_image(apr, img).data.view(np.int16)).cuda()
+    P = raw.numel()
+    u = torch.empty(P, dtype=torch.float32, device="cuda")
+    Lr.rl_iterations(apr, raw, u, psf, 10, resume=False)
+    u0 = u.clone()
+    Lr.rl_iterations(apr, raw, u, psf, 10, resume=True)
+    u1 = u.clone()
+    net = Lr.ProposalCNN(seed=1)
+    first = net.loss(apr, raw, u0, u1, psf)
+    for _ in range(40):
+        net.train_step(apr, raw, u0, u1, psf, lr=3e-3)
+    last = net.loss(apr, raw, u0, u1, psf)
+    print("proposal loss %.4e -> %.4e" % (first, last))
+    assert np.isfinite(last) and last < 0.5 * first
+    # the padded channels stay zero
+    assert float(net.W[0, :, :, 3:].abs().max()) == 0.0
+    assert float(net.W[3, :, 1:, :].abs().max()) == 0.0
