@@ -304,30 +304,11 @@ def bench_rl(A, L, _lib, torch, stream, sptr, args):
     time per iteration, and its relative L2 error after 20/100/500 iterations
     against the FP64 RL (the reference's double instantiation on the GPU, which
     the tests pin bit-exact to the FP64 oracle) after 500 iterations."""
-    import torch.nn.functional as F
+    from libapr_b200 import learned as Lr
     shape = tuple(int(v) for v in args.rl_shape.split(","))
     n = shape[0] * shape[1] * shape[2]
-    gt = torch.empty(shape, dtype=torch.float32, device="cuda")
-    A.synth_ground_truth_device(gt, max(1, int(RL_BLOBS * n / (256 * 1024 * 1024))), (1.0, 4.0), (500.0, 5000.0),
-                                50.0, seed=3000, stream=stream)
-    psf = gaussian_psf()
-    k = torch.from_numpy(psf).cuda().view(1, 1, 5, 5, 5)
-    blurred = F.conv3d(F.pad(gt[None, None], (2, 2, 2, 2, 2, 2), mode="replicate"), k)[0, 0]
-    del gt
-    gen = torch.Generator(device="cuda")
-    gen.manual_seed(3001)
-    noisy = torch.poisson(blurred, generator=gen).clamp_(0, 65535)
-    img = noisy.to(torch.int32).to(torch.int16).contiguous()  # low 16 bits: the uint16 value
-    del blurred, noisy
-    conv = A.APRConverter("float")
-    conv.par = lib_params()
-    apr = A.APR()
-    assert conv.get_apr(apr, img)
+    apr, parts, psf, n_blobs = Lr.deconvolution_workload(shape, seed=3000, stream=stream)
     P = apr.total_number_particles()
-    parts = torch.empty(max(P, 1), dtype=torch.int16, device="cuda")
-    _lib.check(L.aprb_sample_image_device(apr._h, C.c_void_p(img.data_ptr()), C.c_void_p(parts.data_ptr()), sptr))
-    del img
-    apr.init_tree()
     T = apr.total_number_tree_particles()
     pp = C.c_void_p(parts.data_ptr())
     st = C.c_void_p(psf.ctypes.data)
@@ -379,13 +360,16 @@ def bench_rl(A, L, _lib, torch, stream, sptr, args):
             errs[done] = e
             errs_same[done] = float(torch.linalg.norm(o32[:P].double() - f64[done])) / float(
                 torch.linalg.norm(f64[done]))
+    learned = None
+    if not args.no_learned and os.path.exists(Lr.WEIGHTS_FILE):
+        learned = bench_learned(Lr, torch, apr, parts, psf, ref, rnorm, ms32, k_hit, stream)
     bytes_it = 2 * (10 * P + 10 * T) + 2 * P
     hbm, kind = peaks()
     res = {
         "workload": "deconvolution: %dx%dx%d (z,x,y) blob ground truth (bg 50, %d blobs sigma U[1,4], amp "
                     "U[500,5000]) * normalised 5^3 Gaussian PSF sigma 1.2, Poisson, uint16; APR lambda=3 E=0.1 "
                     "Ip_th=0 sigma_th=50 grad_th=10; PSF as APR stencil, downsampled + normalised"
-                    % (shape + (max(1, int(RL_BLOBS * n / (256 * 1024 * 1024))),)),
+                    % (shape + (n_blobs,)),
         "particles": P, "tree_nodes": T,
         "fp32_ms_per_iteration": ms32, "fp32_gpart_per_s": P / (ms32 / 1e3) / 1e9,
         "fp64_ms_per_iteration": ms64 / 500,
@@ -397,9 +381,50 @@ def bench_rl(A, L, _lib, torch, stream, sptr, args):
         "iterations_to_1e-3_of_fp64_500": k_hit,
         "time_to_1e-3_ms": None if k_hit is None else k_hit * ms32,
     }
+    if learned is not None:
+        res["learned_proposal"] = learned
     del o32, o64, parts, f64, ref
     apr._free()
     return res
+
+
+def bench_learned(Lr, torch, apr, raw, psf, ref, rnorm, ms_plain, k_plain, stream, budget=600):
+    """Learned-proposal RL on the same workload (a seed the network was not
+    trained on): device time until the estimate is within 1e-3 relative L2
+    of the FP64 500-iteration solution, beside plain RL's."""
+    net = Lr.ProposalCNN.load()
+    P = raw.numel()
+    u = torch.empty(P, dtype=torch.float32, device="cuda")
+    # time of one proposal (features + 4 layers + apply) for reference
+    Lr.rl_iterations(apr, raw, u, psf, 10, resume=False, stream=stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    scratch = u.clone()
+    e0.record(stream)
+    net.propose(apr, raw, scratch, psf, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_prop = e0.elapsed_time(e1)
+    del scratch
+    acc = Lr.AcceleratedRL(apr, raw, u, psf, net, every=10, warmup=10, stream=stream)
+    total_ms, hit_ms, hit_it, best = 0.0, None, None, float("inf")
+    while acc.iterations < budget:
+        e0.record(stream)
+        acc.step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        total_ms += e0.elapsed_time(e1)
+        err = float(torch.linalg.norm(u.double() - ref)) / rnorm
+        best = min(best, err)
+        if err < 1e-3:
+            hit_ms, hit_it = total_ms, acc.iterations
+            break
+    plain_ms = None if k_plain is None else k_plain * ms_plain
+    return {"weights": os.path.relpath(Lr.WEIGHTS_FILE, ROOT),
+            "network": "4 layers of per-level 3x3x3 stencils, channels 3-16-16-16-1, bf16 tensor-core operands",
+            "proposal_ms": ms_prop, "proposals_tried": acc.tried, "proposals_kept": acc.kept,
+            "time_to_1e-3_ms": hit_ms, "rl_iterations_to_1e-3": hit_it, "best_rel_l2": best,
+            "plain_time_to_1e-3_ms": plain_ms,
+            "time_ratio_learned_over_plain": (hit_ms / plain_ms) if (hit_ms and plain_ms) else None}
 
 
 def main():
@@ -413,6 +438,7 @@ def main():
     ap.add_argument("--no-conv", action="store_true")
     ap.add_argument("--no-batch", action="store_true")
     ap.add_argument("--no-rl", action="store_true")
+    ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--rl-shape", default="256,1024,1024", help="z,x,y of the deconvolution workload")
     ap.add_argument("--image-type", default="float", choices=["float", "uint16"],
                     help="APRConverter ImageType; uint16 throws the reference's overflow error on this volume")

@@ -156,6 +156,57 @@ class ProposalCNN:
         check(lib().aprb_cnn_apply_device(apr._h, _p(acts[-1]), _p(u), _s(stream)))
 
 
+DECONV_PARAMS = dict(lambda_=3.0, rel_error=0.1, Ip_th=0.0, sigma_th=50.0, grad_th=10.0)
+DECONV_BLOBS = 20000  # per 256 x 1024 x 1024 voxels
+
+
+def gaussian_psf(sigma=1.2, ks=5):
+    """Normalised ks^3 Gaussian PSF (float32, z-x-y order)."""
+    g = np.exp(-((np.arange(ks) - ks // 2) ** 2) / (2 * sigma * sigma)).astype(np.float32)
+    p = (g[:, None, None] * g[None, :, None] * g[None, None, :]).astype(np.float32)
+    return (p / p.sum()).astype(np.float32)
+
+
+def deconvolution_workload(shape, seed, image_type="float", stream=None):
+    """The seeded deconvolution workload on the GPU: float ground truth
+    (background 50, Gaussian blobs sigma U[1,4], amplitude U[500,5000], 20000
+    per 256x1024x1024 voxels) blurred by the normalised 5^3 Gaussian PSF
+    (sigma 1.2, replicate border), Poisson noise, uint16; APR with lambda=3,
+    E=0.1, Ip_th=0, sigma_th=50, grad_th=10, its tree built.  Returns
+    (apr, data particles as an int16 CUDA tensor holding uint16 values, psf,
+    number of blobs)."""
+    import torch
+    import torch.nn.functional as F
+    from . import APR, APRConverter, APRParameters, synth_ground_truth_device
+    z, x, y = shape
+    n = z * x * y
+    nb = max(1, int(round(DECONV_BLOBS * n / (256 * 1024 * 1024))))
+    gt = torch.empty(shape, dtype=torch.float32, device="cuda")
+    synth_ground_truth_device(gt, nb, (1.0, 4.0), (500.0, 5000.0), 50.0, seed=seed, stream=stream)
+    psf = gaussian_psf()
+    k = torch.from_numpy(psf).cuda().view(1, 1, 5, 5, 5)
+    blurred = F.conv3d(F.pad(gt[None, None], (2, 2, 2, 2, 2, 2), mode="replicate"), k)[0, 0]
+    del gt
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(seed + 1)
+    noisy = torch.poisson(blurred, generator=gen).clamp_(0, 65535)
+    img = noisy.to(torch.int32).to(torch.int16).contiguous()  # low 16 bits: the uint16 value
+    del blurred, noisy
+    conv = APRConverter(image_type)
+    par = APRParameters()
+    for key, v in DECONV_PARAMS.items():
+        setattr(par, key, v)
+    conv.par = par
+    apr = APR()
+    assert conv.get_apr(apr, img)
+    P = apr.total_number_particles()
+    raw = torch.empty(max(P, 1), dtype=torch.int16, device="cuda")
+    check(lib().aprb_sample_image_device(apr._h, _p(img), _p(raw), _s(stream)))
+    del img
+    apr.init_tree()
+    return apr, raw[:P], psf, nb
+
+
 def rl_objective(apr, raw, u, psf, stream=None):
     """RL's Poisson data-fit objective sum(k - d log k), k = conv(psf_flipped, u)."""
     st = np.ascontiguousarray(psf, np.float32).ravel()
@@ -175,26 +226,32 @@ def rl_iterations(apr, raw, u, psf, n, resume=True, stream=None):
                                             int(resume), _s(stream)))
 
 
-def accelerated_rl(apr, raw, u, psf, net, n_iterations, every=10, warmup=10, stream=None):
-    """RL with learned proposals: after `warmup` plain iterations, every
-    `every` iterations the network proposes a ten-iteration jump; plain RL
-    resumes from it, and the proposal is kept only when RL's data-fit
-    objective does not rise.  Returns (proposals tried, proposals kept)."""
-    import torch
-    tried = kept = 0
-    rl_iterations(apr, raw, u, psf, warmup, resume=False, stream=stream)
-    done = warmup
-    while done < n_iterations:
-        before = rl_objective(apr, raw, u, psf, stream)
-        backup = u.clone()
-        net.propose(apr, raw, u, psf, stream)
-        tried += 1
-        after = rl_objective(apr, raw, u, psf, stream)
-        if not (after <= before) or not torch.isfinite(u).all():
-            u.copy_(backup)
+class AcceleratedRL:
+    """RL with learned proposals, one stage at a time: `warmup` plain
+    iterations first, then per stage the network proposes a ten-iteration
+    jump, the proposal is kept only when RL's data-fit objective does not rise
+    (plain RL is the fallback), and `every` plain iterations follow."""
+
+    def __init__(self, apr, raw, u, psf, net, every=10, warmup=10, stream=None):
+        self.apr, self.raw, self.u, self.psf, self.net = apr, raw, u, psf, net
+        self.every, self.warmup, self.stream = every, warmup, stream
+        self.iterations = 0
+        self.tried = self.kept = 0
+
+    def step(self):
+        import torch
+        if self.iterations == 0:
+            rl_iterations(self.apr, self.raw, self.u, self.psf, self.warmup, resume=False, stream=self.stream)
+            self.iterations = self.warmup
+            return
+        before = rl_objective(self.apr, self.raw, self.u, self.psf, self.stream)
+        backup = self.u.clone()
+        self.net.propose(self.apr, self.raw, self.u, self.psf, self.stream)
+        self.tried += 1
+        after = rl_objective(self.apr, self.raw, self.u, self.psf, self.stream)
+        if not (after <= before) or not bool(torch.isfinite(self.u).all()):
+            self.u.copy_(backup)
         else:
-            kept += 1
-        step = min(every, n_iterations - done)
-        rl_iterations(apr, raw, u, psf, step, resume=True, stream=stream)
-        done += step
-    return tried, kept
+            self.kept += 1
+        rl_iterations(self.apr, self.raw, self.u, self.psf, self.every, resume=True, stream=self.stream)
+        self.iterations += self.every
