@@ -225,7 +225,17 @@ __global__ void __launch_bounds__(256) densify_kernel(ConvLevelArgs a, const uin
     const int yn = a.d.yn;
     T *Rw = D + row * (uint64_t)yn;
     const T miss = VT<T>::miss();
-    for (int y = lane; y < yn; y += 32) Rw[y] = miss;
+    if ((yn * sizeof(T)) % 16 == 0) {  // 16-byte rows: vector stores
+        constexpr int V = 16 / sizeof(T);
+        T pack[V];
+#pragma unroll
+        for (int k = 0; k < V; ++k) pack[k] = miss;
+        const uint4 m4 = *reinterpret_cast<const uint4 *>(pack);
+        uint4 *R4 = reinterpret_cast<uint4 *>(Rw);
+        for (int k = lane; k < yn / V; k += 32) R4[k] = m4;
+    } else {
+        for (int y = lane; y < yn; y += 32) Rw[y] = miss;
+    }
     __syncwarp();
     {
         const uint64_t b = xz_end[a.row_base + row - 1], e = xz_end[a.row_base + row];
@@ -423,24 +433,27 @@ void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, 
     unsigned long long *stale = fb.stale.as<unsigned long long>(1);
     APRB_CUDA(cudaMemsetAsync(stale, 0, sizeof(unsigned long long), s));
     // tree means, fine to coarse
-    for (int t = tg.l_max; t >= tg.l_min; --t) {
-        const int l = t + 1;  // child level
-        if (l > L || l < g.l_min) continue;
-        TreeLevelArgs ta;
-        ta.dt = ld(tg, t);
-        ta.dc = ld(g, l);
-        ta.t_row_base = tg.level_xz[t];
-        ta.c_row_base = g.level_xz[l];
-        ta.ct_row_base = (l <= tg.l_max) ? tg.level_xz[l] : 0;
-        ta.t_cidx = cbase + fi.tree_off[t];
-        ta.c_cidx = cbase + fi.apr_off[l];
-        ta.ct_cidx = (l <= tg.l_max) ? cbase + fi.tree_off[l] : nullptr;
-        const uint64_t rows = (uint64_t)ta.dt.xn * ta.dt.zn;
-        const unsigned ych = (unsigned)((ta.dt.yn + kTW - 1) / kTW);
-        if (rows == 0 || ych == 0) continue;
-        dim3 grid((unsigned)rows, ych);
-        tree_mean_kernel<T><<<grid, 128, 0, s>>>(ta, xz_end, y_vec, in, t_xz_end, t_y_vec, tree);
-        count_launch();
+    {
+        APRB_PROF("tree_mean", s);
+        for (int t = tg.l_max; t >= tg.l_min; --t) {
+            const int l = t + 1;  // child level
+            if (l > L || l < g.l_min) continue;
+            TreeLevelArgs ta;
+            ta.dt = ld(tg, t);
+            ta.dc = ld(g, l);
+            ta.t_row_base = tg.level_xz[t];
+            ta.c_row_base = g.level_xz[l];
+            ta.ct_row_base = (l <= tg.l_max) ? tg.level_xz[l] : 0;
+            ta.t_cidx = cbase + fi.tree_off[t];
+            ta.c_cidx = cbase + fi.apr_off[l];
+            ta.ct_cidx = (l <= tg.l_max) ? cbase + fi.tree_off[l] : nullptr;
+            const uint64_t rows = (uint64_t)ta.dt.xn * ta.dt.zn;
+            const unsigned ych = (unsigned)((ta.dt.yn + kTW - 1) / kTW);
+            if (rows == 0 || ych == 0) continue;
+            dim3 grid((unsigned)rows, ych);
+            tree_mean_kernel<T><<<grid, 128, 0, s>>>(ta, xz_end, y_vec, in, t_xz_end, t_y_vec, tree);
+            count_launch();
+        }
     }
     APRB_CHECK_LAUNCH();
     if (!plan) return;

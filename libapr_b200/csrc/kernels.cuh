@@ -125,7 +125,7 @@ struct CnnGeom {
     uint64_t T;                  // tree nodes
 };
 struct CnnScratch {
-    DevBuf tree, gtree, dense, gdense, gp, wt;
+    DevBuf tree, gtree, dense, gdense, gp, wt, wbf;
 };
 void cnn_build_rows(const Geom &g, const uint64_t *xz_end, uint32_t *prow, cudaStream_t s);
 // one layer: out = act(conv3x3x3(in) + b), W[27][16 co][16 ci] fp32 (bf16 on the tensor cores)

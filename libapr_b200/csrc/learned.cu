@@ -105,14 +105,11 @@ __global__ void tree_up_kernel(TreeMap m, const uint64_t *__restrict__ c_xz_end,
         float w;
         const uint64_t p = tree_parent(m, t_xz_end, t_y_vec, zc, xc, c_y_vec[i], w);
         const float4 *src = reinterpret_cast<const float4 *>(cval + i * kC);
-        float *dst = tree + p * kC;
+        float4 *dst = reinterpret_cast<float4 *>(tree + p * kC);
 #pragma unroll
         for (int q = 0; q < kC / 4; ++q) {
             const float4 v = src[q];
-            atomicAdd(dst + 4 * q + 0, w * v.x);
-            atomicAdd(dst + 4 * q + 1, w * v.y);
-            atomicAdd(dst + 4 * q + 2, w * v.z);
-            atomicAdd(dst + 4 * q + 3, w * v.w);
+            atomicAdd(dst + q, make_float4(w * v.x, w * v.y, w * v.z, w * v.w));  // vector atomic (sm_90+)
         }
     }
 }
@@ -225,88 +222,117 @@ struct ConvArgs {
     int relu;
 };
 
+constexpr int kTilesPerWarp = 8;
+
+// weights as bfloat16, converted once per call: Wb[t][co][ci]
+__global__ void to_bf16_kernel(const float *__restrict__ W, __nv_bfloat16 *__restrict__ Wb, int n) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) Wb[k] = __float2bfloat16_rn(W[k]);
+}
+
 template <int TARGETS>
-__global__ void __launch_bounds__(128) conv16_kernel(ConvArgs a) {
+__global__ void __launch_bounds__(128) conv16_kernel(ConvArgs a, const __nv_bfloat16 *__restrict__ Wb) {
     __shared__ __align__(16) __nv_bfloat16 Ws[kTaps * kC * kC];
     __shared__ float bs[kC];
-    for (int k = threadIdx.x; k < kTaps * kC * kC; k += blockDim.x) Ws[k] = __float2bfloat16_rn(a.W[k]);
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(Wb);
+        uint4 *dst = reinterpret_cast<uint4 *>(Ws);
+        for (int k = threadIdx.x; k < kTaps * kC * kC / 8; k += blockDim.x) dst[k] = src[k];
+    }
     if (threadIdx.x < kC) bs[threadIdx.x] = a.bias ? a.bias[threadIdx.x] : 0.0f;
     __syncthreads();
     const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-    const uint64_t tile = (uint64_t)blockIdx.x * 4 + (threadIdx.x >> 5);
     const uint64_t n = TARGETS == 0 ? a.p1 - a.p0 : ncells(a.d);
-    if (tile * 16 >= n) return;
-    // coordinates of targets g and g + 8 of the tile
-    int tz[2], tx[2], ty[2];
-    bool tv[2];
-    uint64_t tid[2];
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const uint64_t k = tile * 16 + g + 8 * h;
-        tv[h] = k < n;
-        const uint64_t kk = tv[h] ? k : tile * 16;
-        if (TARGETS == 0) {
-            tid[h] = a.p0 + kk;
-            const uint32_t r = a.prow[tid[h]];
-            tz[h] = (int)(r / (uint32_t)a.d.xn);
-            tx[h] = (int)(r % (uint32_t)a.d.xn);
-            ty[h] = a.y_vec[tid[h]];
-        } else {
-            tid[h] = kk;
-            ty[h] = (int)(kk % (uint64_t)a.d.yn);
-            const uint64_t r = kk / (uint64_t)a.d.yn;
-            tx[h] = (int)(r % (uint64_t)a.d.xn);
-            tz[h] = (int)(r / (uint64_t)a.d.xn);
-        }
-    }
-    float c[2][4];
-#pragma unroll
-    for (int nt = 0; nt < 2; ++nt)
-#pragma unroll
-        for (int k = 0; k < 4; ++k) c[nt][k] = 0.0f;
     const uint32_t *D32 = reinterpret_cast<const uint32_t *>(a.D);
     const uint32_t *W32 = reinterpret_cast<const uint32_t *>(Ws);
-#pragma unroll 1
-    for (int t = 0; t < kTaps; ++t) {
-        const int dz = t / 9 - 1, dx = (t / 3) % 3 - 1, dy = t % 3 - 1;
-        uint32_t lo[2], hi[2];
+    const uint64_t first = ((uint64_t)blockIdx.x * 4 + (threadIdx.x >> 5)) * kTilesPerWarp;
+    for (uint64_t tile = first; tile < first + kTilesPerWarp; ++tile) {
+        if (tile * 16 >= n) return;
+        // coordinates of targets g and g + 8 of the tile
+        int tz[2], tx[2], ty[2];
+        bool tv[2];
+        uint64_t tid[2];
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            const int zz = tz[h] + dz, xx = tx[h] + dx, yy = ty[h] + dy;
-            if (zz >= 0 && zz < a.d.zn && xx >= 0 && xx < a.d.xn && yy >= 0 && yy < a.d.yn) {
-                const uint64_t base = (((uint64_t)zz * a.d.xn + xx) * a.d.yn + yy) * (kC / 2);  // in uint32
-                lo[h] = D32[base + q];
-                hi[h] = D32[base + 4 + q];
+            const uint64_t k = tile * 16 + g + 8 * h;
+            tv[h] = k < n;
+            const uint64_t kk = tv[h] ? k : tile * 16;
+            if (TARGETS == 0) {
+                tid[h] = a.p0 + kk;
+                const uint32_t r = a.prow[tid[h]];
+                tz[h] = (int)(r / (uint32_t)a.d.xn);
+                tx[h] = (int)(r % (uint32_t)a.d.xn);
+                ty[h] = a.y_vec[tid[h]];
             } else {
-                lo[h] = 0;
-                hi[h] = 0;
+                tid[h] = kk;
+                ty[h] = (int)(kk % (uint64_t)a.d.yn);
+                const uint64_t r = kk / (uint64_t)a.d.yn;
+                tx[h] = (int)(r % (uint64_t)a.d.xn);
+                tz[h] = (int)(r / (uint64_t)a.d.xn);
             }
         }
-        const uint32_t A[4] = {lo[0], lo[1], hi[0], hi[1]};
+        float c[2][4];
 #pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-            const int co = nt * 8 + g;
-            const uint32_t b0 = W32[(t * kC + co) * (kC / 2) + q];
-            const uint32_t b1 = W32[(t * kC + co) * (kC / 2) + 4 + q];
-            mma_bf16(c[nt], A, b0, b1);
-        }
-    }
+        for (int nt = 0; nt < 2; ++nt)
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        if (!tv[h]) continue;
-        float *o = a.out + tid[h] * kC;
+            for (int k = 0; k < 4; ++k) c[nt][k] = 0.0f;
+#pragma unroll 1
+        for (int t0 = 0; t0 < kTaps; t0 += 3) {  // one (iz, ix) neighbour row, iy = 0..2, loads first
+            const int dz = t0 / 9 - 1, dx = (t0 / 3) % 3 - 1;
+            uint32_t lo[3][2], hi[3][2];
 #pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-            const int co = nt * 8 + 2 * q;
-            float v0 = c[nt][2 * h] + (TARGETS == 0 ? bs[co] : 0.0f);
-            float v1 = c[nt][2 * h + 1] + (TARGETS == 0 ? bs[co + 1] : 0.0f);
-            if (a.relu) {
-                v0 = fmaxf(v0, 0.0f);
-                v1 = fmaxf(v1, 0.0f);
+            for (int h = 0; h < 2; ++h) {
+                const int zz = tz[h] + dz, xx = tx[h] + dx;
+                const bool rin = zz >= 0 && zz < a.d.zn && xx >= 0 && xx < a.d.xn;
+                const uint64_t rbase = ((uint64_t)(rin ? zz : 0) * a.d.xn + (rin ? xx : 0)) * a.d.yn;
+#pragma unroll
+                for (int iy = 0; iy < 3; ++iy) {
+                    const int yy = ty[h] + iy - 1;
+                    if (rin && yy >= 0 && yy < a.d.yn) {
+                        const uint64_t base = (rbase + yy) * (kC / 2);  // in uint32
+                        lo[iy][h] = D32[base + q];
+                        hi[iy][h] = D32[base + 4 + q];
+                    } else {
+                        lo[iy][h] = 0;
+                        hi[iy][h] = 0;
+                    }
+                }
             }
-            *reinterpret_cast<float2 *>(o + co) = make_float2(v0, v1);
+#pragma unroll
+            for (int iy = 0; iy < 3; ++iy) {
+                const int t = t0 + iy;
+                const uint32_t A[4] = {lo[iy][0], lo[iy][1], hi[iy][0], hi[iy][1]};
+#pragma unroll
+                for (int nt = 0; nt < 2; ++nt) {
+                    const int co = nt * 8 + g;
+                    const uint32_t b0 = W32[(t * kC + co) * (kC / 2) + q];
+                    const uint32_t b1 = W32[(t * kC + co) * (kC / 2) + 4 + q];
+                    mma_bf16(c[nt], A, b0, b1);
+                }
+            }
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (!tv[h]) continue;
+            float *o = a.out + tid[h] * kC;
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                const int co = nt * 8 + 2 * q;
+                float v0 = c[nt][2 * h] + (TARGETS == 0 ? bs[co] : 0.0f);
+                float v1 = c[nt][2 * h + 1] + (TARGETS == 0 ? bs[co + 1] : 0.0f);
+                if (a.relu) {
+                    v0 = fmaxf(v0, 0.0f);
+                    v1 = fmaxf(v1, 0.0f);
+                }
+                *reinterpret_cast<float2 *>(o + co) = make_float2(v0, v1);
+            }
         }
     }
+}
+
+unsigned conv16_grid(uint64_t targets) {
+    const uint64_t tiles = (targets + 15) / 16;
+    return blocks_for((tiles + kTilesPerWarp - 1) / kTilesPerWarp, 4);
 }
 
 // ---------------------------------------------------------------------------
@@ -570,15 +596,28 @@ void cnn_layer_forward(const CnnGeom &cg, const float *in, const float *W, const
     APRB_PROF("cnn_forward", s);
     const Geom &g = *cg.g, &tg = *cg.tg;
     float *tree = (float *)sc.tree.get((cg.T ? cg.T : 1) * kC * sizeof(float));
-    tree_means16(g, cg.xz_end, cg.y_vec, tg, cg.t_xz_end, cg.t_y_vec, *cg.fi, in, tree, cg.T, s);
+    __nv_bfloat16 *Wb = (__nv_bfloat16 *)sc.wbf.get(kTaps * kC * kC * sizeof(__nv_bfloat16));
+    to_bf16_kernel<<<blocks_for(kTaps * kC * kC, 256), 256, 0, s>>>(W, Wb, kTaps * kC * kC);
+    count_launch();
+    {
+        APRB_PROF("cnn_tree", s);
+        tree_means16(g, cg.xz_end, cg.y_vec, tg, cg.t_xz_end, cg.t_y_vec, *cg.fi, in, tree, cg.T, s);
+    }
     for (int l = g.l_max; l >= g.l_min; --l) {
         const uint64_t p0 = cg.level_begin[l], p1 = cg.level_begin[l + 1];
         if (p1 == p0) continue;
         const DenseArgs da = dense_args(g, tg, l);
         __nv_bfloat16 *D = (__nv_bfloat16 *)sc.dense.get(ncells(da.d) * kC * sizeof(__nv_bfloat16));
-        densify16_kernel<<<row_grid(da.d), 256, 0, s>>>(da, cg.xz_end, cg.y_vec, in, cg.t_xz_end, cg.t_y_vec, tree, D);
+        {
+            APRB_PROF("cnn_densify", s);
+            densify16_kernel<<<row_grid(da.d), 256, 0, s>>>(da, cg.xz_end, cg.y_vec, in, cg.t_xz_end, cg.t_y_vec,
+                                                            tree, D);
+        }
         ConvArgs ca{da.d, p0, p1, cg.prow, cg.y_vec, D, W, b, out, relu};
-        conv16_kernel<0><<<blocks_for((p1 - p0 + 15) / 16, 4), 128, 0, s>>>(ca);
+        {
+            APRB_PROF("cnn_conv", s);
+            conv16_kernel<0><<<conv16_grid(p1 - p0), 128, 0, s>>>(ca, Wb);
+        }
         count_launch(2);
     }
     APRB_CHECK_LAUNCH();
@@ -596,7 +635,9 @@ void cnn_layer_backward(const CnnGeom &cg, const float *in, const float *W, cons
     tree_means16(g, cg.xz_end, cg.y_vec, tg, cg.t_xz_end, cg.t_y_vec, *cg.fi, in, tree, cg.T, s);
     relu_mask_kernel<<<blocks_for(P * kC, 256), 256, 0, s>>>(g_out, out, gp, P * kC, relu);
     flip_transpose_kernel<<<blocks_for(kTaps * kC * kC, 256), 256, 0, s>>>(W, Wt);
-    count_launch(2);
+    __nv_bfloat16 *Wtb = (__nv_bfloat16 *)sc.wbf.get(kTaps * kC * kC * sizeof(__nv_bfloat16));
+    to_bf16_kernel<<<blocks_for(kTaps * kC * kC, 256), 256, 0, s>>>(Wt, Wtb, kTaps * kC * kC);
+    count_launch(3);
     APRB_CUDA(cudaMemsetAsync(g_in, 0, (P ? P : 1) * kC * sizeof(float), s));
     APRB_CUDA(cudaMemsetAsync(gtree, 0, (cg.T ? cg.T : 1) * kC * sizeof(float), s));
     for (int l = g.l_max; l >= g.l_min; --l) {
@@ -614,7 +655,7 @@ void cnn_layer_backward(const CnnGeom &cg, const float *in, const float *W, cons
         scatter_grad_kernel<<<row_grid(da.d), 256, 0, s>>>(da.d, cg.xz_end, g.level_xz[l], cg.y_vec, gp, D);
         float *G = (float *)sc.gdense.get(nc * kC * sizeof(float));
         ConvArgs cb{da.d, 0, 0, nullptr, nullptr, D, Wt, nullptr, G, 0};
-        conv16_kernel<1><<<blocks_for((nc + 15) / 16, 4), 128, 0, s>>>(cb);
+        conv16_kernel<1><<<conv16_grid(nc), 128, 0, s>>>(cb, Wtb);
         route_kernel<<<row_grid(da.d), 256, 0, s>>>(da.d, cg.xz_end, g.level_xz[l], cg.y_vec, G, g_in, 0, da.d);
         count_launch(5);
         if (da.trow_base) {
