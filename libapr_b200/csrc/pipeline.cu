@@ -7,6 +7,8 @@
 // reference's order (ComputeGradient.hpp, LocalIntensityScale.hpp,
 // LocalParticleCellSet.hpp, APRConverter.hpp); recurrences that the reference
 // runs sequentially along a line run sequentially in one thread here.
+#include <type_traits>
+
 #include "kernels.cuh"
 
 namespace aprb {
@@ -325,8 +327,19 @@ __global__ void offset_copy_kernel(const uint16_t *__restrict__ src, IT *__restr
 // the full-resolution tile plus a one-sample halo, stored with the index
 // clamping both reference functions use (replicate boundary).
 // ---------------------------------------------------------------------------
-constexpr int kGX = 8, kGY = 64, kGZ = 8, kGThreads = 256;
+// 4-byte asynchronous global -> shared copy (cp.async, sm_80+) and the wait
+// for all of a thread's outstanding copies
+__device__ __forceinline__ void cp_async4(float *smem, const float *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+constexpr int kGX = 8, kGY = 64, kGZ = 8, kGThreads = 256, kGSlots = 6;
 constexpr int kTX = 2 * kGX + 2, kTY = 2 * kGY + 2;
+constexpr size_t kGradSmem = sizeof(float) * kGSlots * kTX * kTY;
 
 // PW2: every 2h is a power of two, so dividing by it is the exact multiply by
 // its reciprocal (both round the same real number once).
@@ -334,28 +347,35 @@ template <typename IT, bool PW2>
 __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict__ im, int yn, int xn, int zn,
                                                             IT *__restrict__ grad, float *__restrict__ ids, int yd,
                                                             int xd, int zd, float hx, float hy, float hz) {
-    __shared__ float ring[4][kTX][kTY];
+    // six plane slots: the four planes a step reads and the two the next
+    // step needs, which (ImageType float) arrive by cp.async during the step
+    extern __shared__ float grad_smem[];
+    float(*ring)[kTX][kTY] = reinterpret_cast<float(*)[kTX][kTY]>(grad_smem);
     const int yd0 = blockIdx.x * kGY, xd0 = blockIdx.y * kGX, zd0 = blockIdx.z * kGZ;
     const int zd1 = min(zd0 + kGZ, zd);
     const int xf0 = 2 * xd0 - 1, yf0 = 2 * yd0 - 1;
     const float hx2 = 2 * hx, hy2 = 2 * hy, hz2 = 2 * hz;
     const float ihx2 = 1.0f / hx2, ihy2 = 1.0f / hy2, ihz2 = 1.0f / hz2;
+    constexpr bool kAsync = std::is_same<IT, float>::value;  // 4-byte elements copy asynchronously
 
     auto load = [&](int zf) {  // zf >= -1
-        float(*S)[kTY] = ring[(zf + 4) & 3];
+        float(*S)[kTY] = ring[(zf + kGSlots) % kGSlots];
         const int zc = min(max(zf, 0), zn - 1);
         for (int t = threadIdx.x; t < kTX * kTY; t += kGThreads) {
             const int r = t / kTY, cc = t % kTY;
             const int xg = min(max(xf0 + r, 0), xn - 1), yg = min(max(yf0 + cc, 0), yn - 1);
-            S[r][cc] = (float)im[idx3(yg, xg, zc, yn, xn)];
+            if (kAsync)
+                cp_async4(&S[r][cc], reinterpret_cast<const float *>(im) + idx3(yg, xg, zc, yn, xn));
+            else
+                S[r][cc] = (float)im[idx3(yg, xg, zc, yn, xn)];
         }
     };
     auto gmag = [&](int zf, int xf, int yf) -> float {  // full-res coordinates inside the volume
         if (yn < 2) return 0.0f;
         const int r = xf - xf0, cc = yf - yf0;
-        const float(*C)[kTY] = ring[(zf + 4) & 3];
-        const float(*U)[kTY] = ring[(zf + 3) & 3];
-        const float(*D)[kTY] = ring[(zf + 5) & 3];
+        const float(*C)[kTY] = ring[(zf + kGSlots) % kGSlots];
+        const float(*U)[kTY] = ring[(zf - 1 + kGSlots) % kGSlots];
+        const float(*D)[kTY] = ring[(zf + 1 + kGSlots) % kGSlots];
         float gx, gz, gy;
         if (PW2) {
             gx = (C[r + 1][cc] - C[r - 1][cc]) * ihx2;
@@ -374,10 +394,23 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
 
     load(2 * zd0 - 1);
     load(2 * zd0);
+    if (kAsync) {
+        load(2 * zd0 + 1);
+        load(2 * zd0 + 2);
+        cp_async_wait_all();
+    }
     for (int z = zd0; z < zd1; ++z) {
-        load(2 * z + 1);
-        load(2 * z + 2);
-        __syncthreads();
+        if (kAsync) {
+            __syncthreads();
+            if (z + 1 < zd1) {  // the next step's planes arrive while this step computes
+                load(2 * z + 3);
+                load(2 * z + 4);
+            }
+        } else {
+            load(2 * z + 1);
+            load(2 * z + 2);
+            __syncthreads();
+        }
         for (int t = threadIdx.x; t < kGX * kGY; t += kGThreads) {
             const int xl = t / kGY, yl = t % kGY;
             const int xk = xd0 + xl, k = yd0 + yl;
@@ -393,8 +426,8 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
             const uint64_t o = idx3(k, xk, z, yd, xd);
             grad[o] = to_it<IT>(gmax);
             // mean with the clamped indices of downsample (held by the tile)
-            const float(*A)[kTY] = ring[(z0 + 4) & 3];
-            const float(*B)[kTY] = ring[(z0 + 5) & 3];
+            const float(*A)[kTY] = ring[(z0 + kGSlots) % kGSlots];
+            const float(*B)[kTY] = ring[(z0 + 1 + kGSlots) % kGSlots];
             const int r0 = x0 - xf0, c0 = y0 - yf0;
             float s = A[r0][c0];
             s = s + A[r0][c0 + 1];
@@ -406,6 +439,7 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
             s = s + B[r0 + 1][c0 + 1];
             ids[o] = s * 0.125f;  // == s / 8 exactly
         }
+        if (kAsync) cp_async_wait_all();
         __syncthreads();
     }
 }
@@ -433,10 +467,21 @@ __global__ void __launch_bounds__(256) inv_bspline_kernel(const float *__restric
     float *S = inv_smem;                         // input tile with halo [zz][xx][yy], later the x pass
     float *Yb = inv_smem + kIZH * kIXH * kIYH;  // y pass over the tile's y range [zz][xx][yy]
     const int y0 = blockIdx.x * kIY, x0 = blockIdx.y * kIX, z0 = blockIdx.z * kIZ;
-    for (int t = threadIdx.x; t < kIZH * kIXH * kIYH; t += blockDim.x) {
-        const int yy = t % kIYH, xx = (t / kIYH) % kIXH, zz = t / (kIYH * kIXH);
-        const int yg = y0 - 1 + yy, xg = x0 - 1 + xx, zg = z0 - 1 + zz;
-        if (yg >= 0 && yg < yd && xg >= 0 && xg < xd && zg >= 0 && zg < zd) S[t] = in[idx3(yg, xg, zg, yd, xd)];
+    // asynchronous copies of the tile rows (one warp per (z, x) row, lanes
+    // along y), all in flight before the wait; cells outside the volume stay
+    // unwritten and are never read
+    {
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        for (int r = warp; r < kIZH * kIXH; r += blockDim.x / 32) {
+            const int xg = x0 - 1 + r % kIXH, zg = z0 - 1 + r / kIXH;
+            if (xg < 0 || xg >= xd || zg < 0 || zg >= zd) continue;
+            const float *row = in + idx3(0, xg, zg, yd, xd);
+            for (int yy = lane; yy < kIYH; yy += 32) {
+                const int yg = y0 - 1 + yy;
+                if (yg >= 0 && yg < yd) cp_async4(S + r * kIYH + yy, row + yg);
+            }
+        }
+        cp_async_wait_all();
     }
     __syncthreads();
     // y pass: (z, x) over the tile and its halo, y over the tile
@@ -623,24 +668,24 @@ struct LisOut {
     float rescale;
 };
 
-// x / z box mean (:364-494): one thread per strided line, coalesced over y,
-// with the next sample of the line in flight.
+// x / z box mean (:364-494): one thread per strided line, a warp takes 32
+// lines of adjacent y.  The samples come through shared memory in chunks of
+// 32 (32 coalesced loads in flight per warp); each lane then runs its line's
+// recurrence over the chunk in order.
 template <int OFF, bool FINAL>
 __global__ void __launch_bounds__(128) sat_strided_kernel(const float *__restrict__ in,
                                                           const float *__restrict__ absdiff_ref,
                                                           float *__restrict__ out, int yn, int n, uint64_t stride,
                                                           uint64_t outer_stride, uint64_t nlines, LisOut fo) {
-    constexpr int W = 2 * OFF + 2, U = 1;  // deeper prefetch measured slower
+    constexpr int W = 2 * OFF + 2;
+    __shared__ float tile[4][32][33];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= nlines) return;
-    const uint64_t y = g % (uint64_t)yn, o = g / (uint64_t)yn;
+    const uint64_t g0 = g - lane;  // first line of the warp
+    if (g0 >= nlines) return;
+    const bool valid = g < nlines;
+    const uint64_t y = valid ? g % (uint64_t)yn : 0, o = valid ? g / (uint64_t)yn : 0;
     const uint64_t base = o * outer_stride + y;
-    auto ld = [&](int j) {
-        const uint64_t a = base + (uint64_t)j * stride;
-        float v = in[a];
-        if (absdiff_ref) v = fabsf(v - absdiff_ref[a]);
-        return v;
-    };
     auto emit = [&](int i, float v) {
         if (!FINAL) {
             out[base + (uint64_t)i * stride] = v;
@@ -654,18 +699,25 @@ __global__ void __launch_bounds__(128) sat_strided_kernel(const float *__restric
     float c[W];
 #pragma unroll
     for (int q = 0; q < W; ++q) c[q] = 0.0f;
-    float pre[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) pre[u] = u < n ? ld(u) : 0.0f;
     float C = 0.0f;
     const float dd = (float)(2 * OFF + 1);
-    for (int j0 = 0; j0 < n; j0 += U) {
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int j = j0 + u;
-            if (j < n) {
-                const float v = pre[u];
-                if (j + U < n) pre[u] = ld(j + U);
+    for (int j0 = 0; j0 < n; j0 += 32) {
+        const int m = min(32, n - j0);
+        // lane l loads sample j0 + k of its own line for k < m (coalesced over
+        // the warp's lines), stored transposed: tile[k][lane]
+        for (int k = 0; k < m; ++k) {
+            if (valid) {
+                const uint64_t a = base + (uint64_t)(j0 + k) * stride;
+                float v = in[a];
+                if (absdiff_ref) v = fabsf(v - absdiff_ref[a]);
+                tile[w][k][lane] = v;
+            }
+        }
+        __syncwarp();
+        if (valid) {
+            for (int k = 0; k < m; ++k) {
+                const int j = j0 + k;
+                const float v = tile[w][k][lane];
                 C = (j == 0) ? v : v + C;
 #pragma unroll
                 for (int q = 0; q < W - 1; ++q) c[q] = c[q + 1];
@@ -679,7 +731,9 @@ __global__ void __launch_bounds__(128) sat_strided_kernel(const float *__restric
                 }
             }
         }
+        __syncwarp();
     }
+    if (!valid) return;
     for (int i = n - OFF; i < n; ++i) {
         if (i < 0) continue;
         const int back = (n - 1) - (i - OFF - 1);
@@ -858,12 +912,17 @@ void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *id
             const float m = std::frexp(2.0f * h, &e);
             return m == 0.5f && e > -120 && e < 120;
         };
-        if (pow2(p.dx) && pow2(p.dy) && pow2(p.dz))
-            grad_ds_kernel<IT, true><<<grid, kGThreads, 0, s>>>(work, yn, xn, zn, grad, ids_raw, yd, xd, zd, p.dx, p.dy,
-                                                                p.dz);
-        else
-            grad_ds_kernel<IT, false><<<grid, kGThreads, 0, s>>>(work, yn, xn, zn, grad, ids_raw, yd, xd, zd, p.dx,
-                                                                 p.dy, p.dz);
+        if (pow2(p.dx) && pow2(p.dy) && pow2(p.dz)) {
+            APRB_CUDA(cudaFuncSetAttribute(grad_ds_kernel<IT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kGradSmem));
+            grad_ds_kernel<IT, true><<<grid, kGThreads, kGradSmem, s>>>(work, yn, xn, zn, grad, ids_raw, yd, xd, zd,
+                                                                        p.dx, p.dy, p.dz);
+        } else {
+            APRB_CUDA(cudaFuncSetAttribute(grad_ds_kernel<IT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int)kGradSmem));
+            grad_ds_kernel<IT, false><<<grid, kGThreads, kGradSmem, s>>>(work, yn, xn, zn, grad, ids_raw, yd, xd, zd,
+                                                                         p.dx, p.dy, p.dz);
+        }
         count_launch();
         APRB_CHECK_LAUNCH();
     }
