@@ -130,46 +130,54 @@ __global__ void __launch_bounds__(128) tree_mean_kernel(TreeLevelArgs a, const u
     const int y0 = blockIdx.y * kTW;
     const int cy0 = 2 * y0, cy1 = min(2 * y0 + 2 * kTW, a.dc.yn);
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // the parent range is independent of the children: fetch it first
+    const int nct = nchunk(a.dt.yn);
+    const uint64_t pb = t_xz_end[a.t_row_base + prow - 1];
+    const uint16_t *PC = a.t_cidx + prow * (uint64_t)(nct + 1);
+    const uint64_t ps = pb + PC[y0 / kYC];
+    const uint64_t pend = pb + PC[min(y0 / kYC + kTW / kYC, nct)];
     for (int k = threadIdx.x; k < 4 * 2 * kTW; k += blockDim.x) (&sk[0][0])[k] = 0;
     __syncthreads();
     {
+        // warp w stages child row (2zp + w/2, 2xp + w%2): its particles and
+        // tree nodes (disjoint cells) in one merged pass
         const int cz = 2 * zp + (w >> 1), cx = 2 * xp + (w & 1);
         if (cz < a.dc.zn && cx < a.dc.xn && cy0 < cy1) {
             const uint64_t row = (uint64_t)cz * a.dc.xn + cx;
             const int ncc = nchunk(a.dc.yn);
-            {
-                const uint64_t b = xz_end[a.c_row_base + row - 1], e = xz_end[a.c_row_base + row];
-                const uint64_t s = b + a.c_cidx[row * (uint64_t)(ncc + 1) + cy0 / kYC];
-                for (uint64_t i = s + lane; i < e; i += 32) {
-                    const int y = y_vec[i];
-                    if (y >= cy1) break;
-                    sv[w][y - cy0] = parts[i];
-                    sk[w][y - cy0] = 1;
-                }
-            }
+            const uint64_t s0 = xz_end[a.c_row_base + row - 1] + a.c_cidx[row * (uint64_t)(ncc + 1) + cy0 / kYC];
+            const uint64_t e0 = xz_end[a.c_row_base + row];
+            uint64_t s1 = 0, e1 = 0;
             if (a.ct_row_base) {
-                const uint64_t b = t_xz_end[a.ct_row_base + row - 1], e = t_xz_end[a.ct_row_base + row];
-                const uint64_t s = b + a.ct_cidx[row * (uint64_t)(ncc + 1) + cy0 / kYC];
-                for (uint64_t i = s + lane; i < e; i += 32) {
-                    const int y = t_y_vec[i];
-                    if (y >= cy1) break;
-                    sv[w][y - cy0] = tree[i];
-                    sk[w][y - cy0] = 2;
+                s1 = t_xz_end[a.ct_row_base + row - 1] + a.ct_cidx[row * (uint64_t)(ncc + 1) + cy0 / kYC];
+                e1 = t_xz_end[a.ct_row_base + row];
+            }
+            bool go0 = true, go1 = a.ct_row_base != 0;
+            for (uint64_t t = lane; go0 || go1; t += 32) {
+                const uint64_t i0 = s0 + t, i1 = s1 + t;
+                const bool h0 = go0 && i0 < e0, h1 = go1 && i1 < e1;
+                const int yv0 = h0 ? (int)y_vec[i0] : 0x7fffffff;
+                const int yv1 = h1 ? (int)t_y_vec[i1] : 0x7fffffff;
+                const T v0 = h0 ? parts[i0] : T(0);
+                const T v1 = h1 ? tree[i1] : T(0);
+                if (yv0 < cy1) {
+                    sv[w][yv0 - cy0] = v0;
+                    sk[w][yv0 - cy0] = 1;
                 }
+                if (yv1 < cy1) {
+                    sv[w][yv1 - cy0] = v1;
+                    sk[w][yv1 - cy0] = 2;
+                }
+                go0 = __all_sync(0xffffffffu, h0 && yv0 < cy1);
+                go1 = __all_sync(0xffffffffu, h1 && yv1 < cy1);
             }
         }
     }
     __syncthreads();
-    const int nct = nchunk(a.dt.yn);
-    const uint64_t pb = t_xz_end[a.t_row_base + prow - 1], pe = t_xz_end[a.t_row_base + prow];
-    const uint16_t *PC = a.t_cidx + prow * (uint64_t)(nct + 1);
-    const uint64_t ps = pb + PC[y0 / kYC];
-    const uint64_t pend = pb + PC[min(y0 / kYC + kTW / kYC, nct)];
     float sxz = (float)((((2 * a.dt.xn != a.dc.xn) && (xp == a.dt.xn - 1)) +
                          ((2 * a.dt.zn != a.dc.zn) && (zp == a.dt.zn - 1))) * 2);
     if (sxz == 0) sxz = 1;
     const float syxz = (2 * a.dt.yn != a.dc.yn) ? sxz * 2 : sxz;
-    (void)pe;
     for (uint64_t i = ps + threadIdx.x; i < pend; i += blockDim.x) {
         const int y = t_y_vec[i];
         const float s = (y == a.dt.yn - 1) ? syxz : sxz;

@@ -614,6 +614,9 @@ __global__ void __launch_bounds__(kYWarps * 32) sat_y_kernel(const float *__rest
     }
     for (int y0 = 0; y0 < n; y0 += kTile) {
         const int my = (pm.on_in | pm.on_ref) ? reflect101(y0 + lane - pm.sy, pm.yd) : 0;
+        // partial unrolling: 8 loads in flight per thread at a register count
+        // that keeps 48 warps per SM resident
+#pragma unroll 8
         for (int j = 0; j < kTile; ++j) {
             const uint64_t ln = line0 + j;
             const uint64_t bj = __shfl_sync(0xffffffffu, mbase, j);
@@ -639,6 +642,7 @@ __global__ void __launch_bounds__(kYWarps * 32) sat_y_kernel(const float *__rest
             }
         }
         __syncwarp();
+#pragma unroll 8
         for (int j = 0; j < kTile; ++j) {
             uint64_t ln = line0 + j;
             int i = y0 + lane - OFF;
