@@ -209,6 +209,7 @@ struct ConvLevelArgs {
     const uint16_t *cidx, *pcidx, *tcidx;
     int reflect;
     int mode;
+    int rad;  // stencil radius of the level (densify skips rows no stencil reaches)
 };
 
 // ---------------------------------------------------------------------------
@@ -230,6 +231,21 @@ __global__ void __launch_bounds__(256) densify_kernel(ConvLevelArgs a, const uin
     const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (row >= (uint64_t)a.d.xn * a.d.zn) return;
+    {
+        // only rows within the stencil radius of a row holding particles of the
+        // level are ever read by conv_gather
+        const int z = (int)(row / (uint64_t)a.d.xn), x = (int)(row % (uint64_t)a.d.xn);
+        const int S = 2 * a.rad + 1;
+        bool any = false;
+        for (int k = lane; k < S * S; k += 32) {
+            const int zz = z + k / S - a.rad, xx = x + k % S - a.rad;
+            if (zz >= 0 && zz < a.d.zn && xx >= 0 && xx < a.d.xn) {
+                const uint64_t r = (uint64_t)zz * a.d.xn + xx;
+                any = any || xz_end[a.row_base + r] > xz_end[a.row_base + r - 1];
+            }
+        }
+        if (!__any_sync(0xffffffffu, any)) return;
+    }
     const int yn = a.d.yn;
     T *Rw = D + row * (uint64_t)yn;
     const T miss = VT<T>::miss();
@@ -483,6 +499,7 @@ void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, 
         a.tcidx = l <= tg.l_max ? cbase + fi.tree_off[l] : nullptr;
         a.reflect = plan->reflect;
         a.mode = mode;
+        a.rad = r;
         const T *st = d_stencils + plan->offsets[sn];
         T *D = (T *)fb.dense.get(ncell_of(a.d) * sizeof(T));
         if (side == 3)
