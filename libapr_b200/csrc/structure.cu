@@ -158,6 +158,90 @@ __global__ void fill_parent_kernel(const uint8_t *__restrict__ child, LevelDims 
             }
 }
 
+// Vector forms of set_filler, fill_parent and the equivalence optimisation for
+// levels whose rows are multiples of 8 cells (child) / 4 cells (parent): a
+// thread moves 8 child cells (uint2) or 4 parent cells (uint32) at once, with
+// the same per-cell rules as the scalar kernels.
+__device__ __forceinline__ uint8_t byte_of(uint64_t v, int b) { return (uint8_t)(v >> (8 * b)); }
+
+__global__ void set_filler8_kernel(const uint8_t *__restrict__ parent, LevelDims dp, uint8_t *__restrict__ child,
+                                   LevelDims dc) {
+    const int groups = dc.yn / 8;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (uint64_t)dc.xn * dc.zn * groups) return;
+    const uint64_t row = t / (uint64_t)groups;
+    const int y0 = (int)(t % (uint64_t)groups) * 8;
+    const int x = (int)(row % (uint64_t)dc.xn), z = (int)(row / (uint64_t)dc.xn);
+    uint2 *cp = reinterpret_cast<uint2 *>(child + row * (uint64_t)dc.yn + y0);
+    const uint2 cv = *cp;
+    uint64_t c = ((uint64_t)cv.y << 32) | cv.x;
+    const uint32_t pv = *reinterpret_cast<const uint32_t *>(parent + idx3(y0 / 2, x / 2, z / 2, dp.yn, dp.xn));
+    uint64_t nc = c;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const uint8_t ps = (uint8_t)(pv >> (8 * (b / 2)));
+        if (byte_of(c, b) == kEmpty && (ps == kAscendantNeighbour || ps == kPropagate))
+            nc = (nc & ~(0xffull << (8 * b))) | ((uint64_t)kFiller << (8 * b));
+    }
+    if (nc != c) *cp = make_uint2((uint32_t)nc, (uint32_t)(nc >> 32));
+}
+
+__global__ void eqopt8_kernel(const uint8_t *__restrict__ parent, LevelDims dp, uint8_t *__restrict__ st,
+                              LevelDims d, int min_type) {
+    const int groups = d.yn / 8;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (uint64_t)d.xn * d.zn * groups) return;
+    const uint64_t row = t / (uint64_t)groups;
+    const int y0 = (int)(t % (uint64_t)groups) * 8;
+    const int x = (int)(row % (uint64_t)d.xn), z = (int)(row / (uint64_t)d.xn);
+    const uint32_t pv = *reinterpret_cast<const uint32_t *>(parent + idx3(y0 / 2, x / 2, z / 2, dp.yn, dp.xn));
+    bool any = false;
+#pragma unroll
+    for (int b = 0; b < 4; ++b) {
+        const uint8_t ps = (uint8_t)(pv >> (8 * b));
+        any = any || (ps > 0 && ps <= min_type);
+    }
+    if (!any) return;
+    uint2 *cp = reinterpret_cast<uint2 *>(st + row * (uint64_t)d.yn + y0);
+    const uint2 cv = *cp;
+    uint64_t c = ((uint64_t)cv.y << 32) | cv.x;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const uint8_t ps = (uint8_t)(pv >> (8 * (b / 2)));
+        if (ps > 0 && ps <= min_type) c = (c & ~(0xffull << (8 * b))) | ((uint64_t)kUpsamplingSeed << (8 * b));
+    }
+    *cp = make_uint2((uint32_t)c, (uint32_t)(c >> 32));
+}
+
+__global__ void fill_parent4_kernel(const uint8_t *__restrict__ child, LevelDims dc, uint8_t *__restrict__ parent,
+                                    LevelDims dp) {
+    const int groups = dp.yn / 4;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (uint64_t)dp.xn * dp.zn * groups) return;
+    const uint64_t row = t / (uint64_t)groups;
+    const int y0 = (int)(t % (uint64_t)groups) * 4;
+    const int x = (int)(row % (uint64_t)dp.xn), z = (int)(row / (uint64_t)dp.xn);
+    uint32_t *pp = reinterpret_cast<uint32_t *>(parent + row * (uint64_t)dp.yn + y0);
+    const uint32_t pv = *pp;
+    uint32_t hit = 0;  // bit b: parent y0 + b has a SEED / PROPOGATE / ASCENDANT child
+    for (int cz = 2 * z; cz < min(2 * z + 2, dc.zn); ++cz)
+        for (int cx = 2 * x; cx < min(2 * x + 2, dc.xn); ++cx) {
+            const uint2 cv = *reinterpret_cast<const uint2 *>(child + idx3(2 * y0, cx, cz, dc.yn, dc.xn));
+            const uint64_t c = ((uint64_t)cv.y << 32) | cv.x;
+#pragma unroll
+            for (int b = 0; b < 8; ++b) {
+                const uint8_t q = byte_of(c, b);
+                if (q == kSeed || q == kPropagate || q == kAscendant) hit |= 1u << (b / 2);
+            }
+        }
+    uint32_t nv = pv;
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+        if ((hit >> b & 1) && (uint8_t)(pv >> (8 * b)) != kSeed)
+            nv = (nv & ~(0xffu << (8 * b))) | ((uint32_t)kAscendant << (8 * b));
+    if (nv != pv) *pp = nv;
+}
+
 // equivalence optimisation (LinearAccess.hpp:262-293) for one level
 __global__ void eqopt_kernel(const uint8_t *__restrict__ parent, LevelDims dp, uint8_t *__restrict__ st, LevelDims d,
                              int min_type) {
@@ -378,6 +462,32 @@ __global__ void pyr_mean_u16_kernel(const uint16_t *__restrict__ in, LevelDims d
 // sample_parts_from_img_downsampled_patch (ParticleData.hpp:330-372): the
 // particles of global rows (zlo + offz .. zhi - 1 + offz, x) of one level take
 // the tile's pyramid value at tile-local plane z.
+// The same mean for input rows that are multiples of 4 samples: a thread
+// reads 4 x uint2 (4 samples each) and writes two outputs as one uint32.
+__global__ void pyr_mean_u16x2_kernel(const uint16_t *__restrict__ in, LevelDims di, uint16_t *__restrict__ out,
+                                      LevelDims d) {
+    const int groups = d.yn / 2;
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (uint64_t)d.xn * d.zn * groups) return;
+    const uint64_t row = t / (uint64_t)groups;
+    const int y = (int)(t % (uint64_t)groups) * 2;
+    const int x = (int)(row % (uint64_t)d.xn), z = (int)(row / (uint64_t)d.xn);
+    const int x1 = min(2 * x + 1, di.xn - 1), z1 = min(2 * z + 1, di.zn - 1);
+    const int xs[2] = {2 * x, x1}, zs[2] = {2 * z, z1};
+    unsigned s0 = 0, s1 = 0;
+    // same summation order per output as pyr_mean_u16_kernel: (y0,x0,z0) (y1,x0,z0)
+    // (y0,x1,z0) (y1,x1,z0) then z1; integer sums, so the order is immaterial
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const uint2 v = *reinterpret_cast<const uint2 *>(in + idx3(2 * y, xs[b], zs[a], di.yn, di.xn));
+            s0 += (v.x & 0xffffu) + (v.x >> 16);
+            s1 += (v.y & 0xffffu) + (v.y >> 16);
+        }
+    *reinterpret_cast<uint32_t *>(out + row * (uint64_t)d.yn + y) = (s0 >> 3) | ((s1 >> 3) << 16);
+}
+
 __global__ void gather_patch_kernel(const uint16_t *__restrict__ im, LevelDims dp, int zlo, int zhi, int offz,
                                     int gzn, const uint64_t *__restrict__ xz_end, uint64_t row_base,
                                     const uint16_t *__restrict__ y_vec, uint16_t *__restrict__ parts) {
@@ -485,15 +595,24 @@ void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s, bool fill
         const dim3 dgrid((g.y_num[l] + kDY - 1) / kDY, (g.x_num[l] + kDX - 1) / kDX, (g.z_num[l] + kDZ - 1) / kDZ);
         if (l != top) {
             dilate_kernel<0><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
-            set_filler_kernel<<<blocks_for(ncell(g, l + 1), 256), 256, 0, s>>>(pm.status[l], dims(g, l),
-                                                                              pm.status[l + 1], dims(g, l + 1));
+            if (g.y_num[l + 1] % 8 == 0)
+                set_filler8_kernel<<<blocks_for(ncell(g, l + 1) / 8, 256), 256, 0, s>>>(pm.status[l], dims(g, l),
+                                                                                       pm.status[l + 1],
+                                                                                       dims(g, l + 1));
+            else
+                set_filler_kernel<<<blocks_for(ncell(g, l + 1), 256), 256, 0, s>>>(pm.status[l], dims(g, l),
+                                                                                  pm.status[l + 1], dims(g, l + 1));
             count_launch(2);
         }
         dilate_kernel<1><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
         count_launch();
         if (l - 1 >= lmin) {
-            fill_parent_kernel<<<blocks_for(ncell(g, l - 1), 256), 256, 0, s>>>(pm.status[l], dims(g, l),
-                                                                               pm.status[l - 1], dims(g, l - 1));
+            if (g.y_num[l] % 8 == 0)
+                fill_parent4_kernel<<<blocks_for(ncell(g, l - 1) / 4, 256), 256, 0, s>>>(
+                    pm.status[l], dims(g, l), pm.status[l - 1], dims(g, l - 1));
+            else
+                fill_parent_kernel<<<blocks_for(ncell(g, l - 1), 256), 256, 0, s>>>(pm.status[l], dims(g, l),
+                                                                                   pm.status[l - 1], dims(g, l - 1));
             count_launch();
         }
     }
@@ -506,8 +625,12 @@ uint64_t launch_linear_counts(const Geom &g, Pyramid &pm, uint64_t *xz_end, uint
     const int L = g.l_max, lmin = g.l_min;
     APRB_CUDA(cudaMemsetAsync(xz_end, 0, n_xz * sizeof(uint64_t), s));
     for (int l = lmin + 1; l < L; ++l) {
-        eqopt_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(pm.status[l - 1], dims(g, l - 1), pm.status[l],
-                                                                 dims(g, l), min_type);
+        if (g.y_num[l] % 8 == 0)
+            eqopt8_kernel<<<blocks_for(ncell(g, l) / 8, 256), 256, 0, s>>>(pm.status[l - 1], dims(g, l - 1),
+                                                                          pm.status[l], dims(g, l), min_type);
+        else
+            eqopt_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(pm.status[l - 1], dims(g, l - 1), pm.status[l],
+                                                                     dims(g, l), min_type);
         count_launch();
     }
     for (int l = lmin; l < L - 1; ++l) {
@@ -567,7 +690,12 @@ void launch_sample(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec,
     lev[L] = img;
     for (int l = L - 1; l >= lmin; --l) {
         uint16_t *o = base + off[l];
-        pyr_mean_u16_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(lev[l + 1], dims(g, l + 1), o, dims(g, l));
+        if (g.y_num[l + 1] % 4 == 0 && (l + 1 < L || ((uintptr_t)img & 7) == 0))
+            pyr_mean_u16x2_kernel<<<blocks_for(ncell(g, l) / 2, 256), 256, 0, s>>>(lev[l + 1], dims(g, l + 1), o,
+                                                                                dims(g, l));
+        else
+            pyr_mean_u16_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(lev[l + 1], dims(g, l + 1), o,
+                                                                            dims(g, l));
         count_launch();
         lev[l] = o;
     }
