@@ -132,6 +132,9 @@ TRAFFIC_PER_VOXEL = {
     "gradient_ds": ((537.404672e6 + 120.107008e6) / (128 * 1024 * 1024),
                     "ncu, 128x1024x1024 float capture scaled by voxels "
                     "(profiles/grad_ds_kernel_float_128x1024x1024.md)"),
+    "bspline_y": ((651.044608e6 + 883.089920e6) / (128 * 1024 * 1024),
+                  "ncu, 128x1024x1024 float capture scaled by voxels "
+                  "(profiles/iir_y_kernel_float_128x1024x1024.md)"),
     "bspline_x": ((1.010519e9 + 970.695680e6) / (128 * 1024 * 1024),
                   "ncu, 128x1024x1024 float capture scaled by voxels "
                   "(profiles/iir_strided_kernel_float_128x1024x1024.md)"),

@@ -358,16 +358,30 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
     const float ihx2 = 1.0f / hx2, ihy2 = 1.0f / hy2, ihz2 = 1.0f / hz2;
     constexpr bool kAsync = std::is_same<IT, float>::value;  // 4-byte elements copy asynchronously
 
+    // a thread fills the same (clamped) tile positions t = threadIdx.x + k *
+    // kGThreads of every plane: their in-plane source offsets once
+    constexpr int kLoads = (kTX * kTY + kGThreads - 1) / kGThreads;
+    uint64_t src_off[kLoads];
+#pragma unroll
+    for (int k = 0; k < kLoads; ++k) {
+        const int t = threadIdx.x + k * kGThreads;
+        const int r = t / kTY, cc = t % kTY;
+        const int xg = min(max(xf0 + r, 0), xn - 1), yg = min(max(yf0 + cc, 0), yn - 1);
+        src_off[k] = (uint64_t)xg * (uint64_t)yn + (uint64_t)yg;
+    }
     auto load = [&](int zf) {  // zf >= -1
-        float(*S)[kTY] = ring[(zf + kGSlots) % kGSlots];
+        float *S = &ring[(zf + kGSlots) % kGSlots][0][0];
         const int zc = min(max(zf, 0), zn - 1);
-        for (int t = threadIdx.x; t < kTX * kTY; t += kGThreads) {
-            const int r = t / kTY, cc = t % kTY;
-            const int xg = min(max(xf0 + r, 0), xn - 1), yg = min(max(yf0 + cc, 0), yn - 1);
-            if (kAsync)
-                cp_async4(&S[r][cc], reinterpret_cast<const float *>(im) + idx3(yg, xg, zc, yn, xn));
-            else
-                S[r][cc] = (float)im[idx3(yg, xg, zc, yn, xn)];
+        const IT *plane = im + (uint64_t)zc * (uint64_t)xn * (uint64_t)yn;
+#pragma unroll
+        for (int k = 0; k < kLoads; ++k) {
+            const int t = threadIdx.x + k * kGThreads;
+            if (t < kTX * kTY) {
+                if (kAsync)
+                    cp_async4(S + t, reinterpret_cast<const float *>(plane) + src_off[k]);
+                else
+                    S[t] = (float)plane[src_off[k]];
+            }
         }
     };
     auto gmag = [&](int zf, int xf, int yf) -> float {  // full-res coordinates inside the volume
