@@ -4,11 +4,13 @@
 // point returns an aprb_status.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <memory>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "kernels.cuh"
@@ -70,6 +72,8 @@ void *pool_alloc(size_t bytes, cudaStream_t s) {
 // calling thread uses on one device (they only live for the duration of one
 // call).  Calls issued by one thread on different streams that overlap on the
 // GPU share these buffers; use one thread per concurrent stream.
+constexpr int kBatchWorkers = 6;  // host threads of the batch entry point
+
 struct ThreadScratch {
     DevBuf scan_tmp, tree_vals, pyr, parts_f, parts_u16, out_f, rb, stencils, stencils_f, io_in, t_flags, obj;
     FilterBuffers fb;
@@ -305,17 +309,17 @@ PixelOut<IT> pixel_stages(aprb_converter *c, const aprb_params &p, const uint16_
     const int yd = (yn + 1) / 2, xd = (xn + 1) / 2, zd = (zn + 1) / 2;
     const uint64_t n = (uint64_t)yn * xn * zn, nd = (uint64_t)yd * xd * zd;
     const bool is_u16 = sizeof(IT) == 2;
-    unsigned *mm = c->mm.as<unsigned>(2);
-    float *d_off = c->offset.as<float>(1);
-    unsigned *d_err = c->err.as<unsigned>(1);
+    unsigned *mm = c->mm.as_on<unsigned>(2, s);
+    float *d_off = c->offset.as_on<float>(1, s);
+    unsigned *d_err = c->err.as_on<unsigned>(1, s);
     launch_minmax_offset(img, n, mm, d_off, is_u16 && p.lambda > 0, s);
-    IT *work = c->work.as<IT>(n);
+    IT *work = c->work.as_on<IT>(n, s);
     launch_smooth<IT>(img, work, yn, xn, zn, p.lambda, d_off, d_err, s);
-    IT *grad = c->grad.as<IT>(nd);
-    float *ids_raw = c->ids_raw.as<float>(nd);
-    float *ids = c->ids.as<float>(nd);
+    IT *grad = c->grad.as_on<IT>(nd, s);
+    float *ids_raw = c->ids_raw.as_on<float>(nd, s);
+    float *ids = c->ids.as_on<float>(nd, s);
     launch_gradient<IT>(work, yn, xn, zn, grad, ids_raw, ids, yd, xd, zd, p, s);
-    float *lis = c->lis.as<float>(nd);
+    float *lis = c->lis.as_on<float>(nd, s);
     launch_local_intensity_scale(ids, lis, yd, xd, zd, p, c->lisb, s);
     return PixelOut<IT>{grad, lis, ids, d_off, nd};
 }
@@ -365,14 +369,14 @@ void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, i
     a->org[2] = zn;
     const int L = g.l_max;
     const uint64_t nd = (uint64_t)((yn + 1) / 2) * ((xn + 1) / 2) * ((zn + 1) / 2);
-    APRB_CUDA(cudaMemsetAsync(c->err.as<unsigned>(1), 0, sizeof(unsigned), s));
+    APRB_CUDA(cudaMemsetAsync(c->err.as_on<unsigned>(1, s), 0, sizeof(unsigned), s));
     PixelOut<IT> po = pixel_stages<IT>(c, p, img, yn, xn, zn, s);
     IT *grad = po.grad;
     float *lis = po.lis, *ids = po.ids;
     const float *d_off = po.d_off;
     if (c->keep) {
-        APRB_CUDA(cudaMemcpyAsync(c->grad_keep.as<IT>(nd), grad, nd * sizeof(IT), cudaMemcpyDeviceToDevice, s));
-        APRB_CUDA(cudaMemcpyAsync(c->lis_keep.as<float>(nd), lis, nd * sizeof(float), cudaMemcpyDeviceToDevice, s));
+        APRB_CUDA(cudaMemcpyAsync(c->grad_keep.as_on<IT>(nd, s), grad, nd * sizeof(IT), cudaMemcpyDeviceToDevice, s));
+        APRB_CUDA(cudaMemcpyAsync(c->lis_keep.as_on<float>(nd, s), lis, nd * sizeof(float), cudaMemcpyDeviceToDevice, s));
     }
 
     // particle-cell pyramid: pct levels l_min..L-1 (PullingScheme.hpp:92-104)
@@ -383,8 +387,8 @@ void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, i
         off[l] = tot;
         tot += ((uint64_t)g.y_num[l] * g.x_num[l] * g.z_num[l] + 15) & ~uint64_t(15);
     }
-    uint8_t *st = c->pyr_status.as<uint8_t>(tot ? tot : 16);
-    uint8_t *lv = c->pyr_level.as<uint8_t>(tot ? tot : 16);
+    uint8_t *st = c->pyr_status.as_on<uint8_t>(tot ? tot : 16, s);
+    uint8_t *lv = c->pyr_level.as_on<uint8_t>(tot ? tot : 16, s);
     for (int l = g.l_min; l <= top; ++l) {
         pm.status[l] = st + off[l];
         pm.level[l] = lv + off[l];
@@ -392,7 +396,7 @@ void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, i
     if (top >= g.l_min) {
         launch_levels<IT>(grad, lis, ids, nd, d_off, p, L, top, pm.level[top], pm.status[top], c->keep, s);
     } else {
-        uint8_t *lvl = c->pyr_level.as<uint8_t>(nd), *sts = c->pyr_status.as<uint8_t>(nd);
+        uint8_t *lvl = c->pyr_level.as_on<uint8_t>(nd, s), *sts = c->pyr_status.as_on<uint8_t>(nd, s);
         launch_levels<IT>(grad, lis, ids, nd, d_off, p, L, top, lvl, sts, c->keep, s);
     }
     if (L > 2) launch_pulling_scheme(g, pm, s);
@@ -416,21 +420,21 @@ void run_get_apr_by_block(aprb_converter *c, const aprb_params &p, const uint16_
     a->org[1] = xn;
     a->org[2] = zn;
     const int L = g.l_max, top = L - 1;
-    APRB_CUDA(cudaMemsetAsync(c->err.as<unsigned>(1), 0, sizeof(unsigned), s));
+    APRB_CUDA(cudaMemsetAsync(c->err.as_on<unsigned>(1, s), 0, sizeof(unsigned), s));
     Pyramid pm;
     uint64_t tot = 0, off[32] = {};
     for (int l = g.l_min; l <= top; ++l) {
         off[l] = tot;
         tot += ((uint64_t)g.y_num[l] * g.x_num[l] * g.z_num[l] + 15) & ~uint64_t(15);
     }
-    uint8_t *st = c->pyr_status.as<uint8_t>(tot ? tot : 16);
+    uint8_t *st = c->pyr_status.as_on<uint8_t>(tot ? tot : 16, s);
     APRB_CUDA(cudaMemsetAsync(st, 0, tot ? tot : 16, s));
     for (int l = g.l_min; l <= top; ++l) pm.status[l] = st + off[l];
     const int nb = std::max(zn / zblock, 1);
     for (int b = 0; b < nb; ++b) {
         const ZTile t = z_tile(b, nb, zn, zblock, ghost);
         PixelOut<IT> po = pixel_stages<IT>(c, p, img + (uint64_t)(t.z0 - t.gl) * xn * yn, yn, xn, t.pz, s);
-        uint8_t *lev = c->pyr_level.as<uint8_t>(po.nd);
+        uint8_t *lev = c->pyr_level.as_on<uint8_t>(po.nd, s);
         launch_levels<IT>(po.grad, po.lis, po.ids, po.nd, po.d_off, p, L, top, lev, nullptr, 0, s);
         launch_fill_patch(g, pm, lev, t, c->tile_pyr, s);
     }
@@ -494,7 +498,7 @@ aprb_status aprb_get_apr_by_block(aprb_converter *c, const aprb_params *p, const
         ARG_CHECK(c && img, "null argument");
         const uint64_t n = (uint64_t)y_num * x_num * z_num;
         cudaStream_t s = cudaStreamPerThread;
-        uint16_t *d = c->img.as<uint16_t>(n);
+        uint16_t *d = c->img.as_on<uint16_t>(n, s);
         APRB_CUDA(cudaMemcpyAsync(d, img, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
         get_apr_by_block_impl(c, p, d, y_num, x_num, z_num, z_block_size, ghost_z, s, out);
     });
@@ -504,19 +508,51 @@ aprb_status aprb_get_apr_batch_device(aprb_converter *c, const aprb_params *p, i
                                       const aprb_volume *volumes, int z_block_size, int ghost_z, void *stream,
                                       aprb_apr **outs) {
     return guarded([&] {
-        ARG_CHECK(n_volumes >= 0 && (n_volumes == 0 || (volumes && outs)), "invalid volume list");
+        require_device();
+        ARG_CHECK(c && p && n_volumes >= 0 && (n_volumes == 0 || (volumes && outs)), "invalid volume list");
         for (int i = 0; i < n_volumes; ++i) outs[i] = nullptr;
-        try {
-            for (int i = 0; i < n_volumes; ++i)
-                get_apr_by_block_impl(c, p, volumes[i].img_dev, volumes[i].y_num, volumes[i].x_num,
-                                      volumes[i].z_num, z_block_size, ghost_z, (cudaStream_t)stream, &outs[i]);
-        } catch (...) {
-            for (int i = 0; i < n_volumes; ++i) {
-                delete outs[i];
-                outs[i] = nullptr;
+        if (n_volumes == 0) return;
+        // the inputs are ready once the caller's stream is
+        APRB_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+        int dev = 0;
+        APRB_CUDA(cudaGetDevice(&dev));
+        // Volumes are independent: kBatchWorkers host threads, each with its
+        // own converter (same ImageType) and stream, take volumes in turn, so
+        // the small volumes' launches and particle-count reads overlap.
+        const int nw = std::min(n_volumes, kBatchWorkers);
+        std::vector<aprb_status> st(nw, APRB_OK);
+        std::vector<std::string> msg(nw);
+        std::atomic<int> next(0);
+        auto work = [&](int w) {
+            cudaSetDevice(dev);
+            aprb_converter wc;
+            wc.image_type = c->image_type;
+            cudaStream_t ws = nullptr;
+            st[w] = guarded([&] {
+                APRB_CUDA(cudaStreamCreateWithFlags(&ws, cudaStreamNonBlocking));
+                for (int i = next.fetch_add(1); i < n_volumes; i = next.fetch_add(1))
+                    get_apr_by_block_impl(&wc, p, volumes[i].img_dev, volumes[i].y_num, volumes[i].x_num,
+                                          volumes[i].z_num, z_block_size, ghost_z, ws, &outs[i]);
+            });
+            if (st[w] != APRB_OK) msg[w] = aprb_last_error();
+            if (ws) {
+                cudaStreamSynchronize(ws);
+                cudaStreamDestroy(ws);
             }
-            throw;
-        }
+        };
+        std::vector<std::thread> threads;
+        for (int w = 1; w < nw; ++w) threads.emplace_back(work, w);
+        work(0);
+        for (auto &t : threads) t.join();
+        for (int w = 0; w < nw; ++w)
+            if (st[w] != APRB_OK) {
+                for (int i = 0; i < n_volumes; ++i) {
+                    delete outs[i];
+                    outs[i] = nullptr;
+                }
+                set_error(msg[w]);
+                throw Error{st[w]};
+            }
     });
 }
 
@@ -532,7 +568,7 @@ aprb_status aprb_get_apr(aprb_converter *c, const aprb_params *p, const uint16_t
         ARG_CHECK(c && img, "null argument");
         const uint64_t n = (uint64_t)y_num * x_num * z_num;
         cudaStream_t s = cudaStreamPerThread;
-        uint16_t *d = c->img.as<uint16_t>(n);
+        uint16_t *d = c->img.as_on<uint16_t>(n, s);
         APRB_CUDA(cudaMemcpyAsync(d, img, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
         get_apr_impl(c, p, d, y_num, x_num, z_num, s, out);
     });

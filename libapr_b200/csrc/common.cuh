@@ -93,6 +93,31 @@ struct DevBuf {
     T *as_pooled(size_t n, cudaStream_t s) {
         return (T *)get_pooled(n * sizeof(T), s);
     }
+    // Grows through the pool without a device synchronisation: the old block
+    // is freed in the order of stream s.  For buffers whose every use is on
+    // the stream of a call that synchronises that stream before it returns
+    // (the converter's), so no other stream can still be using the block.
+    void *get_on(size_t bytes, cudaStream_t s) {
+        if (bytes > cap) {
+            if (p) {
+                if (pooled)
+                    cudaFreeAsync(p, s);
+                else
+                    cudaFree(p);
+            }
+            p = nullptr;
+            cap = 0;
+            const size_t want = bytes ? bytes : 16;
+            p = pool_alloc(want, s);
+            cap = want;
+            pooled = true;
+        }
+        return p;
+    }
+    template <typename T>
+    T *as_on(size_t n, cudaStream_t s) {
+        return (T *)get_on(n * sizeof(T), s);
+    }
     void release() {
         if (p) {
             if (pooled) {

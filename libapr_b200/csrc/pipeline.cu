@@ -1001,7 +1001,7 @@ void launch_local_intensity_scale(const float *ids, float *lis, int yd, int xd, 
     const LisWindow w = lis_window(p, yd, xd, zd);
     const uint64_t nd = (uint64_t)yd * xd * zd;
     if (p.constant_intensity_scale || w.n_active == 0) {
-        double *sum = b.scalars.as<double>(2);
+        double *sum = b.scalars.as_on<double>(2, s);
         unsigned *mb = (unsigned *)(sum + 1);
         unsigned init_min = 0xffffffffu;
         APRB_CUDA(cudaMemsetAsync(sum, 0, sizeof(double), s));
@@ -1037,11 +1037,11 @@ void launch_local_intensity_scale(const float *ids, float *lis, int yd, int xd, 
     // window itself.
     const bool fold_pad = w.active[0], fold_unpad = last >= 1;
     const uint64_t pn = (uint64_t)py * px * pz;
-    float *A = b.a.as<float>(pn);
-    float *C2 = b.c.as<float>(pn);
+    float *A = b.a.as_on<float>(pn, s);
+    float *C2 = b.c.as_on<float>(pn, s);
     const float *padded = ids;
     if (!fold_pad) {
-        float *B = b.padded.as<float>(pn);
+        float *B = b.padded.as_on<float>(pn, s);
         pad_reflect_kernel<<<blocks_for(pn, 256), 256, 0, s>>>(ids, yd, xd, zd, B, sy, sx, sz, py, px, pz);
         count_launch();
         APRB_CHECK_LAUNCH();

@@ -573,7 +573,7 @@ unsigned row_blocks(uint64_t rows) { return blocks_for(rows * 32, 256); }
 
 void inclusive_scan_u64(uint64_t *data, uint64_t n, DevBuf &tmp, cudaStream_t s) {
     const uint64_t nb = (n + kScanBlock - 1) / kScanBlock;
-    uint64_t *sums = tmp.as<uint64_t>(nb + 1);
+    uint64_t *sums = tmp.as_on<uint64_t>(nb + 1, s);
     scan_sums_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(data, n, sums);
     scan_sums_serial_kernel<<<1, 1024, 0, s>>>(sums, nb);
     scan_apply_kernel<<<(unsigned)nb, kScanThreads, 0, s>>>(data, n, sums);
@@ -760,7 +760,7 @@ void launch_fill_patch(const Geom &g, Pyramid &pm, const uint8_t *lev_top, const
         off[l] = total;
         total += ((uint64_t)pd[l].yn * pd[l].xn * pd[l].zn + 15) & ~uint64_t(15);
     }
-    uint8_t *base = tmp.as<uint8_t>(total ? total : 16);
+    uint8_t *base = tmp.as_on<uint8_t>(total ? total : 16, s);
     const uint8_t *lev = lev_top;
     for (int l = top; l >= lmin; --l) {
         uint8_t *cur = nullptr;
