@@ -73,6 +73,29 @@ void *pool_alloc(size_t bytes, cudaStream_t s) {
 // call).  Calls issued by one thread on different streams that overlap on the
 // GPU share these buffers; use one thread per concurrent stream.
 constexpr int kBatchWorkers = 6;  // host threads of the batch entry point
+constexpr int kSampleChunk = 16;  // fewest planes per transfer chunk of host-buffer sampling (even)
+
+// Copy streams of the calling thread and device: uploads and downloads run
+// beside the compute stream.
+struct Streams3 {
+    cudaStream_t up = nullptr, down = nullptr;
+    ~Streams3() {
+        if (up) cudaStreamDestroy(up);
+        if (down) cudaStreamDestroy(down);
+    }
+};
+static Streams3 &transfer_streams() {
+    thread_local std::map<int, std::unique_ptr<Streams3>> per_device;
+    int dev = 0;
+    APRB_CUDA(cudaGetDevice(&dev));
+    auto &p = per_device[dev];
+    if (!p) {
+        p.reset(new Streams3());
+        APRB_CUDA(cudaStreamCreateWithFlags(&p->up, cudaStreamNonBlocking));
+        APRB_CUDA(cudaStreamCreateWithFlags(&p->down, cudaStreamNonBlocking));
+    }
+    return *p;
+}
 
 struct ThreadScratch {
     DevBuf scan_tmp, tree_vals, pyr, parts_f, parts_u16, out_f, rb, stencils, stencils_f, io_in, t_flags, obj;
@@ -303,18 +326,25 @@ struct PixelOut {
     uint64_t nd;
 };
 
+// With `host` set, img is the device buffer that the volume is copied into
+// from host memory, chunk by chunk on stream `up`, overlapped with smoothing.
 template <typename IT>
 PixelOut<IT> pixel_stages(aprb_converter *c, const aprb_params &p, const uint16_t *img, int yn, int xn, int zn,
-                          cudaStream_t s) {
+                          cudaStream_t s, const uint16_t *host = nullptr, cudaStream_t up = nullptr) {
     const int yd = (yn + 1) / 2, xd = (xn + 1) / 2, zd = (zn + 1) / 2;
     const uint64_t n = (uint64_t)yn * xn * zn, nd = (uint64_t)yd * xd * zd;
     const bool is_u16 = sizeof(IT) == 2;
     unsigned *mm = c->mm.as_on<unsigned>(2, s);
     float *d_off = c->offset.as_on<float>(1, s);
     unsigned *d_err = c->err.as_on<unsigned>(1, s);
-    launch_minmax_offset(img, n, mm, d_off, is_u16 && p.lambda > 0, s);
     IT *work = c->work.as_on<IT>(n, s);
-    launch_smooth<IT>(img, work, yn, xn, zn, p.lambda, d_off, d_err, s);
+    if (host) {
+        launch_upload_smooth<IT>(host, const_cast<uint16_t *>(img), work, yn, xn, zn, p.lambda, mm, d_off,
+                                 is_u16 && p.lambda > 0, d_err, s, up);
+    } else {
+        launch_minmax_offset(img, n, mm, d_off, is_u16 && p.lambda > 0, s);
+        launch_smooth<IT>(img, work, yn, xn, zn, p.lambda, d_off, d_err, s);
+    }
     IT *grad = c->grad.as_on<IT>(nd, s);
     float *ids_raw = c->ids_raw.as_on<float>(nd, s);
     float *ids = c->ids.as_on<float>(nd, s);
@@ -361,7 +391,7 @@ void build_structure(aprb_converter *c, const aprb_params &p, Pyramid &pm, aprb_
 
 template <typename IT>
 void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, int yn, int xn, int zn,
-                 cudaStream_t s, aprb_apr *a) {
+                 cudaStream_t s, aprb_apr *a, const uint16_t *host = nullptr, cudaStream_t up = nullptr) {
     Geom &g = a->g;
     a->n_xz = apr_geometry(yn, xn, zn, g);
     a->org[0] = yn;
@@ -370,7 +400,7 @@ void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, i
     const int L = g.l_max;
     const uint64_t nd = (uint64_t)((yn + 1) / 2) * ((xn + 1) / 2) * ((zn + 1) / 2);
     APRB_CUDA(cudaMemsetAsync(c->err.as_on<unsigned>(1, s), 0, sizeof(unsigned), s));
-    PixelOut<IT> po = pixel_stages<IT>(c, p, img, yn, xn, zn, s);
+    PixelOut<IT> po = pixel_stages<IT>(c, p, img, yn, xn, zn, s, host, up);
     IT *grad = po.grad;
     float *lis = po.lis, *ids = po.ids;
     const float *d_off = po.d_off;
@@ -444,7 +474,7 @@ void run_get_apr_by_block(aprb_converter *c, const aprb_params &p, const uint16_
 }
 
 void get_apr_impl(aprb_converter *c, const aprb_params *p, const uint16_t *img_dev, int y, int x, int z,
-                  cudaStream_t s, aprb_apr **out) {
+                  cudaStream_t s, aprb_apr **out, const uint16_t *host = nullptr, cudaStream_t up = nullptr) {
     require_device();
     ARG_CHECK(c && p && img_dev && out, "null argument");
     ARG_CHECK(y >= 1 && x >= 1 && z >= 1, "dimensions must be positive");
@@ -457,9 +487,9 @@ void get_apr_impl(aprb_converter *c, const aprb_params *p, const uint16_t *img_d
     ARG_CHECK(par.rel_error > 0, "rel_error must be positive");
     std::unique_ptr<aprb_apr> a(new aprb_apr());
     if (c->image_type == APRB_IMAGE_U16)
-        run_get_apr<uint16_t>(c, par, img_dev, y, x, z, s, a.get());
+        run_get_apr<uint16_t>(c, par, img_dev, y, x, z, s, a.get(), host, up);
     else
-        run_get_apr<float>(c, par, img_dev, y, x, z, s, a.get());
+        run_get_apr<float>(c, par, img_dev, y, x, z, s, a.get(), host, up);
     *out = a.release();
 }
 
@@ -569,8 +599,15 @@ aprb_status aprb_get_apr(aprb_converter *c, const aprb_params *p, const uint16_t
         const uint64_t n = (uint64_t)y_num * x_num * z_num;
         cudaStream_t s = cudaStreamPerThread;
         uint16_t *d = c->img.as_on<uint16_t>(n, s);
-        APRB_CUDA(cudaMemcpyAsync(d, img, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
-        get_apr_impl(c, p, d, y_num, x_num, z_num, s, out);
+        // the copy goes in z-chunks on the transfer stream, overlapped with
+        // the smoothing of the chunks already on the device
+        cudaStream_t up = transfer_streams().up;
+        try {
+            get_apr_impl(c, p, d, y_num, x_num, z_num, s, out, img, up);
+        } catch (...) {
+            cudaStreamSynchronize(up);  // no copy from the caller's buffer outlives the call
+            throw;
+        }
     });
 }
 
@@ -741,13 +778,80 @@ aprb_status aprb_sample_image(const aprb_apr *a, const uint16_t *img, uint16_t *
         require_device();
         ARG_CHECK(a && img && parts, "null argument");
         cudaStream_t s = cudaStreamPerThread;
-        const uint64_t n = (uint64_t)a->org[0] * a->org[1] * a->org[2];
+        const Geom &g = a->g;
+        const int L = g.l_max, zn = a->org[2];
+        const uint64_t n = (uint64_t)a->org[0] * a->org[1] * zn;
+        const uint64_t plane = (uint64_t)a->org[0] * a->org[1];
         uint16_t *di = scratch().io_in.as<uint16_t>(n);
         uint16_t *dp = scratch().parts_u16.as<uint16_t>(a->P ? a->P : 1);
-        APRB_CUDA(cudaMemcpyAsync(di, img, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
-        launch_sample(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, di, dp, scratch().pyr, s);
-        if (a->P) APRB_CUDA(cudaMemcpyAsync(parts, dp, a->P * sizeof(uint16_t), cudaMemcpyDeviceToHost, s));
+        const uint64_t *xz = (const uint64_t *)a->xz_end.p;
+        const uint16_t *yv = (const uint16_t *)a->y_vec.p;
+        // about 2^26 voxels (128 MiB) per chunk, an even number of planes
+        const uint64_t want = ((uint64_t(1) << 26) / std::max<uint64_t>(plane, 1)) & ~uint64_t(1);
+        const int chunk = (int)std::max<uint64_t>(kSampleChunk, want);
+        if (zn < 2 * chunk || L <= g.l_min || a->P == 0) {
+            APRB_CUDA(cudaMemcpyAsync(di, img, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+            launch_sample(g, xz, yv, di, dp, scratch().pyr, s);
+            if (a->P) APRB_CUDA(cudaMemcpyAsync(parts, dp, a->P * sizeof(uint16_t), cudaMemcpyDeviceToHost, s));
+            APRB_CUDA(cudaStreamSynchronize(s));
+            return;
+        }
+        // Pipelined over z-chunks: chunk k's upload
+        // (stream up), its level l_max gather and means (stream s) and the
+        // download of its particles (stream down) overlap the neighbouring
+        // chunks'.  The level l_max particles of planes [z0, z1) are one
+        // contiguous range of the output; the coarser levels come last.
+        Streams3 &st3 = transfer_streams();
+        const int nch = (zn + chunk - 1) / chunk;
+        std::vector<uint64_t> bnd(nch + 1);
+        for (int k = 0; k <= nch; ++k) {
+            const uint64_t row = (uint64_t)std::min(k * chunk, zn) * g.x_num[L];
+            APRB_CUDA(cudaMemcpyAsync(&bnd[k], xz + g.level_xz[L] + row - 1, sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                      s));
+        }
         APRB_CUDA(cudaStreamSynchronize(s));
+        uint64_t off[32] = {};
+        uint16_t *base = sample_pyramid(g, scratch().pyr, off);
+        std::vector<cudaEvent_t> ev(2 * nch + 2, nullptr);
+        try {
+            for (auto &e : ev) APRB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            APRB_CUDA(cudaEventRecord(ev[2 * nch + 1], s));
+            APRB_CUDA(cudaStreamWaitEvent(st3.up, ev[2 * nch + 1], 0));
+            for (int k = 0; k < nch; ++k) {
+                const int z0 = k * chunk, z1 = std::min(zn, z0 + chunk);
+                APRB_CUDA(cudaMemcpyAsync(di + (uint64_t)z0 * plane, img + (uint64_t)z0 * plane,
+                                          (uint64_t)(z1 - z0) * plane * sizeof(uint16_t), cudaMemcpyHostToDevice,
+                                          st3.up));
+                APRB_CUDA(cudaEventRecord(ev[2 * k], st3.up));
+                APRB_CUDA(cudaStreamWaitEvent(s, ev[2 * k], 0));
+                launch_sample_slab(g, xz, yv, di, z0, z1, base + off[L - 1], dp, s);
+                APRB_CUDA(cudaEventRecord(ev[2 * k + 1], s));
+            }
+            launch_sample_coarse(g, xz, yv, base, off, dp, s);
+            APRB_CUDA(cudaEventRecord(ev[2 * nch], s));
+            // downloads are queued after all uploads: a copy to pageable
+            // memory returns only once done, which would hold back the
+            // next chunk's upload
+            for (int k = 0; k < nch; ++k) {
+                APRB_CUDA(cudaStreamWaitEvent(st3.down, ev[2 * k + 1], 0));
+                if (bnd[k + 1] > bnd[k])
+                    APRB_CUDA(cudaMemcpyAsync(parts + bnd[k], dp + bnd[k], (bnd[k + 1] - bnd[k]) * sizeof(uint16_t),
+                                              cudaMemcpyDeviceToHost, st3.down));
+            }
+            APRB_CUDA(cudaStreamWaitEvent(st3.down, ev[2 * nch], 0));
+            if (bnd[0] > 0)
+                APRB_CUDA(cudaMemcpyAsync(parts, dp, bnd[0] * sizeof(uint16_t), cudaMemcpyDeviceToHost, st3.down));
+            APRB_CUDA(cudaStreamSynchronize(st3.down));
+            APRB_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            cudaStreamSynchronize(st3.up);
+            cudaStreamSynchronize(st3.down);
+            cudaStreamSynchronize(s);
+            for (auto &e : ev)
+                if (e) cudaEventDestroy(e);
+            throw;
+        }
+        for (auto &e : ev) cudaEventDestroy(e);
     });
 }
 

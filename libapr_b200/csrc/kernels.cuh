@@ -19,6 +19,7 @@ constexpr uint8_t kEmpty = 0, kSeed = 1, kBoundary = 2, kFiller = 3, kUpsampling
 struct IIRDev {
     float b1, b2, norm;
     int minLen;
+    const float *bc;  // folded boundary vectors bc1..bc4, [4][minLen]
 };
 
 struct LisBuffers {
@@ -30,6 +31,10 @@ void launch_minmax_offset(const uint16_t *img, uint64_t n, unsigned *mm, float *
 template <typename IT>
 void launch_smooth(const uint16_t *img, IT *work, int yn, int xn, int zn, float lambda, const float *d_offset,
                    unsigned *d_err, cudaStream_t s);
+template <typename IT>
+void launch_upload_smooth(const uint16_t *host, uint16_t *img, IT *work, int yn, int xn, int zn, float lambda,
+                          unsigned *mm, float *d_offset, int apply, unsigned *d_err, cudaStream_t s,
+                          cudaStream_t up);
 template <typename IT>
 void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *ids_raw, float *ids, int yd, int xd,
                      int zd, const aprb_params &p, cudaStream_t s);
@@ -70,6 +75,13 @@ void inclusive_scan_u64(uint64_t *data, uint64_t n, DevBuf &tmp, cudaStream_t s)
 // sampling (ParticleData.hpp:222-261)
 void launch_sample(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const uint16_t *img,
                    uint16_t *parts, DevBuf &pyr, cudaStream_t s);
+
+// pieces of sampling for a host-buffer call that pipelines its transfers
+uint16_t *sample_pyramid(const Geom &g, DevBuf &pyr, uint64_t off[32]);
+void launch_sample_slab(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const uint16_t *img, int z0,
+                        int z1, uint16_t *pyr_top, uint16_t *parts, cudaStream_t s);
+void launch_sample_coarse(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, uint16_t *base,
+                          const uint64_t off[32], uint16_t *parts, cudaStream_t s);
 
 // sampling into caller-provided scratch (no allocation): the pyramid levels
 // below l_max need sample_scratch_elems(g) uint16 elements

@@ -7,13 +7,14 @@
 // reference's order (ComputeGradient.hpp, LocalIntensityScale.hpp,
 // LocalParticleCellSet.hpp, APRConverter.hpp); recurrences that the reference
 // runs sequentially along a line run sequentially in one thread here.
+#include <map>
+#include <mutex>
 #include <type_traits>
+#include <vector>
 
 #include "kernels.cuh"
 
 namespace aprb {
-
-__constant__ float c_bc[4][kMaxK0];
 
 // ---------------------------------------------------------------------------
 // a1: compute_bspline_offset (AutoParameters.hpp:164-197) -- min/max reduction
@@ -121,13 +122,13 @@ __global__ void __launch_bounds__(kYWarps * 32) iir_y_kernel(const uint16_t *__r
         const uint16_t *L = src + myline * (uint64_t)yn;
         for (int k = 0; k < c.minLen; ++k) {
             float v = raw_to_it<IT>(L[k], off);
-            t1 = t1 + c_bc[0][k] * v;
-            t2 = t2 + c_bc[1][k] * v;
+            t1 = t1 + __ldg(c.bc + k) * v;
+            t2 = t2 + __ldg(c.bc + c.minLen + k) * v;
         }
         for (int k = 0; k < c.minLen; ++k) {
             float v = raw_to_it<IT>(L[yn - 1 - k], off);
-            t3 = t3 + c_bc[2][k] * v;
-            t4 = t4 + c_bc[3][k] * v;
+            t3 = t3 + __ldg(c.bc + 2 * c.minLen + k) * v;
+            t4 = t4 + __ldg(c.bc + 3 * c.minLen + k) * v;
         }
     }
     const int ya = 2 * lane, yb = 2 * lane + 1;  // columns this lane moves
@@ -256,10 +257,10 @@ __global__ void iir_strided_kernel(IT *__restrict__ im, int yn, int n, uint64_t 
     for (int i = 0; i < c.minLen; ++i) {
         float a = (float)L[(uint64_t)i * stride];
         float b = (float)L[(uint64_t)(n - 1 - i) * stride];
-        v1 = v1 + c_bc[0][i] * a;
-        v2 = v2 + c_bc[1][i] * a;
-        v3 = v3 + c_bc[2][i] * b;
-        v4 = v4 + c_bc[3][i] * b;
+        v1 = v1 + __ldg(c.bc + i) * a;
+        v2 = v2 + __ldg(c.bc + c.minLen + i) * a;
+        v3 = v3 + __ldg(c.bc + 2 * c.minLen + i) * b;
+        v4 = v4 + __ldg(c.bc + 3 * c.minLen + i) * b;
     }
     L[0] = to_it<IT>(rnd_it<IT>(v2, err));
     L[stride] = to_it<IT>(rnd_it<IT>(v1, err));
@@ -835,19 +836,31 @@ __global__ void levels_kernel(IT *__restrict__ grad, float *__restrict__ lis, co
 // ---------------------------------------------------------------------------
 // host drivers
 // ---------------------------------------------------------------------------
-void upload_bc(const IIRCoef &c, cudaStream_t s) {
+// Folded boundary vectors ([4][minLen] floats) of one filter, uploaded once
+// per device and content and then kept: converters on other host threads and
+// streams may use other filters at the same time, so no launch's vectors are
+// ever overwritten.
+static const float *bc_table(const IIRCoef &c) {
     if (c.minLen > kMaxK0) {
         set_error("recursive filter support exceeds the supported maximum (lambda too large)");
         throw Error{APRB_ERR_UNSUPPORTED};
     }
-    float h[4][kMaxK0] = {};
-    for (int k = 0; k < c.minLen; ++k) {
-        h[0][k] = c.bc1[k];
-        h[1][k] = c.bc2[k];
-        h[2][k] = c.bc3[k];
-        h[3][k] = c.bc4[k];
-    }
-    APRB_CUDA(cudaMemcpyToSymbolAsync(c_bc, h, sizeof(h), 0, cudaMemcpyHostToDevice, s));
+    int dev = 0;
+    APRB_CUDA(cudaGetDevice(&dev));
+    std::vector<float> h;
+    h.reserve(4 * c.minLen + 1);
+    h.push_back((float)dev);
+    for (const auto *v : {&c.bc1, &c.bc2, &c.bc3, &c.bc4}) h.insert(h.end(), v->begin(), v->begin() + c.minLen);
+    static std::mutex mu;
+    static std::map<std::vector<float>, float *> *tab = new std::map<std::vector<float>, float *>();
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = tab->find(h);
+    if (it != tab->end()) return it->second;
+    float *d = nullptr;
+    APRB_CUDA(cudaMalloc(&d, std::max<size_t>(4 * c.minLen, 1) * sizeof(float)));
+    if (c.minLen) APRB_CUDA(cudaMemcpy(d, h.data() + 1, 4 * c.minLen * sizeof(float), cudaMemcpyHostToDevice));
+    tab->emplace(std::move(h), d);
+    return d;
 }
 
 static IIRDev dev_coef(const IIRCoef &c) {
@@ -856,6 +869,7 @@ static IIRDev dev_coef(const IIRCoef &c) {
     d.b2 = c.b2;
     d.norm = c.norm;
     d.minLen = c.minLen;
+    d.bc = bc_table(c);
     return d;
 }
 
@@ -874,23 +888,21 @@ void launch_minmax_offset(const uint16_t *img, uint64_t n, unsigned *mm, float *
     APRB_CHECK_LAUNCH();
 }
 
+// y pass (or the plain offset copy) then x pass of planes that the caller
+// chose: both only read lines that lie inside the planes.
 template <typename IT>
-void launch_smooth(const uint16_t *img, IT *work, int yn, int xn, int zn, float lambda, const float *d_offset,
-                   unsigned *d_err, cudaStream_t s) {
+static void launch_smooth_yx(const uint16_t *img, IT *work, int yn, int xn, int zn, float lambda,
+                             const float *d_offset, unsigned *d_err, cudaStream_t s) {
     const uint64_t n = (uint64_t)yn * xn * zn;
-    bool copied = false;
     if (lambda > 0 && yn > 2) {
         APRB_PROF("bspline_y", s);
-        IIRCoef c = iir_coefficients(lambda, yn);
-        upload_bc(c, s);
+        const IIRDev c = dev_coef(iir_coefficients(lambda, yn));
         const uint64_t nlines = (uint64_t)xn * zn;
         const unsigned blocks = blocks_for(nlines, kYWarps * kTile);
-        iir_y_kernel<IT><<<blocks, kYWarps * 32, 0, s>>>(img, work, yn, nlines, dev_coef(c), d_offset, d_err);
+        iir_y_kernel<IT><<<blocks, kYWarps * 32, 0, s>>>(img, work, yn, nlines, c, d_offset, d_err);
         count_launch();
         APRB_CHECK_LAUNCH();
-        copied = true;
-    }
-    if (!copied) {
+    } else {
         APRB_PROF("offset_copy", s);
         unsigned blocks = (unsigned)std::min<uint64_t>(blocks_for(n, 256), 148u * 32u);
         offset_copy_kernel<IT><<<blocks, 256, 0, s>>>(img, work, n, d_offset);
@@ -899,24 +911,96 @@ void launch_smooth(const uint16_t *img, IT *work, int yn, int xn, int zn, float 
     }
     if (lambda > 0 && xn > 2) {
         APRB_PROF("bspline_x", s);
-        IIRCoef c = iir_coefficients(lambda, xn);
-        upload_bc(c, s);
+        const IIRDev c = dev_coef(iir_coefficients(lambda, xn));
         const uint64_t nlines = (uint64_t)yn * zn;
         iir_strided_kernel<IT><<<blocks_for(nlines, 128), 128, 0, s>>>(work, yn, xn, (uint64_t)yn,
-                                                                     (uint64_t)xn * yn, nlines, dev_coef(c), d_err);
+                                                                     (uint64_t)xn * yn, nlines, c, d_err);
         count_launch();
         APRB_CHECK_LAUNCH();
     }
+}
+
+template <typename IT>
+static void launch_smooth_z(IT *work, int yn, int xn, int zn, float lambda, unsigned *d_err, cudaStream_t s) {
     if (lambda > 0 && zn > 2) {
         APRB_PROF("bspline_z", s);
-        IIRCoef c = iir_coefficients(lambda, zn);
-        upload_bc(c, s);
+        const IIRDev c = dev_coef(iir_coefficients(lambda, zn));
         const uint64_t nlines = (uint64_t)yn * xn;
         iir_strided_kernel<IT><<<blocks_for(nlines, 128), 128, 0, s>>>(work, yn, zn, (uint64_t)xn * yn, (uint64_t)yn,
-                                                                     nlines, dev_coef(c), d_err);
+                                                                     nlines, c, d_err);
         count_launch();
         APRB_CHECK_LAUNCH();
     }
+}
+
+template <typename IT>
+void launch_smooth(const uint16_t *img, IT *work, int yn, int xn, int zn, float lambda, const float *d_offset,
+                   unsigned *d_err, cudaStream_t s) {
+    launch_smooth_yx<IT>(img, work, yn, xn, zn, lambda, d_offset, d_err, s);
+    launch_smooth_z<IT>(work, yn, xn, zn, lambda, d_err, s);
+}
+
+// Offset and smoothing of a volume that is still in host memory: it is copied
+// to `img` in z-chunks on stream `up`, and each chunk's work starts on s as
+// soon as its copy has landed, while the later chunks are still on the bus.
+// With an offset that needs the whole volume's min/max (uint16 ImageType with
+// smoothing) the chunks overlap the min/max reduction only; otherwise they
+// overlap the y and x passes.  The z pass needs every plane and runs last.
+template <typename IT>
+void launch_upload_smooth(const uint16_t *host, uint16_t *img, IT *work, int yn, int xn, int zn, float lambda,
+                          unsigned *mm, float *d_offset, int apply, unsigned *d_err, cudaStream_t s,
+                          cudaStream_t up) {
+    const uint64_t plane = (uint64_t)yn * xn;
+    const int chunk = (int)std::max<uint64_t>(4, (uint64_t(1) << 27) / std::max<uint64_t>(plane, 1));
+    const int nch = (zn + chunk - 1) / chunk;
+    std::vector<cudaEvent_t> ev(nch, nullptr);
+    for (auto &e : ev) APRB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    struct Release {
+        std::vector<cudaEvent_t> &ev;
+        ~Release() {
+            for (auto e : ev)
+                if (e) cudaEventDestroy(e);
+        }
+    } release{ev};
+    if (apply) {
+        const unsigned init[2] = {0xffffu, 0u};
+        APRB_CUDA(cudaMemcpyAsync(mm, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    }
+    // the copies start after all of s's earlier work, which includes the
+    // stream-ordered allocation of img
+    cudaEvent_t ready = nullptr;
+    APRB_CUDA(cudaEventCreateWithFlags(&ready, cudaEventDisableTiming));
+    ev.push_back(ready);
+    APRB_CUDA(cudaEventRecord(ready, s));
+    APRB_CUDA(cudaStreamWaitEvent(up, ready, 0));
+    for (int k = 0; k < nch; ++k) {
+        const int z0 = k * chunk, z1 = std::min(zn, z0 + chunk);
+        const uint64_t o = (uint64_t)z0 * plane, cnt = (uint64_t)(z1 - z0) * plane;
+        APRB_CUDA(cudaMemcpyAsync(img + o, host + o, cnt * sizeof(uint16_t), cudaMemcpyHostToDevice, up));
+        APRB_CUDA(cudaEventRecord(ev[k], up));
+        APRB_CUDA(cudaStreamWaitEvent(s, ev[k], 0));
+        if (apply) {
+            APRB_PROF("offset", s);
+            unsigned blocks = (unsigned)std::min<uint64_t>(blocks_for(cnt, 256), 148u * 16u);
+            minmax_u16_kernel<<<blocks, 256, 0, s>>>(img + o, cnt, mm);
+            count_launch();
+            APRB_CHECK_LAUNCH();
+        } else {
+            if (k == 0) {
+                offset_kernel<<<1, 32, 0, s>>>(mm, d_offset, 0);
+                count_launch();
+                APRB_CHECK_LAUNCH();
+            }
+            launch_smooth_yx<IT>(img + o, work + o, yn, xn, z1 - z0, lambda, d_offset, d_err, s);
+        }
+    }
+    if (apply) {
+        offset_kernel<<<1, 32, 0, s>>>(mm, d_offset, 1);
+        count_launch();
+        APRB_CHECK_LAUNCH();
+        launch_smooth_yx<IT>(img, work, yn, xn, zn, lambda, d_offset, d_err, s);
+    }
+    launch_smooth_z<IT>(work, yn, xn, zn, lambda, d_err, s);
 }
 
 template <typename IT>
@@ -1095,6 +1179,10 @@ void launch_levels(IT *grad, float *lis, const float *ids, uint64_t nd, const fl
     APRB_CHECK_LAUNCH();
 }
 
+template void launch_upload_smooth<uint16_t>(const uint16_t *, uint16_t *, uint16_t *, int, int, int, float,
+                                             unsigned *, float *, int, unsigned *, cudaStream_t, cudaStream_t);
+template void launch_upload_smooth<float>(const uint16_t *, uint16_t *, float *, int, int, int, float, unsigned *,
+                                          float *, int, unsigned *, cudaStream_t, cudaStream_t);
 template void launch_smooth<uint16_t>(const uint16_t *, uint16_t *, int, int, int, float, const float *, unsigned *,
                                       cudaStream_t);
 template void launch_smooth<float>(const uint16_t *, float *, int, int, int, float, const float *, unsigned *,

@@ -706,6 +706,62 @@ void launch_sample(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec,
     APRB_CHECK_LAUNCH();
 }
 
+// Pieces of launch_sample for a host-buffer call that overlaps its transfers:
+// the level l_max - 1 means and the level l_max gather of the full-resolution
+// planes [z0, z1) (z0 even; z1 even or the last plane), then the coarser
+// levels once level l_max - 1 is complete.
+uint16_t *sample_pyramid(const Geom &g, DevBuf &pyr, uint64_t off[32]) {
+    uint64_t total = 0;
+    for (int l = g.l_min; l < g.l_max; ++l) {
+        off[l] = total;
+        total += (ncell(g, l) + 7) & ~uint64_t(7);
+    }
+    return pyr.as<uint16_t>(total ? total : 8);
+}
+
+void launch_sample_slab(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const uint16_t *img, int z0,
+                        int z1, uint16_t *pyr_top, uint16_t *parts, cudaStream_t s) {
+    const int L = g.l_max;
+    const uint64_t plane = (uint64_t)g.y_num[L] * g.x_num[L];
+    const LevelDims di{g.y_num[L], g.x_num[L], z1 - z0};
+    const uint16_t *slab = img + (uint64_t)z0 * plane;
+    if (L > g.l_min) {
+        const LevelDims d{g.y_num[L - 1], g.x_num[L - 1], (z1 - z0 + 1) / 2};
+        uint16_t *o = pyr_top + (uint64_t)(z0 / 2) * d.yn * d.xn;
+        const uint64_t nout = (uint64_t)d.yn * d.xn * d.zn;
+        if (di.yn % 4 == 0 && ((uintptr_t)slab & 7) == 0)
+            pyr_mean_u16x2_kernel<<<blocks_for(nout / 2, 256), 256, 0, s>>>(slab, di, o, d);
+        else
+            pyr_mean_u16_kernel<<<blocks_for(nout, 256), 256, 0, s>>>(slab, di, o, d);
+        count_launch();
+    }
+    const uint64_t rows = (uint64_t)(z1 - z0) * di.xn;
+    gather_kernel<<<row_blocks(rows), 256, 0, s>>>(slab, di, xz_end, g.level_xz[L] + (uint64_t)z0 * di.xn, y_vec,
+                                                   parts);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+}
+
+void launch_sample_coarse(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, uint16_t *base,
+                          const uint64_t off[32], uint16_t *parts, cudaStream_t s) {
+    const int L = g.l_max, lmin = g.l_min;
+    for (int l = L - 2; l >= lmin; --l) {
+        uint16_t *o = base + off[l];
+        const uint16_t *in = base + off[l + 1];
+        if (g.y_num[l + 1] % 4 == 0)
+            pyr_mean_u16x2_kernel<<<blocks_for(ncell(g, l) / 2, 256), 256, 0, s>>>(in, dims(g, l + 1), o, dims(g, l));
+        else
+            pyr_mean_u16_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(in, dims(g, l + 1), o, dims(g, l));
+        count_launch();
+    }
+    for (int l = lmin; l < L; ++l) {
+        gather_kernel<<<row_blocks(nrow(g, l)), 256, 0, s>>>(base + off[l], dims(g, l), xz_end, g.level_xz[l], y_vec,
+                                                            parts);
+        count_launch();
+    }
+    APRB_CHECK_LAUNCH();
+}
+
 uint64_t sample_scratch_elems(const Geom &g) {
     uint64_t total = 0;
     for (int l = g.l_min; l < g.l_max; ++l) total += (ncell(g, l) + 7) & ~uint64_t(7);

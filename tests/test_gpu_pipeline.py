@@ -111,3 +111,35 @@ def test_empty_and_flat_inputs():
     assert conv.get_apr(apr, tiny)
     e, acc, _ = B.orc_get_apr(tiny, oracle_params(), 1)
     assert np.array_equal(apr.linear_access()[2], acc.y_vec)
+
+
+@pytest.mark.parametrize("image_type", ["float", "uint16"])
+def test_host_calls_copy_in_chunks_like_device_calls(image_type):
+    """Host-buffer get_apr and sample_image copy a volume with large planes in
+    z-chunks, overlapped with the smoothing and the sampling; the structure
+    and the particles equal those of the device-buffer calls.  2048 x 2048
+    planes, 33 of them: several chunks, an odd last plane."""
+    import ctypes as C
+
+    import torch
+    from libapr_b200._lib import check, lib
+
+    z, x, y = 33, 2048, 2048
+    dev = torch.empty((z, x, y), dtype=torch.int16, device="cuda")
+    A.synth_blobs_device(dev, 2000, sigma=(2.0, 8.0), amp=(500.0, 6000.0), seed=17)
+    torch.cuda.synchronize()
+    host = dev.cpu().numpy().view(np.uint16)
+    conv = A.APRConverter(image_type)
+    conv.par = lib_params()
+    a_dev, a_host = A.APR(), A.APR()
+    assert conv.get_apr(a_dev, dev)
+    assert conv.get_apr(a_host, host)
+    for u, v in zip(a_dev.linear_access(), a_host.linear_access()):
+        assert np.array_equal(u, v)
+    P = a_dev.total_number_particles()
+    assert a_dev.level_max() > a_dev.level_min() and P > 0
+    pd = torch.empty(P, dtype=torch.int16, device="cuda")
+    check(lib().aprb_sample_image_device(a_dev._h, C.c_void_p(dev.data_ptr()), C.c_void_p(pd.data_ptr()), None))
+    torch.cuda.synchronize()
+    ph = A.ParticleData().sample_image(a_host, host).data
+    assert np.array_equal(ph, pd.cpu().numpy().view(np.uint16))
