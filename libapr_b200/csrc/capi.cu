@@ -183,7 +183,7 @@ struct aprb_converter {
     int keep = 0;
     int dims[3] = {0, 0, 0};  // y, x, z of the last call
     DevBuf img, work, grad, grad_keep, ids_raw, ids, lis, lis_keep, pyr_status, pyr_level, mm, offset, err;
-    DevBuf scan_tmp, tile_pyr;
+    DevBuf scan_tmp, tile_pyr, iir_ckpt;
     LisBuffers lisb;
     bool have = false;
 };
@@ -340,10 +340,10 @@ PixelOut<IT> pixel_stages(aprb_converter *c, const aprb_params &p, const uint16_
     IT *work = c->work.as_on<IT>(n, s);
     if (host) {
         launch_upload_smooth<IT>(host, const_cast<uint16_t *>(img), work, yn, xn, zn, p.lambda, mm, d_off,
-                                 is_u16 && p.lambda > 0, d_err, s, up);
+                                 is_u16 && p.lambda > 0, d_err, c->iir_ckpt, s, up);
     } else {
         launch_minmax_offset(img, n, mm, d_off, is_u16 && p.lambda > 0, s);
-        launch_smooth<IT>(img, work, yn, xn, zn, p.lambda, d_off, d_err, s);
+        launch_smooth<IT>(img, work, yn, xn, zn, p.lambda, d_off, d_err, c->iir_ckpt, s);
     }
     IT *grad = c->grad.as_on<IT>(nd, s);
     float *ids_raw = c->ids_raw.as_on<float>(nd, s);

@@ -30,11 +30,11 @@ struct LisBuffers {
 void launch_minmax_offset(const uint16_t *img, uint64_t n, unsigned *mm, float *offset, int apply, cudaStream_t s);
 template <typename IT>
 void launch_smooth(const uint16_t *img, IT *work, int yn, int xn, int zn, float lambda, const float *d_offset,
-                   unsigned *d_err, cudaStream_t s);
+                   unsigned *d_err, DevBuf &ckpt, cudaStream_t s);
 template <typename IT>
 void launch_upload_smooth(const uint16_t *host, uint16_t *img, IT *work, int yn, int xn, int zn, float lambda,
-                          unsigned *mm, float *d_offset, int apply, unsigned *d_err, cudaStream_t s,
-                          cudaStream_t up);
+                          unsigned *mm, float *d_offset, int apply, unsigned *d_err, DevBuf &ckpt,
+                          cudaStream_t s, cudaStream_t up);
 template <typename IT>
 void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *ids_raw, float *ids, int yd, int xd,
                      int zd, const aprb_params &p, cudaStream_t s);

@@ -338,6 +338,185 @@ __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
+// ---------------------------------------------------------------------------
+// a2 (y), recomputing form: the same recurrences as iir_y_kernel without the
+// round trip of the causal values through memory.  The causal sweep keeps
+// only the recurrence state at the start of every 32-sample tile (ckpt,
+// [tile][line] pairs); the anti-causal sweep then walks the tiles from the
+// end, recomputes each tile's causal values from its saved state and the
+// input -- the same operations on the same values, so the same bits -- and
+// runs the anti-causal recurrence over them.  Traffic per sample: the input
+// read twice and the result written once (2 + 2 + 4 bytes for uint16 input
+// and float ImageType) instead of 2 + 4 + 4 + 4.
+// A warp owns 32 lines; tiles arrive by cp.async one tile ahead of the
+// arithmetic, every copy one aligned 32-bit word (two uint16 samples): rows
+// must start on 4 bytes, i.e. yn even.
+// ---------------------------------------------------------------------------
+constexpr int kAY = 32;                         // samples per tile
+constexpr int kAWords = 2 * 32 * 17 + 32 * 33;  // shared words per warp
+__device__ __forceinline__ void cp_async4w(void *smem, const void *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_grp() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one_grp() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+template <typename IT>
+__global__ void __launch_bounds__(128) iir_y_rc_kernel(const uint16_t *__restrict__ src, IT *__restrict__ dst, int yn,
+                                                       uint64_t nlines, IIRDev c, const float *__restrict__ d_offset,
+                                                       unsigned *err_out, float2 *__restrict__ ckpt) {
+    __shared__ uint32_t smem_all[4][kAWords];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t line0 = ((uint64_t)blockIdx.x * 4 + w) * 32;
+    if (line0 >= nlines) return;
+    const uint64_t myline = line0 + lane;
+    const bool valid = myline < nlines;
+    const int nl = (int)min((uint64_t)32, nlines - line0);
+    const float off = d_offset ? *d_offset : 0.0f;
+    uint32_t *S = smem_all[w];
+    uint32_t *U0 = S, *U1 = S + 32 * 17;                      // raw stages [2][32][17] words
+    float *F = reinterpret_cast<float *>(S + 2 * 32 * 17);  // tile values [32][33]
+    unsigned err = 0;
+
+    float t1 = 0, t2 = 0, t3 = 0, t4 = 0;
+    if (valid) {
+        const uint16_t *L = src + myline * (uint64_t)yn;
+        for (int k = 0; k < c.minLen; ++k) {
+            float v = raw_to_it<IT>(L[k], off);
+            t1 = t1 + __ldg(c.bc + k) * v;
+            t2 = t2 + __ldg(c.bc + c.minLen + k) * v;
+        }
+        for (int k = 0; k < c.minLen; ++k) {
+            float v = raw_to_it<IT>(L[yn - 1 - k], off);
+            t3 = t3 + __ldg(c.bc + 2 * c.minLen + k) * v;
+            t4 = t4 + __ldg(c.bc + 3 * c.minLen + k) * v;
+        }
+    }
+    const int ntile = (yn + kAY - 1) / kAY;
+    const int cq = lane & 15, ch = lane >> 4;  // copies: word cq of lines 2 jj + ch
+    auto issue = [&](int t, uint32_t *buf) {
+        const int y = t * kAY + 2 * cq;
+        if (y < yn) {
+#pragma unroll 4
+            for (int jj = 0; jj < 16; ++jj) {
+                const int j = 2 * jj + ch;
+                if (j < nl) cp_async4w(buf + j * 17 + cq, src + (line0 + j) * (uint64_t)yn + y);
+            }
+        }
+        cp_async_commit_grp();
+    };
+    auto sample = [&](const uint32_t *U, int k) -> float {
+        const uint32_t wd = U[lane * 17 + (k >> 1)];
+        return raw_to_it<IT>((uint16_t)((k & 1) ? (wd >> 16) : (wd & 0xffffu)), off);
+    };
+
+    // ---- causal sweep: the state at every tile start
+    issue(0, U0);
+    for (int t = 0; t < ntile; ++t) {
+        const uint32_t *U = (t & 1) ? U1 : U0;
+        if (t + 1 < ntile)
+            issue(t + 1, (t & 1) ? U0 : U1);
+        else
+            cp_async_commit_grp();
+        cp_async_wait_one_grp();
+        __syncwarp();
+        const int y0 = t * kAY;
+        if (valid) {
+            ckpt[(uint64_t)t * nlines + myline] = make_float2(t1, t2);
+            if (y0 >= 2 && y0 + kAY <= yn) {
+#pragma unroll
+                for (int k = 0; k < kAY; ++k) {
+                    const float temp = t1 * c.b1 + t2 * c.b2 + sample(U, k);
+                    t2 = t1;
+                    t1 = temp;
+                }
+            } else {
+                const int kend = min(kAY, yn - y0);
+                for (int k = 0; k < kend; ++k) {
+                    if (y0 + k < 2) continue;
+                    const float temp = t1 * c.b1 + t2 * c.b2 + sample(U, k);
+                    t2 = t1;
+                    t1 = temp;
+                }
+            }
+        }
+        __syncwarp();
+    }
+
+    // ---- anti-causal sweep, recomputing each tile's causal values
+    float b2v = 0, b1v = 0;
+    if (valid) {
+        unsigned e0 = 0;
+        b2v = rnd_it<IT>(t4 * c.norm, e0) / c.norm;
+        b1v = rnd_it<IT>(t3 * c.norm, e0) / c.norm;
+    }
+    const int last = ntile - 1;
+    issue(last, (last & 1) ? U1 : U0);
+    for (int t = last; t >= 0; --t) {
+        const uint32_t *U = (t & 1) ? U1 : U0;
+        if (t > 0)
+            issue(t - 1, (t & 1) ? U0 : U1);
+        else
+            cp_async_commit_grp();
+        cp_async_wait_one_grp();
+        __syncwarp();
+        const int y0 = t * kAY;
+        if (valid) {
+            const float2 st = ckpt[(uint64_t)t * nlines + myline];
+            float r1 = st.x, r2 = st.y;
+            if (y0 >= 2 && y0 + kAY <= yn - 2) {
+#pragma unroll
+                for (int k = 0; k < kAY; ++k) {
+                    const float temp = r1 * c.b1 + r2 * c.b2 + sample(U, k);
+                    F[lane * 33 + k] = rnd_it<IT>(temp, err);
+                    r2 = r1;
+                    r1 = temp;
+                }
+#pragma unroll
+                for (int k = kAY - 1; k >= 0; --k) {
+                    const float temp = b1v * c.b1 + b2v * c.b2 + F[lane * 33 + k];
+                    F[lane * 33 + k] = rnd_it<IT>(temp * c.norm, err);
+                    b2v = b1v;
+                    b1v = temp;
+                }
+            } else {
+                const int kend = min(kAY, yn - y0);
+                for (int k = 0; k < kend; ++k) {
+                    const int y = y0 + k;
+                    float out;
+                    if (y == 0) {
+                        out = store_cvt<IT>(r2);
+                    } else if (y == 1) {
+                        out = store_cvt<IT>(r1);
+                    } else {
+                        const float temp = r1 * c.b1 + r2 * c.b2 + sample(U, k);
+                        out = rnd_it<IT>(temp, err);
+                        r2 = r1;
+                        r1 = temp;
+                    }
+                    if (y == yn - 2) out = rnd_it<IT>(t3 * c.norm, err);
+                    if (y == yn - 1) out = rnd_it<IT>(t4 * c.norm, err);
+                    F[lane * 33 + k] = out;
+                }
+                for (int k = kend - 1; k >= 0; --k) {
+                    if (y0 + k > yn - 3) continue;
+                    const float temp = b1v * c.b1 + b2v * c.b2 + F[lane * 33 + k];
+                    F[lane * 33 + k] = rnd_it<IT>(temp * c.norm, err);
+                    b2v = b1v;
+                    b1v = temp;
+                }
+            }
+        }
+        __syncwarp();
+        if (y0 + lane < yn) {
+#pragma unroll 4
+            for (int j = 0; j < nl; ++j) dst[(line0 + j) * (uint64_t)yn + y0 + lane] = to_it<IT>(F[j * 33 + lane]);
+        }
+        __syncwarp();
+    }
+    if (err) atomicAdd(err_out, err);
+}
+
 constexpr int kGX = 8, kGY = 64, kGZ = 8, kGThreads = 256, kGSlots = 6;
 constexpr int kTX = 2 * kGX + 2, kTY = 2 * kGY + 2;
 constexpr size_t kGradSmem = sizeof(float) * kGSlots * kTX * kTY;
@@ -679,6 +858,122 @@ __global__ void __launch_bounds__(kYWarps * 32) sat_y_kernel(const float *__rest
     }
 }
 
+// The same y box mean with the samples staged by cp.async one tile ahead of
+// the recurrence: a warp owns 32 lines and walks them in tiles of kSY
+// samples, so no registers hold the prefetch and more warps stay resident.
+// In tiles that touch neither end of the line the recurrence runs fully
+// unrolled (the window shift becomes register renaming).  REF: the input is
+// |in - ref| (the second pass of each window).
+constexpr int kSY = 16;
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
+
+template <int OFF, bool REF>
+__global__ void __launch_bounds__(128) sat_y_async_kernel(const float *__restrict__ in, const float *__restrict__ ref,
+                                                          float *__restrict__ out, int n, uint64_t nlines,
+                                                          PadMap pm) {
+    constexpr int W = 2 * OFF + 2;
+    constexpr int NB = REF ? 2 : 1;
+    __shared__ float sm[4][2][NB][32][kSY + 1];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint64_t line0 = ((uint64_t)blockIdx.x * 4 + w) * 32;
+    if (line0 >= nlines) return;
+    const bool valid = line0 + lane < nlines;
+    const float d = (float)(2 * OFF + 1);
+    const bool refl = pm.on_in | pm.on_ref;
+    uint64_t mbase = 0;
+    if (refl && valid) {
+        const uint64_t ln = line0 + lane;
+        const int xp = (int)(ln % (uint64_t)pm.px), zp = (int)(ln / (uint64_t)pm.px);
+        mbase = idx3(0, reflect101(xp - pm.sx, pm.xd), reflect101(zp - pm.sz, pm.zd), pm.yd, pm.xd);
+    }
+    // copy / store mapping: a warp instruction moves two lines of kSY samples
+    const int cy = lane & (kSY - 1), cj = lane >> 4;
+    const int ntile = (n + kSY - 1) / kSY;
+    auto issue = [&](int t, int b) {
+        const int y = t * kSY + cy;
+        const int my = (refl && y < n) ? reflect101(y - pm.sy, pm.yd) : 0;
+#pragma unroll 2
+        for (int jj = 0; jj < 16; ++jj) {
+            const int j = 2 * jj + cj;
+            const uint64_t bj = __shfl_sync(0xffffffffu, mbase, j);
+            const uint64_t ln = line0 + j;
+            if (ln < nlines && y < n) {
+                const uint64_t a = ln * (uint64_t)n + y, am = bj + (uint64_t)my;
+                cp_async4(&sm[w][b][0][j][cy], in + (pm.on_in ? am : a));
+                if (REF) cp_async4(&sm[w][b][NB - 1][j][cy], ref + (pm.on_ref ? am : a));
+            }
+        }
+        cp_async_commit();
+    };
+    float c[W];
+#pragma unroll
+    for (int q = 0; q < W; ++q) c[q] = 0.0f;
+    float C = 0.0f;
+    issue(0, 0);
+    for (int t = 0; t < ntile; ++t) {
+        const int b = t & 1;
+        if (t + 1 < ntile)
+            issue(t + 1, b ^ 1);
+        else
+            cp_async_commit();
+        cp_async_wait_one();
+        __syncwarp();
+        float(*T)[kSY + 1] = sm[w][b][0];
+        float(*R)[kSY + 1] = sm[w][b][NB - 1];
+        const int y0 = t * kSY;
+        if (valid) {
+            if (y0 > 2 * OFF && y0 + kSY <= n) {
+#pragma unroll
+                for (int k = 0; k < kSY; ++k) {
+                    float v = T[lane][k];
+                    if (REF) v = fabsf(v - R[lane][k]);
+                    C = C + v;
+#pragma unroll
+                    for (int q = 0; q < W - 1; ++q) c[q] = c[q + 1];
+                    c[W - 1] = C;
+                    float o = -c[0] / d;
+                    T[lane][k] = o + C / d;
+                }
+            } else {
+                const int kend = min(kSY, n - y0);
+                for (int k = 0; k < kend; ++k) {
+                    float v = T[lane][k];
+                    if (REF) v = fabsf(v - R[lane][k]);
+                    C = C + v;
+#pragma unroll
+                    for (int q = 0; q < W - 1; ++q) c[q] = c[q + 1];
+                    c[W - 1] = C;
+                    const int i = y0 + k - OFF;
+                    if (i >= 0 && i < n - OFF) T[lane][k] = sat_y_value<OFF>(i, n, d, c[0], C, 0.0f);
+                }
+            }
+        }
+        __syncwarp();
+        const int yy = y0 + cy, i = yy - OFF;
+        if (yy < n && i >= 0 && i < n - OFF) {
+#pragma unroll 4
+            for (int jj = 0; jj < 16; ++jj) {
+                const int j = 2 * jj + cj;
+                const uint64_t ln = line0 + j;
+                if (ln < nlines) out[ln * (uint64_t)n + i] = T[j][cy];
+            }
+        }
+        __syncwarp();
+    }
+    if (valid) {
+        for (int i = n - OFF; i < n; ++i) {
+            if (i < 0) continue;
+            const int back = (n - 1) - (i - OFF - 1);
+            float cm = 0.0f;
+#pragma unroll
+            for (int q = 0; q < W; ++q)
+                if (q == W - 1 - back) cm = c[q];
+            out[(line0 + lane) * (uint64_t)n + i] = sat_y_value<OFF>(i, n, d, cm, 0.0f, C);
+        }
+    }
+}
+
 // Final pass writing the unpadded window times the rescale factor
 // (unpaddPixels + rescale_var, LocalIntensityScale.hpp:174-184) directly.
 struct LisOut {
@@ -892,14 +1187,20 @@ void launch_minmax_offset(const uint16_t *img, uint64_t n, unsigned *mm, float *
 // chose: both only read lines that lie inside the planes.
 template <typename IT>
 static void launch_smooth_yx(const uint16_t *img, IT *work, int yn, int xn, int zn, float lambda,
-                             const float *d_offset, unsigned *d_err, cudaStream_t s) {
+                             const float *d_offset, unsigned *d_err, DevBuf &ckpt, cudaStream_t s) {
     const uint64_t n = (uint64_t)yn * xn * zn;
     if (lambda > 0 && yn > 2) {
         APRB_PROF("bspline_y", s);
         const IIRDev c = dev_coef(iir_coefficients(lambda, yn));
         const uint64_t nlines = (uint64_t)xn * zn;
-        const unsigned blocks = blocks_for(nlines, kYWarps * kTile);
-        iir_y_kernel<IT><<<blocks, kYWarps * 32, 0, s>>>(img, work, yn, nlines, c, d_offset, d_err);
+        if (yn % 2 == 0 && ((uintptr_t)img & 3) == 0) {
+            const int ntile = (yn + kAY - 1) / kAY;
+            float2 *ck = ckpt.as_on<float2>(nlines * (uint64_t)ntile, s);
+            iir_y_rc_kernel<IT><<<blocks_for(nlines, 128), 128, 0, s>>>(img, work, yn, nlines, c, d_offset, d_err, ck);
+        } else {
+            const unsigned blocks = blocks_for(nlines, kYWarps * kTile);
+            iir_y_kernel<IT><<<blocks, kYWarps * 32, 0, s>>>(img, work, yn, nlines, c, d_offset, d_err);
+        }
         count_launch();
         APRB_CHECK_LAUNCH();
     } else {
@@ -935,8 +1236,8 @@ static void launch_smooth_z(IT *work, int yn, int xn, int zn, float lambda, unsi
 
 template <typename IT>
 void launch_smooth(const uint16_t *img, IT *work, int yn, int xn, int zn, float lambda, const float *d_offset,
-                   unsigned *d_err, cudaStream_t s) {
-    launch_smooth_yx<IT>(img, work, yn, xn, zn, lambda, d_offset, d_err, s);
+                   unsigned *d_err, DevBuf &ckpt, cudaStream_t s) {
+    launch_smooth_yx<IT>(img, work, yn, xn, zn, lambda, d_offset, d_err, ckpt, s);
     launch_smooth_z<IT>(work, yn, xn, zn, lambda, d_err, s);
 }
 
@@ -948,8 +1249,8 @@ void launch_smooth(const uint16_t *img, IT *work, int yn, int xn, int zn, float 
 // overlap the y and x passes.  The z pass needs every plane and runs last.
 template <typename IT>
 void launch_upload_smooth(const uint16_t *host, uint16_t *img, IT *work, int yn, int xn, int zn, float lambda,
-                          unsigned *mm, float *d_offset, int apply, unsigned *d_err, cudaStream_t s,
-                          cudaStream_t up) {
+                          unsigned *mm, float *d_offset, int apply, unsigned *d_err, DevBuf &ckpt,
+                          cudaStream_t s, cudaStream_t up) {
     const uint64_t plane = (uint64_t)yn * xn;
     const int chunk = (int)std::max<uint64_t>(4, (uint64_t(1) << 27) / std::max<uint64_t>(plane, 1));
     const int nch = (zn + chunk - 1) / chunk;
@@ -991,14 +1292,14 @@ void launch_upload_smooth(const uint16_t *host, uint16_t *img, IT *work, int yn,
                 count_launch();
                 APRB_CHECK_LAUNCH();
             }
-            launch_smooth_yx<IT>(img + o, work + o, yn, xn, z1 - z0, lambda, d_offset, d_err, s);
+            launch_smooth_yx<IT>(img + o, work + o, yn, xn, z1 - z0, lambda, d_offset, d_err, ckpt, s);
         }
     }
     if (apply) {
         offset_kernel<<<1, 32, 0, s>>>(mm, d_offset, 1);
         count_launch();
         APRB_CHECK_LAUNCH();
-        launch_smooth_yx<IT>(img, work, yn, xn, zn, lambda, d_offset, d_err, s);
+        launch_smooth_yx<IT>(img, work, yn, xn, zn, lambda, d_offset, d_err, ckpt, s);
     }
     launch_smooth_z<IT>(work, yn, xn, zn, lambda, d_err, s);
 }
@@ -1048,8 +1349,10 @@ static void sat_axis_t(const float *in, const float *absref, float *out, int py,
                        const PadMap &pm, const LisOut *fo, cudaStream_t s) {
     if (axis == 0) {
         const uint64_t nlines = (uint64_t)px * pz;
-        sat_y_kernel<OFF><<<blocks_for(nlines, kYWarps * kTile), kYWarps * 32, 0, s>>>(in, absref, out, py, nlines,
-                                                                                    pm);
+        if (absref)
+            sat_y_async_kernel<OFF, true><<<blocks_for(nlines, 128), 128, 0, s>>>(in, absref, out, py, nlines, pm);
+        else
+            sat_y_async_kernel<OFF, false><<<blocks_for(nlines, 128), 128, 0, s>>>(in, absref, out, py, nlines, pm);
     } else {
         const uint64_t nlines = axis == 1 ? (uint64_t)py * pz : (uint64_t)py * px;
         const int n = axis == 1 ? px : pz;
@@ -1180,13 +1483,14 @@ void launch_levels(IT *grad, float *lis, const float *ids, uint64_t nd, const fl
 }
 
 template void launch_upload_smooth<uint16_t>(const uint16_t *, uint16_t *, uint16_t *, int, int, int, float,
-                                             unsigned *, float *, int, unsigned *, cudaStream_t, cudaStream_t);
+                                             unsigned *, float *, int, unsigned *, DevBuf &, cudaStream_t,
+                                             cudaStream_t);
 template void launch_upload_smooth<float>(const uint16_t *, uint16_t *, float *, int, int, int, float, unsigned *,
-                                          float *, int, unsigned *, cudaStream_t, cudaStream_t);
+                                          float *, int, unsigned *, DevBuf &, cudaStream_t, cudaStream_t);
 template void launch_smooth<uint16_t>(const uint16_t *, uint16_t *, int, int, int, float, const float *, unsigned *,
-                                      cudaStream_t);
+                                      DevBuf &, cudaStream_t);
 template void launch_smooth<float>(const uint16_t *, float *, int, int, int, float, const float *, unsigned *,
-                                   cudaStream_t);
+                                   DevBuf &, cudaStream_t);
 template void launch_gradient<uint16_t>(const uint16_t *, int, int, int, uint16_t *, float *, float *, int, int, int,
                                         const aprb_params &, cudaStream_t);
 template void launch_gradient<float>(const float *, int, int, int, float *, float *, float *, int, int, int,
