@@ -245,14 +245,24 @@ __global__ void __launch_bounds__(kYWarps * 32) iir_y_kernel(const uint16_t *__r
 // neighbouring threads own neighbouring y so every step is a coalesced row.
 // In place.
 // ---------------------------------------------------------------------------
+// The same x / z recurrences without the round trip of the causal values
+// through memory: the causal sweep reads the line and keeps only the
+// recurrence state at the start of every kRC-sample segment (ckpt,
+// [segment][line] pairs); the anti-causal sweep walks the segments from the
+// end, recomputes each segment's causal values from its saved state and the
+// still untouched input -- the same operations on the same values -- and
+// writes the results over it.  Traffic per sample: 4 B read twice and 4 B
+// written, plus 16 B of state per 16 samples, instead of 16 B.
+constexpr int kRC = 16;
 template <typename IT>
-__global__ void iir_strided_kernel(IT *__restrict__ im, int yn, int n, uint64_t stride, uint64_t outer_stride,
-                                   uint64_t nlines, IIRDev c, unsigned *err_out) {
+__global__ void __launch_bounds__(128) iir_strided_rc_kernel(IT *__restrict__ im, int yn, int n, uint64_t stride,
+                                                             uint64_t outer_stride, uint64_t nlines, IIRDev c,
+                                                             unsigned *err_out, float2 *__restrict__ ckpt) {
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= nlines) return;
     const uint64_t y = g % (uint64_t)yn, o = g / (uint64_t)yn;
     IT *L = im + o * outer_stride + y;
-    unsigned err = 0;
+    unsigned err = 0, scratch_err = 0;
     float v1 = 0, v2 = 0, v3 = 0, v4 = 0;
     for (int i = 0; i < c.minLen; ++i) {
         float a = (float)L[(uint64_t)i * stride];
@@ -262,52 +272,99 @@ __global__ void iir_strided_kernel(IT *__restrict__ im, int yn, int n, uint64_t 
         v3 = v3 + __ldg(c.bc + 2 * c.minLen + i) * b;
         v4 = v4 + __ldg(c.bc + 3 * c.minLen + i) * b;
     }
-    L[0] = to_it<IT>(rnd_it<IT>(v2, err));
-    L[stride] = to_it<IT>(rnd_it<IT>(v1, err));
-    constexpr int U = 8;
-    int i = 2;
-    for (; i + U <= n; i += U) {
-        float buf[U];
+    const int nseg = (n + kRC - 1) / kRC;
+    // ---- causal sweep: the state at every segment start
+    float p1 = v1, p2 = v2;
+    for (int sgm = 0; sgm < nseg; ++sgm) {
+        const int i0 = sgm * kRC;
+        ckpt[(uint64_t)sgm * nlines + g] = make_float2(p1, p2);
+        const IT *P = L + (uint64_t)i0 * stride;
+        if (i0 >= 2 && i0 + kRC <= n) {
+            float buf[kRC];
 #pragma unroll
-        for (int u = 0; u < U; ++u) buf[u] = (float)L[(uint64_t)(i + u) * stride];
+            for (int u = 0; u < kRC; ++u) buf[u] = (float)P[(uint64_t)u * stride];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            float nv = rnd_it<IT>(buf[u] + c.b1 * v1 + c.b2 * v2, err);
-            v2 = v1;
-            v1 = nv;
-            buf[u] = nv;
+            for (int u = 0; u < kRC; ++u) {
+                const float nv = rnd_it<IT>(buf[u] + c.b1 * p1 + c.b2 * p2, scratch_err);
+                p2 = p1;
+                p1 = nv;
+            }
+        } else {
+            const int i1 = min(n, i0 + kRC);
+            for (int i = max(i0, 2); i < i1; ++i) {
+                const float nv = rnd_it<IT>((float)L[(uint64_t)i * stride] + c.b1 * p1 + c.b2 * p2, scratch_err);
+                p2 = p1;
+                p1 = nv;
+            }
         }
-#pragma unroll
-        for (int u = 0; u < U; ++u) L[(uint64_t)(i + u) * stride] = to_it<IT>(buf[u]);
     }
-    for (; i < n; ++i) {
-        float nv = rnd_it<IT>((float)L[(uint64_t)i * stride] + c.b1 * v1 + c.b2 * v2, err);
-        v2 = v1;
-        v1 = nv;
-        L[(uint64_t)i * stride] = to_it<IT>(nv);
-    }
-    L[(uint64_t)(n - 1) * stride] = to_it<IT>(rnd_it<IT>(v4 * c.norm, err));
-    L[(uint64_t)(n - 2) * stride] = to_it<IT>(rnd_it<IT>(v3 * c.norm, err));
-    int j = n - 3;
-    for (; j - U + 1 >= 0; j -= U) {
-        float buf[U];
+    // ---- anti-causal sweep, recomputing each segment's causal values
+    float q3 = v3, q4 = v4;
+    for (int sgm = nseg - 1; sgm >= 0; --sgm) {
+        const int i0 = sgm * kRC;
+        const float2 st = ckpt[(uint64_t)sgm * nlines + g];
+        float r1 = st.x, r2 = st.y;
+        IT *P = L + (uint64_t)i0 * stride;
+        if (i0 >= 2 && i0 + kRC <= n - 2) {
+            float buf[kRC];
 #pragma unroll
-        for (int u = 0; u < U; ++u) buf[u] = (float)L[(uint64_t)(j - u) * stride];
+            for (int u = 0; u < kRC; ++u) buf[u] = (float)P[(uint64_t)u * stride];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            float temp = (buf[u] + c.b1 * v3 + c.b2 * v4);
-            buf[u] = rnd_it<IT>(temp * c.norm, err);
-            v4 = v3;
-            v3 = temp;
+            for (int u = 0; u < kRC; ++u) {
+                const float nv = rnd_it<IT>(buf[u] + c.b1 * r1 + c.b2 * r2, err);
+                r2 = r1;
+                r1 = nv;
+                buf[u] = nv;
+            }
+#pragma unroll
+            for (int u = kRC - 1; u >= 0; --u) {
+                const float temp = (buf[u] + c.b1 * q3 + c.b2 * q4);
+                buf[u] = rnd_it<IT>(temp * c.norm, err);
+                q4 = q3;
+                q3 = temp;
+            }
+#pragma unroll
+            for (int u = 0; u < kRC; ++u) P[(uint64_t)u * stride] = to_it<IT>(buf[u]);
+        } else {
+            const int i1 = min(n, i0 + kRC);
+            float buf[kRC];
+#pragma unroll
+            for (int u = 0; u < kRC; ++u) {
+                const int i = i0 + u;
+                if (i >= i1) break;
+                float f;
+                if (i == 0) {
+                    f = rnd_it<IT>(v2, err);
+                } else if (i == 1) {
+                    f = rnd_it<IT>(v1, err);
+                } else {
+                    f = rnd_it<IT>((float)P[(uint64_t)u * stride] + c.b1 * r1 + c.b2 * r2, err);
+                    r2 = r1;
+                    r1 = f;
+                }
+                buf[u] = f;
+            }
+#pragma unroll
+            for (int u = kRC - 1; u >= 0; --u) {
+                const int i = i0 + u;
+                if (i >= i1) continue;
+                float out;
+                if (i == n - 1) {
+                    out = rnd_it<IT>(v4 * c.norm, err);
+                } else if (i == n - 2) {
+                    out = rnd_it<IT>(v3 * c.norm, err);
+                } else {
+                    const float temp = (buf[u] + c.b1 * q3 + c.b2 * q4);
+                    out = rnd_it<IT>(temp * c.norm, err);
+                    q4 = q3;
+                    q3 = temp;
+                }
+                buf[u] = out;
+            }
+#pragma unroll
+            for (int u = 0; u < kRC; ++u)
+                if (i0 + u < i1) P[(uint64_t)u * stride] = to_it<IT>(buf[u]);
         }
-#pragma unroll
-        for (int u = 0; u < U; ++u) L[(uint64_t)(j - u) * stride] = to_it<IT>(buf[u]);
-    }
-    for (; j >= 0; --j) {
-        float temp = ((float)L[(uint64_t)j * stride] + c.b1 * v3 + c.b2 * v4);
-        L[(uint64_t)j * stride] = to_it<IT>(rnd_it<IT>(temp * c.norm, err));
-        v4 = v3;
-        v3 = temp;
     }
     if (err) atomicAdd(err_out, err);
 }
@@ -564,26 +621,23 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
             }
         }
     };
-    auto gmag = [&](int zf, int xf, int yf) -> float {  // full-res coordinates inside the volume
-        if (yn < 2) return 0.0f;
-        const int r = xf - xf0, cc = yf - yf0;
-        const float(*C)[kTY] = ring[(zf + kGSlots) % kGSlots];
-        const float(*U)[kTY] = ring[(zf - 1 + kGSlots) % kGSlots];
-        const float(*D)[kTY] = ring[(zf + 1 + kGSlots) % kGSlots];
+    // squared gradient magnitude at full-res (zf, xf, yf) of plane C with
+    // neighbour planes U, D: the reference's double sum of the squared float
+    // differences, gx^2 + gz^2 then + gy^2.  Each square of a float is exact
+    // in double, so the fused forms round exactly where the sums do.
+    auto gsq = [&](float cxm, float cxp, float cym, float cyp, float u, float d) -> double {
         float gx, gz, gy;
         if (PW2) {
-            gx = (C[r + 1][cc] - C[r - 1][cc]) * ihx2;
-            gz = (D[r][cc] - U[r][cc]) * ihz2;
-            gy = (C[r][cc + 1] - C[r][cc - 1]) * ihy2;
+            gx = (cxp - cxm) * ihx2;
+            gz = (d - u) * ihz2;
+            gy = (cyp - cym) * ihy2;
         } else {
-            gx = (C[r + 1][cc] - C[r - 1][cc]) / hx2;
-            gz = (D[r][cc] - U[r][cc]) / hz2;
-            gy = (C[r][cc + 1] - C[r][cc - 1]) / hy2;
+            gx = (cxp - cxm) / hx2;
+            gz = (d - u) / hz2;
+            gy = (cyp - cym) / hy2;
         }
-        double s = (double)gx * (double)gx + (double)gz * (double)gz;
-        s = s + (double)gy * (double)gy;
-        const double q = sqrt(s);
-        return sizeof(IT) == 2 ? cvt_u16d(q) : (float)q;
+        const double s = fma((double)gx, (double)gx, (double)gz * (double)gz);
+        return fma((double)gy, (double)gy, s);
     };
 
     load(2 * zd0 - 1);
@@ -609,28 +663,62 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
             const int xl = t / kGY, yl = t % kGY;
             const int xk = xd0 + xl, k = yd0 + yl;
             if (xk >= xd || k >= yd) continue;
-            const int y0 = 2 * k, ks = min(2 * k + 1, yn - 1), x0 = 2 * xk, z0 = 2 * z;
+            const int x0 = 2 * xk, z0 = 2 * z;
+            // tile row / column of (x0, y0 = 2k); column cy + 1 is ks = min(2k + 1, yn - 1)
+            // unless that is clamped onto y0
+            const int rx = x0 - xf0, cy = 2 * k - yf0;
+            const bool y1in = 2 * k + 1 < yn, x1in = x0 + 1 < xn, z1in = z0 + 1 < zn;
+            const float(*P0)[kTY] = ring[(z0 - 1 + kGSlots) % kGSlots];
+            const float(*P1)[kTY] = ring[(z0 + kGSlots) % kGSlots];
+            const float(*P2)[kTY] = ring[(z0 + 1 + kGSlots) % kGSlots];
+            const float(*P3)[kTY] = ring[(z0 + 2 + kGSlots) % kGSlots];
             float gmax = 0.0f;
-            for (int zf = z0; zf <= z0 + 1 && zf < zn; ++zf)
-                for (int xf = x0; xf <= x0 + 1 && xf < xn; ++xf) {
-                    const float a = gmag(zf, xf, y0), b = gmag(zf, xf, ks);
-                    const float m = b > gmax ? b : gmax;
-                    gmax = a > m ? a : m;
+            if (yn >= 2) {
+                // the gradient magnitude is max over the 2 x 2 x 2 children; the
+                // conversion sqrt -> ImageType is monotone (below 2^16 for
+                // uint16), so the max is taken over the squares and rooted once
+                auto children = [&](auto &&f) {
+#pragma unroll
+                    for (int dz = 0; dz < 2; ++dz) {
+                        if (dz == 1 && !z1in) break;
+                        const float(*C)[kTY] = dz ? P2 : P1;
+                        const float(*U)[kTY] = dz ? P1 : P0;
+                        const float(*D)[kTY] = dz ? P3 : P2;
+#pragma unroll
+                        for (int dx = 0; dx < 2; ++dx) {
+                            if (dx == 1 && !x1in) break;
+                            const int r = rx + dx;
+                            const float c0 = C[r][cy - 1], c1 = C[r][cy], c2 = C[r][cy + 1], c3 = C[r][cy + 2];
+                            const double a = gsq(C[r - 1][cy], C[r + 1][cy], c0, c2, U[r][cy], D[r][cy]);
+                            f(a);
+                            if (y1in) f(gsq(C[r - 1][cy + 1], C[r + 1][cy + 1], c1, c3, U[r][cy + 1], D[r][cy + 1]));
+                        }
+                    }
+                };
+                double smax = 0.0;  // every square is >= 0
+                children([&](double q) { smax = q > smax ? q : smax; });
+                if (sizeof(IT) == 4 || smax < 4294967296.0) {
+                    const double root = sqrt(smax);
+                    gmax = sizeof(IT) == 2 ? cvt_u16d(root) : (float)root;
+                } else {
+                    // roots of 2^16 and above wrap in the uint16 conversion
+                    children([&](double q) {
+                        const float v = cvt_u16d(sqrt(q));
+                        gmax = v > gmax ? v : gmax;
+                    });
                 }
+            }
             const uint64_t o = idx3(k, xk, z, yd, xd);
             grad[o] = to_it<IT>(gmax);
             // mean with the clamped indices of downsample (held by the tile)
-            const float(*A)[kTY] = ring[(z0 + kGSlots) % kGSlots];
-            const float(*B)[kTY] = ring[(z0 + 1 + kGSlots) % kGSlots];
-            const int r0 = x0 - xf0, c0 = y0 - yf0;
-            float s = A[r0][c0];
-            s = s + A[r0][c0 + 1];
-            s = s + A[r0 + 1][c0];
-            s = s + A[r0 + 1][c0 + 1];
-            s = s + B[r0][c0];
-            s = s + B[r0][c0 + 1];
-            s = s + B[r0 + 1][c0];
-            s = s + B[r0 + 1][c0 + 1];
+            float s = P1[rx][cy];
+            s = s + P1[rx][cy + 1];
+            s = s + P1[rx + 1][cy];
+            s = s + P1[rx + 1][cy + 1];
+            s = s + P2[rx][cy];
+            s = s + P2[rx][cy + 1];
+            s = s + P2[rx + 1][cy];
+            s = s + P2[rx + 1][cy + 1];
             ids[o] = s * 0.125f;  // == s / 8 exactly
         }
         if (kAsync) cp_async_wait_all();
@@ -1214,21 +1302,24 @@ static void launch_smooth_yx(const uint16_t *img, IT *work, int yn, int xn, int 
         APRB_PROF("bspline_x", s);
         const IIRDev c = dev_coef(iir_coefficients(lambda, xn));
         const uint64_t nlines = (uint64_t)yn * zn;
-        iir_strided_kernel<IT><<<blocks_for(nlines, 128), 128, 0, s>>>(work, yn, xn, (uint64_t)yn,
-                                                                     (uint64_t)xn * yn, nlines, c, d_err);
+        float2 *ck = ckpt.as_on<float2>(nlines * (uint64_t)((xn + kRC - 1) / kRC), s);
+        iir_strided_rc_kernel<IT><<<blocks_for(nlines, 128), 128, 0, s>>>(work, yn, xn, (uint64_t)yn,
+                                                                        (uint64_t)xn * yn, nlines, c, d_err, ck);
         count_launch();
         APRB_CHECK_LAUNCH();
     }
 }
 
 template <typename IT>
-static void launch_smooth_z(IT *work, int yn, int xn, int zn, float lambda, unsigned *d_err, cudaStream_t s) {
+static void launch_smooth_z(IT *work, int yn, int xn, int zn, float lambda, unsigned *d_err, DevBuf &ckpt,
+                            cudaStream_t s) {
     if (lambda > 0 && zn > 2) {
         APRB_PROF("bspline_z", s);
         const IIRDev c = dev_coef(iir_coefficients(lambda, zn));
         const uint64_t nlines = (uint64_t)yn * xn;
-        iir_strided_kernel<IT><<<blocks_for(nlines, 128), 128, 0, s>>>(work, yn, zn, (uint64_t)xn * yn, (uint64_t)yn,
-                                                                     nlines, c, d_err);
+        float2 *ck = ckpt.as_on<float2>(nlines * (uint64_t)((zn + kRC - 1) / kRC), s);
+        iir_strided_rc_kernel<IT><<<blocks_for(nlines, 128), 128, 0, s>>>(work, yn, zn, (uint64_t)xn * yn,
+                                                                        (uint64_t)yn, nlines, c, d_err, ck);
         count_launch();
         APRB_CHECK_LAUNCH();
     }
@@ -1238,7 +1329,7 @@ template <typename IT>
 void launch_smooth(const uint16_t *img, IT *work, int yn, int xn, int zn, float lambda, const float *d_offset,
                    unsigned *d_err, DevBuf &ckpt, cudaStream_t s) {
     launch_smooth_yx<IT>(img, work, yn, xn, zn, lambda, d_offset, d_err, ckpt, s);
-    launch_smooth_z<IT>(work, yn, xn, zn, lambda, d_err, s);
+    launch_smooth_z<IT>(work, yn, xn, zn, lambda, d_err, ckpt, s);
 }
 
 // Offset and smoothing of a volume that is still in host memory: it is copied
@@ -1301,7 +1392,7 @@ void launch_upload_smooth(const uint16_t *host, uint16_t *img, IT *work, int yn,
         APRB_CHECK_LAUNCH();
         launch_smooth_yx<IT>(img, work, yn, xn, zn, lambda, d_offset, d_err, ckpt, s);
     }
-    launch_smooth_z<IT>(work, yn, xn, zn, lambda, d_err, s);
+    launch_smooth_z<IT>(work, yn, xn, zn, lambda, d_err, ckpt, s);
 }
 
 template <typename IT>

@@ -113,6 +113,26 @@ def test_empty_and_flat_inputs():
     assert np.array_equal(apr.linear_access()[2], acc.y_vec)
 
 
+def test_gradient_magnitudes_beyond_uint16_range():
+    """uint16 ImageType whose gradient magnitudes exceed 65535 (steps of 65000
+    with dy = 0.25 and no smoothing): the stored gradient wraps as the
+    reference's conversion does, so the per-cell maximum is taken over the
+    converted magnitudes there."""
+    img = np.full((12, 20, 24), 100, np.uint16)
+    img[:, :, 12:] = 65000
+    img[4:8, 5:15, 3:9] = 40000
+    kw = dict(lambda_=0.0, dy=0.25, dx=0.5)
+    e, acc, (off, inter) = B.orc_get_apr(img, oracle_params(**kw), 1)
+    assert e == 0
+    conv, apr = gpu_apr(img, 1, **kw)
+    ds = STAGE_SHAPE_DS(img.shape)
+    assert inter[1].max() > 0
+    for w in range(1, 7):
+        assert bits_equal(conv.intermediate(w, ds), inter[w]), "stage %d" % w
+    lx, xe, yv = apr.linear_access()
+    assert np.array_equal(xe, acc.xz_end) and np.array_equal(yv, acc.y_vec)
+
+
 @pytest.mark.parametrize("image_type", ["float", "uint16"])
 def test_host_calls_copy_in_chunks_like_device_calls(image_type):
     """Host-buffer get_apr and sample_image copy a volume with large planes in
