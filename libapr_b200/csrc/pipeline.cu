@@ -394,6 +394,9 @@ __device__ __forceinline__ void cp_async4(float *smem, const float *gmem) {
 __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// waits until at most the most recently committed group is still in flight
+__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 // ---------------------------------------------------------------------------
 // a2 (y), recomputing form: the same recurrences as iir_y_kernel without the
@@ -415,8 +418,6 @@ __device__ __forceinline__ void cp_async4w(void *smem, const void *gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
-__device__ __forceinline__ void cp_async_commit_grp() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_one_grp() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 template <typename IT>
 __global__ void __launch_bounds__(128) iir_y_rc_kernel(const uint16_t *__restrict__ src, IT *__restrict__ dst, int yn,
@@ -460,7 +461,7 @@ __global__ void __launch_bounds__(128) iir_y_rc_kernel(const uint16_t *__restric
                 if (j < nl) cp_async4w(buf + j * 17 + cq, src + (line0 + j) * (uint64_t)yn + y);
             }
         }
-        cp_async_commit_grp();
+        cp_async_commit();
     };
     auto sample = [&](const uint32_t *U, int k) -> float {
         const uint32_t wd = U[lane * 17 + (k >> 1)];
@@ -474,8 +475,8 @@ __global__ void __launch_bounds__(128) iir_y_rc_kernel(const uint16_t *__restric
         if (t + 1 < ntile)
             issue(t + 1, (t & 1) ? U0 : U1);
         else
-            cp_async_commit_grp();
-        cp_async_wait_one_grp();
+            cp_async_commit();
+        cp_async_wait_one();
         __syncwarp();
         const int y0 = t * kAY;
         if (valid) {
@@ -514,8 +515,8 @@ __global__ void __launch_bounds__(128) iir_y_rc_kernel(const uint16_t *__restric
         if (t > 0)
             issue(t - 1, (t & 1) ? U0 : U1);
         else
-            cp_async_commit_grp();
-        cp_async_wait_one_grp();
+            cp_async_commit();
+        cp_async_wait_one();
         __syncwarp();
         const int y0 = t * kAY;
         if (valid) {
@@ -727,99 +728,135 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
 }
 
 // ---------------------------------------------------------------------------
-// a5: calc_inv_bspline_y/x/z (ComputeGradient.hpp:785-964): the three in-place
-// passes run one after the other on a shared-memory tile of 8 x 8 x 64 outputs
-// plus a one-sample halo in x and z: the y pass over the tile and its halo,
-// the x pass over the tile's x range and the z halo, then the z pass.  Each
-// value is the reference's expression with its operand order, so the tile
-// reproduces the whole-volume passes exactly.
+// a5: calc_inv_bspline_y/x/z (ComputeGradient.hpp:785-964).  A block owns an
+// 8 (x) x 256 (y) column of the ds image and a run of up to 32 planes, and
+// streams along z; a thread owns one y of the column.  Each input plane (with
+// a one-sample x / y halo) arrives by cp.async two planes ahead; the thread
+// runs the y pass of its y on the ten rows, the x pass of the eight outputs
+// from those, and the z pass from the last three planes it holds in
+// registers, so a plane costs one block barrier.  Each value is the
+// reference's expression with its operand order, so the columns reproduce
+// the whole-volume passes exactly.
 // ---------------------------------------------------------------------------
 struct InvB {
     float a1, a2, a3, a13;
 };
 
-constexpr int kIX = 8, kIY = 64, kIZ = 8;
-constexpr int kIXH = kIX + 2, kIZH = kIZ + 2, kIYH = kIY + 2;
+constexpr int kJX = 8, kJY = 256, kJZ = 32;
+constexpr int kJXH = kJX + 2, kJYH = kJY + 2;
 
-constexpr size_t kInvSmem = sizeof(float) * (kIZH * kIXH * kIYH + kIZH * kIXH * kIY);
-
-__global__ void __launch_bounds__(256) inv_bspline_kernel(const float *__restrict__ in, float *__restrict__ O, int yd,
+__global__ void __launch_bounds__(kJY) inv_bspline_kernel(const float *__restrict__ in, float *__restrict__ O, int yd,
                                                           int xd, int zd, int ony, int onx, int onz, InvB c) {
-    extern __shared__ float inv_smem[];
-    float *S = inv_smem;                         // input tile with halo [zz][xx][yy], later the x pass
-    float *Yb = inv_smem + kIZH * kIXH * kIYH;  // y pass over the tile's y range [zz][xx][yy]
-    const int y0 = blockIdx.x * kIY, x0 = blockIdx.y * kIX, z0 = blockIdx.z * kIZ;
-    // asynchronous copies of the tile rows (one warp per (z, x) row, lanes
-    // along y), all in flight before the wait; cells outside the volume stay
-    // unwritten and are never read
-    {
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        for (int r = warp; r < kIZH * kIXH; r += blockDim.x / 32) {
-            const int xg = x0 - 1 + r % kIXH, zg = z0 - 1 + r / kIXH;
-            if (xg < 0 || xg >= xd || zg < 0 || zg >= zd) continue;
-            const float *row = in + idx3(0, xg, zg, yd, xd);
-            for (int yy = lane; yy < kIYH; yy += 32) {
-                const int yg = y0 - 1 + yy;
-                if (yg >= 0 && yg < yd) cp_async4(S + r * kIYH + yy, row + yg);
+    __shared__ float S[3][kJXH][kJYH];  // input planes with halo, two ahead
+    const int y0 = blockIdx.x * kJY, x0 = blockIdx.y * kJX, zs = blockIdx.z * kJZ;
+    const int ze = min(zs + kJZ, zd);
+    const int zb = zs == 0 ? 0 : zs - 1;            // first plane read
+    const int zl = onz ? min(ze, zd - 1) : ze - 1;  // last plane read
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    auto issue = [&](int zi) {
+        if (zi <= zl) {
+            float(*B)[kJYH] = S[(zi - zb) % 3];
+            for (int r = 0; r < kJXH; ++r) {
+                const int xg = x0 - 1 + r;
+                if (xg < 0 || xg >= xd) continue;
+                const float *row = in + idx3(0, xg, zi, yd, xd);
+                for (int yy = threadIdx.x; yy < kJYH; yy += kJY) {
+                    const int yg = y0 - 1 + yy;
+                    if (yg >= 0 && yg < yd) cp_async4(&B[r][yy], row + yg);
+                }
             }
         }
-        cp_async_wait_all();
-    }
-    __syncthreads();
-    // y pass: (z, x) over the tile and its halo, y over the tile
-    for (int t = threadIdx.x; t < kIZH * kIXH * kIY; t += blockDim.x) {
-        const int yy = t % kIY, xx = (t / kIY) % kIXH, zz = t / (kIY * kIXH);
-        const int y = y0 + yy, xg = x0 - 1 + xx, zg = z0 - 1 + zz;
-        if (y >= yd || xg < 0 || xg >= xd || zg < 0 || zg >= zd) continue;
-        const int base = (zz * kIXH + xx) * kIYH + 1 - y0;  // + global y
-        float v;
-        if (!ony)
-            v = S[base + y];
-        else if (y == 0)
-            v = c.a2 * S[base + 0] + c.a13 * S[base + 1];
-        else if (y == yd - 1)
-            v = c.a13 * S[base + yd - 2] + c.a2 * S[base + yd - 1];
-        else
-            v = c.a1 * S[base + y - 1] + c.a2 * S[base + y] + c.a3 * S[base + y + 1];
-        Yb[t] = v;
-    }
-    __syncthreads();
-    // x pass into S, laid out [zz][xx][yy] with x over the tile only
-    for (int t = threadIdx.x; t < kIZH * kIX * kIY; t += blockDim.x) {
-        const int yy = t % kIY, xx = (t / kIY) % kIX, zz = t / (kIY * kIX);
-        const int y = y0 + yy, x = x0 + xx, zg = z0 - 1 + zz;
-        if (y >= yd || x >= xd || zg < 0 || zg >= zd) continue;
-        const int base = zz * kIXH * kIY + yy;  // + (global x - x0 + 1) * kIY
-        auto Y = [&](int xg) { return Yb[base + (xg - x0 + 1) * kIY]; };
-        float v;
-        if (!onx) {
-            v = Y(x);
-        } else if (x == xd - 1) {
-            v = c.a13 * Y(xd - 2) + c.a2 * Y(xd - 1);
-        } else {
-            const int xm = x == 0 ? 1 : x - 1;
-            v = c.a1 * Y(xm) + c.a2 * Y(x) + c.a3 * Y(x + 1);
+        cp_async_commit();
+    };
+    (void)warp;
+    (void)lane;
+    const int y = y0 + threadIdx.x;
+    const bool yin = y < yd;
+    // the thread's x-pass values of planes zi - 2, zi - 1, zi
+    float p2[kJX], p1[kJX], p0[kJX];
+#pragma unroll
+    for (int i = 0; i < kJX; ++i) p2[i] = p1[i] = p0[i] = 0.0f;
+    issue(zb);
+    issue(zb + 1);
+    for (int zi = zb; zi <= zl; ++zi) {
+        cp_async_wait_one();
+        __syncthreads();
+        issue(zi + 2);  // into the buffer of plane zi - 1, read before the barrier
+        const float(*B)[kJYH] = S[(zi - zb) % 3];
+#pragma unroll
+        for (int i = 0; i < kJX; ++i) {
+            p2[i] = p1[i];
+            p1[i] = p0[i];
         }
-        S[t] = v;
-    }
-    __syncthreads();
-    // z pass and store
-    for (int t = threadIdx.x; t < kIZ * kIX * kIY; t += blockDim.x) {
-        const int yy = t % kIY, xx = (t / kIY) % kIX, zz = t / (kIY * kIX);
-        const int y = y0 + yy, x = x0 + xx, z = z0 + zz;
-        if (y >= yd || x >= xd || z >= zd) continue;
-        const int base = xx * kIY + yy;  // + (global z - z0 + 1) * kIX * kIY
-        auto X = [&](int zg) { return S[base + (zg - z0 + 1) * (kIX * kIY)]; };
-        float r;
-        if (!onz) {
-            r = X(z);
-        } else if (z == zd - 1) {
-            r = c.a13 * X(zd - 2) + c.a2 * X(zd - 1);
-        } else {
-            const int zm = z == 0 ? 1 : z - 1;
-            r = c.a1 * X(zm) + c.a2 * X(z) + c.a3 * X(z + 1);
+        if (yin) {
+            // y pass of the ten rows at this y
+            float yb[kJXH];
+#pragma unroll
+            for (int r = 0; r < kJXH; ++r) {
+                const int xg = x0 - 1 + r;
+                const float *Sr = &B[r][0] + 1 - y0;  // [global y]
+                float v = 0.0f;
+                if (xg >= 0 && xg < xd) {
+                    if (!ony)
+                        v = Sr[y];
+                    else if (y == 0)
+                        v = c.a2 * Sr[0] + c.a13 * Sr[1];
+                    else if (y == yd - 1)
+                        v = c.a13 * Sr[yd - 2] + c.a2 * Sr[yd - 1];
+                    else
+                        v = c.a1 * Sr[y - 1] + c.a2 * Sr[y] + c.a3 * Sr[y + 1];
+                }
+                yb[r] = v;
+            }
+            // x pass of the eight outputs
+#pragma unroll
+            for (int i = 0; i < kJX; ++i) {
+                const int x = x0 + i;
+                float v = 0.0f;
+                if (x < xd) {
+                    if (!onx) {
+                        v = yb[i + 1];
+                    } else if (x == xd - 1) {
+                        v = c.a13 * yb[i] + c.a2 * yb[i + 1];
+                    } else if (x == 0) {
+                        v = c.a1 * yb[2] + c.a2 * yb[1] + c.a3 * yb[2];
+                    } else {
+                        v = c.a1 * yb[i] + c.a2 * yb[i + 1] + c.a3 * yb[i + 2];
+                    }
+                }
+                p0[i] = v;
+            }
+            // z pass of the planes now complete
+            auto emit = [&](int z, const float *xm, const float *xc, const float *xp, bool last) {
+#pragma unroll
+                for (int i = 0; i < kJX; ++i) {
+                    const int x = x0 + i;
+                    if (x >= xd) continue;
+                    float r;
+                    if (!onz)
+                        r = xc[i];
+                    else if (last)
+                        r = c.a13 * xm[i] + c.a2 * xc[i];
+                    else
+                        r = c.a1 * xm[i] + c.a2 * xc[i] + c.a3 * xp[i];
+                    O[idx3(y, x, z, yd, xd)] = r;
+                }
+            };
+            if (!onz) {
+                if (zi >= zs) emit(zi, p0, p0, p0, false);
+            } else {
+                const int z = zi - 1;
+                if (z >= zs) {
+                    if (z == zd - 1)
+                        emit(z, p2, p1, p0, true);
+                    else if (z == 0)
+                        emit(z, p0, p1, p0, false);  // zm = 1 = zi
+                    else
+                        emit(z, p2, p1, p0, false);
+                }
+                if (zi == zd - 1 && zi >= zs) emit(zi, p1, p0, p0, true);
+            }
         }
-        O[idx3(y, x, z, yd, xd)] = r;
     }
 }
 
@@ -953,8 +990,6 @@ __global__ void __launch_bounds__(kYWarps * 32) sat_y_kernel(const float *__rest
 // unrolled (the window shift becomes register renaming).  REF: the input is
 // |in - ref| (the second pass of each window).
 constexpr int kSY = 16;
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 
 template <int OFF, bool REF>
 __global__ void __launch_bounds__(128) sat_y_async_kernel(const float *__restrict__ in, const float *__restrict__ ref,
@@ -1427,10 +1462,8 @@ void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *id
     c.a2 = (float)(4.0 / 6.0);
     c.a3 = (float)(1.0 / 6.0);
     c.a13 = c.a1 + c.a3;
-    dim3 grid((yd + kIY - 1) / kIY, (xd + kIX - 1) / kIX, (zd + kIZ - 1) / kIZ);
-    APRB_CUDA(cudaFuncSetAttribute(inv_bspline_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kInvSmem));
-    inv_bspline_kernel<<<grid, 256, kInvSmem, s>>>(ids_raw, ids, yd, xd, zd, on && yn > 2, on && xn > 2, on && zn > 2,
-                                                   c);
+    dim3 grid((yd + kJY - 1) / kJY, (xd + kJX - 1) / kJX, (zd + kJZ - 1) / kJZ);
+    inv_bspline_kernel<<<grid, kJY, 0, s>>>(ids_raw, ids, yd, xd, zd, on && yn > 2, on && xn > 2, on && zn > 2, c);
     count_launch();
     APRB_CHECK_LAUNCH();
 }
