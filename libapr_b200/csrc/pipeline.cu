@@ -281,8 +281,9 @@ __global__ void __launch_bounds__(128) iir_strided_rc_kernel(IT *__restrict__ im
         const IT *P = L + (uint64_t)i0 * stride;
         if (i0 >= 2 && i0 + kRC <= n) {
             float buf[kRC];
+            const IT *q = P;
 #pragma unroll
-            for (int u = 0; u < kRC; ++u) buf[u] = (float)P[(uint64_t)u * stride];
+            for (int u = 0; u < kRC; ++u, q += stride) buf[u] = (float)*q;
 #pragma unroll
             for (int u = 0; u < kRC; ++u) {
                 const float nv = rnd_it<IT>(buf[u] + c.b1 * p1 + c.b2 * p2, scratch_err);
@@ -307,8 +308,9 @@ __global__ void __launch_bounds__(128) iir_strided_rc_kernel(IT *__restrict__ im
         IT *P = L + (uint64_t)i0 * stride;
         if (i0 >= 2 && i0 + kRC <= n - 2) {
             float buf[kRC];
+            const IT *q = P;
 #pragma unroll
-            for (int u = 0; u < kRC; ++u) buf[u] = (float)P[(uint64_t)u * stride];
+            for (int u = 0; u < kRC; ++u, q += stride) buf[u] = (float)*q;
 #pragma unroll
             for (int u = 0; u < kRC; ++u) {
                 const float nv = rnd_it<IT>(buf[u] + c.b1 * r1 + c.b2 * r2, err);
@@ -323,8 +325,9 @@ __global__ void __launch_bounds__(128) iir_strided_rc_kernel(IT *__restrict__ im
                 q4 = q3;
                 q3 = temp;
             }
+            IT *w = P;
 #pragma unroll
-            for (int u = 0; u < kRC; ++u) P[(uint64_t)u * stride] = to_it<IT>(buf[u]);
+            for (int u = 0; u < kRC; ++u, w += stride) *w = to_it<IT>(buf[u]);
         } else {
             const int i1 = min(n, i0 + kRC);
             float buf[kRC];
@@ -452,14 +455,16 @@ __global__ void __launch_bounds__(128) iir_y_rc_kernel(const uint16_t *__restric
     }
     const int ntile = (yn + kAY - 1) / kAY;
     const int cq = lane & 15, ch = lane >> 4;  // copies: word cq of lines 2 jj + ch
+    const uint16_t *src_w = src + (line0 + ch) * (uint64_t)yn + 2 * cq;  // this lane's first copy source
+    const uint64_t src_step = 2 * (uint64_t)yn;
     auto issue = [&](int t, uint32_t *buf) {
         const int y = t * kAY + 2 * cq;
         if (y < yn) {
+            const uint16_t *p = src_w + t * kAY;
+            uint32_t *d = buf + ch * 17 + cq;
 #pragma unroll 4
-            for (int jj = 0; jj < 16; ++jj) {
-                const int j = 2 * jj + ch;
-                if (j < nl) cp_async4w(buf + j * 17 + cq, src + (line0 + j) * (uint64_t)yn + y);
-            }
+            for (int jj = 0; jj < 16; ++jj, p += src_step, d += 34)
+                if (2 * jj + ch < nl) cp_async4w(d, p);
         }
         cp_async_commit();
     };
@@ -567,8 +572,9 @@ __global__ void __launch_bounds__(128) iir_y_rc_kernel(const uint16_t *__restric
         }
         __syncwarp();
         if (y0 + lane < yn) {
+            IT *q = dst + line0 * (uint64_t)yn + y0 + lane;
 #pragma unroll 4
-            for (int j = 0; j < nl; ++j) dst[(line0 + j) * (uint64_t)yn + y0 + lane] = to_it<IT>(F[j * 33 + lane]);
+            for (int j = 0; j < nl; ++j, q += yn) *q = to_it<IT>(F[j * 33 + lane]);
         }
         __syncwarp();
     }
@@ -1016,15 +1022,17 @@ __global__ void __launch_bounds__(128) sat_y_async_kernel(const float *__restric
     auto issue = [&](int t, int b) {
         const int y = t * kSY + cy;
         const int my = (refl && y < n) ? reflect101(y - pm.sy, pm.yd) : 0;
+        const float *pa = in + (line0 + cj) * (uint64_t)n + y;  // unreflected source of line cj
+        const float *ra = REF ? ref + (line0 + cj) * (uint64_t)n + y : nullptr;
+        const uint64_t step = 2 * (uint64_t)n;
 #pragma unroll 2
-        for (int jj = 0; jj < 16; ++jj) {
+        for (int jj = 0; jj < 16; ++jj, pa += step, ra += REF ? step : 0) {
             const int j = 2 * jj + cj;
             const uint64_t bj = __shfl_sync(0xffffffffu, mbase, j);
-            const uint64_t ln = line0 + j;
-            if (ln < nlines && y < n) {
-                const uint64_t a = ln * (uint64_t)n + y, am = bj + (uint64_t)my;
-                cp_async4(&sm[w][b][0][j][cy], in + (pm.on_in ? am : a));
-                if (REF) cp_async4(&sm[w][b][NB - 1][j][cy], ref + (pm.on_ref ? am : a));
+            if (line0 + j < nlines && y < n) {
+                const uint64_t am = bj + (uint64_t)my;
+                cp_async4(&sm[w][b][0][j][cy], pm.on_in ? in + am : pa);
+                if (REF) cp_async4(&sm[w][b][NB - 1][j][cy], pm.on_ref ? ref + am : ra);
             }
         }
         cp_async_commit();
@@ -1075,12 +1083,11 @@ __global__ void __launch_bounds__(128) sat_y_async_kernel(const float *__restric
         __syncwarp();
         const int yy = y0 + cy, i = yy - OFF;
         if (yy < n && i >= 0 && i < n - OFF) {
+            float *q = out + (line0 + cj) * (uint64_t)n + i;
+            const uint64_t step = 2 * (uint64_t)n;
 #pragma unroll 4
-            for (int jj = 0; jj < 16; ++jj) {
-                const int j = 2 * jj + cj;
-                const uint64_t ln = line0 + j;
-                if (ln < nlines) out[ln * (uint64_t)n + i] = T[j][cy];
-            }
+            for (int jj = 0; jj < 16; ++jj, q += step)
+                if (line0 + 2 * jj + cj < nlines) *q = T[2 * jj + cj][cy];
         }
         __syncwarp();
     }
