@@ -256,6 +256,13 @@ aprb_status aprb_synth_blobs_f32(float *img_dev, int y_num, int x_num, int z_num
                                  float sigma_hi, float amp_lo, float amp_hi, float background, uint64_t seed,
                                  void *stream);
 
+/* --- self-check of the division by a kernel constant ---------------------------
+ * The box means divide by a window length fixed per launch with a corrected
+ * reciprocal product instead of the IEEE division; this runs both on all 2^32
+ * float inputs for divisor d on the current device and returns how many
+ * results differ in their bits (NaNs compare equal) and the first such input. */
+aprb_status aprb_check_division_by_constant(float d, uint64_t *mismatches, uint32_t *first_bits);
+
 /* number of kernel launches this thread issued through the library so far */
 uint64_t aprb_kernel_launch_count(void);
 

@@ -86,6 +86,7 @@ SIGNATURES = {
     "aprb_synth_blobs_u16": ([_vp, _i, _i, _i, _i, _f, _f, _f, _f, _f, _u64, _vp], _i),
     "aprb_synth_blobs_f32": ([_vp, _i, _i, _i, _i, _f, _f, _f, _f, _f, _u64, _vp], _i),
     "aprb_kernel_launch_count": ([], _u64),
+    "aprb_check_division_by_constant": ([C.c_float, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)], _i),
     "aprb_profile_enable": ([_i], _i),
     "aprb_profile_reset": ([], _i),
     "aprb_profile_read": ([C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_uint64), _i], _i),

@@ -208,6 +208,23 @@ const char *aprb_status_string(aprb_status s) {
 const char *aprb_last_error(void) { return g_last_error.c_str(); }
 uint64_t aprb_kernel_launch_count(void) { return g_launches; }
 
+aprb_status aprb_check_division_by_constant(float d, uint64_t *mismatches, uint32_t *first_bits) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(mismatches && first_bits, "null argument");
+        cudaStream_t s = cudaStreamPerThread;
+        unsigned long long *dev = (unsigned long long *)scratch().obj.get(2 * sizeof(unsigned long long));
+        const unsigned long long init[2] = {0ull, ~0ull};
+        APRB_CUDA(cudaMemcpyAsync(dev, init, sizeof(init), cudaMemcpyHostToDevice, s));
+        launch_check_div_const(d, dev, s);
+        unsigned long long h[2];
+        APRB_CUDA(cudaMemcpyAsync(h, dev, sizeof(h), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaStreamSynchronize(s));
+        *mismatches = h[0];
+        *first_bits = h[1] == ~0ull ? 0u : (uint32_t)h[1];
+    });
+}
+
 aprb_status aprb_profile_enable(int on) {
     g_prof_on = on != 0;
     return APRB_OK;

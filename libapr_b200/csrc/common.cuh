@@ -161,6 +161,24 @@ __device__ __forceinline__ uint32_t cvt_u32(float v) {
     return (uint32_t)(long long)v;
 }
 
+// x / d, correctly rounded, for a divisor d fixed over a kernel with r its
+// correctly rounded reciprocal: Markstein's correction of the product
+// (P. Markstein, IA-64 and Elementary Functions, 2000, Theorem 8.10): q =
+// RN(x r) is within one ulp of x / d, the remainder e = x - q d is exact in
+// one fused multiply-add, and RN(q + e r) is the correctly rounded quotient.
+// Quotients that are zero, tiny or not finite take the IEEE division.
+// aprb_check_division_by_constant compares it with the IEEE division on all
+// 2^32 inputs.
+#ifdef __CUDACC__
+__device__ __forceinline__ float div_const(float x, float d, float r) {
+    const float q = __fmul_rn(x, r);
+    const float aq = fabsf(q);
+    if (!(aq >= 0x1p-100f && aq <= 0x1p100f)) return __fdiv_rn(x, d);
+    const float e = __fmaf_rn(-q, d, x);
+    return __fmaf_rn(e, r, q);
+}
+#endif
+
 __host__ __device__ __forceinline__ size_t idx3(int y, int x, int z, int yn, int xn) {
     return ((size_t)z * (size_t)xn + (size_t)x) * (size_t)yn + (size_t)y;
 }

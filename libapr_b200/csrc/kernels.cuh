@@ -27,6 +27,7 @@ struct LisBuffers {
 };
 
 // ---- pipeline.cu
+void launch_check_div_const(float d, unsigned long long *out, cudaStream_t s);
 void launch_minmax_offset(const uint16_t *img, uint64_t n, unsigned *mm, float *offset, int apply, cudaStream_t s);
 template <typename IT>
 void launch_smooth(const uint16_t *img, IT *work, int yn, int xn, int zn, float lambda, const float *d_offset,

@@ -1019,6 +1019,7 @@ __global__ void __launch_bounds__(128) sat_y_async_kernel(const float *__restric
     // copy / store mapping: a warp instruction moves two lines of kSY samples
     const int cy = lane & (kSY - 1), cj = lane >> 4;
     const int ntile = (n + kSY - 1) / kSY;
+    const float rd = __frcp_rn(d);
     auto issue = [&](int t, int b) {
         const int y = t * kSY + cy;
         const int my = (refl && y < n) ? reflect101(y - pm.sy, pm.yd) : 0;
@@ -1063,8 +1064,8 @@ __global__ void __launch_bounds__(128) sat_y_async_kernel(const float *__restric
 #pragma unroll
                     for (int q = 0; q < W - 1; ++q) c[q] = c[q + 1];
                     c[W - 1] = C;
-                    float o = -c[0] / d;
-                    T[lane][k] = o + C / d;
+                    const float o = div_const(-c[0], d, rd);
+                    T[lane][k] = o + div_const(C, d, rd);
                 }
             } else {
                 const int kend = min(kSY, n - y0);
@@ -1144,13 +1145,29 @@ __global__ void __launch_bounds__(128) sat_strided_kernel(const float *__restric
 #pragma unroll
     for (int q = 0; q < W; ++q) c[q] = 0.0f;
     float C = 0.0f;
-    const float dd = (float)(2 * OFF + 1);
+    const float dd = (float)(2 * OFF + 1), rdd = __frcp_rn(dd);
     for (int j0 = 0; j0 < n; j0 += 32) {
         const int m = min(32, n - j0);
         // lane l loads sample j0 + k of its own line for k < m (coalesced over
-        // the warp's lines), stored transposed: tile[k][lane]
-        for (int k = 0; k < m; ++k) {
-            if (valid) {
+        // the warp's lines), stored transposed: tile[k][lane]; whole chunks
+        // keep eight loads in flight per thread
+        if (valid && m == 32) {
+            const float *p = in + base + (uint64_t)j0 * stride;
+            const float *q = absdiff_ref ? absdiff_ref + base + (uint64_t)j0 * stride : nullptr;
+#pragma unroll 1
+            for (int k0 = 0; k0 < 32; k0 += 8) {
+                float v[8];
+#pragma unroll
+                for (int u = 0; u < 8; ++u) v[u] = p[(uint64_t)(k0 + u) * stride];
+                if (q) {
+#pragma unroll
+                    for (int u = 0; u < 8; ++u) v[u] = fabsf(v[u] - q[(uint64_t)(k0 + u) * stride]);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; ++u) tile[w][k0 + u][lane] = v[u];
+            }
+        } else if (valid) {
+            for (int k = 0; k < m; ++k) {
                 const uint64_t a = base + (uint64_t)(j0 + k) * stride;
                 float v = in[a];
                 if (absdiff_ref) v = fabsf(v - absdiff_ref[a]);
@@ -1171,7 +1188,7 @@ __global__ void __launch_bounds__(128) sat_strided_kernel(const float *__restric
                     if (i < OFF + 1)
                         emit(i, C / (float)(i + OFF + 1));
                     else if (i < n - OFF)
-                        emit(i, (C - c[0]) / dd);
+                        emit(i, div_const(C - c[0], dd, rdd));
                 }
             }
         }
@@ -1630,5 +1647,32 @@ template void launch_levels<uint16_t>(uint16_t *, float *, const float *, uint64
                                       int, int, uint8_t *, uint8_t *, int, cudaStream_t);
 template void launch_levels<float>(float *, float *, const float *, uint64_t, const float *, const aprb_params &, int,
                                    int, uint8_t *, uint8_t *, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// exhaustive comparison of div_const with the IEEE division
+// ---------------------------------------------------------------------------
+__global__ void check_div_const_kernel(float d, unsigned long long *out) {
+    const float r = __frcp_rn(d);
+    unsigned long long bad = 0, first = ~0ull;
+    for (uint64_t b = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; b < (1ull << 32);
+         b += (uint64_t)gridDim.x * blockDim.x) {
+        const float x = __uint_as_float((uint32_t)b);
+        const float a = div_const(x, d, r), e = __fdiv_rn(x, d);
+        if (__float_as_uint(a) != __float_as_uint(e) && !(a != a && e != e)) {
+            ++bad;
+            first = b < first ? b : first;
+        }
+    }
+    if (bad) {
+        atomicAdd(&out[0], bad);
+        atomicMin(&out[1], first);
+    }
+}
+
+void launch_check_div_const(float d, unsigned long long *out, cudaStream_t s) {
+    check_div_const_kernel<<<148 * 16, 256, 0, s>>>(d, out);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+}
 
 }  // namespace aprb
