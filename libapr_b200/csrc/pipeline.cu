@@ -581,13 +581,23 @@ __global__ void __launch_bounds__(128) iir_y_rc_kernel(const uint16_t *__restric
     if (err) atomicAdd(err_out, err);
 }
 
-constexpr int kGX = 8, kGY = 64, kGZ = 8, kGThreads = 256, kGSlots = 6;
-constexpr int kTX = 2 * kGX + 2, kTY = 2 * kGY + 2;
+// 8 x 60 ds cells per plane step: tile columns start four samples before
+// 2 * yd0 so that rows split into aligned 16-byte pieces, and six slots of
+// 18 x 128 floats let four blocks share an SM
+constexpr int kGX = 8, kGY = 60, kGZ = 8, kGThreads = 256, kGSlots = 6;
+constexpr int kTX = 2 * kGX + 2, kTY = 2 * kGY + 8;
 constexpr size_t kGradSmem = sizeof(float) * kGSlots * kTX * kTY;
 
+__device__ __forceinline__ void cp_async16(float *smem, const float *gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+
 // PW2: every 2h is a power of two, so dividing by it is the exact multiply by
-// its reciprocal (both round the same real number once).
-template <typename IT, bool PW2>
+// its reciprocal (both round the same real number once).  VEC (float
+// ImageType, yn a multiple of 4, 16-byte aligned image): tile rows arrive in
+// 16-byte copies.
+template <typename IT, bool PW2, bool VEC>
 __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict__ im, int yn, int xn, int zn,
                                                             IT *__restrict__ grad, float *__restrict__ ids, int yd,
                                                             int xd, int zd, float hx, float hy, float hz) {
@@ -597,34 +607,52 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
     float(*ring)[kTX][kTY] = reinterpret_cast<float(*)[kTX][kTY]>(grad_smem);
     const int yd0 = blockIdx.x * kGY, xd0 = blockIdx.y * kGX, zd0 = blockIdx.z * kGZ;
     const int zd1 = min(zd0 + kGZ, zd);
-    const int xf0 = 2 * xd0 - 1, yf0 = 2 * yd0 - 1;
+    const int xf0 = 2 * xd0 - 1, yf0 = 2 * yd0 - 4;
     const float hx2 = 2 * hx, hy2 = 2 * hy, hz2 = 2 * hz;
     const float ihx2 = 1.0f / hx2, ihy2 = 1.0f / hy2, ihz2 = 1.0f / hz2;
     constexpr bool kAsync = std::is_same<IT, float>::value;  // 4-byte elements copy asynchronously
 
     // a thread fills the same (clamped) tile positions t = threadIdx.x + k *
     // kGThreads of every plane: their in-plane source offsets once
-    constexpr int kLoads = (kTX * kTY + kGThreads - 1) / kGThreads;
+    constexpr int kLoads = VEC ? 1 : (kTX * kTY + kGThreads - 1) / kGThreads;
     uint64_t src_off[kLoads];
+    if (!VEC) {
 #pragma unroll
-    for (int k = 0; k < kLoads; ++k) {
-        const int t = threadIdx.x + k * kGThreads;
-        const int r = t / kTY, cc = t % kTY;
-        const int xg = min(max(xf0 + r, 0), xn - 1), yg = min(max(yf0 + cc, 0), yn - 1);
-        src_off[k] = (uint64_t)xg * (uint64_t)yn + (uint64_t)yg;
+        for (int k = 0; k < kLoads; ++k) {
+            const int t = threadIdx.x + k * kGThreads;
+            const int r = t / kTY, cc = t % kTY;
+            const int xg = min(max(xf0 + r, 0), xn - 1), yg = min(max(yf0 + cc, 0), yn - 1);
+            src_off[k] = (uint64_t)xg * (uint64_t)yn + (uint64_t)yg;
+        }
     }
     auto load = [&](int zf) {  // zf >= -1
         float *S = &ring[(zf + kGSlots) % kGSlots][0][0];
         const int zc = min(max(zf, 0), zn - 1);
         const IT *plane = im + (uint64_t)zc * (uint64_t)xn * (uint64_t)yn;
+        if (VEC) {
+            constexpr int kQ = kTY / 4;  // 16-byte pieces per row
+            for (int ci = threadIdx.x; ci < kTX * kQ; ci += kGThreads) {
+                const int r = ci / kQ, q = ci % kQ;
+                const int xg = min(max(xf0 + r, 0), xn - 1), yg = yf0 + 4 * q;
+                const float *row = reinterpret_cast<const float *>(plane) + (uint64_t)xg * (uint64_t)yn;
+                float *d = S + r * kTY + 4 * q;
+                if (yg >= 0 && yg + 3 < yn) {
+                    cp_async16(d, row + yg);
+                } else {
 #pragma unroll
-        for (int k = 0; k < kLoads; ++k) {
-            const int t = threadIdx.x + k * kGThreads;
-            if (t < kTX * kTY) {
-                if (kAsync)
-                    cp_async4(S + t, reinterpret_cast<const float *>(plane) + src_off[k]);
-                else
-                    S[t] = (float)plane[src_off[k]];
+                    for (int e = 0; e < 4; ++e) cp_async4(d + e, row + min(max(yg + e, 0), yn - 1));
+                }
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < kLoads; ++k) {
+                const int t = threadIdx.x + k * kGThreads;
+                if (t < kTX * kTY) {
+                    if (kAsync)
+                        cp_async4(S + t, reinterpret_cast<const float *>(plane) + src_off[k]);
+                    else
+                        S[t] = (float)plane[src_off[k]];
+                }
             }
         }
     };
@@ -679,37 +707,55 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
             const float(*P1)[kTY] = ring[(z0 + kGSlots) % kGSlots];
             const float(*P2)[kTY] = ring[(z0 + 1 + kGSlots) % kGSlots];
             const float(*P3)[kTY] = ring[(z0 + 2 + kGSlots) % kGSlots];
+            // cy is even: the samples come in aligned pairs (y, y + 1)
+            auto ld2 = [](const float *q) { return *reinterpret_cast<const float2 *>(q); };
+            struct Nb {
+                float2 m, p;          // rows rx - 1 and rx + 2 at (cy, cy + 1)
+                float2 a0, a1, a2;    // row rx at cy - 2, cy, cy + 2
+                float2 b0, b1, b2;    // row rx + 1
+            };
+            auto nb = [&](const float(*P)[kTY]) {
+                Nb q;
+                q.m = ld2(&P[rx - 1][cy]);
+                q.p = ld2(&P[rx + 2][cy]);
+                q.a0 = ld2(&P[rx][cy - 2]);
+                q.a1 = ld2(&P[rx][cy]);
+                q.a2 = ld2(&P[rx][cy + 2]);
+                q.b0 = ld2(&P[rx + 1][cy - 2]);
+                q.b1 = ld2(&P[rx + 1][cy]);
+                q.b2 = ld2(&P[rx + 1][cy + 2]);
+                return q;
+            };
+            const Nb n1 = nb(P1), n2 = nb(P2);
             float gmax = 0.0f;
             if (yn >= 2) {
                 // the gradient magnitude is max over the 2 x 2 x 2 children; the
                 // conversion sqrt -> ImageType is monotone (below 2^16 for
                 // uint16), so the max is taken over the squares and rooted once
-                auto children = [&](auto &&f) {
-#pragma unroll
-                    for (int dz = 0; dz < 2; ++dz) {
-                        if (dz == 1 && !z1in) break;
-                        const float(*C)[kTY] = dz ? P2 : P1;
-                        const float(*U)[kTY] = dz ? P1 : P0;
-                        const float(*D)[kTY] = dz ? P3 : P2;
-#pragma unroll
-                        for (int dx = 0; dx < 2; ++dx) {
-                            if (dx == 1 && !x1in) break;
-                            const int r = rx + dx;
-                            const float c0 = C[r][cy - 1], c1 = C[r][cy], c2 = C[r][cy + 1], c3 = C[r][cy + 2];
-                            const double a = gsq(C[r - 1][cy], C[r + 1][cy], c0, c2, U[r][cy], D[r][cy]);
-                            f(a);
-                            if (y1in) f(gsq(C[r - 1][cy + 1], C[r + 1][cy + 1], c1, c3, U[r][cy + 1], D[r][cy + 1]));
-                        }
+                const float2 u0a = ld2(&P0[rx][cy]), u0b = ld2(&P0[rx + 1][cy]);
+                const float2 d3a = ld2(&P3[rx][cy]), d3b = ld2(&P3[rx + 1][cy]);
+                // children of plane C with neighbour planes U (rows rx, rx + 1)
+                // and D: (x, y) = (rx, cy) (rx, cy+1) (rx+1, cy) (rx+1, cy+1)
+                auto children = [&](const Nb &C, float2 ua, float2 ub, float2 da, float2 db, auto &&f) {
+                    f(gsq(C.m.x, C.b1.x, C.a0.y, C.a1.y, ua.x, da.x));
+                    if (y1in) f(gsq(C.m.y, C.b1.y, C.a1.x, C.a2.x, ua.y, da.y));
+                    if (x1in) {
+                        f(gsq(C.a1.x, C.p.x, C.b0.y, C.b1.y, ub.x, db.x));
+                        if (y1in) f(gsq(C.a1.y, C.p.y, C.b1.x, C.b2.x, ub.y, db.y));
                     }
                 };
+                auto all = [&](auto &&f) {
+                    children(n1, u0a, u0b, n2.a1, n2.b1, f);
+                    if (z1in) children(n2, n1.a1, n1.b1, d3a, d3b, f);
+                };
                 double smax = 0.0;  // every square is >= 0
-                children([&](double q) { smax = q > smax ? q : smax; });
+                all([&](double q) { smax = q > smax ? q : smax; });
                 if (sizeof(IT) == 4 || smax < 4294967296.0) {
                     const double root = sqrt(smax);
                     gmax = sizeof(IT) == 2 ? cvt_u16d(root) : (float)root;
                 } else {
                     // roots of 2^16 and above wrap in the uint16 conversion
-                    children([&](double q) {
+                    all([&](double q) {
                         const float v = cvt_u16d(sqrt(q));
                         gmax = v > gmax ? v : gmax;
                     });
@@ -718,14 +764,14 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
             const uint64_t o = idx3(k, xk, z, yd, xd);
             grad[o] = to_it<IT>(gmax);
             // mean with the clamped indices of downsample (held by the tile)
-            float s = P1[rx][cy];
-            s = s + P1[rx][cy + 1];
-            s = s + P1[rx + 1][cy];
-            s = s + P1[rx + 1][cy + 1];
-            s = s + P2[rx][cy];
-            s = s + P2[rx][cy + 1];
-            s = s + P2[rx + 1][cy];
-            s = s + P2[rx + 1][cy + 1];
+            float s = n1.a1.x;
+            s = s + n1.a1.y;
+            s = s + n1.b1.x;
+            s = s + n1.b1.y;
+            s = s + n2.a1.x;
+            s = s + n2.a1.y;
+            s = s + n2.b1.x;
+            s = s + n2.b1.y;
             ids[o] = s * 0.125f;  // == s / 8 exactly
         }
         if (kAsync) cp_async_wait_all();
@@ -1252,27 +1298,91 @@ __global__ void const_scale_fill_kernel(float *out, uint64_t n, const double *su
 // and PullingScheme::fill at the top pct level (PullingScheme.hpp:137-149).
 // ---------------------------------------------------------------------------
 template <typename IT>
+__device__ __forceinline__ void level_of(IT &gv, float &sv, float idv, float th, float sigma_th, float sigma_th_max,
+                                         float grad_th, float mult, int top_level, uint8_t &lev8, uint8_t &st8) {
+    float g = (float)gv;
+    float s = sv;
+    if (idv <= th) g = 0.0f;
+    if (s < sigma_th) s = (s < sigma_th_max) ? 60000.0f : sigma_th;
+    if (g < grad_th) g = 0.0f;
+    gv = to_it<IT>(g);
+    sv = s;
+    const float q = g / s;
+    const uint32_t u = cvt_u32(q * mult);
+    const int lev = u == 0 ? 0 : 31 - __clz(u);
+    lev8 = (uint8_t)lev;
+    st8 = ((float)lev >= (float)top_level) ? kSeed : kEmpty;
+}
+
+// Four cells per thread with vector loads and stores when the arrays allow it
+// (VEC), else one.
+template <typename IT, bool VEC>
 __global__ void levels_kernel(IT *__restrict__ grad, float *__restrict__ lis, const float *__restrict__ ids,
                               uint64_t nd, const float *__restrict__ d_offset, float Ip_th, float sigma_th,
                               float sigma_th_max, float grad_th, float mult, int top_level, uint8_t *__restrict__ level,
                               uint8_t *__restrict__ status, int keep) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nd) return;
     const float th = Ip_th + (d_offset ? *d_offset : 0.0f);
-    float g = (float)grad[i];
+    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (VEC) {
+        const uint64_t i = 4 * t;
+        if (i >= nd) return;
+        if (i + 4 <= nd) {
+            IT g[4];
+            float s[4], d[4];
+            if (sizeof(IT) == 4) {
+                const float4 v = *reinterpret_cast<const float4 *>(grad + i);
+                g[0] = (IT)v.x, g[1] = (IT)v.y, g[2] = (IT)v.z, g[3] = (IT)v.w;
+            } else {
+                const ushort4 v = *reinterpret_cast<const ushort4 *>(grad + i);
+                g[0] = (IT)v.x, g[1] = (IT)v.y, g[2] = (IT)v.z, g[3] = (IT)v.w;
+            }
+            const float4 sv = *reinterpret_cast<const float4 *>(lis + i);
+            const float4 dv = *reinterpret_cast<const float4 *>(ids + i);
+            s[0] = sv.x, s[1] = sv.y, s[2] = sv.z, s[3] = sv.w;
+            d[0] = dv.x, d[1] = dv.y, d[2] = dv.z, d[3] = dv.w;
+            uint8_t lv[4], st[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                level_of<IT>(g[k], s[k], d[k], th, sigma_th, sigma_th_max, grad_th, mult, top_level, lv[k], st[k]);
+            *reinterpret_cast<uchar4 *>(level + i) = make_uchar4(lv[0], lv[1], lv[2], lv[3]);
+            if (status) *reinterpret_cast<uchar4 *>(status + i) = make_uchar4(st[0], st[1], st[2], st[3]);
+            if (keep) {
+                if (sizeof(IT) == 4)
+                    *reinterpret_cast<float4 *>(grad + i) = make_float4((float)g[0], (float)g[1], (float)g[2],
+                                                                        (float)g[3]);
+                else
+                    *reinterpret_cast<ushort4 *>(grad + i) = make_ushort4((uint16_t)g[0], (uint16_t)g[1],
+                                                                          (uint16_t)g[2], (uint16_t)g[3]);
+                *reinterpret_cast<float4 *>(lis + i) = make_float4(s[0], s[1], s[2], s[3]);
+            }
+            return;
+        }
+        for (uint64_t j = i; j < nd; ++j) {
+            IT g = grad[j];
+            float s = lis[j];
+            uint8_t lv, st;
+            level_of<IT>(g, s, ids[j], th, sigma_th, sigma_th_max, grad_th, mult, top_level, lv, st);
+            level[j] = lv;
+            if (status) status[j] = st;
+            if (keep) {
+                grad[j] = g;
+                lis[j] = s;
+            }
+        }
+        return;
+    }
+    const uint64_t i = t;
+    if (i >= nd) return;
+    IT g = grad[i];
     float s = lis[i];
-    if (ids[i] <= th) g = 0.0f;
-    if (s < sigma_th) s = (s < sigma_th_max) ? 60000.0f : sigma_th;
-    if (g < grad_th) g = 0.0f;
+    uint8_t lv, st;
+    level_of<IT>(g, s, ids[i], th, sigma_th, sigma_th_max, grad_th, mult, top_level, lv, st);
+    level[i] = lv;
+    if (status) status[i] = st;
     if (keep) {
-        grad[i] = to_it<IT>(g);
+        grad[i] = g;
         lis[i] = s;
     }
-    const float q = g / s;
-    const uint32_t u = cvt_u32(q * mult);
-    const int lev = u == 0 ? 0 : 31 - __clz(u);
-    level[i] = (uint8_t)lev;
-    if (status) status[i] = ((float)lev >= (float)top_level) ? kSeed : kEmpty;
 }
 
 // ---------------------------------------------------------------------------
@@ -1465,16 +1575,21 @@ void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *id
             const float m = std::frexp(2.0f * h, &e);
             return m == 0.5f && e > -120 && e < 120;
         };
+        auto run = [&](auto kern) {
+            APRB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGradSmem));
+            kern<<<grid, kGThreads, kGradSmem, s>>>(work, yn, xn, zn, grad, ids_raw, yd, xd, zd, p.dx, p.dy, p.dz);
+        };
+        const bool vec = sizeof(IT) == 4 && yn % 4 == 0 && ((uintptr_t)work & 15) == 0;
         if (pow2(p.dx) && pow2(p.dy) && pow2(p.dz)) {
-            APRB_CUDA(cudaFuncSetAttribute(grad_ds_kernel<IT, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)kGradSmem));
-            grad_ds_kernel<IT, true><<<grid, kGThreads, kGradSmem, s>>>(work, yn, xn, zn, grad, ids_raw, yd, xd, zd,
-                                                                        p.dx, p.dy, p.dz);
+            if (vec)
+                run(grad_ds_kernel<IT, true, true>);
+            else
+                run(grad_ds_kernel<IT, true, false>);
         } else {
-            APRB_CUDA(cudaFuncSetAttribute(grad_ds_kernel<IT, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int)kGradSmem));
-            grad_ds_kernel<IT, false><<<grid, kGThreads, kGradSmem, s>>>(work, yn, xn, zn, grad, ids_raw, yd, xd, zd,
-                                                                         p.dx, p.dy, p.dz);
+            if (vec)
+                run(grad_ds_kernel<IT, false, true>);
+            else
+                run(grad_ds_kernel<IT, false, false>);
         }
         count_launch();
         APRB_CHECK_LAUNCH();
@@ -1623,9 +1738,15 @@ void launch_levels(IT *grad, float *lis, const float *ids, uint64_t nd, const fl
     const float min_dim = mxz < p.dy ? mxz : p.dy;
     const float level_factor = (float)(std::pow(2.0, (double)apr_l_max) * (double)min_dim);
     const float mult = level_factor / p.rel_error;
-    levels_kernel<IT><<<blocks_for(nd, 256), 256, 0, s>>>(grad, lis, ids, nd, d_offset, p.Ip_th, p.sigma_th,
-                                                         p.sigma_th_max, p.grad_th, mult, top_level, level, status,
-                                                         keep);
+    auto al = [](const void *q, int a) { return ((uintptr_t)q % a) == 0; };
+    if (al(grad, 4 * sizeof(IT)) && al(lis, 16) && al(ids, 16) && al(level, 4) && (!status || al(status, 4)))
+        levels_kernel<IT, true><<<blocks_for((nd + 3) / 4, 256), 256, 0, s>>>(
+            grad, lis, ids, nd, d_offset, p.Ip_th, p.sigma_th, p.sigma_th_max, p.grad_th, mult, top_level, level,
+            status, keep);
+    else
+        levels_kernel<IT, false><<<blocks_for(nd, 256), 256, 0, s>>>(grad, lis, ids, nd, d_offset, p.Ip_th,
+                                                                    p.sigma_th, p.sigma_th_max, p.grad_th, mult,
+                                                                    top_level, level, status, keep);
     count_launch();
     APRB_CHECK_LAUNCH();
 }
