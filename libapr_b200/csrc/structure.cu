@@ -139,6 +139,63 @@ __global__ void __launch_bounds__(256) dilate_kernel(uint8_t *__restrict__ st, L
     }
 }
 
+// The same dilation for rows of a multiple of 4 cells: a lane moves 4
+// consecutive cells of a row as one 32-bit word, so a warp reads the block's
+// 128 y of a row in one load, and the shared mask holds per row and lane the
+// 4 bits of the lane's cells.  Phase 2 writes the words whose cells change.
+template <int MODE>
+__global__ void __launch_bounds__(256) dilate4_kernel(uint8_t *__restrict__ st, LevelDims d) {
+    __shared__ uint8_t W[kDRows][32];
+    const int y0 = blockIdx.x * kDY, x0 = blockIdx.y * kDX, z0 = blockIdx.z * kDZ;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y = y0 + 4 * lane;  // first of the lane's cells; yn % 4 == 0, so all 4 are in or out
+    for (int r = w; r < kDRows; r += 8) {
+        const int x = x0 - 1 + r % (kDX + 2), z = z0 - 1 + r / (kDX + 2);
+        const bool row_in = x >= 0 && x < d.xn && z >= 0 && z < d.zn;
+        const uint8_t *R = st + ((uint64_t)(row_in ? z : 0) * d.xn + (row_in ? x : 0)) * (uint64_t)d.yn;
+        const bool in = row_in && y < d.yn;
+        const uint32_t v = in ? *reinterpret_cast<const uint32_t *>(R + y) : 0u;
+        unsigned p = 0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            if (in && dil_source<MODE>((uint8_t)(v >> (8 * e)))) p |= 1u << e;
+        unsigned pl = (__shfl_up_sync(0xffffffffu, p, 1) >> 3) & 1u;
+        unsigned pr = __shfl_down_sync(0xffffffffu, p, 1) & 1u;
+        if (lane == 0) pl = row_in && y >= 1 && y - 1 < d.yn && dil_source<MODE>(R[y - 1]);
+        if (lane == 31) pr = row_in && y + 4 < d.yn && dil_source<MODE>(R[y + 4]);
+        W[r][lane] = (uint8_t)((p | (p << 1) | (p >> 1) | pl | (pr << 3)) & 0xFu);
+    }
+    __syncthreads();
+    for (int task = w; task < kDX * kDZ; task += 8) {
+        const int xx = task % kDX, zz = task / kDX;
+        const int x = x0 + xx, z = z0 + zz;
+        if (x >= d.xn || z >= d.zn || y >= d.yn) continue;
+        unsigned m = 0;
+#pragma unroll
+        for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx) m |= W[(zz + dz) * (kDX + 2) + xx + dx][lane];
+        if (!m) continue;
+        uint32_t *c = reinterpret_cast<uint32_t *>(st + ((uint64_t)z * d.xn + x) * (uint64_t)d.yn + y);
+        const uint32_t v = *c;
+        uint32_t nv = v;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            if (!((m >> e) & 1u)) continue;
+            const uint8_t s = (uint8_t)(v >> (8 * e));
+            uint8_t t = s;
+            if (MODE == 0) {
+                if (s == kEmpty) t = kAscendantNeighbour;
+                else if (s == kSeed) t = kPropagate;
+            } else {
+                if (s == kEmpty) t = kBoundary;
+            }
+            nv = (nv & ~(0xFFu << (8 * e))) | ((uint32_t)t << (8 * e));
+        }
+        if (nv != v) *c = nv;
+    }
+}
+
 // fill_neighbours -> fill_parent (:372-393), as a gather over the parents
 __global__ void fill_parent_kernel(const uint8_t *__restrict__ child, LevelDims dc, uint8_t *__restrict__ parent,
                                    LevelDims dp) {
@@ -593,8 +650,12 @@ void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s, bool fill
     APRB_CHECK_LAUNCH();
     for (int l = top; l >= lmin; --l) {
         const dim3 dgrid((g.y_num[l] + kDY - 1) / kDY, (g.x_num[l] + kDX - 1) / kDX, (g.z_num[l] + kDZ - 1) / kDZ);
+        const bool by4 = g.y_num[l] % 4 == 0 && ((uintptr_t)pm.status[l] & 3) == 0;
         if (l != top) {
-            dilate_kernel<0><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
+            if (by4)
+                dilate4_kernel<0><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
+            else
+                dilate_kernel<0><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
             if (g.y_num[l + 1] % 8 == 0)
                 set_filler8_kernel<<<blocks_for(ncell(g, l + 1) / 8, 256), 256, 0, s>>>(pm.status[l], dims(g, l),
                                                                                        pm.status[l + 1],
@@ -604,7 +665,10 @@ void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s, bool fill
                                                                                   pm.status[l + 1], dims(g, l + 1));
             count_launch(2);
         }
-        dilate_kernel<1><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
+        if (by4)
+            dilate4_kernel<1><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
+        else
+            dilate_kernel<1><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
         count_launch();
         if (l - 1 >= lmin) {
             if (g.y_num[l] % 8 == 0)
