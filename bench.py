@@ -129,15 +129,18 @@ SINGLE_KERNEL_STAGES = ("bspline_y", "bspline_x", "bspline_z", "gradient_ds", "i
 # the 128x1024x1024 case (dram__bytes_read.sum + dram__bytes_write.sum divided
 # by its voxels; the traffic grows in proportion to the volume)
 TRAFFIC_PER_VOXEL = {
-    "gradient_ds": ((537.404672e6 + 120.107008e6) / (128 * 1024 * 1024),
+    "gradient_ds": ((537.159424e6 + 120.076288e6) / (128 * 1024 * 1024),
                     "ncu, 128x1024x1024 float capture scaled by voxels "
                     "(profiles/grad_ds_kernel_float_128x1024x1024.md)"),
-    "bspline_y": ((651.044608e6 + 883.089920e6) / (128 * 1024 * 1024),
+    "bspline_y": ((534.820096e6 + 518.603776e6) / (128 * 1024 * 1024),
                   "ncu, 128x1024x1024 float capture scaled by voxels "
-                  "(profiles/iir_y_kernel_float_128x1024x1024.md)"),
-    "bspline_x": ((1.010519e9 + 970.695680e6) / (128 * 1024 * 1024),
+                  "(profiles/iir_y_rc_kernel_float_128x1024x1024.md)"),
+    "bspline_x": ((985.272832e6 + 546.396928e6) / (128 * 1024 * 1024),
                   "ncu, 128x1024x1024 float capture scaled by voxels "
-                  "(profiles/iir_strided_kernel_float_128x1024x1024.md)"),
+                  "(profiles/iir_strided_rc_kernel_float_128x1024x1024.md)"),
+    "bspline_z": ((566.572800e6 + 544.346880e6) / (128 * 1024 * 1024),
+                  "ncu, 128x1024x1024 float capture scaled by voxels "
+                  "(profiles/iir_strided_rc_kernel_float_128x1024x1024.md)"),
 }
 
 
