@@ -675,6 +675,25 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
         return fma((double)gy, (double)gy, s);
     };
 
+    // the (at most two) ds cells of this thread in every plane step: tile row
+    // and column of their full-res corner (x0, y0 = 2k), whether y0 + 1 and
+    // x0 + 1 lie inside the volume (else the child is clamped onto y0 / x0),
+    // and their output offset in plane 0
+    constexpr int kCells = (kGX * kGY + kGThreads - 1) / kGThreads;
+    bool cell_in[kCells];
+    int cell_rx[kCells], cell_cy[kCells], cell_flags[kCells];
+    uint64_t cell_o[kCells];
+#pragma unroll
+    for (int q = 0; q < kCells; ++q) {
+        const int t = threadIdx.x + q * kGThreads;
+        const int xl = t / kGY, yl = t % kGY;
+        const int xk = xd0 + xl, k = yd0 + yl;
+        cell_in[q] = t < kGX * kGY && xk < xd && k < yd;
+        cell_rx[q] = 2 * xk - xf0;
+        cell_cy[q] = 2 * k - yf0;
+        cell_flags[q] = (2 * k + 1 < yn ? 1 : 0) | (2 * xk + 1 < xn ? 2 : 0);
+        cell_o[q] = idx3(k, xk, 0, yd, xd);
+    }
     load(2 * zd0 - 1);
     load(2 * zd0);
     if (kAsync) {
@@ -694,19 +713,17 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
             load(2 * z + 2);
             __syncthreads();
         }
-        for (int t = threadIdx.x; t < kGX * kGY; t += kGThreads) {
-            const int xl = t / kGY, yl = t % kGY;
-            const int xk = xd0 + xl, k = yd0 + yl;
-            if (xk >= xd || k >= yd) continue;
-            const int x0 = 2 * xk, z0 = 2 * z;
-            // tile row / column of (x0, y0 = 2k); column cy + 1 is ks = min(2k + 1, yn - 1)
-            // unless that is clamped onto y0
-            const int rx = x0 - xf0, cy = 2 * k - yf0;
-            const bool y1in = 2 * k + 1 < yn, x1in = x0 + 1 < xn, z1in = z0 + 1 < zn;
-            const float(*P0)[kTY] = ring[(z0 - 1 + kGSlots) % kGSlots];
-            const float(*P1)[kTY] = ring[(z0 + kGSlots) % kGSlots];
-            const float(*P2)[kTY] = ring[(z0 + 1 + kGSlots) % kGSlots];
-            const float(*P3)[kTY] = ring[(z0 + 2 + kGSlots) % kGSlots];
+        const int z0 = 2 * z;
+        const bool z1in = z0 + 1 < zn;
+        const float(*P0)[kTY] = ring[(z0 - 1 + kGSlots) % kGSlots];
+        const float(*P1)[kTY] = ring[(z0 + kGSlots) % kGSlots];
+        const float(*P2)[kTY] = ring[(z0 + 1 + kGSlots) % kGSlots];
+        const float(*P3)[kTY] = ring[(z0 + 2 + kGSlots) % kGSlots];
+#pragma unroll
+        for (int q = 0; q < kCells; ++q) {
+            if (!cell_in[q]) continue;
+            const int rx = cell_rx[q], cy = cell_cy[q];
+            const bool y1in = (cell_flags[q] & 1) != 0, x1in = (cell_flags[q] & 2) != 0;
             // cy is even: the samples come in aligned pairs (y, y + 1)
             auto ld2 = [](const float *q) { return *reinterpret_cast<const float2 *>(q); };
             struct Nb {
@@ -761,7 +778,7 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
                     });
                 }
             }
-            const uint64_t o = idx3(k, xk, z, yd, xd);
+            const uint64_t o = cell_o[q] + (uint64_t)z * (uint64_t)xd * (uint64_t)yd;
             grad[o] = to_it<IT>(gmax);
             // mean with the clamped indices of downsample (held by the tile)
             float s = n1.a1.x;
