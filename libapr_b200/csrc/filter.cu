@@ -102,10 +102,17 @@ __global__ void chunk_index_kernel(const uint64_t *__restrict__ xz_end, uint64_t
     for (int q = lastc + 1 + lane; q <= nc; q += 32) C[q] = (uint16_t)(e - b);
 }
 
+constexpr int kConvK = 4;  // output particles per lane and pass
+
 // ---------------------------------------------------------------------------
 // tree means of tree level t (children at level t+1)
 // ---------------------------------------------------------------------------
-constexpr int kTW = 256;  // parent cells per CTA along y (a multiple of kYC)
+constexpr int kTR = 2;  // parent rows per CTA
+// parent cells per CTA along y (a multiple of kYC), within 48 KB of staging
+template <typename T>
+__host__ __device__ constexpr int tree_tw() {
+    return sizeof(T) == 8 ? 256 : 512;
+}
 
 struct TreeLevelArgs {
     LD dt;                  // tree level t dims (== APR level t dims)
@@ -117,68 +124,80 @@ struct TreeLevelArgs {
 };
 
 template <typename T>
-__global__ void __launch_bounds__(128) tree_mean_kernel(TreeLevelArgs a, const uint64_t *__restrict__ xz_end,
-                                                        const uint16_t *__restrict__ y_vec,
-                                                        const T *__restrict__ parts,
-                                                        const uint64_t *__restrict__ t_xz_end,
-                                                        const uint16_t *__restrict__ t_y_vec,
-                                                        T *__restrict__ tree) {
-    __shared__ T sv[4][2 * kTW];
-    __shared__ uint8_t sk[4][2 * kTW];
-    const uint64_t prow = blockIdx.x;  // parent row z*xt + x
-    const int xp = (int)(prow % (uint64_t)a.dt.xn), zp = (int)(prow / (uint64_t)a.dt.xn);
-    const int y0 = blockIdx.y * kTW;
-    const int cy0 = 2 * y0, cy1 = min(2 * y0 + 2 * kTW, a.dc.yn);
+__global__ void __launch_bounds__(128 * kTR) tree_mean_kernel(TreeLevelArgs a, uint64_t rows,
+                                                              const uint64_t *__restrict__ xz_end,
+                                                              const uint16_t *__restrict__ y_vec,
+                                                              const T *__restrict__ parts,
+                                                              const uint64_t *__restrict__ t_xz_end,
+                                                              const uint16_t *__restrict__ t_y_vec,
+                                                              T *__restrict__ tree) {
+    // kTR parent rows per CTA, four warps (one per child row) for each
+    constexpr int TW = tree_tw<T>();
+    __shared__ T sv[kTR][4][2 * TW];
+    __shared__ __align__(4) uint8_t sk[kTR][4][2 * TW];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pr = w >> 2, q4 = w & 3;
+    const uint64_t prow = (uint64_t)blockIdx.x * kTR + pr;  // parent row z*xt + x
+    const bool row_ok = prow < rows;
+    const int xp = row_ok ? (int)(prow % (uint64_t)a.dt.xn) : 0, zp = row_ok ? (int)(prow / (uint64_t)a.dt.xn) : 0;
+    const int y0 = blockIdx.y * TW;
+    const int cy0 = 2 * y0, cy1 = min(2 * y0 + 2 * TW, a.dc.yn);
     // the parent range is independent of the children: fetch it first
-    const int nct = nchunk(a.dt.yn);
-    const uint64_t pb = t_xz_end[a.t_row_base + prow - 1];
-    const uint16_t *PC = a.t_cidx + prow * (uint64_t)(nct + 1);
-    const uint64_t ps = pb + PC[y0 / kYC];
-    const uint64_t pend = pb + PC[min(y0 / kYC + kTW / kYC, nct)];
-    for (int k = threadIdx.x; k < 4 * 2 * kTW; k += blockDim.x) (&sk[0][0])[k] = 0;
+    uint64_t ps = 0, pend = 0;
+    if (row_ok) {
+        const int nct = nchunk(a.dt.yn);
+        const uint64_t pb = t_xz_end[a.t_row_base + prow - 1];
+        const uint16_t *PC = a.t_cidx + prow * (uint64_t)(nct + 1);
+        ps = pb + PC[y0 / kYC];
+        pend = pb + PC[min(y0 / kYC + TW / kYC, nct)];
+    }
+    for (int k = threadIdx.x; k < kTR * 4 * 2 * TW / 4; k += blockDim.x)
+        reinterpret_cast<uint32_t *>(&sk[0][0][0])[k] = 0u;
     __syncthreads();
     {
-        // warp w stages child row (2zp + w/2, 2xp + w%2): its particles and
-        // tree nodes (disjoint cells) in one merged pass
-        const int cz = 2 * zp + (w >> 1), cx = 2 * xp + (w & 1);
-        if (cz < a.dc.zn && cx < a.dc.xn && cy0 < cy1) {
+        // warp (pr, q4) stages child row (2zp + q4/2, 2xp + q4%2): its
+        // particles and tree nodes (disjoint cells) with y in [cy0, cy1).
+        // cy0 and cy1 are chunk starts or the row end, so the chunk index
+        // gives both ends of the ranges and successive passes' loads are
+        // independent.
+        const int cz = 2 * zp + (q4 >> 1), cx = 2 * xp + (q4 & 1);
+        if (row_ok && cz < a.dc.zn && cx < a.dc.xn && cy0 < cy1) {
             const uint64_t row = (uint64_t)cz * a.dc.xn + cx;
             const int ncc = nchunk(a.dc.yn);
-            const uint64_t s0 = xz_end[a.c_row_base + row - 1] + a.c_cidx[row * (uint64_t)(ncc + 1) + cy0 / kYC];
-            const uint64_t e0 = xz_end[a.c_row_base + row];
-            uint64_t s1 = 0, e1 = 0;
-            if (a.ct_row_base) {
-                s1 = t_xz_end[a.ct_row_base + row - 1] + a.ct_cidx[row * (uint64_t)(ncc + 1) + cy0 / kYC];
-                e1 = t_xz_end[a.ct_row_base + row];
+            const uint16_t *CC = a.c_cidx + row * (uint64_t)(ncc + 1);
+            const int c0 = cy0 / kYC, c1 = cy1 == a.dc.yn ? ncc : cy1 / kYC;
+            const uint64_t r0 = xz_end[a.c_row_base + row - 1];
+            const uint64_t s0 = r0 + CC[c0], e0 = r0 + CC[c1];
+            T *V = sv[pr][q4];
+            uint8_t *K = sk[pr][q4];
+#pragma unroll 4
+            for (uint64_t i = s0 + lane; i < e0; i += 32) {
+                const int yv = (int)y_vec[i] - cy0;
+                V[yv] = parts[i];
+                K[yv] = 1;
             }
-            bool go0 = true, go1 = a.ct_row_base != 0;
-            for (uint64_t t = lane; go0 || go1; t += 32) {
-                const uint64_t i0 = s0 + t, i1 = s1 + t;
-                const bool h0 = go0 && i0 < e0, h1 = go1 && i1 < e1;
-                const int yv0 = h0 ? (int)y_vec[i0] : 0x7fffffff;
-                const int yv1 = h1 ? (int)t_y_vec[i1] : 0x7fffffff;
-                const T v0 = h0 ? parts[i0] : T(0);
-                const T v1 = h1 ? tree[i1] : T(0);
-                if (yv0 < cy1) {
-                    sv[w][yv0 - cy0] = v0;
-                    sk[w][yv0 - cy0] = 1;
+            if (a.ct_row_base) {
+                const uint16_t *CT = a.ct_cidx + row * (uint64_t)(ncc + 1);
+                const uint64_t r1 = t_xz_end[a.ct_row_base + row - 1];
+                const uint64_t s1 = r1 + CT[c0], e1 = r1 + CT[c1];
+#pragma unroll 4
+                for (uint64_t i = s1 + lane; i < e1; i += 32) {
+                    const int yv = (int)t_y_vec[i] - cy0;
+                    V[yv] = tree[i];
+                    K[yv] = 2;
                 }
-                if (yv1 < cy1) {
-                    sv[w][yv1 - cy0] = v1;
-                    sk[w][yv1 - cy0] = 2;
-                }
-                go0 = __all_sync(0xffffffffu, h0 && yv0 < cy1);
-                go1 = __all_sync(0xffffffffu, h1 && yv1 < cy1);
             }
         }
     }
     __syncthreads();
+    if (!row_ok) return;
     float sxz = (float)((((2 * a.dt.xn != a.dc.xn) && (xp == a.dt.xn - 1)) +
                          ((2 * a.dt.zn != a.dc.zn) && (zp == a.dt.zn - 1))) * 2);
     if (sxz == 0) sxz = 1;
     const float syxz = (2 * a.dt.yn != a.dc.yn) ? sxz * 2 : sxz;
-    for (uint64_t i = ps + threadIdx.x; i < pend; i += blockDim.x) {
+    // x / 8 == x * 0.125 exactly: both are the correctly rounded x / 8
+    const T eighth = T(0.125);
+    for (uint64_t i = ps + (threadIdx.x & 127); i < pend; i += 128) {
         const int y = t_y_vec[i];
         const float s = (y == a.dt.yn - 1) ? syxz : sxz;
         const int o = 2 * (y - y0);
@@ -189,8 +208,8 @@ __global__ void __launch_bounds__(128) tree_mean_kernel(TreeLevelArgs a, const u
             for (int q = 0; q < 4; ++q)
 #pragma unroll
                 for (int d = 0; d < 2; ++d)
-                    if (o + d < cy1 - cy0 && sk[q][o + d] == kind)
-                        acc = VT<T>::add(VT<T>::div(VT<T>::mul(T(s), sv[q][o + d]), T(8)), acc);
+                    if (o + d < cy1 - cy0 && sk[pr][q][o + d] == kind)
+                        acc = VT<T>::add(VT<T>::mul(VT<T>::mul(T(s), sv[pr][q][o + d]), eighth), acc);
         tree[i] = acc;
     }
 }
@@ -198,8 +217,6 @@ __global__ void __launch_bounds__(128) tree_mean_kernel(TreeLevelArgs a, const u
 // ---------------------------------------------------------------------------
 // convolution of one level
 // ---------------------------------------------------------------------------
-constexpr int kConvK = 4;  // output particles per lane and pass
-
 struct ConvLevelArgs {
     LD d;                 // level dims
     LD dp;                // parent level dims
@@ -350,15 +367,21 @@ __global__ void __launch_bounds__(256) conv_gather_kernel(ConvLevelArgs a, const
                 T stv[S * S];
 #pragma unroll
                 for (int t = 0; t < S * S; ++t) stv[t] = st[iz * S * S + t];
-                const T *plane = D + (uint64_t)(z + iz - R) * a.d.xn * (uint64_t)yn;
+                // each particle's tap pointers step by one row per ix; the
+                // y taps are immediate offsets from them
+                const T *row0 = D + ((uint64_t)(z + iz - R) * a.d.xn + (uint64_t)(x - R)) * (uint64_t)yn - R;
+                const T *p[kConvK];
+#pragma unroll
+                for (int j = 0; j < kConvK; ++j) p[j] = row0 + yv[j];
 #pragma unroll
                 for (int ix = 0; ix < S; ++ix) {
-                    const T *rp = plane + (uint64_t)(x + ix - R) * yn - R;
 #pragma unroll
                     for (int iy = 0; iy < S; ++iy)
 #pragma unroll
                         for (int j = 0; j < kConvK; ++j)
-                            acc[j] = VT<T>::add(acc[j], VT<T>::mul(__ldg(rp + yv[j] + iy), stv[ix * S + iy]));
+                            acc[j] = VT<T>::add(acc[j], VT<T>::mul(__ldg(p[j] + iy), stv[ix * S + iy]));
+#pragma unroll
+                    for (int j = 0; j < kConvK; ++j) p[j] += yn;
                 }
             }
         }
@@ -472,10 +495,10 @@ void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, 
             ta.c_cidx = cbase + fi.apr_off[l];
             ta.ct_cidx = (l <= tg.l_max) ? cbase + fi.tree_off[l] : nullptr;
             const uint64_t rows = (uint64_t)ta.dt.xn * ta.dt.zn;
-            const unsigned ych = (unsigned)((ta.dt.yn + kTW - 1) / kTW);
+            const unsigned ych = (unsigned)((ta.dt.yn + tree_tw<T>() - 1) / tree_tw<T>());
             if (rows == 0 || ych == 0) continue;
-            dim3 grid((unsigned)rows, ych);
-            tree_mean_kernel<T><<<grid, 128, 0, s>>>(ta, xz_end, y_vec, in, t_xz_end, t_y_vec, tree);
+            dim3 grid((unsigned)((rows + kTR - 1) / kTR), ych);
+            tree_mean_kernel<T><<<grid, 128 * kTR, 0, s>>>(ta, rows, xz_end, y_vec, in, t_xz_end, t_y_vec, tree);
             count_launch();
         }
     }
