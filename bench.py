@@ -627,6 +627,31 @@ def main():
                              "frac": ab / (cms / 1e3) / 1e9 / hbm, "algorithmic_bytes": ab},
                 "gflops": flops / (cms / 1e3) / 1e9, "stages_ms": cstages}
         del pf, outp
+        # piecewise-constant reconstruction of the volume from its particles
+        # (reconstruct_constant): writes every pixel once
+        rimg = torch.empty(N, dtype=torch.int16, device="cuda")
+
+        def run_recon():
+            _lib.check(L.aprb_reconstruct_constant_u16_device(last, C.c_void_p(parts.data_ptr()),
+                                                              C.c_void_p(rimg.data_ptr()), sptr))
+
+        for _ in range(2):
+            run_recon()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = max(2, args.steps)
+        e0.record(stream)
+        for _ in range(reps):
+            run_recon()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        rms = e0.elapsed_time(e1) / reps
+        ab = 2 * N + 4 * P
+        conv_res["reconstruct_constant"] = {
+            "value": N / (rms / 1e3) / 1e9, "unit": "GVox/s", "ms": rms,
+            "roofline": {"bound": "hbm", "achieved": ab / (rms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": ab / (rms / 1e3) / 1e9 / hbm, "algorithmic_bytes": ab}}
+        del rimg
     L.aprb_apr_free(last)
 
     # the batch and deconvolution workloads are single-GPU measurements

@@ -174,6 +174,20 @@ aprb_status aprb_sample_image_by_block_device(const aprb_apr *a, const uint16_t 
 aprb_status aprb_sample_image_noalloc(const uint64_t *xz_end_dev, const uint16_t *y_vec_dev, int y_num, int x_num,
                                       int z_num, const uint16_t *img_dev, uint16_t *parts_dev, void *stream);
 
+/* --- reconstruction: APRReconstruction::reconstruct_constant
+ * (APRReconstruction.hpp:80-123) and reconstruct_level (:132-170) ----------------
+ * The full-resolution image (y fastest, org dims) in which every pixel takes
+ * the value (or the level) of the particle whose cell covers it.  parts holds
+ * P values in linear order; img holds y*x*z values. */
+aprb_status aprb_reconstruct_constant_u16(const aprb_apr *a, const uint16_t *parts, uint16_t *img);
+aprb_status aprb_reconstruct_constant_f32(const aprb_apr *a, const float *parts, float *img);
+aprb_status aprb_reconstruct_level(const aprb_apr *a, uint8_t *img);
+aprb_status aprb_reconstruct_constant_u16_device(const aprb_apr *a, const uint16_t *parts_dev, uint16_t *img_dev,
+                                                 void *stream);
+aprb_status aprb_reconstruct_constant_f32_device(const aprb_apr *a, const float *parts_dev, float *img_dev,
+                                                 void *stream);
+aprb_status aprb_reconstruct_level_device(const aprb_apr *a, uint8_t *img_dev, void *stream);
+
 /* --- APR tree: APR::initialize_tree_dense (APR.hpp:633-689) ---------------------- */
 aprb_status aprb_apr_init_tree(aprb_apr *a);
 aprb_status aprb_apr_export_tree(aprb_apr *a, uint64_t *level_xz, uint64_t *xz_end, uint16_t *y_vec);

@@ -308,6 +308,35 @@ class ParticleData:
         return self
 
 
+class APRReconstruction:
+    """Piecewise-constant and level images of an APR at full resolution
+    (APRReconstruction::reconstruct_constant / reconstruct_level,
+    src/numerics/APRReconstruction.hpp:80, 132)."""
+
+    @staticmethod
+    def reconstruct_constant(apr, particle_data):
+        """(z, x, y) image of the particles' values; uint16 or float32 like the
+        particle data."""
+        parts = getattr(particle_data, "data", particle_data)
+        if hasattr(parts, "data_ptr"):
+            raise TypeError("use the device entry points for CUDA tensors")
+        kind = np.float32 if np.asarray(parts).dtype.kind == "f" else np.uint16
+        p = np.ascontiguousarray(parts, kind)
+        z, x, y = apr.org_dims(2), apr.org_dims(1), apr.org_dims(0)
+        img = np.empty((z, x, y), kind)
+        fn = lib().aprb_reconstruct_constant_f32 if kind is np.float32 else lib().aprb_reconstruct_constant_u16
+        check(fn(apr._h, _ptr(p) if p.size else None, _ptr(img)))
+        return img
+
+    @staticmethod
+    def reconstruct_level(apr):
+        """(z, x, y) uint8 image of the particles' levels."""
+        z, x, y = apr.org_dims(2), apr.org_dims(1), apr.org_dims(0)
+        img = np.empty((z, x, y), np.uint8)
+        check(lib().aprb_reconstruct_level(apr._h, _ptr(img)))
+        return img
+
+
 class APRTreeNumerics:
     @staticmethod
     def fill_tree_mean(apr, particle_data, tree_data=None):

@@ -86,6 +86,12 @@ SIGNATURES = {
     "aprb_synth_blobs_u16": ([_vp, _i, _i, _i, _i, _f, _f, _f, _f, _f, _u64, _vp], _i),
     "aprb_synth_blobs_f32": ([_vp, _i, _i, _i, _i, _f, _f, _f, _f, _f, _u64, _vp], _i),
     "aprb_kernel_launch_count": ([], _u64),
+    "aprb_reconstruct_constant_u16": ([_vp, _vp, _vp], _i),
+    "aprb_reconstruct_constant_f32": ([_vp, _vp, _vp], _i),
+    "aprb_reconstruct_level": ([_vp, _vp], _i),
+    "aprb_reconstruct_constant_u16_device": ([_vp, _vp, _vp, _vp], _i),
+    "aprb_reconstruct_constant_f32_device": ([_vp, _vp, _vp, _vp], _i),
+    "aprb_reconstruct_level_device": ([_vp, _vp, _vp], _i),
     "aprb_check_division_by_constant": ([C.c_float, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)], _i),
     "aprb_profile_enable": ([_i], _i),
     "aprb_profile_reset": ([], _i),

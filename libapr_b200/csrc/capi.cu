@@ -188,6 +188,31 @@ struct aprb_converter {
     bool have = false;
 };
 
+// reconstruct_constant / reconstruct_level on device buffers
+template <typename V>
+static void reconstruct_device(const aprb_apr *a, const V *parts_dev, V *img_dev, bool level, cudaStream_t s) {
+    launch_reconstruct<V>(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, parts_dev, img_dev, level,
+                          s);
+}
+
+// the same from and to host buffers (the volume's worth of pixels is copied
+// back in one piece)
+template <typename V>
+static void reconstruct_host(const aprb_apr *a, const V *parts, V *img, bool level) {
+    cudaStream_t s = cudaStreamPerThread;
+    const uint64_t n = (uint64_t)a->org[0] * a->org[1] * a->org[2];
+    V *dimg = (V *)scratch().out_f.get(n * sizeof(V) ? n * sizeof(V) : 16);
+    const V *dparts = nullptr;
+    if (!level) {
+        V *dp = (V *)scratch().parts_f.get(a->P ? a->P * sizeof(V) : 16);
+        if (a->P) APRB_CUDA(cudaMemcpyAsync(dp, parts, a->P * sizeof(V), cudaMemcpyHostToDevice, s));
+        dparts = dp;
+    }
+    reconstruct_device<V>(a, dparts, dimg, level, s);
+    APRB_CUDA(cudaMemcpyAsync(img, dimg, n * sizeof(V), cudaMemcpyDeviceToHost, s));
+    APRB_CUDA(cudaStreamSynchronize(s));
+}
+
 extern "C" {
 
 const char *aprb_status_string(aprb_status s) {
@@ -749,6 +774,51 @@ aprb_status aprb_apr_from_arrays(int y_num, int x_num, int z_num, const uint64_t
             APRB_CUDA(cudaMemcpy(yv, y_vec, n_particles * sizeof(uint16_t), cudaMemcpyHostToDevice));
         }
         *out = a.release();
+    });
+}
+
+aprb_status aprb_reconstruct_constant_u16(const aprb_apr *a, const uint16_t *parts, uint16_t *img) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && img && (parts || a->P == 0), "null argument");
+        reconstruct_host<uint16_t>(a, parts, img, false);
+    });
+}
+aprb_status aprb_reconstruct_constant_f32(const aprb_apr *a, const float *parts, float *img) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && img && (parts || a->P == 0), "null argument");
+        reconstruct_host<float>(a, parts, img, false);
+    });
+}
+aprb_status aprb_reconstruct_level(const aprb_apr *a, uint8_t *img) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && img, "null argument");
+        reconstruct_host<uint8_t>(a, nullptr, img, true);
+    });
+}
+aprb_status aprb_reconstruct_constant_u16_device(const aprb_apr *a, const uint16_t *parts_dev, uint16_t *img_dev,
+                                                 void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && img_dev && (parts_dev || a->P == 0), "null argument");
+        reconstruct_device<uint16_t>(a, parts_dev, img_dev, false, (cudaStream_t)stream);
+    });
+}
+aprb_status aprb_reconstruct_constant_f32_device(const aprb_apr *a, const float *parts_dev, float *img_dev,
+                                                 void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && img_dev && (parts_dev || a->P == 0), "null argument");
+        reconstruct_device<float>(a, parts_dev, img_dev, false, (cudaStream_t)stream);
+    });
+}
+aprb_status aprb_reconstruct_level_device(const aprb_apr *a, uint8_t *img_dev, void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && img_dev, "null argument");
+        reconstruct_device<uint8_t>(a, nullptr, img_dev, true, (cudaStream_t)stream);
     });
 }
 

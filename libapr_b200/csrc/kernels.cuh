@@ -77,6 +77,11 @@ void inclusive_scan_u64(uint64_t *data, uint64_t n, DevBuf &tmp, cudaStream_t s)
 void launch_sample(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const uint16_t *img,
                    uint16_t *parts, DevBuf &pyr, cudaStream_t s);
 
+// piecewise-constant (or level) image of an APR at full resolution
+template <typename V>
+void launch_reconstruct(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const V *parts, V *img,
+                        bool level, cudaStream_t s);
+
 // pieces of sampling for a host-buffer call that pipelines its transfers
 uint16_t *sample_pyramid(const Geom &g, DevBuf &pyr, uint64_t off[32]);
 void launch_sample_slab(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const uint16_t *img, int z0,

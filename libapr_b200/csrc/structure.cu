@@ -412,6 +412,41 @@ __global__ void row_fill_top_kernel(const uint8_t *__restrict__ st, LevelDims d,
     }
 }
 
+// ---------------------------------------------------------------------------
+// APRReconstruction::reconstruct_constant / reconstruct_level
+// (APRReconstruction.hpp:80-123, 132-170): every full-resolution pixel takes
+// the value, or the level, of the particle whose cell covers it.  A warp per
+// pixel row (z, x) walks the covering row (z >> d, x >> d) of every level
+// l = l_max - d; a particle of level l fills its 2^d samples of the row,
+// clipped at the image edge.  The particle cells partition the image, so
+// every pixel is written once.
+// ---------------------------------------------------------------------------
+template <typename V, bool LEVEL>
+__global__ void reconstruct_kernel(Geom g, const uint64_t *__restrict__ xz_end, const uint16_t *__restrict__ y_vec,
+                                   const V *__restrict__ parts, V *__restrict__ img) {
+    const int L = g.l_max;
+    const int yn = g.y_num[L], xn = g.x_num[L];
+    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= (uint64_t)xn * g.z_num[L]) return;
+    const int x = (int)(row % (uint64_t)xn), z = (int)(row / (uint64_t)xn);
+    V *R = img + row * (uint64_t)yn;
+    for (int l = L; l >= g.l_min; --l) {
+        const int d = L - l;
+        const uint64_t r = (uint64_t)(z >> d) * g.x_num[l] + (x >> d);
+        const uint64_t b = xz_end[g.level_xz[l] + r - 1], e = xz_end[g.level_xz[l] + r];
+        if (d == 0) {
+            for (uint64_t i = b + lane; i < e; i += 32) R[y_vec[i]] = LEVEL ? (V)l : parts[i];
+        } else {
+            for (uint64_t i = b + lane; i < e; i += 32) {
+                const int y0 = (int)y_vec[i] << d, y1 = min(y0 + (1 << d), yn);
+                const V v = LEVEL ? (V)l : parts[i];
+                for (int y = y0; y < y1; ++y) R[y] = v;
+            }
+        }
+    }
+}
+
 // l_max <= 2: every pixel is a particle (LinearAccess.hpp:226-259)
 __global__ void full_res_counts_kernel(uint64_t *xz_end, uint64_t base, int yn, uint64_t rows) {
     const uint64_t r = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -627,6 +662,28 @@ uint64_t nrow(const Geom &g, int l) { return (uint64_t)g.x_num[l] * g.z_num[l]; 
 unsigned row_blocks(uint64_t rows) { return blocks_for(rows * 32, 256); }
 
 }  // namespace
+
+template <typename V>
+void launch_reconstruct(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const V *parts, V *img,
+                        bool level, cudaStream_t s) {
+    APRB_PROF("reconstruct", s);
+    const uint64_t rows = nrow(g, g.l_max);
+    if (!rows) return;
+    if (level)
+        reconstruct_kernel<V, true><<<row_blocks(rows), 256, 0, s>>>(g, xz_end, y_vec, parts, img);
+    else
+        reconstruct_kernel<V, false><<<row_blocks(rows), 256, 0, s>>>(g, xz_end, y_vec, parts, img);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+}
+template void launch_reconstruct<uint16_t>(const Geom &, const uint64_t *, const uint16_t *, const uint16_t *,
+                                           uint16_t *, bool, cudaStream_t);
+template void launch_reconstruct<float>(const Geom &, const uint64_t *, const uint16_t *, const float *, float *, bool,
+                                        cudaStream_t);
+template void launch_reconstruct<uint8_t>(const Geom &, const uint64_t *, const uint16_t *, const uint8_t *,
+                                          uint8_t *, bool, cudaStream_t);
+
+
 
 void inclusive_scan_u64(uint64_t *data, uint64_t n, DevBuf &tmp, cudaStream_t s) {
     const uint64_t nb = (n + kScanBlock - 1) / kScanBlock;

@@ -255,6 +255,36 @@ def orc_sample(acc, img):
     return out
 
 
+def orc_reconstruct(acc, parts=None):
+    """APRReconstruction::reconstruct_constant (parts given) or
+    reconstruct_level (src/numerics/APRReconstruction.hpp:80-123, 132-170)
+    restated in numpy: every full-resolution pixel takes the value (or the
+    level) of the particle whose cell covers it; a particle of level l covers
+    2^(l_max - l) samples per axis, clipped at the image edge.  Returns a
+    (z, x, y) array: the parts' dtype, or uint8 levels."""
+    L = acc.l_max
+    Y, X, Z = acc.y_num[L], acc.x_num[L], acc.z_num[L]
+    lev, zz, xx, yy = acc.particle_coords()
+    vals = lev.astype(np.uint8) if parts is None else np.asarray(parts)
+    out = np.empty((Z, X, Y), vals.dtype)
+    for l in range(acc.l_min, L + 1):
+        m = np.nonzero(lev == l)[0]
+        if not len(m):
+            continue
+        st = 1 << (L - l)
+        if st <= 8:
+            for dz in range(st):
+                for dx in range(st):
+                    for dy in range(st):
+                        z, x, y = zz[m] * st + dz, xx[m] * st + dx, yy[m] * st + dy
+                        ok = (z < Z) & (x < X) & (y < Y)
+                        out[z[ok], x[ok], y[ok]] = vals[m[ok]]
+        else:
+            for i in m:
+                out[zz[i] * st:(zz[i] + 1) * st, xx[i] * st:(xx[i] + 1) * st, yy[i] * st:(yy[i] + 1) * st] = vals[i]
+    return out
+
+
 def orc_tree(acc):
     L = lib()
     t = OrcAccess()

@@ -55,6 +55,18 @@ def test_structure_from_saved_grad_scale(golden_dir, case):
         assert np.array_equal(ref.astype(np.int64), val[ok].astype(np.int64)), name
 
 
+@pytest.mark.parametrize("case", CASES)
+def test_reconstruction_matches_saved_images(golden_dir, case):
+    """reconstruct_level and reconstruct_constant of the stored APR are the
+    reference's per-pixel level and piecewise-constant images
+    (APRReconstruction.hpp:80, 132; the fixtures of test/APRTest.cpp:2600-2665)."""
+    d = load(golden_dir, case)
+    img = d["original"]
+    acc = B.orc_get_apr_custom(d["gradient_saved"].astype(np.float32), d["scale_saved"], img.shape, case_params(d))
+    assert np.array_equal(B.orc_reconstruct(acc).astype(np.uint16), d["img_level"])
+    assert np.array_equal(B.orc_reconstruct(acc, B.orc_sample(acc, img)), d["img_pc"])
+
+
 ref_missing = pytest.mark.skipif(not B.ref_available(), reason="oracle/_ref not built (needs the LibAPR tree)")
 
 
