@@ -208,6 +208,33 @@ inline void richardson_lucy(APR &apr, ParticleData<uint16_t> &in, ParticleData<f
 }
 }  // namespace APRNumerics
 
+namespace APRReconstruction {
+/* reconstruct_constant (APRReconstruction.hpp:80-123): uint16 or float values */
+template <typename U, typename S>
+inline void reconstruct_constant(APR &apr, PixelData<U> &img, const ParticleData<S> &parts) {
+    img.init((int)apr.org_dims(0), (int)apr.org_dims(1), (int)apr.org_dims(2));
+    if (std::is_floating_point<U>::value) {
+        std::vector<float> p(parts.data.begin(), parts.data.end());
+        std::vector<float> out(img.mesh.size());
+        check(aprb_reconstruct_constant_f32(apr.handle(), p.data(), out.data()));
+        img.mesh.assign(out.begin(), out.end());
+    } else {
+        std::vector<uint16_t> p(parts.data.begin(), parts.data.end());
+        std::vector<uint16_t> out(img.mesh.size());
+        check(aprb_reconstruct_constant_u16(apr.handle(), p.data(), out.data()));
+        img.mesh.assign(out.begin(), out.end());
+    }
+}
+/* reconstruct_level (APRReconstruction.hpp:132-170) */
+template <typename U>
+inline void reconstruct_level(APR &apr, PixelData<U> &img) {
+    img.init((int)apr.org_dims(0), (int)apr.org_dims(1), (int)apr.org_dims(2));
+    std::vector<uint8_t> out(img.mesh.size());
+    check(aprb_reconstruct_level(apr.handle(), out.data()));
+    img.mesh.assign(out.begin(), out.end());
+}
+}  // namespace APRReconstruction
+
 }  // namespace compat
 }  // namespace aprb200
 

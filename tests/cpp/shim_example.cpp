@@ -1,6 +1,7 @@
 // Drop-in use of the C++ host layer (include/aprb200.hpp): the calls below
 // have the shape of LibAPR code (Example_get_apr.cpp / Example_apr_filter.cpp).
-// Prints "P=<particles> sum=<sum of intensities> conv=<sum of conv output>".
+// Prints "P=<particles> sum=<sum of intensities> conv=<sum of conv output>
+// recon=<sum of the piecewise-constant image> levels=<sum of the level image>".
 #include <cstdio>
 #include <cstdlib>
 
@@ -35,6 +36,14 @@ int main(int argc, char **argv) {
     APRFilter::convolve_pencil(apr, st, in, out, true, true, false);
     double cs = 0;
     for (float v : out.data) cs += v;
-    std::printf("P=%llu sum=%llu conv=%.6f\n", (unsigned long long)apr.total_number_particles(), sum, cs);
+    PixelData<uint16_t> pc;
+    APRReconstruction::reconstruct_constant(apr, pc, parts);
+    PixelData<uint8_t> lv;
+    APRReconstruction::reconstruct_level(apr, lv);
+    unsigned long long rs = 0, ls = 0;
+    for (uint16_t v : pc.mesh) rs += v;
+    for (uint8_t v : lv.mesh) ls += v;
+    std::printf("P=%llu sum=%llu conv=%.6f recon=%llu levels=%llu\n", (unsigned long long)apr.total_number_particles(),
+                sum, cs, rs, ls);
     return 0;
 }

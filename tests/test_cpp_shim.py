@@ -38,7 +38,9 @@ def test_cpp_shim_matches_python_path(tmp_path):
     assert conv.get_apr(apr, img)
     parts = A.ParticleData().sample_image(apr, img).data
     c = A.APRFilter.convolve_pencil(apr, np.full(27, 1.0 / 27, np.float32), parts.astype(np.float32))
-    P, s, cs = out.split()
+    P, s, cs, rs, ls = out.split()
+    assert int(rs.split("=")[1]) == int(A.APRReconstruction.reconstruct_constant(apr, parts).astype(np.uint64).sum())
+    assert int(ls.split("=")[1]) == int(A.APRReconstruction.reconstruct_level(apr).astype(np.uint64).sum())
     assert int(P.split("=")[1]) == apr.total_number_particles()
     assert int(s.split("=")[1]) == int(parts.astype(np.uint64).sum())
     assert abs(float(cs.split("=")[1]) - float(c.astype(np.float64).sum())) <= 1e-3 * max(1.0, abs(float(c.sum())))
