@@ -206,6 +206,17 @@ aprb_status aprb_convolve(aprb_apr *a, const float *stencil, int ksize, const fl
 aprb_status aprb_convolve_device(aprb_apr *a, const float *stencil, int ksize, const float *in_dev, float *out_dev,
                                  int reflect, int use_stencil_downsample, int normalize, void *stream);
 
+/* --- APR gradients: APRNumerics::gradient_cfd / gradient_sobel of one
+ * dimension (0 y, 1 x, 2 z; APRNumerics.hpp:165-215) and
+ * gradient_magnitude_cfd / _sobel (:218-287) with grid spacings deltas[3]
+ * (y, x, z).  in and out hold P floats in linear order. */
+aprb_status aprb_gradient(aprb_apr *a, const float *in, float *out, int dimension, float delta, int sobel);
+aprb_status aprb_gradient_device(aprb_apr *a, const float *in_dev, float *out_dev, int dimension, float delta,
+                                 int sobel, void *stream);
+aprb_status aprb_gradient_magnitude(aprb_apr *a, const float *in, float *out, const float *deltas, int sobel);
+aprb_status aprb_gradient_magnitude_device(aprb_apr *a, const float *in_dev, float *out_dev, const float *deltas,
+                                           int sobel, void *stream);
+
 /* --- APR Richardson-Lucy --------------------------------------------------------
  * APRNumerics::richardson_lucy (APRNumerics.hpp:576-593) /
  * APRNumericsGPU::richardson_lucy (APRNumericsGPU.hpp:105-108).  psf: ksize^3

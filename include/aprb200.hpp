@@ -206,6 +206,36 @@ inline void richardson_lucy(APR &apr, ParticleData<uint16_t> &in, ParticleData<f
     check(aprb_richardson_lucy(apr.handle(), in.data.data(), out.data.data(), st.data(), psf.y_num, number_iterations,
                                use_stencil_downsample, normalize, resume));
 }
+/* gradient_cfd / gradient_sobel (APRNumerics.hpp:165-215), float particles */
+template <typename In>
+inline void gradient_cfd(APR &apr, const ParticleData<In> &in, ParticleData<float> &out, int dimension,
+                         float delta = 1.0f) {
+    std::vector<float> x(in.data.begin(), in.data.end());
+    out.init(x.size());
+    check(aprb_gradient(apr.handle(), x.data(), out.data.data(), dimension, delta, 0));
+}
+template <typename In>
+inline void gradient_sobel(APR &apr, const ParticleData<In> &in, ParticleData<float> &out, int dimension,
+                           float delta = 1.0f) {
+    std::vector<float> x(in.data.begin(), in.data.end());
+    out.init(x.size());
+    check(aprb_gradient(apr.handle(), x.data(), out.data.data(), dimension, delta, 1));
+}
+/* gradient_magnitude_cfd / _sobel (APRNumerics.hpp:218-287) */
+template <typename In>
+inline void gradient_magnitude_cfd(APR &apr, const ParticleData<In> &in, ParticleData<float> &out,
+                                   const std::vector<float> &deltas = {1.0f, 1.0f, 1.0f}) {
+    std::vector<float> x(in.data.begin(), in.data.end());
+    out.init(x.size());
+    check(aprb_gradient_magnitude(apr.handle(), x.data(), out.data.data(), deltas.data(), 0));
+}
+template <typename In>
+inline void gradient_magnitude_sobel(APR &apr, const ParticleData<In> &in, ParticleData<float> &out,
+                                     const std::vector<float> &deltas = {1.0f, 1.0f, 1.0f}) {
+    std::vector<float> x(in.data.begin(), in.data.end());
+    out.init(x.size());
+    check(aprb_gradient_magnitude(apr.handle(), x.data(), out.data.data(), deltas.data(), 1));
+}
 }  // namespace APRNumerics
 
 namespace APRReconstruction {

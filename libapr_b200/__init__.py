@@ -393,6 +393,43 @@ def isotropic_convolve_555(apr, particle_input, stencil, reflective_bc=True, use
 
 class APRNumerics:
     @staticmethod
+    def gradient_cfd(apr, particle_input, dimension, delta=1.0):
+        """APRNumerics::gradient_cfd (APRNumerics.hpp:165-184): central
+        difference along dimension 0 (y), 1 (x) or 2 (z); float32 particles."""
+        return APRNumerics._gradient(apr, particle_input, dimension, delta, 0)
+
+    @staticmethod
+    def gradient_sobel(apr, particle_input, dimension, delta=1.0):
+        """APRNumerics::gradient_sobel (APRNumerics.hpp:187-215)."""
+        return APRNumerics._gradient(apr, particle_input, dimension, delta, 1)
+
+    @staticmethod
+    def gradient_magnitude_cfd(apr, particle_input, deltas=(1.0, 1.0, 1.0)):
+        """APRNumerics::gradient_magnitude_cfd (APRNumerics.hpp:218-251)."""
+        return APRNumerics._magnitude(apr, particle_input, deltas, 0)
+
+    @staticmethod
+    def gradient_magnitude_sobel(apr, particle_input, deltas=(1.0, 1.0, 1.0)):
+        """APRNumerics::gradient_magnitude_sobel (APRNumerics.hpp:254-287)."""
+        return APRNumerics._magnitude(apr, particle_input, deltas, 1)
+
+    @staticmethod
+    def _gradient(apr, particle_input, dimension, delta, sobel):
+        x = np.ascontiguousarray(getattr(particle_input, "data", particle_input), np.float32)
+        out = np.zeros(max(x.size, 1), np.float32)
+        check(lib().aprb_gradient(apr._h, _ptr(x) if x.size else None, _ptr(out), int(dimension), float(delta),
+                                  int(sobel)))
+        return out[: x.size]
+
+    @staticmethod
+    def _magnitude(apr, particle_input, deltas, sobel):
+        x = np.ascontiguousarray(getattr(particle_input, "data", particle_input), np.float32)
+        out = np.zeros(max(x.size, 1), np.float32)
+        d = np.ascontiguousarray(deltas, np.float32)
+        check(lib().aprb_gradient_magnitude(apr._h, _ptr(x) if x.size else None, _ptr(out), _ptr(d), int(sobel)))
+        return out[: x.size]
+
+    @staticmethod
     def richardson_lucy(apr, particle_input, particle_output, psf, number_iterations, use_stencil_downsample=True,
                         normalize=False, resume=False, dtype=np.float32):
         """APRNumerics::richardson_lucy (APRNumerics.hpp:132-134, 551-593).

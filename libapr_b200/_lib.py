@@ -86,6 +86,10 @@ SIGNATURES = {
     "aprb_synth_blobs_u16": ([_vp, _i, _i, _i, _i, _f, _f, _f, _f, _f, _u64, _vp], _i),
     "aprb_synth_blobs_f32": ([_vp, _i, _i, _i, _i, _f, _f, _f, _f, _f, _u64, _vp], _i),
     "aprb_kernel_launch_count": ([], _u64),
+    "aprb_gradient": ([_vp, _vp, _vp, _i, _f, _i], _i),
+    "aprb_gradient_device": ([_vp, _vp, _vp, _i, _f, _i, _vp], _i),
+    "aprb_gradient_magnitude": ([_vp, _vp, _vp, _vp, _i], _i),
+    "aprb_gradient_magnitude_device": ([_vp, _vp, _vp, _vp, _i, _vp], _i),
     "aprb_reconstruct_constant_u16": ([_vp, _vp, _vp], _i),
     "aprb_reconstruct_constant_f32": ([_vp, _vp, _vp], _i),
     "aprb_reconstruct_level": ([_vp, _vp], _i),

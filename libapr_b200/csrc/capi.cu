@@ -995,6 +995,100 @@ void convolve_impl(aprb_apr *a, const float *stencil, int ks, const float *in, f
     a->last_stale = filter_stale_count(scratch().fb, s);
 }
 
+// ---------------------------------------------------------------------------
+// APRNumerics::gradient_cfd / gradient_sobel (APRNumerics.hpp:165-215) and the
+// gradient magnitudes (:218-287).  The reference convolves with a 3x1x1
+// central difference (cfd), a 3x3x3 Sobel stencil (3-D data) or a 3x3x1 one
+// (2-D data), rescaled by 1/2^d for level delta d (APRStencil.hpp:135-152,
+// 254-299).  Here the 1-D and 2-D shapes sit in the middle of a 3x3x3 cube
+// with zero taps around them, which add nothing to the tap sums, so the
+// cubic convolution reproduces the reference's values bit for bit.
+// ---------------------------------------------------------------------------
+static std::vector<float> gradient_stencils(const aprb_apr *a, int dim, int sobel, float delta, int nlev) {
+    const int nd = (a->org[0] > 1) + (a->org[1] > 1) + (a->org[2] > 1);
+    const float two_d = 2.0f * delta;
+    const float diff[3] = {-1.0f / two_d, 0.0f, 1.0f / two_d};
+    const float smooth[3] = {0.25f, 0.5f, 0.25f};
+    float base[27] = {};  // [z][x][y]
+    if (sobel && nd == 3) {
+        const float *bank[3] = {dim == 0 ? diff : smooth, dim == 1 ? diff : smooth, dim == 2 ? diff : smooth};
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                for (int k = 0; k < 3; ++k) base[(k * 3 + j) * 3 + i] = bank[0][i] * bank[1][j] * bank[2][k];
+    } else if (sobel && nd == 2 && dim != 2) {
+        const float *bank[2] = {dim == 0 ? diff : smooth, dim == 1 ? diff : smooth};
+        for (int j = 0; j < 3; ++j)
+            for (int i = 0; i < 3; ++i) base[(1 * 3 + j) * 3 + i] = bank[0][i] * bank[1][j];
+    } else {
+        for (int t = 0; t < 3; ++t) {
+            int idx[3] = {1, 1, 1};  // z, x, y
+            idx[2 - dim] = t;
+            base[(idx[0] * 3 + idx[1]) * 3 + idx[2]] = diff[t];
+        }
+    }
+    std::vector<float> out;
+    for (int d = 0; d < nlev; ++d) {
+        const float step = (float)std::pow(2.0, (double)d);
+        for (int k = 0; k < 27; ++k) out.push_back(base[k] / step);
+    }
+    return out;
+}
+
+__global__ void square_kernel(float *o, uint64_t n) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) o[i] = __fmul_rn(o[i], o[i]);
+}
+__global__ void add_square_kernel(float *o, const float *g, uint64_t n) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) o[i] = __fadd_rn(o[i], __fmul_rn(g[i], g[i]));
+}
+__global__ void sqrt_kernel(float *o, uint64_t n) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) o[i] = __fsqrt_rn(o[i]);
+}
+
+// gradient of dimension dim, device buffers
+static void gradient_dim(aprb_apr *a, const float *in, float *out, int dim, int sobel, float delta, cudaStream_t s) {
+    ensure_tree(a, s);
+    const int nlev = std::max(a->g.l_max - a->g.l_min, 1);
+    const std::vector<float> host = gradient_stencils(a, dim, sobel, delta, nlev);
+    ConvPlan plan;
+    plan.nstencils = nlev;
+    for (int d = 0; d < nlev; ++d) {
+        plan.sides.push_back(3);
+        plan.offsets.push_back(27 * d);
+    }
+    plan.reflect = true;
+    float *dst = scratch().stencils.as<float>(host.size());
+    APRB_CUDA(cudaMemcpyAsync(dst, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice, s));
+    float *tree = scratch().tree_vals.as<float>(a->T ? a->T : 1);
+    filter_apply<float>(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
+                        (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, a->fi, in, tree, &plan, dst,
+                        out, 0, nullptr, scratch().fb, s);
+    a->last_stale = filter_stale_count(scratch().fb, s);
+}
+
+// gradient magnitude: y^2, then + x^2 and + z^2 for axes longer than 1, then
+// the square root, in the reference's order
+static void gradient_magnitude(aprb_apr *a, const float *in, float *out, const float *deltas, int sobel,
+                               cudaStream_t s) {
+    const uint64_t P = a->P;
+    const unsigned blocks = blocks_for(P, 256);
+    gradient_dim(a, in, out, 0, sobel, deltas[0], s);
+    if (P) square_kernel<<<blocks, 256, 0, s>>>(out, P);
+    count_launch();
+    float *tmp = (float *)scratch().rb.get((P ? P : 1) * sizeof(float));
+    for (int d = 1; d < 3; ++d) {
+        if (a->org[d] <= 1) continue;
+        gradient_dim(a, in, tmp, d, sobel, deltas[d], s);
+        if (P) add_square_kernel<<<blocks, 256, 0, s>>>(out, tmp, P);
+        count_launch();
+    }
+    if (P) sqrt_kernel<<<blocks, 256, 0, s>>>(out, P);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+}
+
 template <typename T>
 __global__ void fill_kernel(T *p, uint64_t n, T v) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1096,6 +1190,54 @@ aprb_status aprb_convolve_device(aprb_apr *a, const float *stencil, int ksize, c
         ARG_CHECK(a && stencil && in_dev && out_dev, "null argument");
         convolve_impl(a, stencil, ksize, in_dev, out_dev, reflect, use_stencil_downsample, normalize,
                       (cudaStream_t)stream);
+    });
+}
+
+aprb_status aprb_gradient(aprb_apr *a, const float *in, float *out, int dimension, float delta, int sobel) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && out && (in || a->P == 0), "null argument");
+        ARG_CHECK(dimension >= 0 && dimension <= 2, "dimension must be 0 (y), 1 (x) or 2 (z)");
+        cudaStream_t s = cudaStreamPerThread;
+        float *din = scratch().parts_f.as<float>(a->P ? a->P : 1);
+        float *dout = scratch().out_f.as<float>(a->P ? a->P : 1);
+        if (a->P) APRB_CUDA(cudaMemcpyAsync(din, in, a->P * sizeof(float), cudaMemcpyHostToDevice, s));
+        gradient_dim(a, din, dout, dimension, sobel, delta, s);
+        if (a->P) APRB_CUDA(cudaMemcpyAsync(out, dout, a->P * sizeof(float), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+aprb_status aprb_gradient_device(aprb_apr *a, const float *in_dev, float *out_dev, int dimension, float delta,
+                                 int sobel, void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && out_dev && (in_dev || a->P == 0), "null argument");
+        ARG_CHECK(dimension >= 0 && dimension <= 2, "dimension must be 0 (y), 1 (x) or 2 (z)");
+        gradient_dim(a, in_dev, out_dev, dimension, sobel, delta, (cudaStream_t)stream);
+    });
+}
+
+aprb_status aprb_gradient_magnitude(aprb_apr *a, const float *in, float *out, const float *deltas, int sobel) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && out && deltas && (in || a->P == 0), "null argument");
+        cudaStream_t s = cudaStreamPerThread;
+        float *din = scratch().parts_f.as<float>(a->P ? a->P : 1);
+        float *dout = scratch().out_f.as<float>(a->P ? a->P : 1);
+        if (a->P) APRB_CUDA(cudaMemcpyAsync(din, in, a->P * sizeof(float), cudaMemcpyHostToDevice, s));
+        gradient_magnitude(a, din, dout, deltas, sobel, s);
+        if (a->P) APRB_CUDA(cudaMemcpyAsync(out, dout, a->P * sizeof(float), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaStreamSynchronize(s));
+    });
+}
+
+aprb_status aprb_gradient_magnitude_device(aprb_apr *a, const float *in_dev, float *out_dev, const float *deltas,
+                                           int sobel, void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(a && out_dev && deltas && (in_dev || a->P == 0), "null argument");
+        gradient_magnitude(a, in_dev, out_dev, deltas, sobel, (cudaStream_t)stream);
     });
 }
 

@@ -95,6 +95,8 @@ def ref(fast=False):
         R.ref_get_apr.argtypes = [C.POINTER(C.c_uint16), C.c_int, C.c_int, C.c_int, C.POINTER(OrcParams), C.c_int,
                                   C.POINTER(vp)]
         R.ref_get_apr_plain.argtypes = R.ref_get_apr.argtypes
+        R.ref_gradient.argtypes = [vp, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int,
+                                   C.POINTER(C.c_float)]
         R.ref_get_apr_custom.argtypes = [C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int,
                                          C.POINTER(OrcParams), C.POINTER(vp)]
         R.ref_free.argtypes = [vp]
@@ -323,6 +325,74 @@ def orc_convolve(acc, tree, stencil, parts, reflect=True, use_stencil_ds=True, n
     return out, int(stale.value)
 
 
+def gradient_stencils(dim, sobel, delta, ndims, nlev):
+    """Per-level 3x3x3 stencils (flattened, z-major, y fastest) of
+    APRNumerics::gradient_cfd / gradient_sobel (APRNumerics.hpp:165-215):
+    the central difference {-1/(2 delta), 0, 1/(2 delta)} along dim, for Sobel
+    times {0.25, 0.5, 0.25} along the other axes (APRStencil.hpp:254-299),
+    each divided by 2^d for level delta d (rescale_stencil, :135-142).  The
+    3x1x1 / 3x3x1 shapes of the reference sit in the middle of the cube with
+    zeros around them: zero taps add nothing to the tap sums."""
+    f32 = np.float32
+    two_d = f32(2) * f32(delta)
+    diff = [f32(-1.0) / two_d, f32(0.0), f32(1.0) / two_d]
+    smooth = [f32(0.25), f32(0.5), f32(0.25)]
+    base = np.zeros((3, 3, 3), np.float32)  # [z][x][y]
+    if sobel and ndims == 3:
+        bank = [diff if dim == k else smooth for k in range(3)]
+        for i in range(3):
+            for j in range(3):
+                for k in range(3):
+                    base[k, j, i] = f32(f32(bank[0][i] * bank[1][j]) * bank[2][k])
+    elif sobel and ndims == 2 and dim != 2:
+        bank = [diff if dim == k else smooth for k in range(2)]
+        for j in range(3):
+            for i in range(3):
+                base[1, j, i] = f32(bank[0][i] * bank[1][j])
+    else:
+        for t in range(3):
+            idx = [1, 1, 1]
+            idx[2 - dim] = t
+            base[idx[0], idx[1], idx[2]] = diff[t]
+    nlev = max(nlev, 1)
+    st = np.concatenate([(base / f32(2.0 ** d)).astype(np.float32).ravel() for d in range(nlev)])
+    return st, np.full(nlev, 3, np.int32)
+
+
+def orc_convolve_stencils(acc, tree, st, sides, parts, reflect=True):
+    """orc_convolve with explicit per-level stencils (flattened) and sides."""
+    p = np.ascontiguousarray(parts, dtype=np.float32)
+    out = np.zeros(acc.P, np.float32)
+    stale = C.c_uint64()
+    st = np.ascontiguousarray(st, np.float32)
+    sides = np.ascontiguousarray(sides, np.int32)
+    lib().orc_convolve(C.byref(acc.c()), C.byref(tree.c()), _ptr(st, C.c_float), _ptr(sides, C.c_int), len(sides),
+                       _ptr(p, C.c_float), _ptr(out, C.c_float), int(reflect), C.byref(stale))
+    return out, int(stale.value)
+
+
+def orc_gradient(acc, tree, parts, dim=-1, sobel=False, deltas=(1.0, 1.0, 1.0)):
+    """gradient_cfd / _sobel of dimension dim, or the gradient magnitude
+    (dim < 0: y^2, then + x^2 and + z^2 for axes longer than 1, then sqrtf,
+    APRNumerics.hpp:218-287), from the oracle's convolution."""
+    nd = sum(1 for v in acc.org if v > 1)
+    nlev = acc.l_max - acc.l_min
+
+    def grad(d):
+        st, sides = gradient_stencils(d, sobel, deltas[d], nd, nlev)
+        return orc_convolve_stencils(acc, tree, st, sides, parts)[0]
+
+    if dim >= 0:
+        return grad(dim)
+    out = grad(0)
+    out = (out * out).astype(np.float32)
+    for d in (1, 2):
+        if acc.org[d] > 1:
+            g = grad(d)
+            out = (out + (g * g).astype(np.float32)).astype(np.float32)
+    return np.sqrt(out).astype(np.float32)
+
+
 def orc_richardson_lucy(acc, tree, parts_u16, psf, niter, use_stencil_ds=True, normalize=False, use_double=False,
                         init=None):
     p = np.ascontiguousarray(parts_u16, dtype=np.uint16)
@@ -417,6 +487,16 @@ class RefAPR:
         out = np.zeros(len(p), np.float32)
         self.R.ref_convolve_pencil(self.h, _ptr(st, C.c_float), ks, _ptr(p, C.c_float), _ptr(out, C.c_float),
                                    int(reflect), int(use_stencil_ds), int(normalize))
+        return out
+
+    def gradient(self, parts, dim=-1, sobel=False, deltas=(1.0, 1.0, 1.0)):
+        """APRNumerics::gradient_cfd / _sobel of dimension dim, or the
+        gradient magnitude (dim < 0), computed by the reference itself."""
+        p = np.ascontiguousarray(parts, dtype=np.float32)
+        out = np.zeros(p.size, np.float32)
+        dl = np.ascontiguousarray(deltas, dtype=np.float32)
+        self.R.ref_gradient(self.h, _ptr(p, C.c_float), _ptr(out, C.c_float), int(dim), int(sobel),
+                            _ptr(dl, C.c_float))
         return out
 
     def richardson_lucy(self, parts_u16, psf, niter, use_stencil_ds=True, normalize=False, use_double=False,

@@ -347,6 +347,29 @@ int ref_convolve_pencil(void *hv, const float *stencil, int ks, const float *in,
     return 0;
 }
 
+/* APRNumerics::gradient_cfd / gradient_sobel (APRNumerics.hpp:165-215) of
+ * dimension dim, and gradient_magnitude_cfd / _sobel (:218-287) when dim < 0. */
+int ref_gradient(void *hv, const float *in, float *out, int dim, int sobel, const float *deltas) {
+    RefHandle *h = (RefHandle *)hv;
+    ParticleData<float> pin(h->apr.total_number_particles());
+    std::memcpy(pin.data.begin(), in, sizeof(float) * pin.size());
+    ParticleData<float> pout;
+    if (dim < 0) {
+        const std::vector<float> d = {deltas[0], deltas[1], deltas[2]};
+        if (sobel)
+            APRNumerics::gradient_magnitude_sobel(h->apr, pin, pout, d);
+        else
+            APRNumerics::gradient_magnitude_cfd(h->apr, pin, pout, d);
+    } else {
+        if (sobel)
+            APRNumerics::gradient_sobel(h->apr, pin, pout, dim, deltas[dim]);
+        else
+            APRNumerics::gradient_cfd(h->apr, pin, pout, dim, deltas[dim]);
+    }
+    std::memcpy(out, pout.data.begin(), sizeof(float) * pout.size());
+    return 0;
+}
+
 /* APRNumerics::richardson_lucy (APRNumerics.hpp:576-593), FP32 or FP64. */
 int ref_richardson_lucy(void *hv, const uint16_t *in, void *out, const float *psf, int ks, int niter,
                         int use_stencil_ds, int normalize, int resume, int use_double) {

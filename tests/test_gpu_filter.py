@@ -81,3 +81,25 @@ def test_richardson_lucy_fp64_bit_exact(pair):
     out2 = A.APRNumerics.richardson_lucy(apr, parts, po, psf, 2, normalize=True, resume=True)
     ref2 = B.orc_richardson_lucy(acc, tr, parts, psf, 2, normalize=True, use_double=True, init=ref)
     assert np.array_equal(out2.view(np.uint64), ref2.view(np.uint64))
+
+
+@pytest.mark.parametrize("shape", [(40, 48, 56), (1, 63, 64), (17, 33, 70)])
+def test_gradients_match_reference_build(shape):
+    """APR gradients (APRNumerics::gradient_cfd / gradient_sobel and the two
+    magnitudes, APRNumerics.hpp:165-287) equal the reference's own results
+    bit for bit (oracle/_ref, the reference compiled from its headers)."""
+    if not B.ref_available():
+        pytest.skip("oracle/_ref not built")
+    img = volume(shape, 12, 5)
+    conv = A.APRConverter("uint16")
+    conv.par = lib_params()
+    apr = A.APR()
+    assert conv.get_apr(apr, img)
+    _, r = B.ref_get_apr(img, oracle_params(), 1)
+    parts = A.ParticleData().sample_image(apr, img).data.astype(np.float32)
+    deltas = (1.0, 0.5, 2.0)
+    for dim in (0, 1, 2):
+        assert bits_equal(A.APRNumerics.gradient_cfd(apr, parts, dim, deltas[dim]), r.gradient(parts, dim, False, deltas))
+        assert bits_equal(A.APRNumerics.gradient_sobel(apr, parts, dim, deltas[dim]), r.gradient(parts, dim, True, deltas))
+    assert bits_equal(A.APRNumerics.gradient_magnitude_cfd(apr, parts, deltas), r.gradient(parts, -1, False, deltas))
+    assert bits_equal(A.APRNumerics.gradient_magnitude_sobel(apr, parts, deltas), r.gradient(parts, -1, True, deltas))

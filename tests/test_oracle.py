@@ -111,6 +111,25 @@ def test_oracle_filters_match_reference_build():
 
 
 @ref_missing
+@pytest.mark.parametrize("shape", [(40, 48, 56), (1, 63, 64), (17, 33, 70)])
+def test_oracle_gradients_match_reference_build(shape):
+    """APRNumerics::gradient_cfd / gradient_sobel and the two gradient
+    magnitudes (APRNumerics.hpp:165-287), computed by the oracle convolution
+    with the reference's 1-D / 2-D stencils embedded in 3x3x3 cubes, equal the
+    reference's own results bit for bit."""
+    img = volume(shape, 12, 5)
+    e, acc, _ = B.orc_get_apr(img, oracle_params(), 1)
+    _, r = B.ref_get_apr(img, oracle_params(), 1)
+    tr = B.orc_tree(acc)
+    parts = B.orc_sample(acc, img).astype(np.float32)
+    deltas = (1.0, 0.5, 2.0)
+    for sobel in (False, True):
+        for dim in (0, 1, 2):
+            assert bits_equal(B.orc_gradient(acc, tr, parts, dim, sobel, deltas), r.gradient(parts, dim, sobel, deltas))
+        assert bits_equal(B.orc_gradient(acc, tr, parts, -1, sobel, deltas), r.gradient(parts, -1, sobel, deltas))
+
+
+@ref_missing
 def test_overflow_detected_like_reference():
     """test_u16_overflow_detection (test/APRTest.cpp:2850-2867)."""
     img = volume((20, 24, 28), 5, 7)
