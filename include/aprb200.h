@@ -55,6 +55,8 @@ typedef struct {
     int constant_intensity_scale;    /* default 0 */
     int check_input;                 /* default 0 (APRConverter.hpp:86) */
     int swap_dimensions;             /* default 0 */
+    int auto_parameters;             /* default 0 (APRParameters.hpp:32): grad_th and sigma_th
+                                        by autoParametersLiEntropy before applyParameters */
 } aprb_params;
 
 /* ImageType of APRConverter<ImageType> */
@@ -133,9 +135,31 @@ aprb_status aprb_get_apr_batch_device(aprb_converter *c, const aprb_params *p, i
 /* copy one APRB_STAGE_* intermediate of the last get_apr to the host (n = element count) */
 aprb_status aprb_converter_intermediate(const aprb_converter *c, int stage, float *dst, size_t n);
 
+/* --- automatic parameters (AutoParameters.hpp) ----------------------------------
+ * With aprb_params.auto_parameters set, get_apr (APRConverter.hpp:556-561) and each
+ * tile of the blocked converter (APRConverterBatch.hpp:243-247) replace grad_th and
+ * sigma_th by Li's minimum cross entropy thresholds of the gradient and the local
+ * intensity scale before applyParameters; aprb_apr_get_parameters returns them.
+ * Sums are FP64 in a fixed order (the reference sums in FP32 in an order set by its
+ * OpenMP thread count); with no foreground pixel both thresholds are 0 (the
+ * reference divides by zero there); at most 1000 Li steps. */
+
+/* threshold_li<T> (AutoParameters.hpp:50-100) on n host values of T held as float:
+ * integer_values != 0 for T = uint16_t (tolerance 0.5), else T = float. */
+aprb_status aprb_threshold_li(const float *values, uint64_t n, int integer_values, float *threshold);
+/* autoParametersLiEntropy(par, image, localIntensityScale, grad, bspline_offset)
+ * (AutoParameters.hpp:103-153) on n host cells: image = the down-sampled image
+ * (local_scale_temp2), lis = local intensity scale, grad = gradient holding ImageType
+ * values (grad_integer != 0 for uint16_t).  Sets par->grad_th and par->sigma_th. */
+aprb_status aprb_auto_parameters(aprb_params *par, const float *image, const float *lis, const float *grad,
+                                 uint64_t n, int grad_integer, float bspline_offset);
+
 /* --- the APR object ------------------------------------------------------------ */
 aprb_status aprb_apr_free(aprb_apr *a);
 aprb_status aprb_apr_get_info(const aprb_apr *a, aprb_apr_info *info);
+/* APR::get_apr_parameters (APR.hpp:99-101): the parameters the APR was built with,
+ * grad_th / sigma_th as chosen by the automatic parameters when those were on */
+aprb_status aprb_apr_get_parameters(const aprb_apr *a, aprb_params *par);
 /* LinearAccess arrays to host (any pointer may be NULL) */
 aprb_status aprb_apr_export(const aprb_apr *a, uint64_t *level_xz, uint64_t *xz_end, uint16_t *y_vec);
 /* device pointers of the LinearAccess arrays (owned by the APR) */

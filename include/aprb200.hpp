@@ -67,7 +67,18 @@ struct APRParameters {
         p.reflect_bc_lis = reflect_bc_lis; p.neighborhood_optimization = neighborhood_optimization;
         p.constant_intensity_scale = constant_intensity_scale; p.check_input = check_input;
         p.swap_dimensions = swap_dimensions;
+        p.auto_parameters = auto_parameters;
         return p;
+    }
+    static APRParameters from_c(const aprb_params &p) {
+        APRParameters r;
+        r.dx = p.dx; r.dy = p.dy; r.dz = p.dz; r.psfx = p.psfx; r.psfy = p.psfy; r.psfz = p.psfz;
+        r.Ip_th = p.Ip_th; r.lambda = p.lambda; r.rel_error = p.rel_error; r.sigma_th = p.sigma_th;
+        r.sigma_th_max = p.sigma_th_max; r.grad_th = p.grad_th;
+        r.reflect_bc_lis = p.reflect_bc_lis != 0; r.neighborhood_optimization = p.neighborhood_optimization != 0;
+        r.constant_intensity_scale = p.constant_intensity_scale != 0; r.check_input = p.check_input != 0;
+        r.swap_dimensions = p.swap_dimensions != 0; r.auto_parameters = p.auto_parameters != 0;
+        return r;
     }
 };
 
@@ -106,6 +117,12 @@ class APR {
     int level_min() const { return info().l_min; }
     uint64_t total_number_particles() const { return info().total_number_particles; }
     uint64_t org_dims(int d) const { return (uint64_t)info().org_dims[d]; }
+    /* APR::get_apr_parameters (APR.hpp:99-101) */
+    APRParameters get_apr_parameters() const {
+        aprb_params p;
+        check(aprb_apr_get_parameters(h_, &p));
+        return APRParameters::from_c(p);
+    }
     /* LinearAccess arrays (LinearAccess.hpp:33-35) */
     void linear_access(std::vector<uint64_t> &level_xz, std::vector<uint64_t> &xz_end, std::vector<uint16_t> &y_vec) const {
         aprb_apr_info i = info();
@@ -142,6 +159,11 @@ class APRConverter {
         check(s);
         apr.reset(h);
         bspline_offset = apr.info().bspline_offset;
+        if (par.auto_parameters) {  // autoParametersLiEntropy writes the converter's par (APRConverter.hpp:558)
+            const APRParameters used = apr.get_apr_parameters();
+            par.grad_th = used.grad_th;
+            par.sigma_th = used.sigma_th;
+        }
         return true;
     }
 

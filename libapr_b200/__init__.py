@@ -55,16 +55,16 @@ class APRParameters:
 
     _FIELDS = ("dx", "dy", "dz", "psfx", "psfy", "psfz", "Ip_th", "lambda_", "rel_error", "sigma_th",
                "sigma_th_max", "grad_th", "reflect_bc_lis", "neighborhood_optimization", "constant_intensity_scale",
-               "check_input", "swap_dimensions")
+               "check_input", "swap_dimensions", "auto_parameters")
+    _FLAGS = ("reflect_bc_lis", "neighborhood_optimization", "constant_intensity_scale", "check_input",
+              "swap_dimensions", "auto_parameters")
 
     def __init__(self, **kw):
         p = _lib.aprb_params()
         lib().aprb_default_params(C.byref(p))
         for f in self._FIELDS:
             v = getattr(p, f)
-            object.__setattr__(self, f, bool(v) if f in ("reflect_bc_lis", "neighborhood_optimization",
-                                                           "constant_intensity_scale", "check_input",
-                                                           "swap_dimensions") else float(v))
+            object.__setattr__(self, f, bool(v) if f in self._FLAGS else float(v))
         for k, v in kw.items():
             setattr(self, k, v)
 
@@ -85,6 +85,14 @@ class APRParameters:
         for f in self._FIELDS:
             setattr(p, f, getattr(self, f))
         return p
+
+    @classmethod
+    def _from_c(cls, p):
+        par = cls()
+        for f in cls._FIELDS:
+            v = getattr(p, f)
+            object.__setattr__(par, f, bool(v) if f in cls._FLAGS else float(v))
+        return par
 
 
 class APR:
@@ -154,6 +162,13 @@ class APR:
     def bspline_offset(self):
         return float(self.info().bspline_offset)
 
+    def get_apr_parameters(self):
+        """APR::get_apr_parameters (APR.hpp:99-101): the parameters the APR was
+        built with, grad_th / sigma_th as the automatic parameters chose them."""
+        p = _lib.aprb_params()
+        check(lib().aprb_apr_get_parameters(self._h, C.byref(p)))
+        return APRParameters._from_c(p)
+
     def linear_access(self):
         """(level_xz, xz_end, y_vec) numpy copies of LinearAccess (LinearAccess.hpp:33-35)."""
         i = self.info()
@@ -211,6 +226,9 @@ class APRConverter:
         check(st)
         apr._set(h)
         self.bspline_offset = apr.bspline_offset()
+        if self.par.auto_parameters:  # autoParametersLiEntropy writes the converter's par (APRConverter.hpp:558)
+            used = apr.get_apr_parameters()
+            self.par.grad_th, self.par.sigma_th = used.grad_th, used.sigma_th
         return True
 
     def get_apr(self, apr, img):
@@ -487,6 +505,32 @@ class APRStencil:
         if normalize:
             st = (st / s).astype(f32)
         return st
+
+
+def threshold_li(values, integer_values=False):
+    """threshold_li<T> (src/algorithm/AutoParameters.hpp:50-100): Li's minimum
+    cross entropy threshold of the values (T = uint16 when integer_values,
+    else float), computed on the GPU with FP64 sums."""
+    v = np.ascontiguousarray(values, np.float32).ravel()
+    out = C.c_float()
+    check(lib().aprb_threshold_li(_ptr(v) if v.size else None, v.size, int(bool(integer_values)), C.byref(out)))
+    return out.value
+
+
+def auto_parameters_li_entropy(par, image, local_intensity_scale, grad, bspline_offset=0.0, grad_integer=True):
+    """autoParametersLiEntropy (src/algorithm/AutoParameters.hpp:103-153) on
+    down-sampled arrays of one shape: sets par.grad_th and par.sigma_th from the
+    cells whose image value exceeds par.Ip_th + bspline_offset.  grad holds
+    ImageType values (grad_integer for uint16)."""
+    im, ls, g = (np.ascontiguousarray(a, np.float32).ravel() for a in (image, local_intensity_scale, grad))
+    if not (im.size == ls.size == g.size):
+        raise ValueError("image, local_intensity_scale and grad must have the same size")
+    p = par.c()
+    check(lib().aprb_auto_parameters(C.byref(p), _ptr(im), _ptr(ls), _ptr(g), im.size, int(bool(grad_integer)),
+                                     float(bspline_offset)))
+    par.grad_th = float(p.grad_th)
+    par.sigma_th = float(p.sigma_th)
+    return par
 
 
 def kernel_launch_count():

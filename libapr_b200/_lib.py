@@ -22,7 +22,7 @@ class aprb_params(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("dx", "dy", "dz", "psfx", "psfy", "psfz", "Ip_th", "lambda_", "rel_error",
                                          "sigma_th", "sigma_th_max", "grad_th")] + \
                [(n, C.c_int) for n in ("reflect_bc_lis", "neighborhood_optimization", "constant_intensity_scale",
-                                       "check_input", "swap_dimensions")]
+                                       "check_input", "swap_dimensions", "auto_parameters")]
 
 
 class aprb_apr_info(C.Structure):
@@ -57,6 +57,9 @@ SIGNATURES = {
     "aprb_converter_intermediate": ([_vp, _i, _vp, C.c_size_t], _i),
     "aprb_apr_free": ([_vp], _i),
     "aprb_apr_get_info": ([_vp, C.POINTER(aprb_apr_info)], _i),
+    "aprb_apr_get_parameters": ([_vp, C.POINTER(aprb_params)], _i),
+    "aprb_threshold_li": ([_vp, _u64, _i, C.POINTER(C.c_float)], _i),
+    "aprb_auto_parameters": ([C.POINTER(aprb_params), _vp, _vp, _vp, _u64, _i, _f], _i),
     "aprb_apr_export": ([_vp, _vp, _vp, _vp], _i),
     "aprb_apr_device_arrays": ([_vp, _vp, _vp, _vp], _i),
     "aprb_apr_from_arrays": ([_i, _i, _i, _vp, _u64, _vp, _u64, _vp, _u64, C.POINTER(_vp)], _i),

@@ -165,6 +165,7 @@ struct aprb_apr {
     int org[3] = {0, 0, 0};
     uint64_t n_xz = 0, P = 0;
     float offset = 0;
+    aprb_params par{};  // the parameters it was built with (APR.hpp:61)
     DevBuf xz_end, y_vec;  // pooled
     // tree
     bool tree_built = false;
@@ -185,6 +186,7 @@ struct aprb_converter {
     DevBuf img, work, grad, grad_keep, ids_raw, ids, lis, lis_keep, pyr_status, pyr_level, mm, offset, err;
     DevBuf scan_tmp, tile_pyr, iir_ckpt;
     LisBuffers lisb;
+    AutoParBuffers autop;
     bool have = false;
 };
 
@@ -312,6 +314,7 @@ void aprb_default_params(aprb_params *p) {
     p->constant_intensity_scale = 0;
     p->check_input = 0;
     p->swap_dimensions = 0;
+    p->auto_parameters = 0;
 }
 
 aprb_status aprb_converter_create(int image_type, aprb_converter **out) {
@@ -431,8 +434,17 @@ void build_structure(aprb_converter *c, const aprb_params &p, Pyramid &pm, aprb_
     APRB_CUDA(cudaStreamSynchronize(s));
 }
 
+// autoParametersLiEntropy before applyParameters (APRConverter.hpp:556-561,
+// APRConverterBatch.hpp:243-247): image = local_scale_temp2 (ids).
 template <typename IT>
-void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, int yn, int xn, int zn,
+void apply_auto_parameters(aprb_converter *c, aprb_params &p, const PixelOut<IT> &po, cudaStream_t s) {
+    if (!p.auto_parameters) return;
+    auto_parameters<IT>(po.ids, po.grad, po.lis, po.nd, po.d_off, p.Ip_th, sizeof(IT) == 2, c->autop, s,
+                        &p.grad_th, &p.sigma_th, nullptr);
+}
+
+template <typename IT>
+void run_get_apr(aprb_converter *c, aprb_params p, const uint16_t *img, int yn, int xn, int zn,
                  cudaStream_t s, aprb_apr *a, const uint16_t *host = nullptr, cudaStream_t up = nullptr) {
     Geom &g = a->g;
     a->n_xz = apr_geometry(yn, xn, zn, g);
@@ -450,6 +462,8 @@ void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, i
         APRB_CUDA(cudaMemcpyAsync(c->grad_keep.as_on<IT>(nd, s), grad, nd * sizeof(IT), cudaMemcpyDeviceToDevice, s));
         APRB_CUDA(cudaMemcpyAsync(c->lis_keep.as_on<float>(nd, s), lis, nd * sizeof(float), cudaMemcpyDeviceToDevice, s));
     }
+    apply_auto_parameters<IT>(c, p, po, s);
+    a->par = p;
 
     // particle-cell pyramid: pct levels l_min..L-1 (PullingScheme.hpp:92-104)
     Pyramid pm;
@@ -484,7 +498,7 @@ void run_get_apr(aprb_converter *c, const aprb_params &p, const uint16_t *img, i
 // particle-cell pyramid (fill_global_particle_cell_tree, :282-314), then one
 // pulling scheme and one linear structure for the volume.
 template <typename IT>
-void run_get_apr_by_block(aprb_converter *c, const aprb_params &p, const uint16_t *img, int yn, int xn, int zn,
+void run_get_apr_by_block(aprb_converter *c, aprb_params p, const uint16_t *img, int yn, int xn, int zn,
                           int zblock, int ghost, cudaStream_t s, aprb_apr *a) {
     Geom &g = a->g;
     a->n_xz = apr_geometry(yn, xn, zn, g);
@@ -506,12 +520,14 @@ void run_get_apr_by_block(aprb_converter *c, const aprb_params &p, const uint16_
     for (int b = 0; b < nb; ++b) {
         const ZTile t = z_tile(b, nb, zn, zblock, ghost);
         PixelOut<IT> po = pixel_stages<IT>(c, p, img + (uint64_t)(t.z0 - t.gl) * xn * yn, yn, xn, t.pz, s);
+        apply_auto_parameters<IT>(c, p, po, s);
         uint8_t *lev = c->pyr_level.as_on<uint8_t>(po.nd, s);
         launch_levels<IT>(po.grad, po.lis, po.ids, po.nd, po.d_off, p, L, top, lev, nullptr, 0, s);
         launch_fill_patch(g, pm, lev, t, c->tile_pyr, s);
     }
     if (L > 2) launch_pulling_scheme(g, pm, s, false);
     build_structure(c, p, pm, a, s);
+    a->par = p;  // the last tile's thresholds, as the reference's par keeps them
     c->have = false;  // intermediates are per tile
 }
 
@@ -703,6 +719,50 @@ aprb_status aprb_converter_intermediate(const aprb_converter *c, int stage, floa
 aprb_status aprb_apr_free(aprb_apr *a) {
     delete a;
     return APRB_OK;
+}
+
+aprb_status aprb_apr_get_parameters(const aprb_apr *a, aprb_params *par) {
+    return guarded([&] {
+        ARG_CHECK(a && par, "null argument");
+        *par = a->par;
+    });
+}
+
+aprb_status aprb_threshold_li(const float *values, uint64_t n, int integer_values, float *threshold) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(threshold && (values || n == 0), "null argument");
+        cudaStream_t s = cudaStreamPerThread;
+        AutoParBuffers b;
+        float *v = n ? b.sub_g.as_on<float>(n, s) : nullptr;
+        if (n) APRB_CUDA(cudaMemcpyAsync(v, values, n * sizeof(float), cudaMemcpyHostToDevice, s));
+        const float *vv[2] = {v, v};
+        const int integer[2] = {integer_values != 0, 0}, active[2] = {1, 0};
+        float out[2];
+        threshold_li_pair(vv, n, integer, active, b, s, out);
+        *threshold = out[0];
+    });
+}
+
+aprb_status aprb_auto_parameters(aprb_params *par, const float *image, const float *lis, const float *grad,
+                                 uint64_t n, int grad_integer, float bspline_offset) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(par && ((image && lis && grad) || n == 0), "null argument");
+        cudaStream_t s = cudaStreamPerThread;
+        AutoParBuffers b;
+        DevBuf d_img, d_lis, d_grad, d_off;
+        float *di = d_img.as_on<float>(n ? n : 1, s), *dl = d_lis.as_on<float>(n ? n : 1, s);
+        float *dg = d_grad.as_on<float>(n ? n : 1, s), *doff = d_off.as_on<float>(1, s);
+        if (n) {
+            APRB_CUDA(cudaMemcpyAsync(di, image, n * sizeof(float), cudaMemcpyHostToDevice, s));
+            APRB_CUDA(cudaMemcpyAsync(dl, lis, n * sizeof(float), cudaMemcpyHostToDevice, s));
+            APRB_CUDA(cudaMemcpyAsync(dg, grad, n * sizeof(float), cudaMemcpyHostToDevice, s));
+        }
+        APRB_CUDA(cudaMemcpyAsync(doff, &bspline_offset, sizeof(float), cudaMemcpyHostToDevice, s));
+        auto_parameters<float>(di, dg, dl, n, doff, par->Ip_th, grad_integer, b, s, &par->grad_th, &par->sigma_th,
+                               nullptr);
+    });
 }
 
 aprb_status aprb_apr_get_info(const aprb_apr *a, aprb_apr_info *info) {

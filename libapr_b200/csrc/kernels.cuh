@@ -165,4 +165,24 @@ template <typename OutT>
 void launch_synth_blobs(OutT *img, int yn, int xn, int zn, int n_blobs, float slo, float shi, float alo, float ahi,
                         float bg, uint64_t seed, DevBuf &blobs, cudaStream_t s);
 
+// ---- autopar.cu
+// Scratch of the automatic-parameter step, kept by a converter.
+struct AutoParBuffers {
+    DevBuf counts, offs, sub_g, sub_l, part, res, ticket;
+    bool ticket_ready = false;
+};
+// threshold_li (AutoParameters.hpp:50-100) on up to two device arrays of m
+// values each (T values as float; integer[q] for T = uint16); inactive
+// arrays give 0.  Synchronises s.
+void threshold_li_pair(const float *const v[2], uint64_t m, const int integer[2], const int active[2],
+                       AutoParBuffers &b, cudaStream_t s, float out[2]);
+// autoParametersLiEntropy (AutoParameters.hpp:103-153) on the ds image ids,
+// gradient grad (ImageType values; grad_integer for uint16_t) and local
+// intensity scale lis, nd cells; synchronises s.  n_subsample (may be null)
+// receives the subsample length.
+template <typename IT>
+void auto_parameters(const float *ids, const IT *grad, const float *lis, uint64_t nd, const float *d_off,
+                     float Ip_th, int grad_integer, AutoParBuffers &b, cudaStream_t s, float *grad_th,
+                     float *sigma_th, uint64_t *n_subsample);
+
 }  // namespace aprb

@@ -1449,3 +1449,93 @@ int orc_richardson_lucy(const orc_access *a, const orc_access *t, const uint16_t
     }
     return ORC_OK;
 }
+
+/* ------------------------------------------------------------------ automatic parameters */
+
+/* Means of the values above / at-or-below t (compute_means,
+ * src/algorithm/AutoParameters.hpp:17-36): float sums in index order, or
+ * double sums. */
+static void li_means(const float *v, size_t n, float t, int fp32_sums, float *mean_back, float *mean_fore) {
+    if (fp32_sums) {
+        float sf = 0.f, sb = 0.f;
+        size_t cf = 0, cb = 0;
+        for (size_t i = 0; i < n; ++i) {
+            if (v[i] > t) { sf += v[i]; cf++; } else { sb += v[i]; cb++; }
+        }
+        *mean_fore = sf / (float)cf;
+        *mean_back = sb / (float)cb;
+    } else {
+        double sf = 0, sb = 0;
+        size_t cf = 0, cb = 0;
+        for (size_t i = 0; i < n; ++i) {
+            if (v[i] > t) { sf += v[i]; cf++; } else { sb += v[i]; cb++; }
+        }
+        *mean_fore = (float)(sf / (double)cf);
+        *mean_back = (float)(sb / (double)cb);
+    }
+}
+
+/* threshold_li<T> (src/algorithm/AutoParameters.hpp:50-100) with the
+ * iteration bounded by ORC_LI_MAX_ITER steps. */
+#define ORC_LI_MAX_ITER 1000
+float orc_threshold_li(const float *v, size_t n, int integer_values, int fp32_sums) {
+    if (n == 0) return 0.f;
+    float mn = v[0], mx = v[0];
+    for (size_t i = 1; i < n; ++i) {
+        if (v[i] < mn) mn = v[i];
+        if (v[i] > mx) mx = v[i];
+    }
+    if (mn == mx) return mn;
+    float tol = 0.5f;
+    if (!integer_values) {
+        const float range = mx - mn;
+        tol = fminf(0.01f, range * 1e-4f);
+    }
+    float t_next;
+    if (fp32_sums) {
+        float s = 0.f;
+        for (size_t i = 0; i < n; ++i) s += v[i];
+        t_next = s / (float)n;
+    } else {
+        double s = 0;
+        for (size_t i = 0; i < n; ++i) s += v[i];
+        t_next = (float)(s / (double)n);
+    }
+    float t_curr = -2.f * tol;
+    if (integer_values && t_next < 1.f) {
+        const float mid = (mn + mx) / 2.f;
+        t_next = mid < 1.5f ? mid : 1.5f;
+    }
+    for (int it = 0; it < ORC_LI_MAX_ITER && fabsf(t_next - t_curr) > tol; ++it) {
+        t_curr = t_next;
+        float mb, mf;
+        li_means(v, n, t_curr, fp32_sums, &mb, &mf);
+        if (mb == 0) return t_curr;
+        t_next = (mf - mb) / (logf(mf) - logf(mb));
+    }
+    return t_next;
+}
+
+/* autoParametersLiEntropy (src/algorithm/AutoParameters.hpp:103-153). */
+int orc_auto_parameters(const float *image, const float *lis, const float *grad, size_t n, float threshold,
+                        int grad_integer, int fp32_sums, float *grad_th, float *sigma_th, float *sub_grad,
+                        float *sub_lis, size_t *m_out) {
+    float *fg = (float *)malloc(sizeof(float) * (n ? n : 1)), *fl = (float *)malloc(sizeof(float) * (n ? n : 1));
+    if (!fg || !fl) { free(fg); free(fl); return ORC_ERR_ALLOC; }
+    size_t nf = 0;
+    for (size_t i = 0; i < n; ++i)
+        if (image[i] > threshold) { fg[nf] = grad[i]; fl[nf] = lis[i]; nf++; }
+    const size_t cap = (size_t)32 * 512 * 512;
+    const size_t m = nf < cap ? nf : cap;
+    /* the reference divides by m here; with no foreground pixel both
+     * thresholds are those of an empty input */
+    const size_t delta = m ? nf / m : 0;
+    for (size_t i = 0; i < m; ++i) { fg[i] = fg[i * delta]; fl[i] = fl[i * delta]; }
+    *grad_th = orc_threshold_li(fg, m, grad_integer, fp32_sums);
+    *sigma_th = orc_threshold_li(fl, m, 0, fp32_sums);
+    if (sub_grad) memcpy(sub_grad, fg, sizeof(float) * m);
+    if (sub_lis) memcpy(sub_lis, fl, sizeof(float) * m);
+    if (m_out) *m_out = m;
+    free(fg); free(fl);
+    return ORC_OK;
+}

@@ -127,6 +127,24 @@ int orc_richardson_lucy(const orc_access *acc, const orc_access *tree, const uin
  * (src/algorithm/ComputeGradient.hpp:249-779); returns overflow count. */
 uint64_t orc_bspline_axis(float *img, int y, int x, int z, int axis, float lambda, int is_u16);
 
+/* Li's minimum cross entropy threshold, threshold_li<T>
+ * (src/algorithm/AutoParameters.hpp:50-100), on T values held as float.
+ * integer_values selects T = uint16 (tolerance 0.5, initial value raised
+ * towards 1.5, :63-78), else T = float.  fp32_sums = 1 sums in float in index
+ * order, as the reference does at one OpenMP thread (std::accumulate :71,
+ * compute_means :17-36); fp32_sums = 0 sums in double and rounds each mean to
+ * float once, as libaprb200 does.  At most 1000 Li steps. */
+float orc_threshold_li(const float *v, size_t n, int integer_values, int fp32_sums);
+
+/* autoParametersLiEntropy (src/algorithm/AutoParameters.hpp:103-153): the
+ * gradient and local intensity scale at the pixels whose ds image value
+ * exceeds threshold (= Ip_th + bspline_offset), uniformly subsampled to at
+ * most 32*512*512 values, each thresholded by orc_threshold_li.  sub_grad and
+ * sub_lis (capacity n, may be NULL) receive the subsample, *m its length. */
+int orc_auto_parameters(const float *image, const float *lis, const float *grad, size_t n, float threshold,
+                        int grad_integer, int fp32_sums, float *grad_th, float *sigma_th, float *sub_grad,
+                        float *sub_lis, size_t *m);
+
 #ifdef __cplusplus
 }
 #endif

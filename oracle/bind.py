@@ -80,6 +80,10 @@ def lib():
                                            C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
         L.orc_sample_image_by_block.argtypes = [C.POINTER(OrcAccess), C.POINTER(C.c_uint16), C.c_int, C.c_int,
                                                 C.POINTER(C.c_uint16)]
+        L.orc_threshold_li.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.c_int, C.c_int]
+        L.orc_threshold_li.restype = C.c_float
+        L.orc_auto_parameters.argtypes = [C.POINTER(C.c_float)] * 3 + [C.c_size_t, C.c_float, C.c_int, C.c_int] + \
+            [C.POINTER(C.c_float)] * 4 + [C.POINTER(C.c_size_t)]
         _lib = L
     return _lib
 
@@ -120,6 +124,12 @@ def ref(fast=False):
         R.ref_sample_image_by_block.argtypes = [vp, C.POINTER(C.c_uint16), C.c_int, C.c_int, C.POINTER(C.c_uint16)]
         R.ref_smooth.argtypes = [C.POINTER(C.c_uint16), C.c_int, C.c_int, C.c_int, C.c_float, C.c_int, C.c_float,
                                  C.POINTER(C.c_float)]
+        R.ref_threshold_li.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.c_int, C.c_int]
+        R.ref_threshold_li.restype = C.c_float
+        R.ref_auto_parameters.argtypes = [C.POINTER(C.c_float)] * 3 + [C.c_int] * 4 + [C.c_float, C.c_float, C.c_int,
+                                                                           C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        R.ref_get_apr_auto.argtypes = [C.POINTER(C.c_uint16), C.c_int, C.c_int, C.c_int, C.POINTER(OrcParams),
+                                       C.c_int, C.c_int, C.POINTER(vp), C.POINTER(C.c_float), C.POINTER(C.c_float)]
         _ref[fast] = R
     return _ref[fast]
 
@@ -540,6 +550,57 @@ def ref_get_apr(img, params, image_type=1, staged=True, fast=False):
     if e != 0:
         return e, None
     return 0, RefAPR(h.value, img.shape, fast)
+
+
+def orc_threshold_li(values, integer_values, fp32_sums):
+    """threshold_li restated: float sums in index order (fp32_sums, the
+    reference at one OpenMP thread) or double sums (the GPU's)."""
+    v = np.ascontiguousarray(values, dtype=np.float32)
+    return float(lib().orc_threshold_li(_ptr(v, C.c_float), v.size, int(integer_values), int(fp32_sums)))
+
+
+def orc_auto_parameters(image, lis, grad, threshold, grad_integer, fp32_sums):
+    """autoParametersLiEntropy restated: (grad_th, sigma_th, sub_grad, sub_lis)."""
+    im, ls, g = (np.ascontiguousarray(a, dtype=np.float32).ravel() for a in (image, lis, grad))
+    n = im.size
+    sg, sl = np.zeros(max(n, 1), np.float32), np.zeros(max(n, 1), np.float32)
+    gt, st, m = C.c_float(), C.c_float(), C.c_size_t()
+    assert lib().orc_auto_parameters(_ptr(im, C.c_float), _ptr(ls, C.c_float), _ptr(g, C.c_float), n, threshold,
+                                     int(grad_integer), int(fp32_sums), C.byref(gt), C.byref(st),
+                                     _ptr(sg, C.c_float), _ptr(sl, C.c_float), C.byref(m)) == 0
+    return gt.value, st.value, sg[: m.value], sl[: m.value]
+
+
+def ref_threshold_li(values, integer_values, nthreads=1):
+    """The reference's threshold_li at nthreads OpenMP threads."""
+    v = np.ascontiguousarray(values, dtype=np.float32)
+    return float(ref().ref_threshold_li(_ptr(v, C.c_float), v.size, int(integer_values), nthreads))
+
+
+def ref_auto_parameters(image, lis, grad, Ip_th, bspline_offset, grad_u16, nthreads=1):
+    """The reference's autoParametersLiEntropy on ds arrays (z, x, y):
+    (grad_th, sigma_th)."""
+    im, ls, g = (np.ascontiguousarray(a, dtype=np.float32) for a in (image, lis, grad))
+    z, x, y = im.shape
+    gt, st = C.c_float(), C.c_float()
+    ref().ref_auto_parameters(_ptr(im, C.c_float), _ptr(ls, C.c_float), _ptr(g, C.c_float), y, x, z, int(grad_u16),
+                              Ip_th, bspline_offset, nthreads, C.byref(gt), C.byref(st))
+    return gt.value, st.value
+
+
+def ref_get_apr_auto(img, params, image_type=1, nthreads=1):
+    """The reference's get_apr with auto_parameters on: (status, RefAPR,
+    grad_th, sigma_th)."""
+    R = ref()
+    img = np.ascontiguousarray(img, dtype=np.uint16)
+    z, x, y = img.shape
+    h = C.c_void_p()
+    gt, st = C.c_float(), C.c_float()
+    e = R.ref_get_apr_auto(_ptr(img, C.c_uint16), y, x, z, C.byref(params), image_type, nthreads, C.byref(h),
+                           C.byref(gt), C.byref(st))
+    if e != 0:
+        return e, None, None, None
+    return 0, RefAPR(h.value, img.shape), gt.value, st.value
 
 
 def ref_get_apr_by_block(img, params, image_type, z_block, ghost, fast=False):

@@ -10,12 +10,15 @@
  */
 #include "algorithm/APRConverter.hpp"
 #include "algorithm/APRConverterBatch.hpp"
+#include "algorithm/AutoParameters.hpp"
 #include "numerics/APRFilter.hpp"
 #include "numerics/APRNumerics.hpp"
 #include "numerics/APRStencil.hpp"
 #include "numerics/APRTreeNumerics.hpp"
 
 #include "apr_oracle.h"
+
+#include <omp.h>
 
 #include <cstring>
 #include <stdexcept>
@@ -252,6 +255,93 @@ int ref_get_apr_custom(const float *grad, const float *lis, int y, int x, int z,
     c.bspline_offset = 0;
     c.initPipelineAPR(h->apr, in);
     c.get_apr_custom_grad_scale(h->apr, g, s);
+    *out = h;
+    return 0;
+}
+
+/* ------------------------------------------------------------------ automatic parameters
+ * The reference's OpenMP reductions sum in an order that depends on the
+ * thread count; nthreads (> 0) fixes it for the call. */
+struct OmpThreads {
+    int saved;
+    explicit OmpThreads(int n) : saved(omp_get_max_threads()) { if (n > 0) omp_set_num_threads(n); }
+    ~OmpThreads() { omp_set_num_threads(saved); }
+};
+
+/* threshold_li<T> (src/algorithm/AutoParameters.hpp:50-100), T = uint16_t
+ * when is_u16, else float; v holds the values as float. */
+float ref_threshold_li(const float *v, size_t n, int is_u16, int nthreads) {
+    OmpThreads th(nthreads);
+    if (is_u16) {
+        std::vector<uint16_t> in(n);
+        for (size_t i = 0; i < n; ++i) in[i] = (uint16_t)v[i];
+        return threshold_li(in);
+    }
+    std::vector<float> in(v, v + n);
+    return threshold_li(in);
+}
+
+/* autoParametersLiEntropy (src/algorithm/AutoParameters.hpp:103-153) on ds
+ * arrays of shape (y, x, z): image = local_scale_temp2, lis =
+ * local_scale_temp, grad = grad_temp holding ImageType values (uint16_t when
+ * grad_u16). */
+int ref_auto_parameters(const float *image, const float *lis, const float *grad, int y, int x, int z, int grad_u16,
+                        float Ip_th, float bspline_offset, int nthreads, float *grad_th, float *sigma_th) {
+    OmpThreads th(nthreads);
+    PixelData<float> im(y, x, z), ls(y, x, z);
+    std::memcpy(im.mesh.begin(), image, im.mesh.size() * sizeof(float));
+    std::memcpy(ls.mesh.begin(), lis, ls.mesh.size() * sizeof(float));
+    APRParameters par;
+    par.Ip_th = Ip_th;
+    if (grad_u16) {
+        PixelData<uint16_t> g(y, x, z);
+        for (size_t i = 0; i < g.mesh.size(); ++i) g.mesh[i] = (uint16_t)grad[i];
+        autoParametersLiEntropy(par, im, ls, g, bspline_offset, false);
+    } else {
+        PixelData<float> g(y, x, z);
+        std::memcpy(g.mesh.begin(), grad, g.mesh.size() * sizeof(float));
+        autoParametersLiEntropy(par, im, ls, g, bspline_offset, false);
+    }
+    *grad_th = par.grad_th;
+    *sigma_th = par.sigma_th;
+    return 0;
+}
+
+/* APRConverter::get_apr with par.auto_parameters = true (the public entry
+ * point, APRConverter.hpp:556-561); the thresholds it chose are read back
+ * from APR::get_apr_parameters. */
+int ref_get_apr_auto(const uint16_t *img, int y, int x, int z, const orc_params *p, int image_type, int nthreads,
+                     void **out, float *grad_th, float *sigma_th) {
+    OmpThreads th(nthreads);
+    *out = nullptr;
+    PixelData<uint16_t> in(y, x, z);
+    std::memcpy(in.mesh.begin(), img, sizeof(uint16_t) * (size_t)y * x * z);
+    RefHandle *h = new RefHandle();
+    try {
+        bool ok;
+        if (image_type == 1) {
+            APRConverter<uint16_t> c;
+            c.verbose = false;
+            set_params(c.par, p);
+            c.par.auto_parameters = true;
+            ok = c.get_apr(h->apr, in);
+            h->offset = c.bspline_offset;
+        } else {
+            APRConverter<float> c;
+            c.verbose = false;
+            set_params(c.par, p);
+            c.par.auto_parameters = true;
+            ok = c.get_apr(h->apr, in);
+            h->offset = c.bspline_offset;
+        }
+        if (!ok) { delete h; return 1; }
+    } catch (std::invalid_argument &) {
+        delete h;
+        return 2;
+    }
+    const APRParameters par = h->apr.get_apr_parameters();
+    *grad_th = par.grad_th;
+    *sigma_th = par.sigma_th;
     *out = h;
     return 0;
 }
