@@ -626,6 +626,31 @@ def main():
                 "roofline": {"bound": "hbm", "achieved": ab / (cms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
                              "frac": ab / (cms / 1e3) / 1e9 / hbm, "algorithmic_bytes": ab},
                 "gflops": flops / (cms / 1e3) / 1e9, "stages_ms": cstages}
+        # gradient magnitude on the particles (APRNumerics::gradient_magnitude_cfd
+        # and _sobel): three directional 3x3x3 convolutions, squares and a root
+        deltas = (C.c_float * 3)(1.0, 1.0, 1.0)
+        for sobel in (0, 1):
+            def run_grad():
+                _lib.check(L.aprb_gradient_magnitude_device(last, C.c_void_p(pf.data_ptr()),
+                                                            C.c_void_p(outp.data_ptr()), deltas, sobel, sptr))
+
+            for _ in range(2):
+                run_grad()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            reps = max(2, args.steps)
+            e0.record(stream)
+            for _ in range(reps):
+                run_grad()
+            e1.record(stream)
+            torch.cuda.synchronize()
+            gms = e0.elapsed_time(e1) / reps
+            ab = 3 * (10 * P + 10 * T)
+            conv_res["gradient_magnitude_sobel" if sobel else "gradient_magnitude_cfd"] = {
+                "value": P / (gms / 1e3) / 1e9, "unit": "Gpart/s", "ms": gms,
+                "roofline": {"bound": "hbm", "achieved": ab / (gms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
+                             "frac": ab / (gms / 1e3) / 1e9 / hbm, "algorithmic_bytes": ab,
+                             "note": "three directional convolutions at 10P + 10T each"}}
         del pf, outp
         # piecewise-constant reconstruction of the volume from its particles
         # (reconstruct_constant): writes every pixel once
@@ -653,6 +678,41 @@ def main():
                          "frac": ab / (rms / 1e3) / 1e9 / hbm, "algorithmic_bytes": ab}}
         del rimg
     L.aprb_apr_free(last)
+
+    # automatic parameters (autoParametersLiEntropy before applyParameters):
+    # the same get_apr with par.auto_parameters on, the step's stage time
+    auto_res = None
+    if rank == 0 and not args.no_conv:
+        par_auto = lib_params().c()
+        par_auto.auto_parameters = 1
+
+        def get_apr_auto():
+            h = C.c_void_p()
+            _lib.check(L.aprb_get_apr_device(conv._h, C.byref(par_auto), iptr, y, x, z, sptr, C.byref(h)))
+            return h
+
+        L.aprb_apr_free(get_apr_auto())
+        torch.cuda.synchronize()
+        L.aprb_profile_reset()
+        L.aprb_profile_enable(1)
+        reps = max(2, args.steps)
+        for _ in range(reps):
+            ha = get_apr_auto()
+            used = _lib.aprb_params()
+            _lib.check(L.aprb_apr_get_parameters(ha, C.byref(used)))
+            L.aprb_apr_free(ha)
+        torch.cuda.synchronize()
+        L.aprb_profile_enable(0)
+        an = (C.c_char_p * 64)()
+        at = (C.c_double * 64)()
+        ac = (C.c_uint64 * 64)()
+        na = L.aprb_profile_read(an, at, ac, 64)
+        astages = {an[i].decode(): at[i] / reps for i in range(na)}
+        L.aprb_profile_reset()
+        ams = astages.get("auto_parameters")
+        auto_res = {"ms": ams, "ds_cells": Nd, "ds_cells_per_s": Nd / (ams / 1e3) if ams else None,
+                    "grad_th": used.grad_th, "sigma_th": used.sigma_th,
+                    "note": "foreground count + scan + subsample + Li steps (host round trip per step)"}
 
     # the batch and deconvolution workloads are single-GPU measurements
     batch_res = None
@@ -699,6 +759,8 @@ def main():
                            "l2": "input 4 GiB > L2, no flush needed",
                            "parallelism": "independent volume per GPU" if world > 1 else "1 GPU"},
                 "gpu_launches": int(launches), "e2e": e2e, "cpu_baseline": cpu, **out, **conv_res}
+        if auto_res:
+            line["auto_parameters"] = auto_res
         if batch_res:
             line["batch_by_block"] = batch_res
         if rl_res:
