@@ -1094,19 +1094,6 @@ static std::vector<float> gradient_stencils(const aprb_apr *a, int dim, int sobe
     return out;
 }
 
-__global__ void square_kernel(float *o, uint64_t n) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) o[i] = __fmul_rn(o[i], o[i]);
-}
-__global__ void add_square_kernel(float *o, const float *g, uint64_t n) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) o[i] = __fadd_rn(o[i], __fmul_rn(g[i], g[i]));
-}
-__global__ void sqrt_kernel(float *o, uint64_t n) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) o[i] = __fsqrt_rn(o[i]);
-}
-
 // gradient of dimension dim, device buffers
 static void gradient_dim(aprb_apr *a, const float *in, float *out, int dim, int sobel, float delta, cudaStream_t s) {
     ensure_tree(a, s);
@@ -1129,24 +1116,25 @@ static void gradient_dim(aprb_apr *a, const float *in, float *out, int dim, int 
 }
 
 // gradient magnitude: y^2, then + x^2 and + z^2 for axes longer than 1, then
-// the square root, in the reference's order
+// the square root, in the reference's order; the three directions share one
+// pass (tree means, neighbourhood images, particles)
 static void gradient_magnitude(aprb_apr *a, const float *in, float *out, const float *deltas, int sobel,
                                cudaStream_t s) {
-    const uint64_t P = a->P;
-    const unsigned blocks = blocks_for(P, 256);
-    gradient_dim(a, in, out, 0, sobel, deltas[0], s);
-    if (P) square_kernel<<<blocks, 256, 0, s>>>(out, P);
-    count_launch();
-    float *tmp = (float *)scratch().rb.get((P ? P : 1) * sizeof(float));
-    for (int d = 1; d < 3; ++d) {
-        if (a->org[d] <= 1) continue;
-        gradient_dim(a, in, tmp, d, sobel, deltas[d], s);
-        if (P) add_square_kernel<<<blocks, 256, 0, s>>>(out, tmp, P);
-        count_launch();
+    ensure_tree(a, s);
+    const int nlev = std::max(a->g.l_max - a->g.l_min, 1);
+    std::vector<float> st[3];
+    const float *stp[3];
+    int active[3];
+    for (int d = 0; d < 3; ++d) {
+        active[d] = d == 0 || a->org[d] > 1;
+        st[d] = gradient_stencils(a, d, sobel, deltas[d], nlev);
+        stp[d] = st[d].data();
     }
-    if (P) sqrt_kernel<<<blocks, 256, 0, s>>>(out, P);
-    count_launch();
-    APRB_CHECK_LAUNCH();
+    float *tree = scratch().tree_vals.as<float>(a->T ? a->T : 1);
+    filter_gradient_magnitude(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, a->tg,
+                              (const uint64_t *)a->t_xz_end.p, (const uint16_t *)a->t_y_vec.p, a->fi, in, tree, stp,
+                              active, nlev, out, scratch().fb, s);
+    a->last_stale = filter_stale_count(scratch().fb, s);
 }
 
 template <typename T>

@@ -428,6 +428,115 @@ void launch_conv_level_dense(const ConvLevelArgs &a, const uint64_t *xz_end, con
     APRB_CHECK_LAUNCH();
 }
 
+// Gradient magnitude of one level (APRNumerics::gradient_magnitude_cfd /
+// _sobel, APRNumerics.hpp:227-287) in one pass over the level's
+// neighbourhood image: every direction's 3x3x3 stencil with its zero taps
+// dropped and the others kept in memory order, then y^2 (+ x^2) (+ z^2) and
+// the square root, as the per-direction path (one convolution per
+// direction, squares and a root) computes them.  A zero tap adds +-0 to a
+// finite sum, which changes the sum only when it is itself zero, and then
+// only its sign, which the square removes.  Each cell of the union of the
+// directions' taps is loaded once.
+struct GradTaps {
+    int nu;         // cells with a nonzero weight in some direction, memory order
+    int active[3];  // direction enters the magnitude
+    float w[27][3]; // weights of those cells per direction (0: tap dropped)
+    signed char dz[27], dx[27], dy[27];
+};
+
+__global__ void __launch_bounds__(256) grad_mag_gather_kernel(ConvLevelArgs a, const uint64_t *__restrict__ xz_end,
+                                                              const uint16_t *__restrict__ y_vec,
+                                                              const float *__restrict__ D, GradTaps gt,
+                                                              float *__restrict__ out, unsigned long long *stale) {
+    __shared__ long long so[27];
+    __shared__ float sw[27][3];
+    const int yn = a.d.yn;
+    for (int k = threadIdx.x; k < 27; k += blockDim.x) {
+        so[k] = ((long long)gt.dz[k] * a.d.xn + gt.dx[k]) * (long long)yn + gt.dy[k];
+        sw[k][0] = gt.w[k][0];
+        sw[k][1] = gt.w[k][1];
+        sw[k][2] = gt.w[k][2];
+    }
+    __syncthreads();
+    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= (uint64_t)a.d.xn * a.d.zn) return;
+    const uint64_t b = xz_end[a.row_base + row - 1], e = xz_end[a.row_base + row];
+    if (b == e) return;
+    const int z = (int)(row / (uint64_t)a.d.xn), x = (int)(row % (uint64_t)a.d.xn);
+    const bool rows_in = z - 1 >= 0 && z + 1 < a.d.zn && x - 1 >= 0 && x + 1 < a.d.xn;
+    const float *Drow = D + ((uint64_t)z * a.d.xn + (uint64_t)x) * (uint64_t)yn;
+    const int nu = gt.nu;
+    unsigned nstale = 0;
+    for (uint64_t base = b; base < e; base += 32 * kConvK) {
+        uint64_t ii[kConvK];
+        int yv[kConvK];
+        bool has[kConvK];
+        bool inner = rows_in;
+#pragma unroll
+        for (int j = 0; j < kConvK; ++j) {
+            ii[j] = base + (uint64_t)(j * 32 + lane);
+            has[j] = ii[j] < e;
+            yv[j] = has[j] ? (int)y_vec[ii[j]] : 1;
+            inner = inner && yv[j] - 1 >= 0 && yv[j] + 1 < yn;
+        }
+        float g[3][kConvK];
+#pragma unroll
+        for (int d = 0; d < 3; ++d)
+#pragma unroll
+            for (int j = 0; j < kConvK; ++j) g[d][j] = 0.0f;
+        if (inner) {
+            // one load per cell, every direction with a weight there in turn:
+            // each direction still sums its taps in memory order
+            for (int c = 0; c < nu; ++c) {
+                const long long o = so[c];
+                const float w0 = sw[c][0], w1 = sw[c][1], w2 = sw[c][2];
+                float v[kConvK];
+#pragma unroll
+                for (int j = 0; j < kConvK; ++j) v[j] = __ldg(Drow + yv[j] + o);
+                if (w0 != 0.0f) {
+#pragma unroll
+                    for (int j = 0; j < kConvK; ++j) g[0][j] = __fadd_rn(g[0][j], __fmul_rn(v[j], w0));
+                }
+                if (w1 != 0.0f) {
+#pragma unroll
+                    for (int j = 0; j < kConvK; ++j) g[1][j] = __fadd_rn(g[1][j], __fmul_rn(v[j], w1));
+                }
+                if (w2 != 0.0f) {
+#pragma unroll
+                    for (int j = 0; j < kConvK; ++j) g[2][j] = __fadd_rn(g[2][j], __fmul_rn(v[j], w2));
+                }
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < kConvK; ++j) {
+            if (!has[j]) continue;
+            float gv[3] = {g[0][j], g[1][j], g[2][j]};
+            bool redo = !inner;
+#pragma unroll
+            for (int d = 0; d < 3; ++d) redo = redo || gv[d] != gv[d];
+            if (redo) {
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    float acc = 0.0f;
+                    for (int c = 0; c < nu; ++c) {
+                        const float w = gt.w[c][d];
+                        if (w == 0.0f) continue;
+                        const float vv = gather_tap(D, a, z + gt.dz[c], x + gt.dx[c], yv[j] + gt.dy[c], nstale);
+                        acc = __fadd_rn(acc, __fmul_rn(vv, w));
+                    }
+                    gv[d] = acc;
+                }
+            }
+            float m = __fmul_rn(gv[0], gv[0]);
+            if (gt.active[1]) m = __fadd_rn(m, __fmul_rn(gv[1], gv[1]));
+            if (gt.active[2]) m = __fadd_rn(m, __fmul_rn(gv[2], gv[2]));
+            out[ii[j]] = __fsqrt_rn(m);
+        }
+    }
+    if (nstale) atomicAdd(stale, (unsigned long long)nstale);
+}
+
 }  // namespace
 
 void build_filter_index(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
@@ -469,6 +578,59 @@ void build_filter_index(const Geom &g, const uint64_t *xz_end, const uint16_t *y
     fi.built = true;
 }
 
+// Tree means of every tree level, fine to coarse.
+template <typename T>
+static void tree_means_all(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
+                           const uint64_t *t_xz_end, const uint16_t *t_y_vec, const FilterIndex &fi, const T *in,
+                           T *tree, cudaStream_t s) {
+    APRB_PROF("tree_mean", s);
+    const int L = g.l_max;
+    const uint16_t *cbase = (const uint16_t *)fi.buf.p;
+    for (int t = tg.l_max; t >= tg.l_min; --t) {
+        const int l = t + 1;  // child level
+        if (l > L || l < g.l_min) continue;
+        TreeLevelArgs ta;
+        ta.dt = ld(tg, t);
+        ta.dc = ld(g, l);
+        ta.t_row_base = tg.level_xz[t];
+        ta.c_row_base = g.level_xz[l];
+        ta.ct_row_base = (l <= tg.l_max) ? tg.level_xz[l] : 0;
+        ta.t_cidx = cbase + fi.tree_off[t];
+        ta.c_cidx = cbase + fi.apr_off[l];
+        ta.ct_cidx = (l <= tg.l_max) ? cbase + fi.tree_off[l] : nullptr;
+        const uint64_t rows = (uint64_t)ta.dt.xn * ta.dt.zn;
+        const unsigned ych = (unsigned)((ta.dt.yn + tree_tw<T>() - 1) / tree_tw<T>());
+        if (rows == 0 || ych == 0) continue;
+        dim3 grid((unsigned)((rows + kTR - 1) / kTR), ych);
+        tree_mean_kernel<T><<<grid, 128 * kTR, 0, s>>>(ta, rows, xz_end, y_vec, in, t_xz_end, t_y_vec, tree);
+        count_launch();
+    }
+    APRB_CHECK_LAUNCH();
+}
+
+// Neighbourhood arguments of level l for a stencil of the given side
+// (parents used up to ceil(log2(r + 2) - 1) levels coarser, APRFilter.hpp:1118-1124).
+static ConvLevelArgs conv_level_args(const Geom &g, const Geom &tg, const FilterIndex &fi, int l, int side,
+                                     int reflect, int mode) {
+    const uint16_t *cbase = (const uint16_t *)fi.buf.p;
+    const int r = (side - 1) / 2;
+    const int max_npl = (int)std::ceil(std::log2((double)(r + 2)) - 1);
+    const int npl = std::min(max_npl, l - g.l_min);
+    ConvLevelArgs a;
+    a.d = ld(g, l);
+    a.dp = l > g.l_min ? ld(g, l - 1) : LD{1, 1, 1};
+    a.row_base = g.level_xz[l];
+    a.prow_base = npl >= 1 ? g.level_xz[l - 1] : 0;
+    a.trow_base = l <= tg.l_max ? tg.level_xz[l] : 0;
+    a.cidx = cbase + fi.apr_off[l];
+    a.pcidx = npl >= 1 ? cbase + fi.apr_off[l - 1] : nullptr;
+    a.tcidx = l <= tg.l_max ? cbase + fi.tree_off[l] : nullptr;
+    a.reflect = reflect;
+    a.mode = mode;
+    a.rad = r;
+    return a;
+}
+
 template <typename T>
 void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
                   const uint64_t *t_xz_end, const uint16_t *t_y_vec, const FilterIndex &fi, const T *in, T *tree,
@@ -476,53 +638,15 @@ void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, 
                   FilterBuffers &fb, cudaStream_t s) {
     APRB_PROF(plan ? "convolve" : "fill_tree_mean", s);
     const int L = g.l_max;
-    const uint16_t *cbase = (const uint16_t *)fi.buf.p;
     unsigned long long *stale = fb.stale.as<unsigned long long>(1);
     APRB_CUDA(cudaMemsetAsync(stale, 0, sizeof(unsigned long long), s));
-    // tree means, fine to coarse
-    {
-        APRB_PROF("tree_mean", s);
-        for (int t = tg.l_max; t >= tg.l_min; --t) {
-            const int l = t + 1;  // child level
-            if (l > L || l < g.l_min) continue;
-            TreeLevelArgs ta;
-            ta.dt = ld(tg, t);
-            ta.dc = ld(g, l);
-            ta.t_row_base = tg.level_xz[t];
-            ta.c_row_base = g.level_xz[l];
-            ta.ct_row_base = (l <= tg.l_max) ? tg.level_xz[l] : 0;
-            ta.t_cidx = cbase + fi.tree_off[t];
-            ta.c_cidx = cbase + fi.apr_off[l];
-            ta.ct_cidx = (l <= tg.l_max) ? cbase + fi.tree_off[l] : nullptr;
-            const uint64_t rows = (uint64_t)ta.dt.xn * ta.dt.zn;
-            const unsigned ych = (unsigned)((ta.dt.yn + tree_tw<T>() - 1) / tree_tw<T>());
-            if (rows == 0 || ych == 0) continue;
-            dim3 grid((unsigned)((rows + kTR - 1) / kTR), ych);
-            tree_mean_kernel<T><<<grid, 128 * kTR, 0, s>>>(ta, rows, xz_end, y_vec, in, t_xz_end, t_y_vec, tree);
-            count_launch();
-        }
-    }
-    APRB_CHECK_LAUNCH();
+    tree_means_all<T>(g, xz_end, y_vec, tg, t_xz_end, t_y_vec, fi, in, tree, s);
     if (!plan) return;
     for (int l = L; l >= g.l_min; --l) {
         if (fi.level_count[l] == 0) continue;
         const int sn = std::min(plan->nstencils - 1, L - l);
         const int side = plan->sides[sn];
-        const int r = (side - 1) / 2;
-        const int max_npl = (int)std::ceil(std::log2((double)(r + 2)) - 1);
-        const int npl = std::min(max_npl, l - g.l_min);
-        ConvLevelArgs a;
-        a.d = ld(g, l);
-        a.dp = l > g.l_min ? ld(g, l - 1) : LD{1, 1, 1};
-        a.row_base = g.level_xz[l];
-        a.prow_base = npl >= 1 ? g.level_xz[l - 1] : 0;
-        a.trow_base = l <= tg.l_max ? tg.level_xz[l] : 0;
-        a.cidx = cbase + fi.apr_off[l];
-        a.pcidx = npl >= 1 ? cbase + fi.apr_off[l - 1] : nullptr;
-        a.tcidx = l <= tg.l_max ? cbase + fi.tree_off[l] : nullptr;
-        a.reflect = plan->reflect;
-        a.mode = mode;
-        a.rad = r;
+        const ConvLevelArgs a = conv_level_args(g, tg, fi, l, side, plan->reflect, mode);
         const T *st = d_stencils + plan->offsets[sn];
         T *D = (T *)fb.dense.get(ncell_of(a.d) * sizeof(T));
         if (side == 3)
@@ -538,6 +662,52 @@ template void filter_apply<float>(const Geom &, const uint64_t *, const uint16_t
 template void filter_apply<double>(const Geom &, const uint64_t *, const uint16_t *, const Geom &, const uint64_t *,
                                    const uint16_t *, const FilterIndex &, const double *, double *, const ConvPlan *,
                                    const double *, double *, int, const uint16_t *, FilterBuffers &, cudaStream_t);
+
+void filter_gradient_magnitude(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
+                               const uint64_t *t_xz_end, const uint16_t *t_y_vec, const FilterIndex &fi,
+                               const float *in, float *tree, const float *const stencils[3], const int active[3],
+                               int nstencils, float *out, FilterBuffers &fb, cudaStream_t s) {
+    APRB_PROF("gradient_magnitude", s);
+    const int L = g.l_max;
+    unsigned long long *stale = fb.stale.as<unsigned long long>(1);
+    APRB_CUDA(cudaMemsetAsync(stale, 0, sizeof(unsigned long long), s));
+    tree_means_all<float>(g, xz_end, y_vec, tg, t_xz_end, t_y_vec, fi, in, tree, s);
+    for (int l = L; l >= g.l_min; --l) {
+        if (fi.level_count[l] == 0) continue;
+        const int sn = std::min(nstencils - 1, L - l);
+        const ConvLevelArgs a = conv_level_args(g, tg, fi, l, 3, 1, 0);
+        GradTaps gt{};
+        for (int d = 0; d < 3; ++d) gt.active[d] = active[d];
+        for (int k = 0; k < 27; ++k) {
+            float w[3];
+            bool any = false;
+            for (int d = 0; d < 3; ++d) {
+                w[d] = active[d] ? stencils[d][27 * sn + k] : 0.0f;
+                if (w[d] == 0.0f) w[d] = 0.0f;  // -0 too: the tap is dropped
+                any = any || w[d] != 0.0f;
+            }
+            if (!any) continue;
+            const int c = gt.nu++;
+            for (int d = 0; d < 3; ++d) gt.w[c][d] = w[d];
+            gt.dz[c] = (signed char)(k / 9 - 1);
+            gt.dx[c] = (signed char)((k / 3) % 3 - 1);
+            gt.dy[c] = (signed char)(k % 3 - 1);
+        }
+        const uint64_t rows = (uint64_t)a.d.xn * a.d.zn;
+        float *D = (float *)fb.dense.get(ncell_of(a.d) * sizeof(float));
+        {
+            APRB_PROF("densify", s);
+            densify_kernel<float><<<blocks_for(rows * 32, 256), 256, 0, s>>>(a, xz_end, y_vec, in, t_xz_end, t_y_vec,
+                                                                           tree, D);
+            count_launch();
+            APRB_CHECK_LAUNCH();
+        }
+        APRB_PROF("grad_mag_gather", s);
+        grad_mag_gather_kernel<<<blocks_for(rows * 32, 256), 256, 0, s>>>(a, xz_end, y_vec, D, gt, out, stale);
+        count_launch();
+        APRB_CHECK_LAUNCH();
+    }
+}
 
 uint64_t filter_stale_count(FilterBuffers &fb, cudaStream_t s) {
     unsigned long long v = 0;

@@ -131,6 +131,14 @@ void filter_apply(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, 
                   const ConvPlan *plan, const T *d_stencils, T *out, int mode, const uint16_t *rl_in,
                   FilterBuffers &fb, cudaStream_t s);
 uint64_t filter_stale_count(FilterBuffers &fb, cudaStream_t s);
+// gradient magnitude (APRNumerics::gradient_magnitude_*): tree means once,
+// then per level one neighbourhood image and one pass over the particles with
+// the three directions' 3x3x3 stencils (host arrays of nstencils x 27, level
+// delta d at stencils[k] + 27 d); active[k] = direction k enters the magnitude
+void filter_gradient_magnitude(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const Geom &tg,
+                               const uint64_t *t_xz_end, const uint16_t *t_y_vec, const FilterIndex &fi,
+                               const float *in, float *tree, const float *const stencils[3], const int active[3],
+                               int nstencils, float *out, FilterBuffers &fb, cudaStream_t s);
 
 // ---- learned.cu: the learned RL proposal (a sparse APR CNN, 16 channels)
 struct CnnGeom {
