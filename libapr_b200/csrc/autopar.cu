@@ -27,15 +27,14 @@ constexpr uint64_t kFgChunk = (uint64_t)kFgThreads * kFgIter;  // cells per bloc
 constexpr uint64_t kSubsampleCap = (uint64_t)32 * 512 * 512;   // AutoParameters.hpp:140
 constexpr int kScanThreads = 1024;
 constexpr int kStatsThreads = 256;
-constexpr int kStatsBlocks = 296;  // 2 per SM; fixed, so the reduction order is too
+constexpr int kStatsBlocks = 1184;  // 8 per SM; fixed, so the reduction order is too
 constexpr int kLiMaxSteps = 1000;  // bound on Li steps (the reference has none)
 
 __device__ __forceinline__ float fg_threshold(const float *d_off, float Ip_th) {
     return Ip_th + (d_off ? *d_off : 0.0f);
 }
 
-// Foreground cells of each kFgChunk-cell chunk; thread t reads cells
-// base + k * kFgThreads + t.
+// Foreground cells of each kFgChunk-cell chunk.
 __global__ void __launch_bounds__(kFgThreads) fg_count_kernel(const float *__restrict__ ids, uint64_t nd,
                                                               const float *__restrict__ d_off, float Ip_th,
                                                               unsigned *__restrict__ counts) {
@@ -83,9 +82,11 @@ __global__ void __launch_bounds__(kScanThreads) fg_scan_kernel(const unsigned *_
 }
 
 // Gathers the gradient and scale of the foreground cells whose rank r (in
-// index order) is a multiple of delta, to position r / delta < m.  The ranks
-// follow the cell order of fg_count_kernel: per step k, warps in order, lanes
-// in order.
+// index order) is a multiple of delta, to position r / delta < m.  Warp w of
+// a block owns the 32 * kFgIter consecutive cells from base + w * 32 *
+// kFgIter: it counts them, the block adds the counts of the warps before it
+// to the chunk's offset (the only barrier), and the warp ranks its cells
+// with ballots in a second read (from L1).
 template <typename IT>
 __global__ void __launch_bounds__(kFgThreads) fg_subsample_kernel(
     const float *__restrict__ ids, const IT *__restrict__ grad, const float *__restrict__ lis, uint64_t nd,
@@ -93,34 +94,36 @@ __global__ void __launch_bounds__(kFgThreads) fg_subsample_kernel(
     uint64_t delta, float *__restrict__ sub_g, float *__restrict__ sub_l) {
     __shared__ unsigned wc[kFgThreads / 32];
     const float th = fg_threshold(d_off, Ip_th);
-    const uint64_t base = (uint64_t)blockIdx.x * kFgChunk;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    const unsigned below = (1u << lane) - 1u;
+    const uint64_t base = (uint64_t)blockIdx.x * kFgChunk + (uint64_t)w * (32 * kFgIter);
+    const uint64_t end = m * delta;
     uint64_t run = offs[blockIdx.x];
-    if (run >= m * delta) return;  // uniform over the block
+    if (run >= end) return;  // uniform over the block
+    unsigned c = 0;
+#pragma unroll 4
     for (int k = 0; k < kFgIter; ++k) {
-        const uint64_t i = base + (uint64_t)k * kFgThreads + threadIdx.x;
+        const uint64_t i = base + (uint64_t)(32 * k + lane);
+        if (i < nd && ids[i] > th) ++c;
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    if (lane == 0) wc[w] = c;
+    __syncthreads();
+    for (int q = 0; q < w; ++q) run += wc[q];
+    if (run >= end) return;  // uniform over the warp
+    const unsigned below = (1u << lane) - 1u;
+    for (int k = 0; k < kFgIter; ++k) {
+        const uint64_t i = base + (uint64_t)(32 * k + lane);
         const bool f = i < nd && ids[i] > th;
         const unsigned bal = __ballot_sync(0xffffffffu, f);
-        if (lane == 0) wc[w] = __popc(bal);
-        __syncthreads();
-        unsigned before = 0, tot = 0;
-#pragma unroll
-        for (int q = 0; q < kFgThreads / 32; ++q) {
-            const unsigned c = wc[q];
-            before += q < w ? c : 0u;
-            tot += c;
-        }
         if (f) {
-            const uint64_t r = run + before + __popc(bal & below);
+            const uint64_t r = run + __popc(bal & below);
             const uint64_t j = delta == 1 ? r : r / delta;
             if (j < m && j * delta == r) {
                 sub_g[j] = (float)grad[i];
                 sub_l[j] = lis[i];
             }
         }
-        run += tot;
-        __syncthreads();
+        run += __popc(bal);
     }
 }
 
@@ -193,8 +196,7 @@ __global__ void __launch_bounds__(kStatsThreads) li_stats_kernel(LiArgs args, ui
         if (args.active[q]) {
             const float *v = args.v[q];
             const float t = args.t[q];
-            for (uint64_t i = (uint64_t)blockIdx.x * kStatsThreads + threadIdx.x; i < m; i += stride) {
-                const float x = v[i];
+            auto take = [&](float x) {
                 if (mode == 0) {
                     s.a += (double)x;
                     s.mn = fminf(s.mn, x);
@@ -205,7 +207,20 @@ __global__ void __launch_bounds__(kStatsThreads) li_stats_kernel(LiArgs args, ui
                 } else {
                     s.b += (double)x;
                 }
+            };
+            // four values per load (the arrays start 16-byte aligned), the
+            // last m % 4 by the first threads
+            const uint64_t m4 = m / 4;
+            const float4 *v4 = reinterpret_cast<const float4 *>(v);
+            for (uint64_t i = (uint64_t)blockIdx.x * kStatsThreads + threadIdx.x; i < m4; i += stride) {
+                const float4 x = __ldg(v4 + i);
+                take(x.x);
+                take(x.y);
+                take(x.z);
+                take(x.w);
             }
+            const uint64_t g = (uint64_t)blockIdx.x * kStatsThreads + threadIdx.x;
+            if (g < m - 4 * m4) take(v[4 * m4 + g]);
         }
         s = li_block_reduce(s);
         if (threadIdx.x == 0) part[(size_t)blockIdx.x * 2 + q] = s;
@@ -306,7 +321,8 @@ void threshold_li_pair(const float *const v[2], uint64_t m, const int integer[2]
     }
     unsigned *ticket = (unsigned *)b.ticket.p;
     LiStats hres[2];
-    const unsigned grid = (unsigned)std::min<uint64_t>(kStatsBlocks, (m + kStatsThreads - 1) / kStatsThreads);
+    const unsigned grid =
+        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(kStatsBlocks, (m / 4 + kStatsThreads - 1) / kStatsThreads));
     auto stats = [&](const LiArgs &args, int mode) {
         li_stats_kernel<<<grid, kStatsThreads, 0, s>>>(args, m, mode, part, res, ticket);
         APRB_CHECK_LAUNCH();
