@@ -38,7 +38,17 @@ def test_cpp_shim_matches_python_path(tmp_path):
     assert conv.get_apr(apr, img)
     parts = A.ParticleData().sample_image(apr, img).data
     c = A.APRFilter.convolve_pencil(apr, np.full(27, 1.0 / 27, np.float32), parts.astype(np.float32))
-    P, s, cs, rs, ls = out.split()
+    P, s, cs, rs, ls, gs, aP, gth, sth = out.split()
+    g = A.APRNumerics.gradient_magnitude_cfd(apr, parts.astype(np.float32))
+    assert abs(float(gs.split("=")[1]) - float(g.astype(np.float64).sum())) <= 1e-3 * max(1.0, abs(float(g.sum())))
+    conv_auto = A.APRConverter("uint16")
+    conv_auto.par = lib_params(auto_parameters=True)
+    apr_auto = A.APR()
+    assert conv_auto.get_apr(apr_auto, img)
+    used = apr_auto.get_apr_parameters()
+    assert np.float32(float(gth.split("=")[1])) == np.float32(used.grad_th)
+    assert np.float32(float(sth.split("=")[1])) == np.float32(used.sigma_th)
+    assert int(aP.split("=")[1]) == apr_auto.total_number_particles()
     assert int(rs.split("=")[1]) == int(A.APRReconstruction.reconstruct_constant(apr, parts).astype(np.uint64).sum())
     assert int(ls.split("=")[1]) == int(A.APRReconstruction.reconstruct_level(apr).astype(np.uint64).sum())
     assert int(P.split("=")[1]) == apr.total_number_particles()
