@@ -135,12 +135,12 @@ TRAFFIC_PER_VOXEL = {
     "bspline_y": ((534.820096e6 + 518.603776e6) / (128 * 1024 * 1024),
                   "ncu, 128x1024x1024 float capture scaled by voxels "
                   "(profiles/iir_y_rc_kernel_float_128x1024x1024.md)"),
-    "bspline_x": ((985.272832e6 + 546.396928e6) / (128 * 1024 * 1024),
+    "bspline_x": ((1074.711e6 + 545.667840e6) / (128 * 1024 * 1024),
                   "ncu, 128x1024x1024 float capture scaled by voxels "
-                  "(profiles/iir_strided_rc_kernel_float_128x1024x1024.md)"),
-    "bspline_z": ((566.572800e6 + 544.346880e6) / (128 * 1024 * 1024),
+                  "(profiles/iir_strided_rcv_kernel_float_128x1024x1024.md)"),
+    "bspline_z": ((716.355e6 + 544.182016e6) / (128 * 1024 * 1024),
                   "ncu, 128x1024x1024 float capture scaled by voxels "
-                  "(profiles/iir_strided_rc_kernel_float_128x1024x1024.md)"),
+                  "(profiles/iir_strided_rcv_kernel_float_128x1024x1024.md)"),
 }
 
 

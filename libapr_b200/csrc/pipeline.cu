@@ -372,6 +372,244 @@ __global__ void __launch_bounds__(128) iir_strided_rc_kernel(IT *__restrict__ im
     if (err) atomicAdd(err_out, err);
 }
 
+// V neighbouring lines (y .. y + V - 1) per thread, V = 2 or 4: the same
+// recurrences as iir_strided_rc_kernel, each line's operations in the same
+// order, with the V samples of a step moved as one 8- or 16-byte access, so
+// that a block of 128 threads covers 128 V consecutive y of each plane (the
+// longer contiguous runs per plane raise the DRAM efficiency of the strided
+// access).  Needs yn a multiple of V and the image aligned to V samples.
+template <typename IT, int V>
+struct VecL;
+template <>
+struct VecL<float, 2> {
+    __device__ __forceinline__ static void get(const float *p, float *a) {
+        const float2 v = *reinterpret_cast<const float2 *>(p);
+        a[0] = v.x;
+        a[1] = v.y;
+    }
+    __device__ __forceinline__ static void put(float *p, const float *a) {
+        *reinterpret_cast<float2 *>(p) = make_float2(a[0], a[1]);
+    }
+};
+template <>
+struct VecL<float, 4> {
+    __device__ __forceinline__ static void get(const float *p, float *a) {
+        const float4 v = *reinterpret_cast<const float4 *>(p);
+        a[0] = v.x;
+        a[1] = v.y;
+        a[2] = v.z;
+        a[3] = v.w;
+    }
+    __device__ __forceinline__ static void put(float *p, const float *a) {
+        *reinterpret_cast<float4 *>(p) = make_float4(a[0], a[1], a[2], a[3]);
+    }
+};
+template <>
+struct VecL<uint16_t, 2> {
+    __device__ __forceinline__ static void get(const uint16_t *p, float *a) {
+        const ushort2 v = *reinterpret_cast<const ushort2 *>(p);
+        a[0] = (float)v.x;
+        a[1] = (float)v.y;
+    }
+    __device__ __forceinline__ static void put(uint16_t *p, const float *a) {
+        *reinterpret_cast<ushort2 *>(p) = make_ushort2(to_it<uint16_t>(a[0]), to_it<uint16_t>(a[1]));
+    }
+};
+template <>
+struct VecL<uint16_t, 4> {
+    __device__ __forceinline__ static void get(const uint16_t *p, float *a) {
+        const ushort4 v = *reinterpret_cast<const ushort4 *>(p);
+        a[0] = (float)v.x;
+        a[1] = (float)v.y;
+        a[2] = (float)v.z;
+        a[3] = (float)v.w;
+    }
+    __device__ __forceinline__ static void put(uint16_t *p, const float *a) {
+        *reinterpret_cast<ushort4 *>(p) = make_ushort4(to_it<uint16_t>(a[0]), to_it<uint16_t>(a[1]),
+                                                       to_it<uint16_t>(a[2]), to_it<uint16_t>(a[3]));
+    }
+};
+
+template <typename IT, int V>
+__global__ void __launch_bounds__(128) iir_strided_rcv_kernel(IT *__restrict__ im, int yn, int n, uint64_t stride,
+                                                              uint64_t outer_stride, uint64_t nlines, IIRDev c,
+                                                              unsigned *err_out, float2 *__restrict__ ckpt) {
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;  // pair index
+    const uint64_t hy = (uint64_t)(yn / V);
+    if (g >= nlines / V) return;
+    const uint64_t y = V * (g % hy), o = g / hy;
+    const uint64_t line = V * g;  // o * yn + y
+    IT *L = im + o * outer_stride + y;
+    unsigned err = 0, scratch_err = 0;
+    float v1[V] = {}, v2[V] = {}, v3[V] = {}, v4[V] = {};
+    for (int i = 0; i < c.minLen; ++i) {
+        float a[V], b[V];
+        VecL<IT, V>::get(L + (uint64_t)i * stride, a);
+        VecL<IT, V>::get(L + (uint64_t)(n - 1 - i) * stride, b);
+        const float k1 = __ldg(c.bc + i), k2 = __ldg(c.bc + c.minLen + i);
+        const float k3 = __ldg(c.bc + 2 * c.minLen + i), k4 = __ldg(c.bc + 3 * c.minLen + i);
+#pragma unroll
+        for (int h = 0; h < V; ++h) {
+            v1[h] = v1[h] + k1 * a[h];
+            v2[h] = v2[h] + k2 * a[h];
+            v3[h] = v3[h] + k3 * b[h];
+            v4[h] = v4[h] + k4 * b[h];
+        }
+    }
+    const int nseg = (n + kRC - 1) / kRC;
+    // ---- causal sweep: the state at every segment start
+    float p1[V], p2[V];
+#pragma unroll
+    for (int h = 0; h < V; ++h) {
+        p1[h] = v1[h];
+        p2[h] = v2[h];
+    }
+    for (int sgm = 0; sgm < nseg; ++sgm) {
+        const int i0 = sgm * kRC;
+        float2 *ck = ckpt + (uint64_t)sgm * nlines + line;
+#pragma unroll
+        for (int h = 0; h < V; ++h) ck[h] = make_float2(p1[h], p2[h]);
+        const IT *P = L + (uint64_t)i0 * stride;
+        if (i0 >= 2 && i0 + kRC <= n) {
+            float buf[kRC][V];
+            const IT *q = P;
+#pragma unroll
+            for (int u = 0; u < kRC; ++u, q += stride) VecL<IT, V>::get(q, buf[u]);
+#pragma unroll
+            for (int u = 0; u < kRC; ++u)
+#pragma unroll
+                for (int h = 0; h < V; ++h) {
+                    const float nv = rnd_it<IT>(buf[u][h] + c.b1 * p1[h] + c.b2 * p2[h], scratch_err);
+                    p2[h] = p1[h];
+                    p1[h] = nv;
+                }
+        } else {
+            const int i1 = min(n, i0 + kRC);
+            for (int i = max(i0, 2); i < i1; ++i) {
+                float a[V];
+                VecL<IT, V>::get(L + (uint64_t)i * stride, a);
+#pragma unroll
+                for (int h = 0; h < V; ++h) {
+                    const float nv = rnd_it<IT>(a[h] + c.b1 * p1[h] + c.b2 * p2[h], scratch_err);
+                    p2[h] = p1[h];
+                    p1[h] = nv;
+                }
+            }
+        }
+    }
+    // ---- anti-causal sweep, recomputing each segment's causal values
+    float q3[V], q4[V];
+#pragma unroll
+    for (int h = 0; h < V; ++h) {
+        q3[h] = v3[h];
+        q4[h] = v4[h];
+    }
+    for (int sgm = nseg - 1; sgm >= 0; --sgm) {
+        const int i0 = sgm * kRC;
+        const float2 *ck = ckpt + (uint64_t)sgm * nlines + line;
+        float r1[V], r2[V];
+#pragma unroll
+        for (int h = 0; h < V; ++h) {
+            const float2 st = ck[h];
+            r1[h] = st.x;
+            r2[h] = st.y;
+        }
+        IT *P = L + (uint64_t)i0 * stride;
+        if (i0 >= 2 && i0 + kRC <= n - 2) {
+            float buf[kRC][V];
+            const IT *q = P;
+#pragma unroll
+            for (int u = 0; u < kRC; ++u, q += stride) VecL<IT, V>::get(q, buf[u]);
+#pragma unroll
+            for (int u = 0; u < kRC; ++u)
+#pragma unroll
+                for (int h = 0; h < V; ++h) {
+                    const float nv = rnd_it<IT>(buf[u][h] + c.b1 * r1[h] + c.b2 * r2[h], err);
+                    r2[h] = r1[h];
+                    r1[h] = nv;
+                    buf[u][h] = nv;
+                }
+#pragma unroll
+            for (int u = kRC - 1; u >= 0; --u)
+#pragma unroll
+                for (int h = 0; h < V; ++h) {
+                    const float temp = (buf[u][h] + c.b1 * q3[h] + c.b2 * q4[h]);
+                    buf[u][h] = rnd_it<IT>(temp * c.norm, err);
+                    q4[h] = q3[h];
+                    q3[h] = temp;
+                }
+            IT *w = P;
+#pragma unroll
+            for (int u = 0; u < kRC; ++u, w += stride) VecL<IT, V>::put(w, buf[u]);
+        } else {
+            const int i1 = min(n, i0 + kRC);
+            float buf[kRC][V];
+#pragma unroll
+            for (int u = 0; u < kRC; ++u) {
+                const int i = i0 + u;
+                if (i >= i1) break;
+                float a[V] = {};
+                if (i >= 2) VecL<IT, V>::get(P + (uint64_t)u * stride, a);
+#pragma unroll
+                for (int h = 0; h < V; ++h) {
+                    float f;
+                    if (i == 0) {
+                        f = rnd_it<IT>(v2[h], err);
+                    } else if (i == 1) {
+                        f = rnd_it<IT>(v1[h], err);
+                    } else {
+                        f = rnd_it<IT>(a[h] + c.b1 * r1[h] + c.b2 * r2[h], err);
+                        r2[h] = r1[h];
+                        r1[h] = f;
+                    }
+                    buf[u][h] = f;
+                }
+            }
+#pragma unroll
+            for (int u = kRC - 1; u >= 0; --u) {
+                const int i = i0 + u;
+                if (i >= i1) continue;
+#pragma unroll
+                for (int h = 0; h < V; ++h) {
+                    float out;
+                    if (i == n - 1) {
+                        out = rnd_it<IT>(v4[h] * c.norm, err);
+                    } else if (i == n - 2) {
+                        out = rnd_it<IT>(v3[h] * c.norm, err);
+                    } else {
+                        const float temp = (buf[u][h] + c.b1 * q3[h] + c.b2 * q4[h]);
+                        out = rnd_it<IT>(temp * c.norm, err);
+                        q4[h] = q3[h];
+                        q3[h] = temp;
+                    }
+                    buf[u][h] = out;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kRC; ++u)
+                if (i0 + u < i1) VecL<IT, V>::put(P + (uint64_t)u * stride, buf[u]);
+        }
+    }
+    if (err) atomicAdd(err_out, err);
+}
+
+// The x / z pass over nlines lines of n samples: four or two lines per thread
+// where y_num and the alignment allow, else one.
+template <typename IT>
+static void launch_strided_iir(IT *work, int yn, int n, uint64_t stride, uint64_t outer_stride, uint64_t nlines,
+                               const IIRDev &c, unsigned *d_err, float2 *ck, cudaStream_t s) {
+    const uintptr_t a = (uintptr_t)work;
+    if (yn % 4 == 0 && a % (4 * sizeof(IT)) == 0)
+        iir_strided_rcv_kernel<IT, 4><<<blocks_for(nlines / 4, 128), 128, 0, s>>>(work, yn, n, stride, outer_stride,
+                                                                                 nlines, c, d_err, ck);
+    else if (yn % 2 == 0 && a % (2 * sizeof(IT)) == 0)
+        iir_strided_rcv_kernel<IT, 2><<<blocks_for(nlines / 2, 128), 128, 0, s>>>(work, yn, n, stride, outer_stride,
+                                                                                 nlines, c, d_err, ck);
+    else
+        iir_strided_rc_kernel<IT><<<blocks_for(nlines, 128), 128, 0, s>>>(work, yn, n, stride, outer_stride, nlines,
+                                                                        c, d_err, ck);
+}
+
 // Copy of the offset input when no smoothing runs (lambda <= 0 or y too short).
 template <typename IT>
 __global__ void offset_copy_kernel(const uint16_t *__restrict__ src, IT *__restrict__ dst, uint64_t n,
@@ -1489,8 +1727,7 @@ static void launch_smooth_yx(const uint16_t *img, IT *work, int yn, int xn, int 
         const IIRDev c = dev_coef(iir_coefficients(lambda, xn));
         const uint64_t nlines = (uint64_t)yn * zn;
         float2 *ck = ckpt.as_on<float2>(nlines * (uint64_t)((xn + kRC - 1) / kRC), s);
-        iir_strided_rc_kernel<IT><<<blocks_for(nlines, 128), 128, 0, s>>>(work, yn, xn, (uint64_t)yn,
-                                                                        (uint64_t)xn * yn, nlines, c, d_err, ck);
+        launch_strided_iir<IT>(work, yn, xn, (uint64_t)yn, (uint64_t)xn * yn, nlines, c, d_err, ck, s);
         count_launch();
         APRB_CHECK_LAUNCH();
     }
@@ -1504,8 +1741,7 @@ static void launch_smooth_z(IT *work, int yn, int xn, int zn, float lambda, unsi
         const IIRDev c = dev_coef(iir_coefficients(lambda, zn));
         const uint64_t nlines = (uint64_t)yn * xn;
         float2 *ck = ckpt.as_on<float2>(nlines * (uint64_t)((zn + kRC - 1) / kRC), s);
-        iir_strided_rc_kernel<IT><<<blocks_for(nlines, 128), 128, 0, s>>>(work, yn, zn, (uint64_t)xn * yn,
-                                                                        (uint64_t)yn, nlines, c, d_err, ck);
+        launch_strided_iir<IT>(work, yn, zn, (uint64_t)xn * yn, (uint64_t)yn, nlines, c, d_err, ck, s);
         count_launch();
         APRB_CHECK_LAUNCH();
     }
