@@ -132,7 +132,7 @@ TRAFFIC_PER_VOXEL = {
     "gradient_ds": ((537.159424e6 + 120.076288e6) / (128 * 1024 * 1024),
                     "ncu, 128x1024x1024 float capture scaled by voxels "
                     "(profiles/grad_ds_kernel_float_128x1024x1024.md)"),
-    "bspline_y": ((534.820096e6 + 518.603776e6) / (128 * 1024 * 1024),
+    "bspline_y": ((477.950720e6 + 496.806912e6) / (128 * 1024 * 1024),
                   "ncu, 128x1024x1024 float capture scaled by voxels "
                   "(profiles/iir_y_rc_kernel_float_128x1024x1024.md)"),
     "bspline_x": ((1074.711e6 + 545.667840e6) / (128 * 1024 * 1024),

@@ -642,39 +642,43 @@ __device__ __forceinline__ void cp_async_wait_one() { asm volatile("cp.async.wai
 // ---------------------------------------------------------------------------
 // a2 (y), recomputing form: the same recurrences as iir_y_kernel without the
 // round trip of the causal values through memory.  The causal sweep keeps
-// only the recurrence state at the start of every 32-sample tile (ckpt,
+// only the recurrence state at the start of every 64-sample tile (ckpt,
 // [tile][line] pairs); the anti-causal sweep then walks the tiles from the
 // end, recomputes each tile's causal values from its saved state and the
 // input -- the same operations on the same values, so the same bits -- and
 // runs the anti-causal recurrence over them.  Traffic per sample: the input
 // read twice and the result written once (2 + 2 + 4 bytes for uint16 input
 // and float ImageType) instead of 2 + 4 + 4 + 4.
-// A warp owns 32 lines; tiles arrive by cp.async one tile ahead of the
-// arithmetic, every copy one aligned 32-bit word (two uint16 samples): rows
-// must start on 4 bytes, i.e. yn even.
+// A warp (one per block) owns 32 lines; tiles arrive by cp.async one tile
+// ahead of the arithmetic, every copy one aligned 32-bit word (two uint16
+// samples) and a warp's copies one 128-byte run of a line: rows must start
+// on 4 bytes, i.e. yn even.  The 64-sample tiles give 128-byte input and
+// 256-byte output runs per line (the DRAM efficiency of the pass rises with
+// the run length).
 // ---------------------------------------------------------------------------
-constexpr int kAY = 32;                         // samples per tile
-constexpr int kAWords = 2 * 32 * 17 + 32 * 33;  // shared words per warp
+constexpr int kAY = 64;                         // samples per tile
+constexpr int kAWords = 2 * 32 * 33 + 32 * 65;  // shared words per warp: two raw stages, the tile values
+constexpr int kAWarps = 1;                       // warps per block
 __device__ __forceinline__ void cp_async4w(void *smem, const void *gmem) {
     const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gmem) : "memory");
 }
 
 template <typename IT>
-__global__ void __launch_bounds__(128) iir_y_rc_kernel(const uint16_t *__restrict__ src, IT *__restrict__ dst, int yn,
+__global__ void __launch_bounds__(32 * kAWarps) iir_y_rc_kernel(const uint16_t *__restrict__ src, IT *__restrict__ dst, int yn,
                                                        uint64_t nlines, IIRDev c, const float *__restrict__ d_offset,
                                                        unsigned *err_out, float2 *__restrict__ ckpt) {
-    __shared__ uint32_t smem_all[4][kAWords];
+    __shared__ uint32_t smem_all[kAWarps][kAWords];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint64_t line0 = ((uint64_t)blockIdx.x * 4 + w) * 32;
+    const uint64_t line0 = ((uint64_t)blockIdx.x * kAWarps + w) * 32;
     if (line0 >= nlines) return;
     const uint64_t myline = line0 + lane;
     const bool valid = myline < nlines;
     const int nl = (int)min((uint64_t)32, nlines - line0);
     const float off = d_offset ? *d_offset : 0.0f;
     uint32_t *S = smem_all[w];
-    uint32_t *U0 = S, *U1 = S + 32 * 17;                      // raw stages [2][32][17] words
-    float *F = reinterpret_cast<float *>(S + 2 * 32 * 17);  // tile values [32][33]
+    uint32_t *U0 = S, *U1 = S + 32 * 33;                      // raw stages [2][32][33] words
+    float *F = reinterpret_cast<float *>(S + 2 * 32 * 33);  // tile values [32][65]
     unsigned err = 0;
 
     float t1 = 0, t2 = 0, t3 = 0, t4 = 0;
@@ -692,22 +696,24 @@ __global__ void __launch_bounds__(128) iir_y_rc_kernel(const uint16_t *__restric
         }
     }
     const int ntile = (yn + kAY - 1) / kAY;
-    const int cq = lane & 15, ch = lane >> 4;  // copies: word cq of lines 2 jj + ch
-    const uint16_t *src_w = src + (line0 + ch) * (uint64_t)yn + 2 * cq;  // this lane's first copy source
-    const uint64_t src_step = 2 * (uint64_t)yn;
+    const uint16_t *src_w = src + line0 * (uint64_t)yn;
     auto issue = [&](int t, uint32_t *buf) {
-        const int y = t * kAY + 2 * cq;
-        if (y < yn) {
-            const uint16_t *p = src_w + t * kAY;
-            uint32_t *d = buf + ch * 17 + cq;
+#pragma unroll
+        for (int h = 0; h < kAY / 64; ++h) {
+            const int cw = lane + 32 * h;  // word of the line
+            const int y = t * kAY + 2 * cw;
+            if (y < yn) {
+                const uint16_t *p = src_w + y;
+                uint32_t *d = buf + cw;
 #pragma unroll 4
-            for (int jj = 0; jj < 16; ++jj, p += src_step, d += 34)
-                if (2 * jj + ch < nl) cp_async4w(d, p);
+                for (int jj = 0; jj < 32; ++jj, p += yn, d += 33)
+                    if (jj < nl) cp_async4w(d, p);
+            }
         }
         cp_async_commit();
     };
     auto sample = [&](const uint32_t *U, int k) -> float {
-        const uint32_t wd = U[lane * 17 + (k >> 1)];
+        const uint32_t wd = U[lane * 33 + (k >> 1)];
         return raw_to_it<IT>((uint16_t)((k & 1) ? (wd >> 16) : (wd & 0xffffu)), off);
     };
 
@@ -769,14 +775,14 @@ __global__ void __launch_bounds__(128) iir_y_rc_kernel(const uint16_t *__restric
 #pragma unroll
                 for (int k = 0; k < kAY; ++k) {
                     const float temp = r1 * c.b1 + r2 * c.b2 + sample(U, k);
-                    F[lane * 33 + k] = rnd_it<IT>(temp, err);
+                    F[lane * 65 + k] = rnd_it<IT>(temp, err);
                     r2 = r1;
                     r1 = temp;
                 }
 #pragma unroll
                 for (int k = kAY - 1; k >= 0; --k) {
-                    const float temp = b1v * c.b1 + b2v * c.b2 + F[lane * 33 + k];
-                    F[lane * 33 + k] = rnd_it<IT>(temp * c.norm, err);
+                    const float temp = b1v * c.b1 + b2v * c.b2 + F[lane * 65 + k];
+                    F[lane * 65 + k] = rnd_it<IT>(temp * c.norm, err);
                     b2v = b1v;
                     b1v = temp;
                 }
@@ -797,22 +803,25 @@ __global__ void __launch_bounds__(128) iir_y_rc_kernel(const uint16_t *__restric
                     }
                     if (y == yn - 2) out = rnd_it<IT>(t3 * c.norm, err);
                     if (y == yn - 1) out = rnd_it<IT>(t4 * c.norm, err);
-                    F[lane * 33 + k] = out;
+                    F[lane * 65 + k] = out;
                 }
                 for (int k = kend - 1; k >= 0; --k) {
                     if (y0 + k > yn - 3) continue;
-                    const float temp = b1v * c.b1 + b2v * c.b2 + F[lane * 33 + k];
-                    F[lane * 33 + k] = rnd_it<IT>(temp * c.norm, err);
+                    const float temp = b1v * c.b1 + b2v * c.b2 + F[lane * 65 + k];
+                    F[lane * 65 + k] = rnd_it<IT>(temp * c.norm, err);
                     b2v = b1v;
                     b1v = temp;
                 }
             }
         }
         __syncwarp();
-        if (y0 + lane < yn) {
-            IT *q = dst + line0 * (uint64_t)yn + y0 + lane;
+#pragma unroll
+        for (int h = 0; h < kAY / 32; ++h) {
+            if (y0 + lane + 32 * h < yn) {
+                IT *q = dst + line0 * (uint64_t)yn + y0 + lane + 32 * h;
 #pragma unroll 4
-            for (int j = 0; j < nl; ++j, q += yn) *q = to_it<IT>(F[j * 33 + lane]);
+                for (int j = 0; j < nl; ++j, q += yn) *q = to_it<IT>(F[j * 65 + lane + 32 * h]);
+            }
         }
         __syncwarp();
     }
@@ -1708,7 +1717,7 @@ static void launch_smooth_yx(const uint16_t *img, IT *work, int yn, int xn, int 
         if (yn % 2 == 0 && ((uintptr_t)img & 3) == 0) {
             const int ntile = (yn + kAY - 1) / kAY;
             float2 *ck = ckpt.as_on<float2>(nlines * (uint64_t)ntile, s);
-            iir_y_rc_kernel<IT><<<blocks_for(nlines, 128), 128, 0, s>>>(img, work, yn, nlines, c, d_offset, d_err, ck);
+            iir_y_rc_kernel<IT><<<blocks_for(nlines, 32 * kAWarps), 32 * kAWarps, 0, s>>>(img, work, yn, nlines, c, d_offset, d_err, ck);
         } else {
             const unsigned blocks = blocks_for(nlines, kYWarps * kTile);
             iir_y_kernel<IT><<<blocks, kYWarps * 32, 0, s>>>(img, work, yn, nlines, c, d_offset, d_err);
