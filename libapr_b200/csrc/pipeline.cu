@@ -1516,6 +1516,102 @@ __global__ void __launch_bounds__(128) sat_strided_kernel(const float *__restric
     }
 }
 
+// The x / z box mean with V neighbouring lines (y .. y + V - 1) per thread:
+// each line's recurrence and divisions exactly as in sat_strided_kernel, the
+// V samples of a step moved as one access (longer runs per plane), eight
+// steps of loads in flight.  Needs yn a multiple of V (used with V = 2: the
+// padded y extent is even whenever the image's is).
+template <int OFF, bool FINAL, int V>
+__global__ void __launch_bounds__(128) sat_stridedv_kernel(const float *__restrict__ in,
+                                                           const float *__restrict__ absdiff_ref,
+                                                           float *__restrict__ out, int yn, int n, uint64_t stride,
+                                                           uint64_t outer_stride, uint64_t nlines, LisOut fo) {
+    constexpr int W = 2 * OFF + 2;
+    const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t hy = (uint64_t)(yn / V);
+    if (g >= nlines / V) return;
+    const uint64_t y = V * (g % hy), o = g / hy;
+    const uint64_t base = o * outer_stride + y;
+    auto emit = [&](int i, const float *v) {
+        if (!FINAL) {
+            VecL<float, V>::put(out + base + (uint64_t)i * stride, v);
+            return;
+        }
+        const int xpad = fo.axis == 1 ? i : (int)o, zpad = fo.axis == 1 ? (int)o : i;
+        const int ux = xpad - fo.sx, uz = zpad - fo.sz;
+        if (ux < 0 || ux >= fo.xd || uz < 0 || uz >= fo.zd) return;
+#pragma unroll
+        for (int h = 0; h < V; ++h) {
+            const int uy = (int)y + h - fo.sy;
+            if (uy >= 0 && uy < fo.yd) fo.out[idx3(uy, ux, uz, fo.yd, fo.xd)] = v[h] * fo.rescale;
+        }
+    };
+    float c[V][W], C[V];
+#pragma unroll
+    for (int h = 0; h < V; ++h) {
+        C[h] = 0.0f;
+#pragma unroll
+        for (int q = 0; q < W; ++q) c[h][q] = 0.0f;
+    }
+    const float dd = (float)(2 * OFF + 1), rdd = __frcp_rn(dd);
+    for (int j0 = 0; j0 < n; j0 += 8) {
+        const int m = min(8, n - j0);
+        float v[8][V];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (u < m) {
+                const uint64_t a = base + (uint64_t)(j0 + u) * stride;
+                VecL<float, V>::get(in + a, v[u]);
+                if (absdiff_ref) {
+                    float r[V];
+                    VecL<float, V>::get(absdiff_ref + a, r);
+#pragma unroll
+                    for (int h = 0; h < V; ++h) v[u][h] = fabsf(v[u][h] - r[h]);
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+            if (u >= m) break;
+            const int j = j0 + u;
+#pragma unroll
+            for (int h = 0; h < V; ++h) {
+                C[h] = (j == 0) ? v[u][h] : v[u][h] + C[h];
+#pragma unroll
+                for (int q = 0; q < W - 1; ++q) c[h][q] = c[h][q + 1];
+                c[h][W - 1] = C[h];
+            }
+            const int i = j - OFF;
+            if (i >= 0) {
+                float e[V];
+                if (i < OFF + 1) {
+#pragma unroll
+                    for (int h = 0; h < V; ++h) e[h] = C[h] / (float)(i + OFF + 1);
+                    emit(i, e);
+                } else if (i < n - OFF) {
+#pragma unroll
+                    for (int h = 0; h < V; ++h) e[h] = div_const(C[h] - c[h][0], dd, rdd);
+                    emit(i, e);
+                }
+            }
+        }
+    }
+    for (int i = n - OFF; i < n; ++i) {
+        if (i < 0) continue;
+        const int back = (n - 1) - (i - OFF - 1);
+        float e[V];
+#pragma unroll
+        for (int h = 0; h < V; ++h) {
+            float cm = 0.0f;
+#pragma unroll
+            for (int q = 0; q < W; ++q)
+                if (q == W - 1 - back) cm = c[h][q];
+            e[h] = (C[h] - cm) / (float)(n - i + OFF);
+        }
+        emit(i, e);
+    }
+}
+
 __global__ void unpad_rescale_kernel(const float *__restrict__ in, int py, int px, float *__restrict__ out, int yn,
                                      int xn, int zn, int oy, int ox, int oz, float rescale) {
     const uint64_t g = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1883,7 +1979,13 @@ static void sat_axis_t(const float *in, const float *absref, float *out, int py,
         const int n = axis == 1 ? px : pz;
         const uint64_t stride = axis == 1 ? (uint64_t)py : (uint64_t)px * py;
         const uint64_t outer = axis == 1 ? (uint64_t)px * py : (uint64_t)py;
-        if (fo)
+        if (py % 2 == 0 && fo)
+            sat_stridedv_kernel<OFF, true, 2><<<blocks_for(nlines / 2, 128), 128, 0, s>>>(in, absref, nullptr, py, n,
+                                                                                      stride, outer, nlines, *fo);
+        else if (py % 2 == 0)
+            sat_stridedv_kernel<OFF, false, 2><<<blocks_for(nlines / 2, 128), 128, 0, s>>>(in, absref, out, py, n,
+                                                                                       stride, outer, nlines, LisOut{});
+        else if (fo)
             sat_strided_kernel<OFF, true><<<blocks_for(nlines, 128), 128, 0, s>>>(in, absref, nullptr, py, n, stride,
                                                                                   outer, nlines, *fo);
         else
