@@ -1302,20 +1302,25 @@ __global__ void __launch_bounds__(kYWarps * 32) sat_y_kernel(const float *__rest
 // The same y box mean with the samples staged by cp.async one tile ahead of
 // the recurrence: a warp owns 32 lines and walks them in tiles of kSY
 // samples, so no registers hold the prefetch and more warps stay resident.
+// 32-sample tiles (a warp's copies and stores are 128-byte runs of a line)
+// in 2-warp blocks keep the static shared memory under 48 KB.
 // In tiles that touch neither end of the line the recurrence runs fully
 // unrolled (the window shift becomes register renaming).  REF: the input is
 // |in - ref| (the second pass of each window).
-constexpr int kSY = 16;
+constexpr int kSY = 32;
+constexpr int kSW = 2;                         // warps per block
+constexpr int kSH = kSY >= 32 ? kSY / 32 : 1;   // y samples per lane and line in a copy
+constexpr int kLPI = kSY >= 32 ? 1 : 32 / kSY;  // lines per warp copy instruction
 
 template <int OFF, bool REF>
-__global__ void __launch_bounds__(128) sat_y_async_kernel(const float *__restrict__ in, const float *__restrict__ ref,
-                                                          float *__restrict__ out, int n, uint64_t nlines,
-                                                          PadMap pm) {
+__global__ void __launch_bounds__(32 * kSW) sat_y_async_kernel(const float *__restrict__ in,
+                                                               const float *__restrict__ ref, float *__restrict__ out,
+                                                               int n, uint64_t nlines, PadMap pm) {
     constexpr int W = 2 * OFF + 2;
     constexpr int NB = REF ? 2 : 1;
-    __shared__ float sm[4][2][NB][32][kSY + 1];
+    __shared__ float sm[kSW][2][NB][32][kSY + 1];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint64_t line0 = ((uint64_t)blockIdx.x * 4 + w) * 32;
+    const uint64_t line0 = ((uint64_t)blockIdx.x * kSW + w) * 32;
     if (line0 >= nlines) return;
     const bool valid = line0 + lane < nlines;
     const float d = (float)(2 * OFF + 1);
@@ -1326,24 +1331,29 @@ __global__ void __launch_bounds__(128) sat_y_async_kernel(const float *__restric
         const int xp = (int)(ln % (uint64_t)pm.px), zp = (int)(ln / (uint64_t)pm.px);
         mbase = idx3(0, reflect101(xp - pm.sx, pm.xd), reflect101(zp - pm.sz, pm.zd), pm.yd, pm.xd);
     }
-    // copy / store mapping: a warp instruction moves two lines of kSY samples
-    const int cy = lane & (kSY - 1), cj = lane >> 4;
+    // copy / store mapping: a warp instruction moves kLPI lines of
+    // min(kSY, 32) samples
+    const int cy0 = kSY < 32 ? (lane & (kSY - 1)) : lane, cj = kSY < 32 ? lane / kSY : 0;
     const int ntile = (n + kSY - 1) / kSY;
     const float rd = __frcp_rn(d);
     auto issue = [&](int t, int b) {
-        const int y = t * kSY + cy;
-        const int my = (refl && y < n) ? reflect101(y - pm.sy, pm.yd) : 0;
-        const float *pa = in + (line0 + cj) * (uint64_t)n + y;  // unreflected source of line cj
-        const float *ra = REF ? ref + (line0 + cj) * (uint64_t)n + y : nullptr;
-        const uint64_t step = 2 * (uint64_t)n;
+#pragma unroll
+        for (int h = 0; h < kSH; ++h) {
+            const int cy = cy0 + 32 * h;
+            const int y = t * kSY + cy;
+            const int my = (refl && y < n) ? reflect101(y - pm.sy, pm.yd) : 0;
+            const float *pa = in + (line0 + cj) * (uint64_t)n + y;  // unreflected source of line cj
+            const float *ra = REF ? ref + (line0 + cj) * (uint64_t)n + y : nullptr;
+            const uint64_t step = kLPI * (uint64_t)n;
 #pragma unroll 2
-        for (int jj = 0; jj < 16; ++jj, pa += step, ra += REF ? step : 0) {
-            const int j = 2 * jj + cj;
-            const uint64_t bj = __shfl_sync(0xffffffffu, mbase, j);
-            if (line0 + j < nlines && y < n) {
-                const uint64_t am = bj + (uint64_t)my;
-                cp_async4(&sm[w][b][0][j][cy], pm.on_in ? in + am : pa);
-                if (REF) cp_async4(&sm[w][b][NB - 1][j][cy], pm.on_ref ? ref + am : ra);
+            for (int jj = 0; jj < 32 / kLPI; ++jj, pa += step, ra += REF ? step : 0) {
+                const int j = kLPI * jj + cj;
+                const uint64_t bj = __shfl_sync(0xffffffffu, mbase, j);
+                if (line0 + j < nlines && y < n) {
+                    const uint64_t am = bj + (uint64_t)my;
+                    cp_async4(&sm[w][b][0][j][cy], pm.on_in ? in + am : pa);
+                    if (REF) cp_async4(&sm[w][b][NB - 1][j][cy], pm.on_ref ? ref + am : ra);
+                }
             }
         }
         cp_async_commit();
@@ -1392,13 +1402,17 @@ __global__ void __launch_bounds__(128) sat_y_async_kernel(const float *__restric
             }
         }
         __syncwarp();
-        const int yy = y0 + cy, i = yy - OFF;
-        if (yy < n && i >= 0 && i < n - OFF) {
-            float *q = out + (line0 + cj) * (uint64_t)n + i;
-            const uint64_t step = 2 * (uint64_t)n;
+#pragma unroll
+        for (int h = 0; h < kSH; ++h) {
+            const int cy = cy0 + 32 * h;
+            const int yy = y0 + cy, i = yy - OFF;
+            if (yy < n && i >= 0 && i < n - OFF) {
+                float *q = out + (line0 + cj) * (uint64_t)n + i;
+                const uint64_t step = kLPI * (uint64_t)n;
 #pragma unroll 4
-            for (int jj = 0; jj < 16; ++jj, q += step)
-                if (line0 + 2 * jj + cj < nlines) *q = T[2 * jj + cj][cy];
+                for (int jj = 0; jj < 32 / kLPI; ++jj, q += step)
+                    if (line0 + kLPI * jj + cj < nlines) *q = T[kLPI * jj + cj][cy];
+            }
         }
         __syncwarp();
     }
@@ -1971,9 +1985,9 @@ static void sat_axis_t(const float *in, const float *absref, float *out, int py,
     if (axis == 0) {
         const uint64_t nlines = (uint64_t)px * pz;
         if (absref)
-            sat_y_async_kernel<OFF, true><<<blocks_for(nlines, 128), 128, 0, s>>>(in, absref, out, py, nlines, pm);
+            sat_y_async_kernel<OFF, true><<<blocks_for(nlines, 32 * kSW), 32 * kSW, 0, s>>>(in, absref, out, py, nlines, pm);
         else
-            sat_y_async_kernel<OFF, false><<<blocks_for(nlines, 128), 128, 0, s>>>(in, absref, out, py, nlines, pm);
+            sat_y_async_kernel<OFF, false><<<blocks_for(nlines, 32 * kSW), 32 * kSW, 0, s>>>(in, absref, out, py, nlines, pm);
     } else {
         const uint64_t nlines = axis == 1 ? (uint64_t)py * pz : (uint64_t)py * px;
         const int n = axis == 1 ? px : pz;
