@@ -444,6 +444,7 @@ struct GradTaps {
     signed char dz[27], dx[27], dy[27];
 };
 
+template <int K>
 __global__ void __launch_bounds__(256) grad_mag_gather_kernel(ConvLevelArgs a, const uint64_t *__restrict__ xz_end,
                                                               const uint16_t *__restrict__ y_vec,
                                                               const float *__restrict__ D, GradTaps gt,
@@ -468,48 +469,48 @@ __global__ void __launch_bounds__(256) grad_mag_gather_kernel(ConvLevelArgs a, c
     const float *Drow = D + ((uint64_t)z * a.d.xn + (uint64_t)x) * (uint64_t)yn;
     const int nu = gt.nu;
     unsigned nstale = 0;
-    for (uint64_t base = b; base < e; base += 32 * kConvK) {
-        uint64_t ii[kConvK];
-        int yv[kConvK];
-        bool has[kConvK];
+    for (uint64_t base = b; base < e; base += 32 * K) {
+        uint64_t ii[K];
+        int yv[K];
+        bool has[K];
         bool inner = rows_in;
 #pragma unroll
-        for (int j = 0; j < kConvK; ++j) {
+        for (int j = 0; j < K; ++j) {
             ii[j] = base + (uint64_t)(j * 32 + lane);
             has[j] = ii[j] < e;
             yv[j] = has[j] ? (int)y_vec[ii[j]] : 1;
             inner = inner && yv[j] - 1 >= 0 && yv[j] + 1 < yn;
         }
-        float g[3][kConvK];
+        float g[3][K];
 #pragma unroll
         for (int d = 0; d < 3; ++d)
 #pragma unroll
-            for (int j = 0; j < kConvK; ++j) g[d][j] = 0.0f;
+            for (int j = 0; j < K; ++j) g[d][j] = 0.0f;
         if (inner) {
             // one load per cell, every direction with a weight there in turn:
             // each direction still sums its taps in memory order
             for (int c = 0; c < nu; ++c) {
                 const long long o = so[c];
                 const float w0 = sw[c][0], w1 = sw[c][1], w2 = sw[c][2];
-                float v[kConvK];
+                float v[K];
 #pragma unroll
-                for (int j = 0; j < kConvK; ++j) v[j] = __ldg(Drow + yv[j] + o);
+                for (int j = 0; j < K; ++j) v[j] = __ldg(Drow + yv[j] + o);
                 if (w0 != 0.0f) {
 #pragma unroll
-                    for (int j = 0; j < kConvK; ++j) g[0][j] = __fadd_rn(g[0][j], __fmul_rn(v[j], w0));
+                    for (int j = 0; j < K; ++j) g[0][j] = __fadd_rn(g[0][j], __fmul_rn(v[j], w0));
                 }
                 if (w1 != 0.0f) {
 #pragma unroll
-                    for (int j = 0; j < kConvK; ++j) g[1][j] = __fadd_rn(g[1][j], __fmul_rn(v[j], w1));
+                    for (int j = 0; j < K; ++j) g[1][j] = __fadd_rn(g[1][j], __fmul_rn(v[j], w1));
                 }
                 if (w2 != 0.0f) {
 #pragma unroll
-                    for (int j = 0; j < kConvK; ++j) g[2][j] = __fadd_rn(g[2][j], __fmul_rn(v[j], w2));
+                    for (int j = 0; j < K; ++j) g[2][j] = __fadd_rn(g[2][j], __fmul_rn(v[j], w2));
                 }
             }
         }
 #pragma unroll
-        for (int j = 0; j < kConvK; ++j) {
+        for (int j = 0; j < K; ++j) {
             if (!has[j]) continue;
             float gv[3] = {g[0][j], g[1][j], g[2][j]};
             bool redo = !inner;
@@ -703,7 +704,12 @@ void filter_gradient_magnitude(const Geom &g, const uint64_t *xz_end, const uint
             APRB_CHECK_LAUNCH();
         }
         APRB_PROF("grad_mag_gather", s);
-        grad_mag_gather_kernel<<<blocks_for(rows * 32, 256), 256, 0, s>>>(a, xz_end, y_vec, D, gt, out, stale);
+        // four particles per lane for the few taps of central differences,
+        // two for the 26 cells of Sobel (fewer registers, more warps)
+        if (gt.nu <= 8)
+            grad_mag_gather_kernel<4><<<blocks_for(rows * 32, 256), 256, 0, s>>>(a, xz_end, y_vec, D, gt, out, stale);
+        else
+            grad_mag_gather_kernel<2><<<blocks_for(rows * 32, 256), 256, 0, s>>>(a, xz_end, y_vec, D, gt, out, stale);
         count_launch();
         APRB_CHECK_LAUNCH();
     }
