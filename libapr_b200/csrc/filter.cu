@@ -321,7 +321,7 @@ __device__ __forceinline__ T gather_tap(const T *__restrict__ D, const ConvLevel
 }
 
 // conv_gather: one warp per row of level l; each lane takes kConvK particles
-// of the row.  A z-slice of the stencil sits in registers; the taps are
+// of the row (two in FP64, where four cost more in registers than they save).  A z-slice of the stencil sits in registers; the taps are
 // summed in the stencil's memory order without contraction
 // (run_convolution_pencil, APRFilter.hpp:706-736).  Particles whose window
 // stays inside the level read D directly; a NaN sum (a sentinel was read) is
@@ -333,6 +333,7 @@ __global__ void __launch_bounds__(256) conv_gather_kernel(ConvLevelArgs a, const
                                                           const uint16_t *__restrict__ rl_in,
                                                           unsigned long long *stale) {
     constexpr int S = 2 * R + 1, S3 = S * S * S;
+    constexpr int K = sizeof(T) == 8 ? 2 : kConvK;  // particles per lane: two in FP64
     __shared__ T st[S3];
     for (int k = threadIdx.x; k < S3; k += blockDim.x) st[k] = stencil[k];
     __syncthreads();
@@ -346,21 +347,21 @@ __global__ void __launch_bounds__(256) conv_gather_kernel(ConvLevelArgs a, const
     // the S x S neighbour rows lie inside the level (warp-uniform)
     const bool rows_in = z - R >= 0 && z + R < a.d.zn && x - R >= 0 && x + R < a.d.xn;
     unsigned nstale = 0;
-    for (uint64_t base = b; base < e; base += 32 * kConvK) {
-        uint64_t ii[kConvK];
-        int yv[kConvK];
-        bool has[kConvK];
+    for (uint64_t base = b; base < e; base += 32 * K) {
+        uint64_t ii[K];
+        int yv[K];
+        bool has[K];
         bool inner = rows_in;
 #pragma unroll
-        for (int j = 0; j < kConvK; ++j) {
+        for (int j = 0; j < K; ++j) {
             ii[j] = base + (uint64_t)(j * 32 + lane);
             has[j] = ii[j] < e;
             yv[j] = has[j] ? (int)y_vec[ii[j]] : R;
             inner = inner && yv[j] - R >= 0 && yv[j] + R < yn;
         }
-        T acc[kConvK];
+        T acc[K];
 #pragma unroll
-        for (int j = 0; j < kConvK; ++j) acc[j] = T(0);
+        for (int j = 0; j < K; ++j) acc[j] = T(0);
         if (inner) {
 #pragma unroll 1
             for (int iz = 0; iz < S; ++iz) {
@@ -370,23 +371,23 @@ __global__ void __launch_bounds__(256) conv_gather_kernel(ConvLevelArgs a, const
                 // each particle's tap pointers step by one row per ix; the
                 // y taps are immediate offsets from them
                 const T *row0 = D + ((uint64_t)(z + iz - R) * a.d.xn + (uint64_t)(x - R)) * (uint64_t)yn - R;
-                const T *p[kConvK];
+                const T *p[K];
 #pragma unroll
-                for (int j = 0; j < kConvK; ++j) p[j] = row0 + yv[j];
+                for (int j = 0; j < K; ++j) p[j] = row0 + yv[j];
 #pragma unroll
                 for (int ix = 0; ix < S; ++ix) {
 #pragma unroll
                     for (int iy = 0; iy < S; ++iy)
 #pragma unroll
-                        for (int j = 0; j < kConvK; ++j)
+                        for (int j = 0; j < K; ++j)
                             acc[j] = VT<T>::add(acc[j], VT<T>::mul(__ldg(p[j] + iy), stv[ix * S + iy]));
 #pragma unroll
-                    for (int j = 0; j < kConvK; ++j) p[j] += yn;
+                    for (int j = 0; j < K; ++j) p[j] += yn;
                 }
             }
         }
 #pragma unroll
-        for (int j = 0; j < kConvK; ++j) {
+        for (int j = 0; j < K; ++j) {
             if (!has[j]) continue;
             T val = acc[j];
             if (!inner || val != val) {
