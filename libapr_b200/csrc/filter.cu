@@ -321,7 +321,8 @@ __device__ __forceinline__ T gather_tap(const T *__restrict__ D, const ConvLevel
 }
 
 // conv_gather: one warp per row of level l; each lane takes kConvK particles
-// of the row (two in FP64, where four cost more in registers than they save).  A z-slice of the stencil sits in registers; the taps are
+// of the row (two in FP64, where four cost more in registers than they
+// save).  A z-slice of the stencil sits in registers; the taps are
 // summed in the stencil's memory order without contraction
 // (run_convolution_pencil, APRFilter.hpp:706-736).  Particles whose window
 // stays inside the level read D directly; a NaN sum (a sentinel was read) is
