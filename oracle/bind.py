@@ -130,6 +130,9 @@ def ref(fast=False):
                                                                            C.POINTER(C.c_float), C.POINTER(C.c_float)]
         R.ref_get_apr_auto.argtypes = [C.POINTER(C.c_uint16), C.c_int, C.c_int, C.c_int, C.POINTER(OrcParams),
                                        C.c_int, C.c_int, C.POINTER(vp), C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        R.ref_get_apr_by_block_auto.argtypes = [C.POINTER(C.c_uint16), C.c_int, C.c_int, C.c_int,
+                                                C.POINTER(OrcParams), C.c_int, C.c_int, C.c_int, C.c_int,
+                                                C.POINTER(vp), C.POINTER(C.c_float), C.POINTER(C.c_float)]
         _ref[fast] = R
     return _ref[fast]
 
@@ -598,6 +601,21 @@ def ref_get_apr_auto(img, params, image_type=1, nthreads=1):
     gt, st = C.c_float(), C.c_float()
     e = R.ref_get_apr_auto(_ptr(img, C.c_uint16), y, x, z, C.byref(params), image_type, nthreads, C.byref(h),
                            C.byref(gt), C.byref(st))
+    if e != 0:
+        return e, None, None, None
+    return 0, RefAPR(h.value, img.shape), gt.value, st.value
+
+
+def ref_get_apr_by_block_auto(img, params, image_type, z_block, ghost, nthreads=1):
+    """The reference's blocked converter with auto_parameters on: (status,
+    RefAPR, grad_th, sigma_th) of the last tile."""
+    R = ref()
+    img = np.ascontiguousarray(img, dtype=np.uint16)
+    z, x, y = img.shape
+    h = C.c_void_p()
+    gt, st = C.c_float(), C.c_float()
+    e = R.ref_get_apr_by_block_auto(_ptr(img, C.c_uint16), y, x, z, C.byref(params), image_type, z_block, ghost,
+                                    nthreads, C.byref(h), C.byref(gt), C.byref(st))
     if e != 0:
         return e, None, None, None
     return 0, RefAPR(h.value, img.shape), gt.value, st.value

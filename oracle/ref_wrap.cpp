@@ -346,6 +346,39 @@ int ref_get_apr_auto(const uint16_t *img, int y, int x, int z, const orc_params 
     return 0;
 }
 
+/* The blocked converter with par.auto_parameters = true: every tile chooses
+ * its thresholds (APRConverterBatch.hpp:243-247) and the APR keeps the last
+ * tile's, read back from APR::get_apr_parameters. */
+int ref_get_apr_by_block_auto(const uint16_t *img, int y, int x, int z, const orc_params *p, int image_type,
+                              int zblock, int ghost, int nthreads, void **out, float *grad_th, float *sigma_th) {
+    OmpThreads th(nthreads);
+    *out = nullptr;
+    PixelData<uint16_t> in(y, x, z);
+    std::memcpy(in.mesh.begin(), img, sizeof(uint16_t) * (size_t)y * x * z);
+    RefHandle *h = new RefHandle();
+    try {
+        if (image_type == 1) {
+            BlockConverter<uint16_t> c;
+            set_params(c.par, p);
+            c.par.auto_parameters = true;
+            c.run(h->apr, in, zblock, ghost);
+        } else {
+            BlockConverter<float> c;
+            set_params(c.par, p);
+            c.par.auto_parameters = true;
+            c.run(h->apr, in, zblock, ghost);
+        }
+    } catch (std::invalid_argument &) {
+        delete h;
+        return 2;
+    }
+    const APRParameters par = h->apr.get_apr_parameters();
+    *grad_th = par.grad_th;
+    *sigma_th = par.sigma_th;
+    *out = h;
+    return 0;
+}
+
 void ref_free(void *hv) { delete (RefHandle *)hv; }
 
 void ref_apr_info(void *hv, int *l_min, int *l_max, uint64_t *n_level_xz, uint64_t *n_xz, uint64_t *P, float *offset) {

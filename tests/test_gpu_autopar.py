@@ -123,3 +123,22 @@ def test_blocked_converter_auto_parameters():
     c = apr2.get_apr_parameters()
     assert c.grad_th > 0 and c.sigma_th > 0
     assert f32_equal(many.par.grad_th, c.grad_th) and f32_equal(many.par.sigma_th, c.sigma_th)
+
+
+@ref_missing
+@pytest.mark.parametrize("shape,z_block,ghost", [((64, 72, 80), 24, 8), ((60, 64, 64), 16, 4)])
+def test_blocked_converter_auto_parameters_near_reference(shape, z_block, ghost):
+    """Per-tile automatic parameters of the blocked converter against the
+    reference's APRConverterBatch with auto_parameters on: the last tile's
+    thresholds, which both APRs keep (tilings the reference keeps in bounds)."""
+    assert B.block_tiling_in_bounds(shape, z_block, ghost)
+    img = volume(shape, 30, 9)
+    e, _, rg, rs = B.ref_get_apr_by_block_auto(img, oracle_params(), 1, z_block, ghost, nthreads=1)
+    assert e == 0
+    conv = A.APRConverterBatch("uint16", z_block_size=z_block, ghost_z=ghost)
+    conv.par = lib_params(auto_parameters=True)
+    apr = A.APR()
+    assert conv.get_apr(apr, img)
+    used = apr.get_apr_parameters()
+    assert abs(used.grad_th - rg) <= LI_REL_TOL * abs(rg) and abs(used.sigma_th - rs) <= LI_REL_TOL * abs(rs), \
+        (used.grad_th, rg, used.sigma_th, rs)
