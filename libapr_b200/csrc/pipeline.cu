@@ -1302,13 +1302,13 @@ __global__ void __launch_bounds__(kYWarps * 32) sat_y_kernel(const float *__rest
 // The same y box mean with the samples staged by cp.async one tile ahead of
 // the recurrence: a warp owns 32 lines and walks them in tiles of kSY
 // samples, so no registers hold the prefetch and more warps stay resident.
-// 32-sample tiles (a warp's copies and stores are 128-byte runs of a line)
-// in 2-warp blocks keep the static shared memory under 48 KB.
+// 32-sample tiles (a warp's copies and stores are 128-byte runs of a line),
+// one warp per block.
 // In tiles that touch neither end of the line the recurrence runs fully
 // unrolled (the window shift becomes register renaming).  REF: the input is
 // |in - ref| (the second pass of each window).
 constexpr int kSY = 32;
-constexpr int kSW = 2;                         // warps per block
+constexpr int kSW = 1;                         // warps per block
 constexpr int kSH = kSY >= 32 ? kSY / 32 : 1;   // y samples per lane and line in a copy
 constexpr int kLPI = kSY >= 32 ? 1 : 32 / kSY;  // lines per warp copy instruction
 
