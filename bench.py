@@ -38,7 +38,6 @@ AMP = (500.0, 6000.0)
 BG = 100.0
 PARAMS = dict(lambda_=3.0, rel_error=0.1, Ip_th=0.0, sigma_th=50.0, grad_th=10.0)
 METRIC = "get_apr GVox/s + APR conv Gpart/s vs HBM roofline; RL time-to-1e-3 learned vs plain"
-CPU_SLAB_Z = 64  # bounded CPU sample: z-slab of the same volume
 
 
 def peaks():
@@ -155,65 +154,119 @@ def algorithmic_bytes(stage, N, Nd, P, T, its=2):
     }.get(stage)
 
 
-def cpu_baseline(host_img, image_type, steps=2):
+def workload_config(image_type, P, world):
+    """The workload description both arms print (the reference arm converts
+    the rank-0 volume of the same generator and parameters)."""
+    z, x, y = SHAPE
+    return {"workload": "get_apr + sample_image, uint16 %dx%dx%d (y,x,z) blob volume, 60000 blobs per "
+                        "2048x2048x512, one volume per process" % (y, x, z),
+            "image_type": image_type, **PARAMS, "particles": P,
+            "l2": "input 4 GiB > L2, no flush needed",
+            "parallelism": "independent volume per GPU" if world > 1 else "one volume"}
+
+
+def cpu_baseline(host_img, image_type):
     """The reference's own CPU get_apr + sample_image (oracle/_ref, Release
-    flags) on a z-slab of the volume, all host threads."""
+    flags -O3 -ffast-math) on the whole volume the GPU converted, all host
+    threads, one run."""
     from oracle import bind as B
     if not B.ref_available(fast=True):
         return None
-    slab = np.ascontiguousarray(host_img[:CPU_SLAB_Z])
     p = B.make_params(**PARAMS)
-    ts = []
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        e, r = B.ref_get_apr(slab, p, image_type, staged=False, fast=True)
-        if e != 0:
-            return {"value": None, "unit": "GVox/s", "cores": os.cpu_count(), "kind": "reference",
-                    "sample": "reference get_apr failed with status %d on the slab" % e}
-        r.sample(slab)
-        ts.append(time.perf_counter() - t0)
-        del r
-    t = min(ts)
-    return {"value": slab.size / t / 1e9, "unit": "GVox/s", "cores": os.cpu_count(), "kind": "reference",
-            "sample": "get_apr + sample_image on a %dx%dx%d z-slab of the volume, best of %d" % (
-                slab.shape[0], slab.shape[1], slab.shape[2], steps), "seconds": t}
+    t0 = time.perf_counter()
+    e, r = B.ref_get_apr(host_img, p, image_type, staged=False, fast=True)
+    if e != 0:
+        return {"value": None, "unit": "GVox/s", "cores": os.cpu_count(), "kind": "reference",
+                "sample": "reference get_apr failed with status %d" % e}
+    r.sample(host_img)
+    t = time.perf_counter() - t0
+    del r
+    return {"value": host_img.size / t / 1e9, "unit": "GVox/s", "cores": os.cpu_count(), "kind": "reference",
+            "sample": "get_apr + sample_image on the whole %dx%dx%d volume the GPU converted, one run"
+                      % host_img.shape[::-1], "seconds": t}
+
+
+def parity_full_volume(A, host_img, dev_img, image_type, rel_tol=1e-5):
+    """Outside the timed region: the GPU's get_apr on the benchmark volume
+    against the reference's own CPU code built with strict IEEE flags
+    (oracle/_ref/libaprref.so) on the same bytes -- linear access structure,
+    uint16 intensities, the down-sampled level of every cell (a differing
+    level is a flip) -- and the number of cells whose level argument lies
+    within rel_tol of a level boundary (LocalParticleCellSet.hpp:129-171)."""
+    from oracle import bind as B
+    if not B.ref_available():
+        return {"skipped": "oracle/_ref/libaprref.so not built"}
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = None
+    if avail is not None and avail < 40e9:
+        return {"skipped": "%.0f GB of host memory available, the reference run needs about 40" % (avail / 1e9)}
+    conv = A.APRConverter(image_type)
+    conv.par = lib_params()
+    conv.keep_intermediates(True)
+    apr = A.APR()
+    conv.get_apr(apr, dev_img)
+    near, active = conv.level_margins(rel_tol)
+    z, x, y = host_img.shape
+    ds = ((z + 1) // 2, (x + 1) // 2, (y + 1) // 2)
+    it = 1 if image_type == "uint16" else 0
+    t0 = time.perf_counter()
+    e, ref = B.ref_get_apr(host_img, B.make_params(**PARAMS), it, staged=True)
+    t_ref = time.perf_counter() - t0
+    if e != 0:
+        return {"reference_status": e}
+    flips = int(np.count_nonzero(conv.intermediate(6, ds) != ref.intermediate(6)))
+    acc = ref.access()
+    lx, xe, yv = apr.linear_access()
+    structure = bool(np.array_equal(lx, acc.level_xz) and np.array_equal(xe, acc.xz_end)
+                     and np.array_equal(yv, acc.y_vec))
+    del lx, xe, yv
+    P = acc.P
+    del acc
+    parts = A.ParticleData().sample_image(apr, dev_img).data
+    same_parts = bool(np.array_equal(parts[:P], ref.sample(host_img)[:P]))
+    del parts, ref
+    apr._free()
+    return {"reference": "oracle/_ref/libaprref.so: the reference's get_apr_cpu + sample_image compiled from "
+                         "its headers with strict IEEE flags, on the same bytes",
+            "structure_equal": structure, "intensities_equal": same_parts, "level_flips": flips,
+            "near_threshold_cells": near, "cells_at_level_1_or_more": active, "rel_tol": rel_tol,
+            "particles": P, "reference_seconds": t_ref}
 
 
 def run_reference(args):
-    """--impl reference: the reference CPU implementation, rank 0 only."""
+    """--impl reference: the reference's own CPU implementation (LibAPR's
+    get_apr_cpu + sample_image compiled from its headers at its Release flags,
+    oracle/_ref/libaprref_fast.so, OpenMP on every host core) on the rank-0
+    volume of the benchmark, rendered on the host by the generator's CPU twin
+    (the same bytes the device generator writes); rank 0 only.  Nothing of
+    the library is loaded."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
     from oracle import bind as B
-    import libapr_b200.synth as S
     if not B.ref_available(fast=True):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref was not built (needs the LibAPR tree)"}))
         return 0
-    slab_shape = (CPU_SLAB_Z, SHAPE[1], SHAPE[2])
-    frac = CPU_SLAB_Z / SHAPE[0]
-    img = None
-    try:
-        import torch
-        import libapr_b200 as A
-        if torch.cuda.is_available():
-            d = torch.empty(slab_shape, dtype=torch.int16, device="cuda")
-            A.synth_blobs_device(d, int(BLOBS * frac), SIGMA, AMP, BG, seed=1000)
-            img = d.cpu().numpy().view(np.uint16)
-    except Exception:
-        img = None
-    if img is None:
-        img = S.blob_volume(slab_shape, int(BLOBS * frac), SIGMA, AMP, BG, seed=1000)
+    t0 = time.perf_counter()
+    img = B.blob_volume_cpu(SHAPE, BLOBS, SIGMA, AMP, BG, volume_seed(0))
+    t_gen = time.perf_counter() - t0
     p = B.make_params(**PARAMS)
-    times = []
+    it = 1 if args.image_type == "uint16" else 0
+    times, P = [], None
     for i in range(args.warmup + args.steps):
         t0 = time.perf_counter()
-        e, r = B.ref_get_apr(img, p, 1 if args.image_type == "uint16" else 0, staged=False, fast=True)
+        e, r = B.ref_get_apr(img, p, it, staged=False, fast=True)
         if e != 0:
             print(json.dumps({"impl": "reference", "unavailable": "reference get_apr failed with status %d" % e}))
             return 0
         r.sample(img)
         dt = time.perf_counter() - t0
+        if P is None:
+            P = r.access().P
         del r
         if i >= args.warmup:
             times.append(dt)
@@ -222,13 +275,13 @@ def run_reference(args):
     line = {"metric": METRIC, "value": v, "unit": "GVox/s", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32" if args.image_type == "float" else "u16", "data": "synthetic",
-            "config": {"workload": "get_apr + sample_image, uint16 2048x2048x512 blob volume (each step a "
-                                   "2048x2048x%d z-slab of it)" % CPU_SLAB_Z, "image_type": args.image_type,
-                       **PARAMS},
+            "config": workload_config(args.image_type, P, 1),
             "impl": "reference",
             "cpu_baseline": {"value": v, "unit": "GVox/s", "cores": os.cpu_count(), "kind": "reference",
-                             "sample": "z-slab %s per step, LibAPR CPU get_apr_cpu + sample_image at Release "
-                                       "flags (-O3 -ffast-math), OpenMP" % (slab_shape,)},
+                             "sample": "the whole %dx%dx%d volume per step: LibAPR's CPU get_apr_cpu + "
+                                       "sample_image at its Release flags (-O3 -ffast-math), OpenMP on all host "
+                                       "cores; volume rendered on the host (%.1f s) by the generator's CPU twin, "
+                                       "bit-identical to the device generator" % (SHAPE[2], SHAPE[1], SHAPE[0], t_gen)},
             "e2e": {"value": v, "unit": "GVox/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -745,20 +798,20 @@ def main():
     te = max_over_ranks((time.perf_counter() - t0) / args.steps, world, "cuda")
     e2e = {"value": N * world / te / 1e9, "unit": "GVox/s", "h2d_bytes_per_step": 4 * N,
            "d2h_bytes_per_step": 2 * P, "ms_per_step": te * 1e3}
-    cpu = None
-    if not args.no_cpu and world == 1:
-        cpu = cpu_baseline(host.numpy().view(np.uint16), it_code)
+    cpu, parity = None, None
+    if not args.no_cpu and world == 1 and shape == SHAPE:
+        hv = host.numpy().view(np.uint16)
+        parity = parity_full_volume(A, hv, img, args.image_type)
+        cpu = cpu_baseline(hv, it_code)
     if rank == 0:
         line = {"metric": METRIC, "value": N * world / (ms_all / 1e3) / 1e9, "unit": "GVox/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_all, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32" if it_code == 0 else "u16",
                 "data": "synthetic",
-                "config": {"workload": "get_apr + sample_image, uint16 %dx%dx%d (y,x,z) blob volume, "
-                                       "60000 blobs per 2048x2048x512, per GPU" % (y, x, z),
-                           "image_type": args.image_type, **PARAMS, "particles": P,
-                           "l2": "input 4 GiB > L2, no flush needed",
-                           "parallelism": "independent volume per GPU" if world > 1 else "1 GPU"},
+                "config": workload_config(args.image_type, P, world),
                 "gpu_launches": int(launches), "e2e": e2e, "cpu_baseline": cpu, **out, **conv_res}
+        if parity:
+            line["parity"] = parity
         if auto_res:
             line["auto_parameters"] = auto_res
         if batch_res:

@@ -134,6 +134,14 @@ aprb_status aprb_get_apr_batch_device(aprb_converter *c, const aprb_params *p, i
                                       aprb_apr **outs);
 /* copy one APRB_STAGE_* intermediate of the last get_apr to the host (n = element count) */
 aprb_status aprb_converter_intermediate(const aprb_converter *c, int stage, float *dst, size_t n);
+/* Level-decision margins of the last get_apr (needs aprb_converter_keep_intermediates).
+ * computeLevels (LocalParticleCellSet.hpp:129-171) gives a down-sampled cell the level
+ * floor(log2(v)), v = (grad / scale) * 2^l_max * min(dx, dy, dz) / E after applyParameters
+ * (APRConverter.hpp:250-297); a computation of v that differs by a relative rel_tol can
+ * decide another level only where v lies within rel_tol of a power of two 2^k (k >= 1).
+ * near_boundary receives the number of such cells, active the number with v >= 1. */
+aprb_status aprb_converter_level_margins(aprb_converter *c, double rel_tol, uint64_t *near_boundary,
+                                         uint64_t *active);
 
 /* --- automatic parameters (AutoParameters.hpp) ----------------------------------
  * With aprb_params.auto_parameters set, get_apr (APRConverter.hpp:556-561) and each
@@ -183,18 +191,21 @@ aprb_status aprb_sample_image_by_block_device(const aprb_apr *a, const uint16_t 
 
 /* Particle sampling that allocates no device memory.  No counterpart in the
  * reference.  For callers that cannot allocate GPU memory while they run:
- * code replayed inside a captured CUDA graph, real-time acquisition loops and
- * plugin hosts that own a fixed device-memory budget and forbid cudaMalloc
- * and cudaFree after start-up.  It takes the APR's device arrays (xz_end,
- * y_vec, e.g. from aprb_apr_device_arrays) and the image dimensions (y, x, z),
- * and keeps its down-sampling pyramid in one 64 MiB buffer that the library
- * reserves in device memory at load time (every GPU the library is loaded on
- * holds it until the process exits).  Volumes whose pyramid below l_max needs
- * more than 32 Mi uint16 values (about 2.2e8 voxels) are rejected with
+ * real-time acquisition loops and plugin hosts that own a fixed device-memory
+ * budget and forbid cudaMalloc and cudaFree after start-up.  It takes the
+ * APR's device arrays (xz_end, y_vec, e.g. from aprb_apr_device_arrays) and
+ * the image dimensions (y, x, z), and keeps its down-sampling pyramid in one
+ * 64 MiB file-scope device buffer of the library.  The buffer is reserved on
+ * a device when the library's module is first used there (at library load
+ * only with eager module loading, CUDA_MODULE_LOADING=EAGER) and stays until
+ * the process exits.  Volumes whose pyramid below l_max needs more than
+ * 32 Mi uint16 values (about 2.2e8 voxels) are rejected with
  * APRB_ERR_INVALID_ARGUMENT.  The first call on a device looks the buffer up
- * for that device; make that first call before any stream capture.  All
- * calls share the buffer: calls that overlap on the GPU (other streams,
- * other host threads) race and must be serialised by the caller. */
+ * for that device (which may load the module); make that first call before
+ * any stream capture.  Later calls outside stream capture look it up again,
+ * so a device reset (which reloads the module) is picked up.  All calls share
+ * the buffer: calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialised by the caller. */
 aprb_status aprb_sample_image_noalloc(const uint64_t *xz_end_dev, const uint16_t *y_vec_dev, int y_num, int x_num,
                                       int z_num, const uint16_t *img_dev, uint16_t *parts_dev, void *stream);
 

@@ -251,6 +251,16 @@ class APRConverter:
         check(lib().aprb_converter_intermediate(self._h, int(stage), _ptr(out), out.size))
         return out
 
+    def level_margins(self, rel_tol=1e-5):
+        """(near_boundary, active) of the last get_apr (needs keep_intermediates):
+        down-sampled cells whose level argument (grad / scale) * 2^l_max *
+        min(dx, dy, dz) / E lies within rel_tol of a power of two (where a level
+        decision of computeLevels, LocalParticleCellSet.hpp:129-171, can flip
+        under a relative error rel_tol), and cells whose argument is >= 1."""
+        n, a = C.c_uint64(), C.c_uint64()
+        check(lib().aprb_converter_level_margins(self._h, float(rel_tol), C.byref(n), C.byref(a)))
+        return int(n.value), int(a.value)
+
 
 class APRConverterBatch(APRConverter):
     """APRConverterBatch<ImageType> (src/algorithm/APRConverterBatch.hpp:32-98):

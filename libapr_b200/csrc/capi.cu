@@ -188,6 +188,9 @@ struct aprb_converter {
     LisBuffers lisb;
     AutoParBuffers autop;
     bool have = false;
+    aprb_params last_par{};  // parameters of the last get_apr after the automatic ones
+    int last_l_max = 0;
+    DevBuf margins;
 };
 
 // reconstruct_constant / reconstruct_level on device buffers
@@ -487,6 +490,8 @@ void run_get_apr(aprb_converter *c, aprb_params p, const uint16_t *img, int yn, 
     }
     if (L > 2) launch_pulling_scheme(g, pm, s);
     build_structure(c, p, pm, a, s);
+    c->last_par = p;
+    c->last_l_max = L;
     c->dims[0] = yn;
     c->dims[1] = xn;
     c->dims[2] = zn;
@@ -713,6 +718,31 @@ aprb_status aprb_converter_intermediate(const aprb_converter *c, int stage, floa
         } else {
             APRB_CUDA(cudaMemcpy(dst, src, cnt * sizeof(float), cudaMemcpyDeviceToHost));
         }
+    });
+}
+
+aprb_status aprb_converter_level_margins(aprb_converter *c, double rel_tol, uint64_t *near_boundary,
+                                         uint64_t *active) {
+    return guarded([&] {
+        ARG_CHECK(c && near_boundary && active, "null argument");
+        ARG_CHECK(rel_tol >= 0.0, "rel_tol must be >= 0");
+        ARG_CHECK(c->have && c->keep, "no intermediates kept (enable aprb_converter_keep_intermediates first)");
+        require_device();
+        const int y = c->dims[0], x = c->dims[1], z = c->dims[2];
+        const uint64_t nd = (uint64_t)((y + 1) / 2) * ((x + 1) / 2) * ((z + 1) / 2);
+        cudaStream_t s = cudaStreamPerThread;
+        unsigned long long *cnt = c->margins.as_on<unsigned long long>(2, s);
+        if (c->image_type == APRB_IMAGE_U16)
+            launch_level_margins<uint16_t>((const uint16_t *)c->grad.p, (const float *)c->lis.p, nd, c->last_par,
+                                           c->last_l_max, rel_tol, cnt, s);
+        else
+            launch_level_margins<float>((const float *)c->grad.p, (const float *)c->lis.p, nd, c->last_par,
+                                        c->last_l_max, rel_tol, cnt, s);
+        unsigned long long h[2];
+        APRB_CUDA(cudaMemcpyAsync(h, cnt, sizeof(h), cudaMemcpyDeviceToHost, s));
+        APRB_CUDA(cudaStreamSynchronize(s));
+        *near_boundary = h[0];
+        *active = h[1];
     });
 }
 

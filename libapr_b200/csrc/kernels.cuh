@@ -44,6 +44,10 @@ void launch_local_intensity_scale(const float *ids, float *lis, int yd, int xd, 
 template <typename IT>
 void launch_levels(IT *grad, float *lis, const float *ids, uint64_t nd, const float *d_offset, const aprb_params &p,
                    int apr_l_max, int top_level, uint8_t *level, uint8_t *status, int keep, cudaStream_t s);
+// cells whose level argument lies within rel of a level boundary, and cells at level >= 1
+template <typename IT>
+void launch_level_margins(const IT *grad, const float *lis, uint64_t nd, const aprb_params &p, int apr_l_max,
+                          double rel, unsigned long long *counts, cudaStream_t s);
 
 // ---- structure.cu
 // Particle-cell pyramid: status[l] for pct levels l_min..l_max-1 (dims of

@@ -1,7 +1,8 @@
 // aprb_sample_image_noalloc: particle sampling for callers that must not
-// allocate device memory while they run (graph replay, real-time loops,
+// allocate device memory while they run (real-time acquisition loops, plugin
 // hosts with a fixed device-memory budget).  The down-sampling pyramid lives
-// in a file-scope device array reserved when the library is loaded; no
+// in a file-scope device array, reserved on a device when this module is
+// first used there (at library load only with eager module loading); no
 // cudaMalloc / cudaFree is called on this path.
 #include <mutex>
 
@@ -19,9 +20,11 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 uint16_t *g_scratch_ptr[kMaxDevices] = {};
 
-// Device address of the scratch array for the current device, looked up
-// once per device with that device current.
-uint16_t *scratch_for_current_device() {
+// Device address of the scratch array for the current device, looked up with
+// that device current.  A call outside stream capture looks it up again (a
+// device reset reloads the module at another address); a call under capture
+// uses the address of the last call on the device.
+uint16_t *scratch_for_current_device(bool refresh) {
     int dev = 0;
     APRB_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kMaxDevices) {
@@ -29,7 +32,7 @@ uint16_t *scratch_for_current_device() {
         throw Error{APRB_ERR_INVALID_ARGUMENT};
     }
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch_ptr[dev]) {
+    if (!g_scratch_ptr[dev] || refresh) {
         void *p = nullptr;
         APRB_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
         g_scratch_ptr[dev] = (uint16_t *)p;
@@ -59,7 +62,9 @@ extern "C" aprb_status aprb_sample_image_noalloc(const uint64_t *xz_end_dev, con
                       " uint16 values, more than the fixed scratch of " + std::to_string(kNoAllocScratchElems));
             return APRB_ERR_INVALID_ARGUMENT;
         }
-        uint16_t *scratch = scratch_for_current_device();
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        APRB_CUDA(cudaStreamIsCapturing((cudaStream_t)stream, &cs));
+        uint16_t *scratch = scratch_for_current_device(cs == cudaStreamCaptureStatusNone);
         launch_sample_scratch(g, xz_end_dev, y_vec_dev, img_dev, parts_dev, scratch, (cudaStream_t)stream);
         return APRB_OK;
     } catch (const Error &e) {

@@ -2129,6 +2129,56 @@ void launch_levels(IT *grad, float *lis, const float *ids, uint64_t nd, const fl
     APRB_CHECK_LAUNCH();
 }
 
+// ---------------------------------------------------------------------------
+// Level-decision margins (diagnostic, outside get_apr): the level of a ds cell
+// is floor(log2(v)) for v = (grad / scale) * mult >= 1 (level_of above,
+// LocalParticleCellSet.hpp:129-171), so a computation of v that is off by a
+// relative r can decide another level only where v lies within r of a power
+// of two 2^k, k >= 1.  Counts those cells and the cells with v >= 1, from the
+// gradient and scale after applyParameters.
+template <typename IT>
+__global__ void level_margin_kernel(const IT *__restrict__ grad, const float *__restrict__ lis, uint64_t nd,
+                                    float mult, double rel, unsigned long long *counts) {
+    unsigned long long near = 0, active = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nd;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float q = (float)grad[i] / lis[i];
+        const double v = (double)(q * mult);
+        if (!(v >= 1.0)) continue;
+        ++active;
+        int e;
+        frexp(v, &e);  // v = m 2^e, m in [0.5, 1): the nearest powers are 2^(e-1) and 2^e
+        const double lo = ldexp(1.0, e - 1), hi = ldexp(1.0, e);
+        if ((e - 1 >= 1 && v - lo <= rel * lo) || hi - v <= rel * hi) ++near;
+    }
+    for (int o = 16; o; o >>= 1) {
+        near += __shfl_down_sync(0xffffffffu, near, o);
+        active += __shfl_down_sync(0xffffffffu, active, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (near | active)) {
+        atomicAdd(&counts[0], near);
+        atomicAdd(&counts[1], active);
+    }
+}
+
+template <typename IT>
+void launch_level_margins(const IT *grad, const float *lis, uint64_t nd, const aprb_params &p, int apr_l_max,
+                          double rel, unsigned long long *counts, cudaStream_t s) {
+    const float mxz = p.dz < p.dx ? p.dz : p.dx;
+    const float min_dim = mxz < p.dy ? mxz : p.dy;
+    const float level_factor = (float)(std::pow(2.0, (double)apr_l_max) * (double)min_dim);
+    const float mult = level_factor / p.rel_error;
+    APRB_CUDA(cudaMemsetAsync(counts, 0, 2 * sizeof(unsigned long long), s));
+    const unsigned blocks = (unsigned)std::min<uint64_t>(blocks_for(nd, 256), 148 * 8);
+    level_margin_kernel<IT><<<blocks, 256, 0, s>>>(grad, lis, nd, mult, rel, counts);
+    count_launch();
+    APRB_CHECK_LAUNCH();
+}
+template void launch_level_margins<uint16_t>(const uint16_t *, const float *, uint64_t, const aprb_params &, int,
+                                             double, unsigned long long *, cudaStream_t);
+template void launch_level_margins<float>(const float *, const float *, uint64_t, const aprb_params &, int, double,
+                                          unsigned long long *, cudaStream_t);
+
 template void launch_upload_smooth<uint16_t>(const uint16_t *, uint16_t *, uint16_t *, int, int, int, float,
                                              unsigned *, float *, int, unsigned *, DevBuf &, cudaStream_t,
                                              cudaStream_t);

@@ -891,6 +891,7 @@ uint64_t sample_scratch_elems(const Geom &g) {
 
 void launch_sample_scratch(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec, const uint16_t *img,
                            uint16_t *parts, uint16_t *scratch, cudaStream_t s) {
+    APRB_PROF("sample", s);
     const int L = g.l_max, lmin = g.l_min;
     uint64_t off = 0;
     const uint16_t *lev[32] = {};
@@ -903,10 +904,13 @@ void launch_sample_scratch(const Geom &g, const uint64_t *xz_end, const uint16_t
     for (int l = L - 1; l >= lmin; --l) {
         pyr_mean_u16_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(lev[l + 1], dims(g, l + 1), slot[l],
                                                                         dims(g, l));
+        count_launch();
         lev[l] = slot[l];
     }
-    for (int l = lmin; l <= L; ++l)
+    for (int l = lmin; l <= L; ++l) {
         gather_kernel<<<row_blocks(nrow(g, l)), 256, 0, s>>>(lev[l], dims(g, l), xz_end, g.level_xz[l], y_vec, parts);
+        count_launch();
+    }
     APRB_CHECK_LAUNCH();
 }
 

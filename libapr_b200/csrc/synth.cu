@@ -5,6 +5,16 @@
 // deviates use a counter-based generator per voxel: multiplication of
 // uniforms for small means, Hoermann's transformed rejection (PTRS, 1993)
 // otherwise.
+//
+// The exponentials, logarithms and log-factorials are this file's own
+// (Cody-Waite range reduction with Taylor, atanh and Stirling series) and
+// use only IEEE-rounded additions, multiplications, divisions, square roots
+// and floors, with no contraction (-fmad=false), so a host program that
+// performs the same operations in the same order reproduces every voxel bit
+// for bit: a CPU run of the same workload can be fed the same bytes without
+// a GPU.
+#include <math_constants.h>
+
 #include <type_traits>
 #include <vector>
 
@@ -42,28 +52,127 @@ struct Rng {
     }
 };
 
+// exp(x) for x <= 0 in float: x = k ln2 + r with the Cody-Waite split of
+// ln2 (|r| <= ln2/2), exp(r) by its Taylor polynomial of degree 7 (truncation
+// below 6e-9 relative), times 2^k built from the exponent bits.  Below -87 the
+// result is 0 (exp(-87) < 2^-125).
+__device__ __forceinline__ float exp_nonpos_f(float x) {
+    if (!(x > -87.0f)) return 0.0f;
+    const float kf = floorf(x * 1.44269504f + 0.5f);
+    const int k = (int)kf;
+    const float r = (x - kf * 0.693145751953125f) - kf * 1.42860677e-06f;
+    float p = 1.98412701e-04f;
+    p = p * r + 1.38888892e-03f;
+    p = p * r + 8.33333377e-03f;
+    p = p * r + 4.16666679e-02f;
+    p = p * r + 1.66666672e-01f;
+    p = p * r + 0.5f;
+    p = p * r + 1.0f;
+    p = p * r + 1.0f;
+    return p * __int_as_float((k + 127) << 23);
+}
+
+// exp(x) for -700 < x <= 0 in double: the same reduction with the fdlibm
+// split of ln2 and the Taylor polynomial of degree 13.
+__device__ __forceinline__ double exp_nonpos_d(double x) {
+    if (!(x > -700.0)) return 0.0;
+    const double kf = floor(x * 1.4426950408889634 + 0.5);
+    const long long k = (long long)kf;
+    const double r = (x - kf * 0.6931471803691238) - kf * 1.9082149292705877e-10;
+    double p = 1.6059043836821613e-10;
+    p = p * r + 2.08767569878681e-09;
+    p = p * r + 2.505210838544172e-08;
+    p = p * r + 2.755731922398589e-07;
+    p = p * r + 2.7557319223985893e-06;
+    p = p * r + 2.48015873015873e-05;
+    p = p * r + 0.0001984126984126984;
+    p = p * r + 0.001388888888888889;
+    p = p * r + 0.008333333333333333;
+    p = p * r + 0.041666666666666664;
+    p = p * r + 0.16666666666666666;
+    p = p * r + 0.5;
+    p = p * r + 1.0;
+    p = p * r + 1.0;
+    return p * __longlong_as_double((k + 1023) << 52);
+}
+
+// log(x) in double: x = m 2^e with m in [sqrt(1/2), sqrt(2)), log(m) =
+// 2 atanh(s), s = (m - 1)/(m + 1), |s| <= 0.1716, by its series to s^23.
+__device__ __forceinline__ double log_d(double x) {
+    if (!(x > 0.0)) return x == 0.0 ? -CUDART_INF : CUDART_NAN;
+    if (x == CUDART_INF) return x;
+    int e = 0;
+    if (x < 2.2250738585072014e-308) {
+        x *= 18014398509481984.0;  // 2^54
+        e = -54;
+    }
+    const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+    e += (int)((b >> 52) & 0x7ff) - 1023;
+    double m = __longlong_as_double((long long)((b & 0xfffffffffffffull) | 0x3ff0000000000000ull));
+    if (m > 1.4142135623730951) {
+        m = m * 0.5;
+        e += 1;
+    }
+    const double s = (m - 1.0) / (m + 1.0);
+    const double s2 = s * s;
+    double p = 0.043478260869565216;
+    p = p * s2 + 0.047619047619047616;
+    p = p * s2 + 0.05263157894736842;
+    p = p * s2 + 0.058823529411764705;
+    p = p * s2 + 0.06666666666666667;
+    p = p * s2 + 0.07692307692307693;
+    p = p * s2 + 0.09090909090909091;
+    p = p * s2 + 0.1111111111111111;
+    p = p * s2 + 0.14285714285714285;
+    p = p * s2 + 0.2;
+    p = p * s2 + 0.3333333333333333;
+    p = p * s2 + 1.0;
+    const double ed = (double)e;
+    return ed * 0.6931471803691238 + ((2.0 * s) * p + ed * 1.9082149292705877e-10);
+}
+
+// log(k!) for k >= 0: the exact product below 18! (exactly representable),
+// else Stirling's series for lgamma(k + 1) to the 1/n^7 term.
+__device__ __forceinline__ double log_factorial(long long k) {
+    if (k < 2) return 0.0;
+    if (k < 18) {
+        double f = 1.0;
+        for (long long i = 2; i <= k; ++i) f = f * (double)i;
+        return log_d(f);
+    }
+    const double n = (double)(k + 1);
+    const double inv = 1.0 / n, inv2 = inv * inv;
+    const double series =
+        inv * (0.08333333333333333 + inv2 * (-0.002777777777777778 +
+                                             inv2 * (0.0007936507936507937 + inv2 * -0.0005952380952380953)));
+    return (((n - 0.5) * log_d(n) - n) + 0.9189385332046727) + series;
+}
+
 __device__ int poisson(double lam, Rng &r) {
     if (lam <= 0) return 0;
     if (lam < 10.0) {
-        const double L = exp(-lam);
+        const double L = exp_nonpos_d(-lam);
         double p = 1.0;
         int k = 0;
         do {
             ++k;
-            p *= r.next();
+            p = p * r.next();
         } while (p > L && k < 1000);
         return k - 1;
     }
-    const double slam = sqrt(lam), loglam = log(lam);
+    const double slam = sqrt(lam), loglam = log_d(lam);
     const double b = 0.931 + 2.53 * slam, a = -0.059 + 0.02483 * b;
-    const double invalpha = 1.1239 + 1.1328 / (b - 3.4), vr = 0.9277 - 3.6224 / (b - 2);
+    const double invalpha = 1.1239 + 1.1328 / (b - 3.4), vr = 0.9277 - 3.6224 / (b - 2.0);
+    const double log_invalpha = log_d(invalpha);
     for (int it = 0; it < 1000; ++it) {
         const double U = r.next() - 0.5, V = r.next();
         const double us = 0.5 - fabs(U);
-        const long long k = (long long)floor((2 * a / us + b) * U + lam + 0.43);
+        const long long k = (long long)floor(((2.0 * a) / us + b) * U + lam + 0.43);
         if (us >= 0.07 && V <= vr) return (int)k;
         if (k < 0 || (us < 0.013 && V > us)) continue;
-        if (log(V) + log(invalpha) - log(a / (us * us) + b) <= -lam + k * loglam - lgamma((double)k + 1)) return (int)k;
+        const double lhs = (log_d(V) + log_invalpha) - log_d(a / (us * us) + b);
+        const double rhs = (-lam + (double)k * loglam) - log_factorial(k);
+        if (lhs <= rhs) return (int)k;
     }
     return (int)lam;
 }
@@ -87,7 +196,7 @@ __global__ void render_kernel(OutT *__restrict__ img, int yn, int xn, int zn, co
         for (uint32_t k = b0; k < b1; ++k) {
             const Blob B = blobs[bidx[k]];
             const float dy = fy - B.cy, dx = fx - B.cx, dz = fz - B.cz;
-            v += B.amp * expf(-(dy * dy + dx * dx + dz * dz) * B.inv2s2);
+            v = v + B.amp * exp_nonpos_f(-((dy * dy + dx * dx) + dz * dz) * B.inv2s2);
         }
         const uint64_t vox = idx3(y, x, z, yn, xn);
         if (NOISE) {

@@ -4,6 +4,8 @@
 * ``_ref/libaprref.so``: LibAPR's own CPU code compiled from its headers
   (strict IEEE flags); ``_ref/libaprref_fast.so`` the same at the reference's
   Release flags (-O3 -ffast-math), used only for timing.
+* ``libblobs.so``: the CPU twin of the library's synthetic-volume generator
+  (the same bytes as ``aprb_synth_blobs_u16`` / ``_f32``, without a GPU).
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this module.  Images are numpy arrays of shape (z, x, y) in C order, i.e. the
@@ -45,6 +47,36 @@ def _ptr(a, t):
 
 _lib = None
 _ref = {}
+_blobs = None
+
+
+def blobs_lib():
+    global _blobs
+    if _blobs is None:
+        L = C.CDLL(os.path.join(HERE, "libblobs.so"))
+        for n, t in (("blobs_render_u16", C.c_uint16), ("blobs_render_f32", C.c_float)):
+            f = getattr(L, n)
+            f.argtypes = [C.POINTER(t), C.c_int, C.c_int, C.c_int, C.c_int] + [C.c_float] * 5 + [C.c_uint64]
+            f.restype = C.c_int
+        _blobs = L
+    return _blobs
+
+
+def blob_volume_cpu(shape_zxy, n_blobs, sigma, amp, background, seed, noise=True, out=None):
+    """The benchmark generator's volume on the host cores: (z, x, y) uint16
+    with Poisson noise, or float32 noise-free intensities; bit-identical to
+    the device generator for the same arguments."""
+    z, x, y = (int(v) for v in shape_zxy)
+    dt = np.uint16 if noise else np.float32
+    if out is None:
+        out = np.empty((z, x, y), dt)
+    assert out.dtype == dt and out.shape == (z, x, y) and out.flags.c_contiguous
+    f = blobs_lib().blobs_render_u16 if noise else blobs_lib().blobs_render_f32
+    e = f(_ptr(out, C.c_uint16 if noise else C.c_float), y, x, z, int(n_blobs), float(sigma[0]), float(sigma[1]),
+          float(amp[0]), float(amp[1]), float(background), int(seed))
+    if e != 0:
+        raise MemoryError("blob generator could not allocate its brick lists")
+    return out
 
 
 def lib():

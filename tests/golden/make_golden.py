@@ -22,7 +22,8 @@ import sys
 
 import numpy as np
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+# the LibAPR source tree: first argument, else $LIBAPR_SRC/.. (LIBAPR_SRC names its src/ directory)
+REF = sys.argv[1] if len(sys.argv) > 1 else os.path.dirname(os.path.normpath(os.environ["LIBAPR_SRC"]))
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 _TYPES = {1: 1, 2: 1, 3: 2, 4: 4, 5: 8, 6: 1, 7: 1, 8: 2, 9: 4, 10: 8, 11: 4, 12: 8, 16: 8}
