@@ -225,7 +225,7 @@ def parity_full_volume(A, host_img, dev_img, image_type, rel_tol=1e-5):
     del lx, xe, yv
     P = acc.P
     del acc
-    parts = A.ParticleData().sample_image(apr, dev_img).data
+    parts = A.ParticleData().sample_image(apr, host_img).data
     same_parts = bool(np.array_equal(parts[:P], ref.sample(host_img)[:P]))
     del parts, ref
     apr._free()

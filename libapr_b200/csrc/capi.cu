@@ -384,7 +384,7 @@ PixelOut<IT> pixel_stages(aprb_converter *c, const aprb_params &p, const uint16_
     const bool is_u16 = sizeof(IT) == 2;
     unsigned *mm = c->mm.as_on<unsigned>(2, s);
     float *d_off = c->offset.as_on<float>(1, s);
-    unsigned *d_err = c->err.as_on<unsigned>(1, s);
+    unsigned *d_err = c->err.as_on<unsigned>(2, s);  // [0] overflow count, [1] TMA wait timeout
     IT *work = c->work.as_on<IT>(n, s);
     if (host) {
         launch_upload_smooth<IT>(host, const_cast<uint16_t *>(img), work, yn, xn, zn, p.lambda, mm, d_off,
@@ -403,9 +403,14 @@ PixelOut<IT> pixel_stages(aprb_converter *c, const aprb_params &p, const uint16_
 }
 
 void throw_if_overflow(aprb_converter *c, cudaStream_t s) {
-    unsigned h_err = 0;
-    APRB_CUDA(cudaMemcpyAsync(&h_err, c->err.p, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    unsigned h[2] = {0, 0};
+    APRB_CUDA(cudaMemcpyAsync(h, c->err.p, 2 * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
     APRB_CUDA(cudaStreamSynchronize(s));
+    if (h[1]) {
+        set_error("a bounded wait for a TMA copy in the B-spline smoothing ran out");
+        throw Error{APRB_ERR_CUDA};
+    }
+    const unsigned h_err = h[0];
     if (h_err) {
         set_error("integer under-/overflow encountered in the B-spline smoothing");
         throw Error{APRB_ERR_INTEGER_OVERFLOW};
@@ -456,7 +461,7 @@ void run_get_apr(aprb_converter *c, aprb_params p, const uint16_t *img, int yn, 
     a->org[2] = zn;
     const int L = g.l_max;
     const uint64_t nd = (uint64_t)((yn + 1) / 2) * ((xn + 1) / 2) * ((zn + 1) / 2);
-    APRB_CUDA(cudaMemsetAsync(c->err.as_on<unsigned>(1, s), 0, sizeof(unsigned), s));
+    APRB_CUDA(cudaMemsetAsync(c->err.as_on<unsigned>(2, s), 0, 2 * sizeof(unsigned), s));
     PixelOut<IT> po = pixel_stages<IT>(c, p, img, yn, xn, zn, s, host, up);
     IT *grad = po.grad;
     float *lis = po.lis, *ids = po.ids;
@@ -511,7 +516,7 @@ void run_get_apr_by_block(aprb_converter *c, aprb_params p, const uint16_t *img,
     a->org[1] = xn;
     a->org[2] = zn;
     const int L = g.l_max, top = L - 1;
-    APRB_CUDA(cudaMemsetAsync(c->err.as_on<unsigned>(1, s), 0, sizeof(unsigned), s));
+    APRB_CUDA(cudaMemsetAsync(c->err.as_on<unsigned>(2, s), 0, 2 * sizeof(unsigned), s));
     Pyramid pm;
     uint64_t tot = 0, off[32] = {};
     for (int l = g.l_min; l <= top; ++l) {

@@ -26,6 +26,16 @@ struct LisBuffers {
     DevBuf padded, a, c, scalars;
 };
 
+// ---- iir_tma.cu
+// The x (zaxis false) or z pass of the recursive smoothing over a float image
+// with TMA-staged segments; false when the layout does not allow it (y_num not
+// a multiple of 4 or below 256, fewer than 16 samples along the axis, an
+// unaligned image), and the caller runs the register-staged kernel instead.
+// A bounded mbarrier wait that runs out sets *d_timeout.  ckpt holds ckpt_elems
+// recurrence states (16-sample segments x lines).
+bool launch_strided_iir_tma(float *work, int yn, int xn, int zn, bool zaxis, const IIRDev &c, unsigned *d_timeout,
+                            float2 *ckpt, uint64_t ckpt_elems, cudaStream_t s);
+
 // ---- pipeline.cu
 void launch_check_div_const(float d, unsigned long long *out, cudaStream_t s);
 void launch_minmax_offset(const uint16_t *img, uint64_t n, unsigned *mm, float *offset, int apply, cudaStream_t s);

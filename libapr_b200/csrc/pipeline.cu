@@ -1845,10 +1845,14 @@ static void launch_smooth_yx(const uint16_t *img, IT *work, int yn, int xn, int 
         APRB_PROF("bspline_x", s);
         const IIRDev c = dev_coef(iir_coefficients(lambda, xn));
         const uint64_t nlines = (uint64_t)yn * zn;
-        float2 *ck = ckpt.as_on<float2>(nlines * (uint64_t)((xn + kRC - 1) / kRC), s);
-        launch_strided_iir<IT>(work, yn, xn, (uint64_t)yn, (uint64_t)xn * yn, nlines, c, d_err, ck, s);
-        count_launch();
-        APRB_CHECK_LAUNCH();
+        const uint64_t nck = nlines * (uint64_t)((xn + kRC - 1) / kRC);
+        float2 *ck = ckpt.as_on<float2>(nck, s);
+        if (!(std::is_same<IT, float>::value &&
+              launch_strided_iir_tma((float *)work, yn, xn, zn, false, c, d_err + 1, ck, nck, s))) {
+            launch_strided_iir<IT>(work, yn, xn, (uint64_t)yn, (uint64_t)xn * yn, nlines, c, d_err, ck, s);
+            count_launch();
+            APRB_CHECK_LAUNCH();
+        }
     }
 }
 
@@ -1859,10 +1863,14 @@ static void launch_smooth_z(IT *work, int yn, int xn, int zn, float lambda, unsi
         APRB_PROF("bspline_z", s);
         const IIRDev c = dev_coef(iir_coefficients(lambda, zn));
         const uint64_t nlines = (uint64_t)yn * xn;
-        float2 *ck = ckpt.as_on<float2>(nlines * (uint64_t)((zn + kRC - 1) / kRC), s);
-        launch_strided_iir<IT>(work, yn, zn, (uint64_t)xn * yn, (uint64_t)yn, nlines, c, d_err, ck, s);
-        count_launch();
-        APRB_CHECK_LAUNCH();
+        const uint64_t nck = nlines * (uint64_t)((zn + kRC - 1) / kRC);
+        float2 *ck = ckpt.as_on<float2>(nck, s);
+        if (!(std::is_same<IT, float>::value &&
+              launch_strided_iir_tma((float *)work, yn, xn, zn, true, c, d_err + 1, ck, nck, s))) {
+            launch_strided_iir<IT>(work, yn, zn, (uint64_t)xn * yn, (uint64_t)yn, nlines, c, d_err, ck, s);
+            count_launch();
+            APRB_CHECK_LAUNCH();
+        }
     }
 }
 

@@ -47,6 +47,25 @@ def test_get_apr_bit_exact(shape, blobs, seed, image_type):
     assert np.array_equal(parts, B.orc_sample(acc, img))
 
 
+# shapes that take the TMA-staged x / z smoothing (float ImageType, y_num a
+# multiple of 4 and >= 256, >= 16 samples along the axis): partial TMA boxes
+# (y_num 600, 260), partial 16-sample segments, and an x extent below 16 that
+# keeps the register-staged x pass
+TMA_SHAPES = [((37, 45, 600), 25, 21), ((16, 300, 260), 30, 22), ((130, 17, 512), 40, 23), ((20, 9, 256), 6, 24)]
+
+
+@pytest.mark.parametrize("shape,blobs,seed", TMA_SHAPES)
+@pytest.mark.parametrize("lam", [3.0, 0.5, 10.0])
+def test_tma_smoothing_bit_exact(shape, blobs, seed, lam):
+    img = volume(shape, blobs, seed)
+    e, acc, (off, inter) = B.orc_get_apr(img, oracle_params(lambda_=lam), 0)
+    assert e == 0
+    conv, apr = gpu_apr(img, 0, lambda_=lam)
+    assert bits_equal(conv.intermediate(0, shape), inter[0]), "smoothed image"
+    lx, xe, yv = apr.linear_access()
+    assert np.array_equal(xe, acc.xz_end) and np.array_equal(yv, acc.y_vec)
+
+
 @pytest.mark.parametrize("kw", [dict(lambda_=0.5), dict(lambda_=10.0), dict(sigma_th=0.0, grad_th=0.0),
                                 dict(neighborhood_optimization=False), dict(Ip_th=150.0, rel_error=0.05),
                                 dict(constant_intensity_scale=True), dict(lambda_=0.0),
