@@ -1,13 +1,13 @@
 // a2 (x, z) for float ImageType: bspline_filt_rec_x (ComputeGradient.hpp:602-779)
 // and bspline_filt_rec_z (:416-599) with TMA-staged segments.
 //
-// A CTA owns 512 consecutive y of one plane of the other axis (one x row for
-// the z pass, one z plane for the x pass): 512 lines along the filtered axis,
-// four neighbouring lines per thread.  The lines move through shared memory in
-// segments of 16 samples, each segment two cp.async.bulk.tensor boxes of
-// 256 y x 16 samples (2 KB contiguous per sample), in a ring of three stages
-// whose mbarriers the copy engine completes; a CTA keeps up to three segments
-// (96 KB) in flight without spending registers on them.
+// A CTA owns a run of consecutive y (one or more boxes of 256) of one plane of
+// the other axis (one x row for the z pass, one z plane for the x pass): one
+// line along the filtered axis per y, a few neighbouring lines per thread.
+// The lines move through shared memory in segments of 16 samples, each
+// segment one cp.async.bulk.tensor box of 256 y x 16 samples per 256 y, in a
+// ring of stages whose mbarriers the copy engine completes; a CTA keeps
+// several segments in flight without spending registers on them.
 //
 // The recurrences are those of the register-staged kernels in pipeline.cu,
 // operation for operation: the causal sweep walks the segments forward and
@@ -21,84 +21,122 @@
 #include "kernels.cuh"
 #include "tma.cuh"
 
+// boxes of 256 y per CTA, lines per thread, stages in flight.  Measured on
+// 2048x2048x512 (B200): 1 box, 2 lines, 4 stages (three 64 KB CTAs per SM)
+// x 4.27 / z 4.03 ms; 2 boxes, 4 lines, 3 stages 4.29 / 4.20; one CTA per SM
+// with 8 stages 5.5 - 7.3 ms (too few warps for the recurrences' latency).
+#ifndef APRB_TMA_Z_SHAPE
+#define APRB_TMA_Z_SHAPE 1, 2, 4
+#endif
+#ifndef APRB_TMA_X_SHAPE
+#define APRB_TMA_X_SHAPE 1, 2, 4
+#endif
+
 namespace aprb {
 
 namespace {
 
-constexpr int kTS = 16;                // samples per segment (one stage)
-constexpr int kTBox = 256;             // y extent of one TMA box
-constexpr int kTY = 2 * kTBox;         // y columns (lines) of a CTA
-constexpr int kTThreads = kTY / 4;     // four lines per thread
-constexpr int kTStages = 3;            // segments in flight per CTA
-constexpr int kStageFloats = kTS * kTY;
-// the stages, then the stages' mbarriers
-constexpr size_t kTSmem = sizeof(float) * kTStages * kStageFloats + 8 * kTStages;
+constexpr int kTS = 16;     // samples per segment (one stage)
+constexpr int kTBox = 256;  // y extent of one TMA box
 
-__device__ __forceinline__ void ld4(const float *p, float *a) {
-    const float4 v = *reinterpret_cast<const float4 *>(p);
-    a[0] = v.x, a[1] = v.y, a[2] = v.z, a[3] = v.w;
-}
-__device__ __forceinline__ void st4(float *p, const float *a) {
-    *reinterpret_cast<float4 *>(p) = make_float4(a[0], a[1], a[2], a[3]);
-}
+template <int V>
+struct LdV;
+template <>
+struct LdV<4> {
+    __device__ __forceinline__ static void ld(const float *p, float *a) {
+        const float4 v = *reinterpret_cast<const float4 *>(p);
+        a[0] = v.x, a[1] = v.y, a[2] = v.z, a[3] = v.w;
+    }
+    __device__ __forceinline__ static void st(float *p, const float *a) {
+        *reinterpret_cast<float4 *>(p) = make_float4(a[0], a[1], a[2], a[3]);
+    }
+};
+template <>
+struct LdV<2> {
+    __device__ __forceinline__ static void ld(const float *p, float *a) {
+        const float2 v = *reinterpret_cast<const float2 *>(p);
+        a[0] = v.x, a[1] = v.y;
+    }
+    __device__ __forceinline__ static void st(float *p, const float *a) {
+        *reinterpret_cast<float2 *>(p) = make_float2(a[0], a[1]);
+    }
+};
+template <>
+struct LdV<1> {
+    __device__ __forceinline__ static void ld(const float *p, float *a) { a[0] = *p; }
+    __device__ __forceinline__ static void st(float *p, const float *a) { *p = a[0]; }
+};
+
+template <int BOXES, int V, int STAGES>
+struct TmaShape {
+    static constexpr int kY = BOXES * kTBox;          // y columns (lines) of a CTA
+    static constexpr int kThreads = kY / V;           // V neighbouring lines per thread
+    static constexpr int kStageFloats = kTS * kY;
+    // the stages, then the stages' mbarriers
+    static constexpr size_t kSmem = sizeof(float) * STAGES * kStageFloats + 8 * STAGES;
+};
 
 // ZAXIS: lines along z (box 256 y x 1 x x 16 z, coordinates (y, o = x, i = z));
 // else lines along x (box 256 y x 16 x x 1 z, coordinates (y, i = x, o = z)).
-template <bool ZAXIS>
-__global__ void __launch_bounds__(kTThreads, 2)
+// A CTA owns BOXES * 256 consecutive y of plane o; thread t the V lines
+// y0 + V t .. y0 + V t + V - 1.
+template <bool ZAXIS, int BOXES, int V, int STAGES>
+__global__ void __launch_bounds__(TmaShape<BOXES, V, STAGES>::kThreads)
     iir_strided_tma_kernel(const __grid_constant__ CUtensorMap tm, const float *__restrict__ im, int yn, int n,
                            uint64_t s1, uint64_t s2, IIRDev c, float2 *__restrict__ ckpt, uint64_t nlines,
                            unsigned *timeout) {
+    using Sh = TmaShape<BOXES, V, STAGES>;
+    constexpr int kY = Sh::kY, kSF = Sh::kStageFloats;
     extern __shared__ __align__(128) float tsm[];
-    uint64_t *full = reinterpret_cast<uint64_t *>(tsm + (size_t)kTStages * kStageFloats);
-    const int ytiles = (yn + kTY - 1) / kTY;
-    const int y0 = (int)(blockIdx.x % ytiles) * kTY;
+    uint64_t *full = reinterpret_cast<uint64_t *>(tsm + (size_t)STAGES * kSF);
+    const int ytiles = (yn + kY - 1) / kY;
+    const int y0 = (int)(blockIdx.x % ytiles) * kY;
     const int o = (int)(blockIdx.x / ytiles);
     const int t = threadIdx.x;
-    const int half = t / (kTBox / 4), col = 4 * (t % (kTBox / 4));
-    const int y = y0 + half * kTBox + col;
+    const int box = (V * t) / kTBox, col = (V * t) % kTBox;
+    const int y = y0 + box * kTBox + col;
     const bool valid = y < yn;
-    const bool second = y0 + kTBox < yn;
-    const uint32_t stage_bytes = (second ? 2u : 1u) * (uint32_t)(kTS * kTBox * sizeof(float));
+    int nbox = 0;  // boxes of the CTA that start inside the image
+    for (int b = 0; b < BOXES; ++b) nbox += (y0 + b * kTBox < yn) ? 1 : 0;
+    const uint32_t stage_bytes = (uint32_t)nbox * (uint32_t)(kTS * kTBox * sizeof(float));
     const int nseg = (n + kTS - 1) / kTS;
     const int njobs = 2 * nseg;
     const uint64_t line = (uint64_t)o * (uint64_t)yn + (uint64_t)y;
 
     if (t == 0) {
-        for (int i = 0; i < kTStages; ++i) mbar_init(&full[i], 1);
+        for (int i = 0; i < STAGES; ++i) mbar_init(&full[i], 1);
         mbar_fence_init();
     }
     __syncthreads();
     // job j < nseg: causal sweep over segment j; else anti-causal over segment 2 nseg - 1 - j
     auto issue = [&](int j) {
         if (j >= njobs) return;
-        const int st = j % kTStages;
-        float *S = tsm + (size_t)st * kStageFloats;
+        const int st = j % STAGES;
+        float *S = tsm + (size_t)st * kSF;
         const int i0 = (j < nseg ? j : njobs - 1 - j) * kTS;
         mbar_arrive_expect_tx(&full[st], stage_bytes);
-        if (ZAXIS) {
-            tma_load_3d(S, &tm, &full[st], y0, o, i0);
-            if (second) tma_load_3d(S + kTS * kTBox, &tm, &full[st], y0 + kTBox, o, i0);
-        } else {
-            tma_load_3d(S, &tm, &full[st], y0, i0, o);
-            if (second) tma_load_3d(S + kTS * kTBox, &tm, &full[st], y0 + kTBox, i0, o);
+        for (int b = 0; b < nbox; ++b) {
+            if (ZAXIS)
+                tma_load_3d(S + b * kTS * kTBox, &tm, &full[st], y0 + b * kTBox, o, i0);
+            else
+                tma_load_3d(S + b * kTS * kTBox, &tm, &full[st], y0 + b * kTBox, i0, o);
         }
     };
     if (t == 0)
-        for (int j = 0; j < kTStages; ++j) issue(j);
+        for (int j = 0; j < STAGES; ++j) issue(j);
 
     // boundary sums over the first and last minLen samples (ComputeGradient.hpp:434-470)
-    float v1[4] = {}, v2[4] = {}, v3[4] = {}, v4[4] = {};
+    float v1[V] = {}, v2[V] = {}, v3[V] = {}, v4[V] = {};
     if (valid) {
         const float *L = im + (uint64_t)o * s2 + (uint64_t)y;
         for (int i = 0; i < c.minLen; ++i) {
-            float a[4], b[4];
-            ld4(L + (uint64_t)i * s1, a);
-            ld4(L + (uint64_t)(n - 1 - i) * s1, b);
+            float a[V], b[V];
+            LdV<V>::ld(L + (uint64_t)i * s1, a);
+            LdV<V>::ld(L + (uint64_t)(n - 1 - i) * s1, b);
             const float k1 = __ldg(c.bc + i), k2 = __ldg(c.bc + c.minLen + i);
             const float k3 = __ldg(c.bc + 2 * c.minLen + i), k4 = __ldg(c.bc + 3 * c.minLen + i);
 #pragma unroll
-            for (int h = 0; h < 4; ++h) {
+            for (int h = 0; h < V; ++h) {
                 v1[h] = v1[h] + k1 * a[h];
                 v2[h] = v2[h] + k2 * a[h];
                 v3[h] = v3[h] + k3 * b[h];
@@ -106,39 +144,39 @@ __global__ void __launch_bounds__(kTThreads, 2)
             }
         }
     }
-    float p1[4], p2[4], q3[4], q4[4];
+    float p1[V], p2[V], q3[V], q4[V];
 #pragma unroll
-    for (int h = 0; h < 4; ++h) p1[h] = v1[h], p2[h] = v2[h], q3[h] = v3[h], q4[h] = v4[h];
+    for (int h = 0; h < V; ++h) p1[h] = v1[h], p2[h] = v2[h], q3[h] = v3[h], q4[h] = v4[h];
 
     for (int j = 0; j < njobs; ++j) {
-        const int st = j % kTStages;
-        const bool ok = mbar_wait_bounded(&full[st], (uint32_t)((j / kTStages) & 1));
+        const int st = j % STAGES;
+        const bool ok = mbar_wait_bounded(&full[st], (uint32_t)((j / STAGES) & 1));
         if (__syncthreads_or(!ok)) {
             if (t == 0) {
                 atomicOr(timeout, 1u);
-                // the loads issued for jobs j .. j + kTStages - 1 may still land: wait for them (bounded)
-                for (int k = j; k < j + kTStages && k < njobs; ++k)
-                    mbar_wait_bounded(&full[k % kTStages], (uint32_t)((k / kTStages) & 1));
+                // the loads issued for jobs j .. j + STAGES - 1 may still land: wait for them (bounded)
+                for (int k = j; k < j + STAGES && k < njobs; ++k)
+                    mbar_wait_bounded(&full[k % STAGES], (uint32_t)((k / STAGES) & 1));
                 bulk_wait_all();
             }
             return;
         }
-        float *S = tsm + (size_t)st * kStageFloats + half * (kTS * kTBox) + col;
+        float *S = tsm + (size_t)st * kSF + box * (kTS * kTBox) + col;
         const bool causal = j < nseg;
         const int sgm = causal ? j : njobs - 1 - j;
         const int i0 = sgm * kTS;
         float2 *ck = ckpt + (uint64_t)sgm * nlines + line;
         if (valid && causal) {
             // ---- causal sweep: the state at the segment start, then the segment
-            reinterpret_cast<float4 *>(ck)[0] = make_float4(p1[0], p2[0], p1[1], p2[1]);
-            reinterpret_cast<float4 *>(ck)[1] = make_float4(p1[2], p2[2], p1[3], p2[3]);
+#pragma unroll
+            for (int h = 0; h < V; ++h) ck[h] = make_float2(p1[h], p2[h]);
             if (i0 >= 2 && i0 + kTS <= n) {
 #pragma unroll
                 for (int u = 0; u < kTS; ++u) {
-                    float a[4];
-                    ld4(S + u * kTBox, a);
+                    float a[V];
+                    LdV<V>::ld(S + u * kTBox, a);
 #pragma unroll
-                    for (int h = 0; h < 4; ++h) {
+                    for (int h = 0; h < V; ++h) {
                         const float nv = a[h] + c.b1 * p1[h] + c.b2 * p2[h];
                         p2[h] = p1[h];
                         p1[h] = nv;
@@ -147,10 +185,10 @@ __global__ void __launch_bounds__(kTThreads, 2)
             } else {
                 const int i1 = min(n, i0 + kTS);
                 for (int i = max(i0, 2); i < i1; ++i) {
-                    float a[4];
-                    ld4(S + (i - i0) * kTBox, a);
+                    float a[V];
+                    LdV<V>::ld(S + (i - i0) * kTBox, a);
 #pragma unroll
-                    for (int h = 0; h < 4; ++h) {
+                    for (int h = 0; h < V; ++h) {
                         const float nv = a[h] + c.b1 * p1[h] + c.b2 * p2[h];
                         p2[h] = p1[h];
                         p1[h] = nv;
@@ -159,17 +197,21 @@ __global__ void __launch_bounds__(kTThreads, 2)
             }
         } else if (valid) {
             // ---- anti-causal sweep, recomputing the segment's causal values
-            const float4 c0 = reinterpret_cast<const float4 *>(ck)[0];
-            const float4 c1 = reinterpret_cast<const float4 *>(ck)[1];
-            float r1[4] = {c0.x, c0.z, c1.x, c1.z}, r2[4] = {c0.y, c0.w, c1.y, c1.w};
-            float buf[kTS][4];
+            float r1[V], r2[V];
+#pragma unroll
+            for (int h = 0; h < V; ++h) {
+                const float2 q = ck[h];
+                r1[h] = q.x;
+                r2[h] = q.y;
+            }
+            float buf[kTS][V];
             if (i0 >= 2 && i0 + kTS <= n - 2) {
 #pragma unroll
                 for (int u = 0; u < kTS; ++u) {
-                    float a[4];
-                    ld4(S + u * kTBox, a);
+                    float a[V];
+                    LdV<V>::ld(S + u * kTBox, a);
 #pragma unroll
-                    for (int h = 0; h < 4; ++h) {
+                    for (int h = 0; h < V; ++h) {
                         const float nv = a[h] + c.b1 * r1[h] + c.b2 * r2[h];
                         r2[h] = r1[h];
                         r1[h] = nv;
@@ -179,13 +221,13 @@ __global__ void __launch_bounds__(kTThreads, 2)
 #pragma unroll
                 for (int u = kTS - 1; u >= 0; --u) {
 #pragma unroll
-                    for (int h = 0; h < 4; ++h) {
+                    for (int h = 0; h < V; ++h) {
                         const float temp = buf[u][h] + c.b1 * q3[h] + c.b2 * q4[h];
                         buf[u][h] = temp * c.norm;
                         q4[h] = q3[h];
                         q3[h] = temp;
                     }
-                    st4(S + u * kTBox, buf[u]);
+                    LdV<V>::st(S + u * kTBox, buf[u]);
                 }
             } else {
                 const int i1 = min(n, i0 + kTS);
@@ -193,10 +235,10 @@ __global__ void __launch_bounds__(kTThreads, 2)
                 for (int u = 0; u < kTS; ++u) {
                     const int i = i0 + u;
                     if (i >= i1) break;
-                    float a[4] = {};
-                    if (i >= 2) ld4(S + u * kTBox, a);
+                    float a[V] = {};
+                    if (i >= 2) LdV<V>::ld(S + u * kTBox, a);
 #pragma unroll
-                    for (int h = 0; h < 4; ++h) {
+                    for (int h = 0; h < V; ++h) {
                         float f;
                         if (i == 0) {
                             f = v2[h];
@@ -215,7 +257,7 @@ __global__ void __launch_bounds__(kTThreads, 2)
                     const int i = i0 + u;
                     if (i >= i1) continue;
 #pragma unroll
-                    for (int h = 0; h < 4; ++h) {
+                    for (int h = 0; h < V; ++h) {
                         float out;
                         if (i == n - 1) {
                             out = v4[h] * c.norm;
@@ -229,7 +271,7 @@ __global__ void __launch_bounds__(kTThreads, 2)
                         }
                         buf[u][h] = out;
                     }
-                    st4(S + u * kTBox, buf[u]);
+                    LdV<V>::st(S + u * kTBox, buf[u]);
                 }
             }
         }
@@ -237,21 +279,33 @@ __global__ void __launch_bounds__(kTThreads, 2)
         __syncthreads();
         if (t == 0) {
             if (!causal) {
-                float *SS = tsm + (size_t)st * kStageFloats;
-                if (ZAXIS) {
-                    tma_store_3d(&tm, SS, y0, o, i0);
-                    if (second) tma_store_3d(&tm, SS + kTS * kTBox, y0 + kTBox, o, i0);
-                } else {
-                    tma_store_3d(&tm, SS, y0, i0, o);
-                    if (second) tma_store_3d(&tm, SS + kTS * kTBox, y0 + kTBox, i0, o);
+                float *SS = tsm + (size_t)st * kSF;
+                for (int b = 0; b < nbox; ++b) {
+                    if (ZAXIS)
+                        tma_store_3d(&tm, SS + b * kTS * kTBox, y0 + b * kTBox, o, i0);
+                    else
+                        tma_store_3d(&tm, SS + b * kTS * kTBox, y0 + b * kTBox, i0, o);
                 }
                 bulk_commit();
                 bulk_wait_read_all();  // the stage is loaded again below
             }
-            issue(j + kTStages);
+            issue(j + STAGES);
         }
     }
     if (t == 0) bulk_wait_all();
+}
+
+template <bool ZAXIS, int BOXES, int V, int STAGES>
+void launch_tma_variant(const CUtensorMap &tm, float *work, int yn, int n, int m, uint64_t s1, uint64_t s2,
+                        const IIRDev &c, float2 *ckpt, unsigned *d_timeout, cudaStream_t s) {
+    using Sh = TmaShape<BOXES, V, STAGES>;
+    auto kern = iir_strided_tma_kernel<ZAXIS, BOXES, V, STAGES>;
+    APRB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::kSmem));
+    const unsigned blocks = (unsigned)((uint64_t)((yn + Sh::kY - 1) / Sh::kY) * (uint64_t)m);
+    kern<<<blocks, Sh::kThreads, Sh::kSmem, s>>>(tm, work, yn, n, s1, s2, c, ckpt, (uint64_t)yn * (uint64_t)m,
+                                                 d_timeout);
+    count_launch();
+    APRB_CHECK_LAUNCH();
 }
 
 }  // namespace
@@ -266,14 +320,11 @@ bool launch_strided_iir_tma(float *work, int yn, int xn, int zn, bool zaxis, con
     const uint64_t d[3] = {(uint64_t)yn, (uint64_t)xn, (uint64_t)zn};
     const uint32_t box[3] = {(uint32_t)kTBox, zaxis ? 1u : (uint32_t)kTS, zaxis ? (uint32_t)kTS : 1u};
     if (!make_tensor_map_3d_f32(&tm, work, d, (uint64_t)yn * 4, (uint64_t)xn * yn * 4, box)) return false;
-    auto kern = zaxis ? iir_strided_tma_kernel<true> : iir_strided_tma_kernel<false>;
-    APRB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTSmem));
-    const uint64_t nlines = (uint64_t)yn * (uint64_t)m;
     const uint64_t s1 = zaxis ? (uint64_t)xn * yn : (uint64_t)yn, s2 = zaxis ? (uint64_t)yn : (uint64_t)xn * yn;
-    const unsigned blocks = (unsigned)((uint64_t)((yn + kTY - 1) / kTY) * (uint64_t)m);
-    kern<<<blocks, kTThreads, kTSmem, s>>>(tm, work, yn, n, s1, s2, c, ckpt, nlines, d_timeout);
-    count_launch();
-    APRB_CHECK_LAUNCH();
+    if (zaxis)
+        launch_tma_variant<true, APRB_TMA_Z_SHAPE>(tm, work, yn, n, m, s1, s2, c, ckpt, d_timeout, s);
+    else
+        launch_tma_variant<false, APRB_TMA_X_SHAPE>(tm, work, yn, n, m, s1, s2, c, ckpt, d_timeout, s);
     return true;
 }
 
