@@ -132,6 +132,30 @@ typedef struct {
 aprb_status aprb_get_apr_batch_device(aprb_converter *c, const aprb_params *p, int n_volumes,
                                       const aprb_volume *volumes, int z_block_size, int ghost_z, void *stream,
                                       aprb_apr **outs);
+/* --- the blocked converter split by z-tiles over several GPUs -------------------
+ * APRConverterBatch (APRConverterBatch.hpp:114-175) fills one global particle-cell tree
+ * from its z-tiles (fill_global_particle_cell_tree :282-314, PullingScheme::fill_patch
+ * PullingScheme.hpp:175-247) and solves it once.  A tile only sets cells to SEED, so the
+ * tree of all tiles is the element-wise maximum of the trees of any partition of the tiles:
+ * each GPU fills a zeroed pyramid from its own tiles, the pyramids are combined by a MAX
+ * all-reduce (one uint8 buffer), and the pulling scheme and linear structure run on the
+ * result.  The layout is the converter's own: pct levels l_min .. l_max - 1, each padded
+ * to 16 bytes. */
+/* bytes of the pyramid buffer of a y x x x z volume */
+aprb_status aprb_pyramid_bytes(int y_num, int x_num, int z_num, uint64_t *bytes);
+/* get_apr_method_patch (:190-271) for tiles [first_tile, first_tile + n_tiles) of the
+ * volume's tiling (z_block_size, ghost_z), filling pyramid_dev (zeroed by the caller before
+ * the first fill); slab_dev holds planes [slab_z0, slab_z0 + slab_z_num) of the volume and
+ * must contain the tiles' planes and ghosts.  Blocks until the overflow check is read. */
+aprb_status aprb_pyramid_fill_tiles_device(aprb_converter *c, const aprb_params *p, uint8_t *pyramid_dev, int y_num,
+                                           int x_num, int z_num, int z_block_size, int ghost_z, int first_tile,
+                                           int n_tiles, const uint16_t *slab_dev, int slab_z0, int slab_z_num,
+                                           void *stream);
+/* pulling_scheme_main + generateDatastructures (APRConverter.hpp:339-363) of a filled
+ * pyramid (consumed: the pulling scheme works in place) */
+aprb_status aprb_get_apr_from_pyramid_device(aprb_converter *c, const aprb_params *p, uint8_t *pyramid_dev, int y_num,
+                                             int x_num, int z_num, void *stream, aprb_apr **out);
+
 /* copy one APRB_STAGE_* intermediate of the last get_apr to the host (n = element count) */
 aprb_status aprb_converter_intermediate(const aprb_converter *c, int stage, float *dst, size_t n);
 /* Level-decision margins of the last get_apr (needs aprb_converter_keep_intermediates).

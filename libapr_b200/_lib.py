@@ -55,6 +55,10 @@ SIGNATURES = {
     "aprb_get_apr_batch_device": ([_vp, C.POINTER(aprb_params), _i, C.POINTER(aprb_volume), _i, _i, _vp,
                                    C.POINTER(_vp)], _i),
     "aprb_converter_intermediate": ([_vp, _i, _vp, C.c_size_t], _i),
+    "aprb_pyramid_bytes": ([_i, _i, _i, C.POINTER(_u64)], _i),
+    "aprb_pyramid_fill_tiles_device": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, _i, _i, _i, _i, _vp, _i, _i,
+                                        _vp], _i),
+    "aprb_get_apr_from_pyramid_device": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, _vp, C.POINTER(_vp)], _i),
     "aprb_converter_level_margins": ([_vp, C.c_double, C.POINTER(_u64), C.POINTER(_u64)], _i),
     "aprb_apr_free": ([_vp], _i),
     "aprb_apr_get_info": ([_vp, C.POINTER(aprb_apr_info)], _i),

@@ -507,38 +507,68 @@ void run_get_apr(aprb_converter *c, aprb_params p, const uint16_t *img, int yn, 
 // levels per z-tile with ghost planes, each tile filling the global
 // particle-cell pyramid (fill_global_particle_cell_tree, :282-314), then one
 // pulling scheme and one linear structure for the volume.
-template <typename IT>
-void run_get_apr_by_block(aprb_converter *c, aprb_params p, const uint16_t *img, int yn, int xn, int zn,
-                          int zblock, int ghost, cudaStream_t s, aprb_apr *a) {
-    Geom &g = a->g;
-    a->n_xz = apr_geometry(yn, xn, zn, g);
-    a->org[0] = yn;
-    a->org[1] = xn;
-    a->org[2] = zn;
-    const int L = g.l_max, top = L - 1;
-    APRB_CUDA(cudaMemsetAsync(c->err.as_on<unsigned>(2, s), 0, 2 * sizeof(unsigned), s));
-    Pyramid pm;
-    uint64_t tot = 0, off[32] = {};
-    for (int l = g.l_min; l <= top; ++l) {
-        off[l] = tot;
+// Particle-cell pyramid of the blocked converter: pct levels l_min .. l_max - 1
+// in one buffer, each level padded to 16 bytes.
+uint64_t pyramid_layout(const Geom &g, uint8_t *base, Pyramid *pm) {
+    uint64_t tot = 0;
+    for (int l = g.l_min; l <= g.l_max - 1; ++l) {
+        if (pm) pm->status[l] = base + tot;
         tot += ((uint64_t)g.y_num[l] * g.x_num[l] * g.z_num[l] + 15) & ~uint64_t(15);
     }
-    uint8_t *st = c->pyr_status.as_on<uint8_t>(tot ? tot : 16, s);
-    APRB_CUDA(cudaMemsetAsync(st, 0, tot ? tot : 16, s));
-    for (int l = g.l_min; l <= top; ++l) pm.status[l] = st + off[l];
+    return tot;
+}
+
+// get_apr_method_patch for z-tiles [first, first + count) of the volume's
+// blocked tiling, each filling the global particle-cell pyramid
+// (fill_global_particle_cell_tree); the tiles' planes, ghosts included, are
+// read from slab, which holds planes [slab_z0, ...) of the volume.
+template <typename IT>
+void fill_tiles(aprb_converter *c, aprb_params &p, const Geom &g, Pyramid &pm, const uint16_t *slab, int slab_z0,
+                int yn, int xn, int zn, int zblock, int ghost, int first, int count, cudaStream_t s) {
+    const int L = g.l_max, top = L - 1;
     const int nb = std::max(zn / zblock, 1);
-    for (int b = 0; b < nb; ++b) {
+    for (int b = first; b < first + count && b < nb; ++b) {
         const ZTile t = z_tile(b, nb, zn, zblock, ghost);
-        PixelOut<IT> po = pixel_stages<IT>(c, p, img + (uint64_t)(t.z0 - t.gl) * xn * yn, yn, xn, t.pz, s);
+        PixelOut<IT> po =
+            pixel_stages<IT>(c, p, slab + (uint64_t)(t.z0 - t.gl - slab_z0) * xn * yn, yn, xn, t.pz, s);
         apply_auto_parameters<IT>(c, p, po, s);
         uint8_t *lev = c->pyr_level.as_on<uint8_t>(po.nd, s);
         launch_levels<IT>(po.grad, po.lis, po.ids, po.nd, po.d_off, p, L, top, lev, nullptr, 0, s);
         launch_fill_patch(g, pm, lev, t, c->tile_pyr, s);
     }
-    if (L > 2) launch_pulling_scheme(g, pm, s, false);
+}
+
+// pulling scheme and linear structure of a filled pyramid (consumed)
+void apr_from_pyramid(aprb_converter *c, const aprb_params &p, Pyramid &pm, aprb_apr *a, cudaStream_t s) {
+    if (a->g.l_max > 2) launch_pulling_scheme(a->g, pm, s, false);
     build_structure(c, p, pm, a, s);
     a->par = p;  // the last tile's thresholds, as the reference's par keeps them
     c->have = false;  // intermediates are per tile
+}
+
+void init_apr_geometry(aprb_apr *a, int yn, int xn, int zn) {
+    a->n_xz = apr_geometry(yn, xn, zn, a->g);
+    a->org[0] = yn;
+    a->org[1] = xn;
+    a->org[2] = zn;
+}
+
+// APRConverterBatch<IT> (APRConverterBatch.hpp:114-175): the pixel stages and
+// levels per z-tile with ghost planes, each tile filling the global
+// particle-cell pyramid (fill_global_particle_cell_tree, :282-314), then one
+// pulling scheme and one linear structure for the volume.
+template <typename IT>
+void run_get_apr_by_block(aprb_converter *c, aprb_params p, const uint16_t *img, int yn, int xn, int zn,
+                          int zblock, int ghost, cudaStream_t s, aprb_apr *a) {
+    init_apr_geometry(a, yn, xn, zn);
+    APRB_CUDA(cudaMemsetAsync(c->err.as_on<unsigned>(2, s), 0, 2 * sizeof(unsigned), s));
+    Pyramid pm;
+    const uint64_t tot = pyramid_layout(a->g, nullptr, nullptr);
+    uint8_t *st = c->pyr_status.as_on<uint8_t>(tot ? tot : 16, s);
+    APRB_CUDA(cudaMemsetAsync(st, 0, tot ? tot : 16, s));
+    pyramid_layout(a->g, st, &pm);
+    fill_tiles<IT>(c, p, a->g, pm, img, 0, yn, xn, zn, zblock, ghost, 0, std::max(zn / zblock, 1), s);
+    apr_from_pyramid(c, p, pm, a, s);
 }
 
 void get_apr_impl(aprb_converter *c, const aprb_params *p, const uint16_t *img_dev, int y, int x, int z,
@@ -599,6 +629,68 @@ aprb_status aprb_get_apr_by_block(aprb_converter *c, const aprb_params *p, const
         uint16_t *d = c->img.as_on<uint16_t>(n, s);
         APRB_CUDA(cudaMemcpyAsync(d, img, n * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
         get_apr_by_block_impl(c, p, d, y_num, x_num, z_num, z_block_size, ghost_z, s, out);
+    });
+}
+
+aprb_status aprb_pyramid_bytes(int y_num, int x_num, int z_num, uint64_t *bytes) {
+    return guarded([&] {
+        ARG_CHECK(bytes && y_num >= 1 && x_num >= 1 && z_num >= 1, "invalid argument");
+        Geom g;
+        apr_geometry(y_num, x_num, z_num, g);
+        const uint64_t tot = pyramid_layout(g, nullptr, nullptr);
+        *bytes = tot ? tot : 16;
+    });
+}
+
+aprb_status aprb_pyramid_fill_tiles_device(aprb_converter *c, const aprb_params *p, uint8_t *pyramid_dev, int y_num,
+                                           int x_num, int z_num, int z_block_size, int ghost_z, int first_tile,
+                                           int n_tiles, const uint16_t *slab_dev, int slab_z0, int slab_z_num,
+                                           void *stream) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(c && p && pyramid_dev && slab_dev, "null argument");
+        ARG_CHECK(y_num >= 1 && x_num >= 1 && z_num >= 1 && y_num <= 65535 && x_num <= 65535 && z_num <= 65535,
+                  "invalid dimensions");
+        ARG_CHECK(z_block_size >= 1 && ghost_z >= 0 && p->rel_error > 0, "invalid tiling or parameters");
+        const int nb = std::max(z_num / z_block_size, 1);
+        ARG_CHECK(first_tile >= 0 && n_tiles >= 0 && first_tile + n_tiles <= nb, "tile range outside the tiling");
+        if (n_tiles == 0) return;
+        const ZTile t0 = z_tile(first_tile, nb, z_num, z_block_size, ghost_z);
+        const ZTile t1 = z_tile(first_tile + n_tiles - 1, nb, z_num, z_block_size, ghost_z);
+        ARG_CHECK(slab_z0 <= t0.z0 - t0.gl && t1.zf + t1.gr <= slab_z0 + slab_z_num,
+                  "the slab does not hold the tiles' planes and ghosts");
+        cudaStream_t s = (cudaStream_t)stream;
+        Geom g;
+        apr_geometry(y_num, x_num, z_num, g);
+        Pyramid pm;
+        pyramid_layout(g, pyramid_dev, &pm);
+        APRB_CUDA(cudaMemsetAsync(c->err.as_on<unsigned>(2, s), 0, 2 * sizeof(unsigned), s));
+        aprb_params par = *p;
+        if (c->image_type == APRB_IMAGE_U16)
+            fill_tiles<uint16_t>(c, par, g, pm, slab_dev, slab_z0, y_num, x_num, z_num, z_block_size, ghost_z,
+                                 first_tile, n_tiles, s);
+        else
+            fill_tiles<float>(c, par, g, pm, slab_dev, slab_z0, y_num, x_num, z_num, z_block_size, ghost_z,
+                              first_tile, n_tiles, s);
+        throw_if_overflow(c, s);
+    });
+}
+
+aprb_status aprb_get_apr_from_pyramid_device(aprb_converter *c, const aprb_params *p, uint8_t *pyramid_dev, int y_num,
+                                             int x_num, int z_num, void *stream, aprb_apr **out) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(c && p && pyramid_dev && out, "null argument");
+        ARG_CHECK(y_num >= 1 && x_num >= 1 && z_num >= 1 && y_num <= 65535 && x_num <= 65535 && z_num <= 65535,
+                  "invalid dimensions");
+        cudaStream_t s = (cudaStream_t)stream;
+        std::unique_ptr<aprb_apr> a(new aprb_apr());
+        init_apr_geometry(a.get(), y_num, x_num, z_num);
+        APRB_CUDA(cudaMemsetAsync(c->err.as_on<unsigned>(2, s), 0, 2 * sizeof(unsigned), s));
+        Pyramid pm;
+        pyramid_layout(a->g, pyramid_dev, &pm);
+        apr_from_pyramid(c, *p, pm, a.get(), s);
+        *out = a.release();
     });
 }
 

@@ -1010,6 +1010,43 @@ static void z_block(int b, int nb, int zn, int zblock, int ghost, int *z0, int *
     *gr = (zn - *zf) < ghost ? (zn - *zf) : ghost;
 }
 
+/* get_apr_method_patch (APRConverterBatch.hpp:190-271) for tiles [first, first +
+ * count) of the blocked tiling, each filling the global particle-cell tree t
+ * (fill_global_particle_cell_tree :282-314); slab holds planes [slab_z0, ...)
+ * of the volume.  *offset receives the last tile's bspline offset. */
+static int fill_tiles(pct_t *t, const uint16_t *slab, int slab_z0, int yn, int xn, int zn, const orc_params *p,
+                      int image_type, int zblock, int ghost, int first, int count, int l_max, float *offset) {
+    int nb = zn / zblock > 1 ? zn / zblock : 1;
+    int e = ORC_OK;
+    for (int b = first; b < first + count && b < nb && e == ORC_OK; ++b) {
+        int z0, zf, gl, gr;
+        z_block(b, nb, zn, zblock, ghost, &z0, &zf, &gl, &gr);
+        int pz = zf + gr - (z0 - gl);
+        float *grad, *ids, *lis;
+        e = pixel_stages(slab + (size_t)(z0 - gl - slab_z0) * xn * yn, yn, xn, pz, p, image_type == 1, offset, &grad,
+                         &ids, &lis, NULL);
+        if (e != ORC_OK) break;
+        int cy = (int)ceil(yn / 2.0), cx = (int)ceil(xn / 2.0), cz = (int)ceil(pz / 2.0);
+        apply_and_levels(NULL, grad, lis, ids, (size_t)cy * cx * cz, *offset, p, l_max);
+        free(grad); free(ids);
+        float *cur = lis;
+        if (t->l_max >= t->l_min) {
+            e = pct_fill_patch(t, t->l_max, cur, cy, cx, cz, gl, gr, z0);
+            for (int l = t->l_max - 1; l >= t->l_min && e == ORC_OK; --l) {
+                int ny = (int)ceil(cy / 2.0), nx = (int)ceil(cx / 2.0), nz = (int)ceil(cz / 2.0);
+                float *nxt = (float *)malloc(sizeof(float) * (size_t)ny * nx * nz);
+                downsample2(cur, cy, cx, cz, nxt, DS_MAX);
+                free(cur);
+                cur = nxt;
+                cy = ny; cx = nx; cz = nz;
+                e = pct_fill_patch(t, l, cur, cy, cx, cz, gl, gr, z0);
+            }
+        }
+        free(cur);
+    }
+    return e;
+}
+
 /* APRConverterBatch<IT>: get_apr_method_patch per z-tile
  * (APRConverterBatch.hpp:190-271), fill_global_particle_cell_tree (:282-314),
  * then one pulling scheme and linear structure for the whole volume. */
@@ -1024,38 +1061,70 @@ int orc_get_apr_by_block(const uint16_t *img, int yn, int xn, int zn, const orc_
     pct_t t;
     pct_init(&t, &r->acc);
     int nb = zn / zblock > 1 ? zn / zblock : 1;
-    int e = ORC_OK;
-    for (int b = 0; b < nb && e == ORC_OK; ++b) {
-        int z0, zf, gl, gr;
-        z_block(b, nb, zn, zblock, ghost, &z0, &zf, &gl, &gr);
-        int pz = zf + gr - (z0 - gl);
-        float *grad, *ids, *lis;
-        e = pixel_stages(img + (size_t)(z0 - gl) * xn * yn, yn, xn, pz, p, image_type == 1, &r->offset, &grad, &ids,
-                         &lis, NULL);
-        if (e != ORC_OK) break;
-        int cy = (int)ceil(yn / 2.0), cx = (int)ceil(xn / 2.0), cz = (int)ceil(pz / 2.0);
-        apply_and_levels(NULL, grad, lis, ids, (size_t)cy * cx * cz, r->offset, p, r->acc.l_max);
-        free(grad); free(ids);
-        float *cur = lis;
-        if (t.l_max >= t.l_min) {
-            e = pct_fill_patch(&t, t.l_max, cur, cy, cx, cz, gl, gr, z0);
-            for (int l = t.l_max - 1; l >= t.l_min && e == ORC_OK; --l) {
-                int ny = (int)ceil(cy / 2.0), nx = (int)ceil(cx / 2.0), nz = (int)ceil(cz / 2.0);
-                float *nxt = (float *)malloc(sizeof(float) * (size_t)ny * nx * nz);
-                downsample2(cur, cy, cx, cz, nxt, DS_MAX);
-                free(cur);
-                cur = nxt;
-                cy = ny; cx = nx; cz = nz;
-                e = pct_fill_patch(&t, l, cur, cy, cx, cz, gl, gr, z0);
-            }
-        }
-        free(cur);
-    }
+    int e = fill_tiles(&t, img, 0, yn, xn, zn, p, image_type, zblock, ghost, 0, nb, r->acc.l_max, &r->offset);
     if (e == ORC_OK) {
         if (t.l_max >= t.l_min) pulling_scheme(&t);
         e = linear_structure(&r->acc, &t, p->neighborhood_optimization);
     }
     pct_free(&t);
+    if (e != ORC_OK) { orc_free(r); return e; }
+    *out = r;
+    return ORC_OK;
+}
+
+/* The particle-cell tree in one caller buffer: levels l_min .. l_max - 1 of the
+ * tree, each y_num x x_num x z_num bytes, concatenated (the arrays of
+ * PullingScheme::particle_cell_tree, PullingScheme.hpp:92-104). */
+static size_t pct_view(pct_t *t, const orc_access *g, uint8_t *buf) {
+    memset(t, 0, sizeof(*t));
+    t->l_max = g->l_max - 1;
+    t->l_min = g->l_min;
+    size_t tot = 0;
+    for (int l = t->l_min; l <= t->l_max; ++l) {
+        double cell = powr(2, t->l_max - l + 1);
+        t->y_num[l] = (int)ceil(g->org[0] / cell);
+        t->x_num[l] = (int)ceil(g->org[1] / cell);
+        t->z_num[l] = (int)ceil(g->org[2] / cell);
+        if (buf) t->m[l] = buf + tot;
+        tot += (size_t)t->y_num[l] * t->x_num[l] * t->z_num[l];
+    }
+    return tot;
+}
+
+size_t orc_pyramid_bytes(int yn, int xn, int zn) {
+    orc_access g;
+    memset(&g, 0, sizeof(g));
+    geninfo_init(&g, yn, xn, zn);
+    pct_t t;
+    size_t n = pct_view(&t, &g, NULL);
+    free(g.xz_end);
+    return n;
+}
+
+int orc_pyramid_fill_tiles(const uint16_t *slab, int slab_z0, int yn, int xn, int zn, const orc_params *p,
+                           int image_type, int zblock, int ghost, int first, int count, uint8_t *pyramid) {
+    if (yn < 1 || xn < 1 || zn < 1 || zblock < 1 || ghost < 0 || first < 0 || count < 0) return ORC_ERR_ARG;
+    orc_access g;
+    memset(&g, 0, sizeof(g));
+    geninfo_init(&g, yn, xn, zn);
+    pct_t t;
+    pct_view(&t, &g, pyramid);
+    float offset = 0;
+    int e = fill_tiles(&t, slab, slab_z0, yn, xn, zn, p, image_type, zblock, ghost, first, count, g.l_max, &offset);
+    free(g.xz_end);
+    return e;
+}
+
+int orc_apr_from_pyramid(uint8_t *pyramid, int yn, int xn, int zn, const orc_params *p, orc_apr **out) {
+    *out = NULL;
+    orc_apr *r = (orc_apr *)calloc(1, sizeof(orc_apr));
+    geninfo_init(&r->acc, yn, xn, zn);
+    r->yn = yn; r->xn = xn; r->zn = zn;
+    r->yd = (int)ceil(yn / 2.0); r->xd = (int)ceil(xn / 2.0); r->zd = (int)ceil(zn / 2.0);
+    pct_t t;
+    pct_view(&t, &r->acc, pyramid);
+    if (t.l_max >= t.l_min) pulling_scheme(&t);
+    int e = linear_structure(&r->acc, &t, p->neighborhood_optimization);
     if (e != ORC_OK) { orc_free(r); return e; }
     *out = r;
     return ORC_OK;

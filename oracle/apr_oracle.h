@@ -75,6 +75,13 @@ int orc_get_apr_by_block(const uint16_t *img, int y, int x, int z, const orc_par
                          int zblock, int ghost, orc_apr **out);
 
 void orc_free(orc_apr *a);
+/* the blocked converter split by tiles: bytes of the flat particle-cell tree,
+ * tiles [first, first + count) filling it (slab = planes [slab_z0, ...) of the
+ * volume), and the APR of a filled tree (pulling scheme in place) */
+size_t orc_pyramid_bytes(int y, int x, int z);
+int orc_pyramid_fill_tiles(const uint16_t *slab, int slab_z0, int y, int x, int z, const orc_params *p,
+                           int image_type, int zblock, int ghost, int first, int count, uint8_t *pyramid);
+int orc_apr_from_pyramid(uint8_t *pyramid, int y, int x, int z, const orc_params *p, orc_apr **out);
 const orc_access *orc_get_access(const orc_apr *a);
 /* Intermediates kept by orc_get_apr (ds = ceil(dim/2) per axis):
  * which: 0 smoothed full-res image (IT values as float), 1 ds gradient after

@@ -112,6 +112,13 @@ def lib():
                                            C.c_int, C.c_int, C.c_int, C.POINTER(C.c_void_p)]
         L.orc_sample_image_by_block.argtypes = [C.POINTER(OrcAccess), C.POINTER(C.c_uint16), C.c_int, C.c_int,
                                                 C.POINTER(C.c_uint16)]
+        L.orc_pyramid_bytes.argtypes = [C.c_int, C.c_int, C.c_int]
+        L.orc_pyramid_bytes.restype = C.c_size_t
+        L.orc_pyramid_fill_tiles.argtypes = [C.POINTER(C.c_uint16), C.c_int, C.c_int, C.c_int, C.c_int,
+                                             C.POINTER(OrcParams), C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                             C.POINTER(C.c_uint8)]
+        L.orc_apr_from_pyramid.argtypes = [C.POINTER(C.c_uint8), C.c_int, C.c_int, C.c_int, C.POINTER(OrcParams),
+                                           C.POINTER(C.c_void_p)]
         L.orc_threshold_li.argtypes = [C.POINTER(C.c_float), C.c_size_t, C.c_int, C.c_int]
         L.orc_threshold_li.restype = C.c_float
         L.orc_auto_parameters.argtypes = [C.POINTER(C.c_float)] * 3 + [C.c_size_t, C.c_float, C.c_int, C.c_int] + \
@@ -285,6 +292,35 @@ def orc_get_apr_by_block(img, params, image_type, z_block, ghost):
     acc = Access.from_c(L.orc_get_access(h).contents)
     L.orc_free(h)
     return 0, acc
+
+
+class OracleTileBackend:
+    """The CPU checker behind libapr_b200.distributed.get_apr_by_block_distributed:
+    the oracle's tile fill and pyramid solve on CPU torch tensors (gloo ranks)."""
+
+    def __init__(self, params, image_type=1):
+        self.p, self.it = params, image_type
+
+    def pyramid(self, shape):
+        import torch
+        z, x, y = shape
+        return torch.zeros(int(lib().orc_pyramid_bytes(y, x, z)), dtype=torch.uint8)
+
+    def fill(self, pyr, shape, z_block, ghost, first, count, slab, slab_z0):
+        z, x, y = shape
+        a = np.ascontiguousarray(slab.numpy() if hasattr(slab, "numpy") else slab, dtype=np.uint16)
+        pv = pyr.numpy()
+        assert lib().orc_pyramid_fill_tiles(_ptr(a, C.c_uint16), slab_z0, y, x, z, C.byref(self.p), self.it,
+                                            z_block, ghost, first, count, _ptr(pv, C.c_uint8)) == 0
+
+    def finish(self, pyr, shape):
+        z, x, y = shape
+        h = C.c_void_p()
+        pv = pyr.numpy()
+        assert lib().orc_apr_from_pyramid(_ptr(pv, C.c_uint8), y, x, z, C.byref(self.p), C.byref(h)) == 0
+        acc = Access.from_c(lib().orc_get_access(h).contents)
+        lib().orc_free(h)
+        return acc
 
 
 def orc_sample_by_block(acc, img, z_block, ghost):

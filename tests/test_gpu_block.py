@@ -54,3 +54,39 @@ def test_batch_matches_per_volume_calls():
         assert conv.get_apr(one, im)
         for a, b in zip(apr.linear_access(), one.linear_access()):
             assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("shape,zb,ghost,image_type,world",
+                         [((100, 40, 48), 32, 8, 1, 2), ((200, 32, 32), 32, 16, 0, 3), ((84, 33, 50), 16, 4, 1, 4),
+                          ((96, 30, 40), 20, 8, 0, 2)])
+def test_split_by_tiles_equals_blocked_converter(shape, zb, ghost, image_type, world):
+    """The multi-GPU split on one GPU: each of `world` emulated ranks fills
+    its own pyramid from its own slab (its tiles and ghosts only), the
+    pyramids are combined by element-wise maximum (what the MAX all-reduce
+    computes) and the structure built from the result equals the blocked
+    converter's and the oracle's."""
+    import torch
+    from libapr_b200 import distributed as D
+    if not B.block_tiling_in_bounds(shape, zb, ghost):
+        pytest.skip("tiling where the reference writes outside a coarse level")
+    img = volume(shape, 30, 3)
+    it = "uint16" if image_type == 1 else "float"
+    be = D.TileBackend(it, lib_params())
+    total = None
+    for r in range(world):
+        lo, hi = D.rank_slab(shape[0], zb, ghost, r, world)
+        first, count = D.rank_tiles(D.tile_count(shape[0], zb), r, world)
+        pyr = be.pyramid(shape)
+        if count:
+            slab = torch.from_numpy(np.ascontiguousarray(img[lo:hi]).view(np.int16)).cuda()
+            be.fill(pyr, shape, zb, ghost, first, count, slab, lo)
+        total = pyr if total is None else torch.maximum(total, pyr)
+    apr = be.finish(total, shape)
+    conv = A.APRConverterBatch(it, z_block_size=zb, ghost_z=ghost)
+    conv.par = lib_params()
+    one = A.APR()
+    assert conv.get_apr(one, img)
+    for a, b in zip(apr.linear_access(), one.linear_access()):
+        assert np.array_equal(a, b)
+    e, acc = B.orc_get_apr_by_block(img, oracle_params(), image_type, zb, ghost)
+    assert e == 0 and np.array_equal(apr.linear_access()[2], acc.y_vec)
