@@ -102,6 +102,14 @@ aprb_status aprb_converter_destroy(aprb_converter *c);
 /* keep_intermediates != 0 keeps the APRB_STAGE_* buffers after get_apr */
 aprb_status aprb_converter_keep_intermediates(aprb_converter *c, int keep);
 
+/* keep != 0: aprb_get_apr (host buffer) hands its device copy of the input image to the
+ * APR it returns, and the first aprb_sample_image of that APR from the same host buffer
+ * samples that copy instead of uploading the image again (the reference's call pair
+ * get_apr(apr, img); sample_image(apr, img) moves the volume to the GPU once).  The caller
+ * must not change the image in between; the copy is released by that sample_image or
+ * with the APR.  No counterpart in the reference (a host-transfer option). */
+aprb_status aprb_converter_keep_input(aprb_converter *c, int keep);
+
 /* APRConverter<IT>::get_apr(APR&, PixelData<uint16_t>&) (APRConverter.hpp:591-600 -> get_apr_cpu :535-582) */
 aprb_status aprb_get_apr(aprb_converter *c, const aprb_params *p, const uint16_t *img, int y_num, int x_num,
                          int z_num, aprb_apr **out);

@@ -245,6 +245,12 @@ class APRConverter:
             st = lib().aprb_get_apr(self._h, C.byref(p), _ptr(a), y, x, z, C.byref(h))
         return self._finish(st, h, apr)
 
+    def keep_input(self, keep=True):
+        """Host-buffer get_apr hands its device copy of the image to the APR, and
+        the next sample_image of that APR from the same numpy array samples it
+        without a second upload (the array must not change in between)."""
+        check(lib().aprb_converter_keep_input(self._h, int(keep)))
+
     def intermediate(self, stage, shape_zxy):
         """Copy of one APRB_STAGE_* buffer of the last get_apr (needs keep_intermediates)."""
         out = np.zeros(shape_zxy, np.float32)

@@ -47,6 +47,7 @@ SIGNATURES = {
     "aprb_converter_create": ([_i, C.POINTER(_vp)], _i),
     "aprb_converter_destroy": ([_vp], _i),
     "aprb_converter_keep_intermediates": ([_vp, _i], _i),
+    "aprb_converter_keep_input": ([_vp, _i], _i),
     "aprb_get_apr": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, C.POINTER(_vp)], _i),
     "aprb_get_apr_device": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, _vp, C.POINTER(_vp)], _i),
     "aprb_get_apr_by_block": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, _i, _i, C.POINTER(_vp)], _i),

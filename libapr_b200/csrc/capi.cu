@@ -177,11 +177,16 @@ struct aprb_apr {
     // learned proposal: level row of every particle (pooled), built on first use
     DevBuf cnn_rows;
     bool cnn_ready = false;
+    // device copy of the host image it was built from (converter keep_input),
+    // used and released by the first sample_image from the same host buffer
+    mutable DevBuf kept_img;
+    mutable const uint16_t *kept_host = nullptr;
 };
 
 struct aprb_converter {
     int image_type = APRB_IMAGE_U16;
     int keep = 0;
+    int keep_input = 0;  // hand the host call's device copy of the input to its APR
     int dims[3] = {0, 0, 0};  // y, x, z of the last call
     DevBuf img, work, grad, grad_keep, ids_raw, ids, lis, lis_keep, pyr_status, pyr_level, mm, offset, err;
     DevBuf scan_tmp, tile_pyr, iir_ckpt;
@@ -768,6 +773,17 @@ aprb_status aprb_get_apr(aprb_converter *c, const aprb_params *p, const uint16_t
             cudaStreamSynchronize(up);  // no copy from the caller's buffer outlives the call
             throw;
         }
+        if (c->keep_input) {
+            (*out)->kept_img.swap(c->img);
+            (*out)->kept_host = img;
+        }
+    });
+}
+
+aprb_status aprb_converter_keep_input(aprb_converter *c, int keep) {
+    return guarded([&] {
+        ARG_CHECK(c, "null argument");
+        c->keep_input = keep != 0;
     });
 }
 
@@ -1056,10 +1072,20 @@ aprb_status aprb_sample_image(const aprb_apr *a, const uint16_t *img, uint16_t *
         const int L = g.l_max, zn = a->org[2];
         const uint64_t n = (uint64_t)a->org[0] * a->org[1] * zn;
         const uint64_t plane = (uint64_t)a->org[0] * a->org[1];
-        uint16_t *di = scratch().io_in.as<uint16_t>(n);
         uint16_t *dp = scratch().parts_u16.as<uint16_t>(a->P ? a->P : 1);
         const uint64_t *xz = (const uint64_t *)a->xz_end.p;
         const uint16_t *yv = (const uint16_t *)a->y_vec.p;
+        if (a->kept_img.p && a->kept_host == img) {
+            // the APR still holds the device copy its converter made of this
+            // host buffer (keep_input): no second upload
+            launch_sample(g, xz, yv, (const uint16_t *)a->kept_img.p, dp, scratch().pyr, s);
+            if (a->P) APRB_CUDA(cudaMemcpyAsync(parts, dp, a->P * sizeof(uint16_t), cudaMemcpyDeviceToHost, s));
+            APRB_CUDA(cudaStreamSynchronize(s));
+            a->kept_img.release();
+            a->kept_host = nullptr;
+            return;
+        }
+        uint16_t *di = scratch().io_in.as<uint16_t>(n);
         // about 2^26 voxels (128 MiB) per chunk, an even number of planes
         const uint64_t want = ((uint64_t(1) << 26) / std::max<uint64_t>(plane, 1)) & ~uint64_t(1);
         const int chunk = (int)std::max<uint64_t>(kSampleChunk, want);

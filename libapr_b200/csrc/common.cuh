@@ -10,6 +10,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <utility>
 
 #include "../../include/aprb200.h"
 
@@ -130,6 +131,11 @@ struct DevBuf {
         p = nullptr;
         cap = 0;
         pooled = false;
+    }
+    void swap(DevBuf &o) {
+        std::swap(p, o.p);
+        std::swap(cap, o.cap);
+        std::swap(pooled, o.pooled);
     }
     ~DevBuf() { release(); }
     DevBuf() = default;

@@ -127,6 +127,33 @@ def lib():
     return _lib
 
 
+_bind = None
+
+
+def bind_available():
+    return os.path.exists(os.path.join(HERE, "_ref", "libaprbind.so"))
+
+
+def bind_lib():
+    """_ref/libaprbind.so: include/aprb200_libapr.hpp driven with LibAPR's own
+    objects (see ref_bind.cu)."""
+    global _bind
+    if _bind is None:
+        L = C.CDLL(os.path.join(HERE, "_ref", "libaprbind.so"))
+        vp, u16p = C.c_void_p, C.POINTER(C.c_uint16)
+        L.bind_get_apr.argtypes = [u16p, C.c_int, C.c_int, C.c_int, C.POINTER(OrcParams), C.c_int,
+                                   C.POINTER(vp), C.POINTER(C.c_uint64), C.POINTER(C.c_float)]
+        L.bind_free.argtypes = [vp]
+        L.bind_free.restype = None
+        L.bind_particles.argtypes = [vp, u16p, u16p, u16p, u16p]
+        L.bind_sample.argtypes = [vp, u16p, u16p]
+        L.bind_convolve.argtypes = [vp, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                    C.c_int, C.c_int, C.c_int, C.c_int]
+        L.bind_rl.argtypes = [vp, u16p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int]
+        _bind = L
+    return _bind
+
+
 def ref_available(fast=False):
     return os.path.exists(os.path.join(HERE, "_ref", "libaprref_fast.so" if fast else "libaprref.so"))
 

@@ -182,3 +182,27 @@ def test_host_calls_copy_in_chunks_like_device_calls(image_type):
     torch.cuda.synchronize()
     ph = A.ParticleData().sample_image(a_host, host).data
     assert np.array_equal(ph, pd.cpu().numpy().view(np.uint16))
+
+
+def test_keep_input_samples_the_uploaded_copy():
+    """keep_input: the host-buffer get_apr hands its device copy to the APR,
+    sample_image from the same array uses it (no second upload) and equals
+    the plain call; a different array is uploaded as usual."""
+    img = volume((48, 64, 72), 30, 31)
+    conv = A.APRConverter("float")
+    conv.par = lib_params()
+    ref_apr = A.APR()
+    assert conv.get_apr(ref_apr, img)
+    ref_parts = A.ParticleData().sample_image(ref_apr, img).data
+    conv.keep_input(True)
+    apr = A.APR()
+    assert conv.get_apr(apr, img)
+    assert np.array_equal(A.ParticleData().sample_image(apr, img).data, ref_parts)
+    # the kept copy was consumed: a second sampling uploads the array again
+    assert np.array_equal(A.ParticleData().sample_image(apr, img).data, ref_parts)
+    other = img.copy()
+    other[::2] //= 2
+    apr2 = A.APR()
+    assert conv.get_apr(apr2, img)
+    assert np.array_equal(A.ParticleData().sample_image(apr2, other).data,
+                          A.ParticleData().sample_image(ref_apr, other).data)
