@@ -338,17 +338,23 @@ bool launch_strided_iir_tma(float *work, int yn, int xn, int zn, bool zaxis, con
 
 namespace aprb {
 
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::once_flag g_encode_once;
+}  // namespace
+
+// (map == nullptr: only looks the driver's encoder up)
 bool make_tensor_map_3d_f32(CUtensorMap *map, const void *base, const uint64_t d[3], uint64_t s1, uint64_t s2,
                             const uint32_t b[3]) {
-    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
+    std::call_once(g_encode_once, [] {
         void *p = nullptr;
         cudaDriverEntryPointQueryResult q;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
             q == cudaDriverEntryPointSuccess)
-            encode = (PFN_cuTensorMapEncodeTiled_v12000)p;
+            g_encode = (PFN_cuTensorMapEncodeTiled_v12000)p;
     });
+    auto encode = g_encode;
+    if (!map) return encode != nullptr;
     if (!encode || ((uintptr_t)base & 15) != 0 || (s1 & 15) != 0 || (s2 & 15) != 0) return false;
     cuuint64_t gdim[3] = {d[0], d[1], d[2]};
     cuuint64_t gstride[2] = {s1, s2};
@@ -357,6 +363,21 @@ bool make_tensor_map_3d_f32(CUtensorMap *map, const void *base, const uint64_t d
     const CUresult r = encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void *>(base), gdim, gstride, box,
                               estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+bool make_tensor_map_2d_sw128(CUtensorMap *map, const void *base, bool f32, const uint64_t d[2], uint64_t s1,
+                              const uint32_t b[2]) {
+    make_tensor_map_3d_f32(nullptr, nullptr, nullptr, 0, 0, nullptr);  // looks the encoder up
+    if (!g_encode || ((uintptr_t)base & 15) != 0 || (s1 & 15) != 0) return false;
+    cuuint64_t gdim[2] = {d[0], d[1]};
+    cuuint64_t gstride[1] = {s1};
+    cuuint32_t box[2] = {b[0], b[1]};
+    cuuint32_t estride[2] = {1, 1};
+    const CUresult r =
+        g_encode(map, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16, 2, const_cast<void *>(base),
+                 gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS;
 }
 

@@ -36,6 +36,15 @@ struct LisBuffers {
 bool launch_strided_iir_tma(float *work, int yn, int xn, int zn, bool zaxis, const IIRDev &c, unsigned *d_timeout,
                             float2 *ckpt, uint64_t ckpt_elems, cudaStream_t s);
 
+// ---- iir_y_tma.cu
+// The y pass of the recursive smoothing of a uint16 image into a float
+// working image with TMA-staged tiles; false when the layout does not allow
+// it (y_num not a multiple of 8 or below 64, fewer than 32 lines, unaligned
+// buffers), and the caller runs the cp.async-staged kernel instead.  ckpt
+// holds ckpt_elems recurrence states (64-sample tiles x lines).
+bool launch_iir_y_tma(const uint16_t *img, float *work, int yn, uint64_t nlines, const IIRDev &c, unsigned *d_timeout,
+                      float2 *ckpt, uint64_t ckpt_elems, cudaStream_t s);
+
 // ---- pipeline.cu
 void launch_check_div_const(float d, unsigned long long *out, cudaStream_t s);
 void launch_minmax_offset(const uint16_t *img, uint64_t n, unsigned *mm, float *offset, int apply, cudaStream_t s);

@@ -1824,15 +1824,19 @@ static void launch_smooth_yx(const uint16_t *img, IT *work, int yn, int xn, int 
         APRB_PROF("bspline_y", s);
         const IIRDev c = dev_coef(iir_coefficients(lambda, yn));
         const uint64_t nlines = (uint64_t)xn * zn;
-        if (yn % 2 == 0 && ((uintptr_t)img & 3) == 0) {
-            const int ntile = (yn + kAY - 1) / kAY;
-            float2 *ck = ckpt.as_on<float2>(nlines * (uint64_t)ntile, s);
+        const uint64_t nck = nlines * (uint64_t)((yn + kAY - 1) / kAY);
+        if (std::is_same<IT, float>::value &&
+            launch_iir_y_tma(img, (float *)work, yn, nlines, c, d_err + 1, ckpt.as_on<float2>(nck, s), nck, s)) {
+            // TMA-staged tiles (iir_y_tma.cu); the launch is counted there
+        } else if (yn % 2 == 0 && ((uintptr_t)img & 3) == 0) {
+            float2 *ck = ckpt.as_on<float2>(nck, s);
             iir_y_rc_kernel<IT><<<blocks_for(nlines, 32 * kAWarps), 32 * kAWarps, 0, s>>>(img, work, yn, nlines, c, d_offset, d_err, ck);
+            count_launch();
         } else {
             const unsigned blocks = blocks_for(nlines, kYWarps * kTile);
             iir_y_kernel<IT><<<blocks, kYWarps * 32, 0, s>>>(img, work, yn, nlines, c, d_offset, d_err);
+            count_launch();
         }
-        count_launch();
         APRB_CHECK_LAUNCH();
     } else {
         APRB_PROF("offset_copy", s);

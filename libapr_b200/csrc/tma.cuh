@@ -19,6 +19,12 @@ namespace aprb {
 // takes a path without TMA.
 bool make_tensor_map_3d_f32(CUtensorMap *map, const void *base, const uint64_t d[3], uint64_t s1, uint64_t s2,
                             const uint32_t b[3]);
+// A 2-D tiled tensor map (d[0] contiguous, row stride s1 bytes) over uint16 or
+// float elements with 128-byte swizzling: the box's rows (128 bytes each) land
+// in shared memory with their 16-byte chunks permuted, chunk j of row r at
+// position j ^ (r % 8) (the destination must be 1024-byte aligned).
+bool make_tensor_map_2d_sw128(CUtensorMap *map, const void *base, bool f32, const uint64_t d[2], uint64_t s1,
+                              const uint32_t b[2]);
 
 // Iterations of a bounded mbarrier wait (each try_wait may suspend the thread
 // for a short, hardware-defined time); a wait that runs out reports failure.
@@ -63,6 +69,21 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, u
         "[%5];" ::"r"(smem_addr(dst)),
         "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(smem_addr(bar))
         : "memory");
+}
+
+__device__ __forceinline__ void tma_load_2d(void *dst, const CUtensorMap *map, uint64_t *bar, int c0, int c1) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap *map, const void *src, int c0, int c1) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%2, %3}], [%1];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(smem_addr(src)), "r"(c0), "r"(c1)
+                 : "memory");
 }
 
 __device__ __forceinline__ void tma_store_3d(const CUtensorMap *map, const void *src, int c0, int c1, int c2) {

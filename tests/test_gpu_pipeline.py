@@ -47,11 +47,14 @@ def test_get_apr_bit_exact(shape, blobs, seed, image_type):
     assert np.array_equal(parts, B.orc_sample(acc, img))
 
 
-# shapes that take the TMA-staged x / z smoothing (float ImageType, y_num a
-# multiple of 4 and >= 256, >= 16 samples along the axis): partial TMA boxes
-# (y_num 600, 260), partial 16-sample segments, and an x extent below 16 that
-# keeps the register-staged x pass
-TMA_SHAPES = [((37, 45, 600), 25, 21), ((16, 300, 260), 30, 22), ((130, 17, 512), 40, 23), ((20, 9, 256), 6, 24)]
+# shapes that take the TMA-staged smoothing (float ImageType): x / z passes
+# with y_num a multiple of 4 and >= 256 and >= 16 samples along the axis --
+# partial TMA boxes (y_num 600, 260), partial 16-sample segments, an x extent
+# below 16 that keeps the register-staged x pass; the y pass with y_num a
+# multiple of 8 and >= 64 and >= 32 lines -- one tile (64), a last tile of 8
+# or 24 samples (72, 600), line counts that are not multiples of 32
+TMA_SHAPES = [((37, 45, 600), 25, 21), ((16, 300, 260), 30, 22), ((130, 17, 512), 40, 23), ((20, 9, 256), 6, 24),
+              ((7, 11, 72), 4, 25), ((9, 5, 64), 3, 26), ((33, 40, 136), 12, 27)]
 
 
 @pytest.mark.parametrize("shape,blobs,seed", TMA_SHAPES)
