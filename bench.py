@@ -131,15 +131,15 @@ TRAFFIC_PER_VOXEL = {
     "gradient_ds": ((537.159424e6 + 120.076288e6) / (128 * 1024 * 1024),
                     "ncu, 128x1024x1024 float capture scaled by voxels "
                     "(profiles/grad_ds_kernel_float_128x1024x1024.md)"),
-    "bspline_y": ((477.950720e6 + 496.806912e6) / (128 * 1024 * 1024),
+    "bspline_y": ((468.568e6 + 496.170496e6) / (128 * 1024 * 1024),
                   "ncu, 128x1024x1024 float capture scaled by voxels "
-                  "(profiles/iir_y_rc_kernel_float_128x1024x1024.md)"),
-    "bspline_x": ((1074.711e6 + 545.667840e6) / (128 * 1024 * 1024),
+                  "(profiles/iir_tma_kernels_float_128x1024x1024.md)"),
+    "bspline_x": ((1019.727e6 + 544.518400e6) / (128 * 1024 * 1024),
                   "ncu, 128x1024x1024 float capture scaled by voxels "
-                  "(profiles/iir_strided_rcv_kernel_float_128x1024x1024.md)"),
-    "bspline_z": ((716.355e6 + 544.182016e6) / (128 * 1024 * 1024),
+                  "(profiles/iir_tma_kernels_float_128x1024x1024.md)"),
+    "bspline_z": ((644.672e6 + 544.285184e6) / (128 * 1024 * 1024),
                   "ncu, 128x1024x1024 float capture scaled by voxels "
-                  "(profiles/iir_strided_rcv_kernel_float_128x1024x1024.md)"),
+                  "(profiles/iir_tma_kernels_float_128x1024x1024.md)"),
 }
 
 
