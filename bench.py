@@ -501,6 +501,67 @@ def bench_learned(Lr, torch, apr, raw, psf, ref, rnorm, ms_plain, k_plain, strea
             "time_ratio_learned_over_plain": (hit_ms / plain_ms) if (hit_ms and plain_ms) else None}
 
 
+def run_split(args):
+    """--split-volume: one 2048x2048x512 volume's blocked construction (z tiles
+    of 128 planes, 16 ghost planes) split by tiles over the ranks
+    (libapr_b200.distributed): each rank converts its tiles from its own slab
+    of planes, one MAX all-reduce of the particle-cell pyramid over NCCL, and
+    every rank builds the volume's structure.  Strong scaling: value = the
+    volume's voxels / the slowest rank's device time per step."""
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    import libapr_b200 as A
+    from libapr_b200 import distributed as D
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    shape = tuple(int(v) for v in args.shape.split(",")) if args.shape else SHAPE
+    zb, ghost = 128, 16
+    img = torch.empty(shape, dtype=torch.int16, device="cuda")
+    A.synth_blobs_device(img, int(BLOBS * img.numel() / (SHAPE[0] * SHAPE[1] * SHAPE[2])), SIGMA, AMP, BG,
+                         seed=volume_seed(0))
+    lo, hi = D.rank_slab(shape[0], zb, ghost, rank, world)
+    slab = img[lo:hi].contiguous() if hi > lo else img[:1].contiguous()
+    del img
+    torch.cuda.synchronize()
+    be = D.TileBackend(args.image_type, lib_params())
+    for _ in range(args.warmup):
+        D.get_apr_by_block_distributed(be, shape, slab, lo, zb, ghost)._free()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    P = 0
+    for _ in range(args.steps):
+        apr = D.get_apr_by_block_distributed(be, shape, slab, lo, zb, ghost)
+        P = apr.total_number_particles()
+        apr._free()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world, "cuda")
+    if rank == 0:
+        z, x, y = shape
+        print(json.dumps({"metric": METRIC, "value": z * x * y / (ms / 1e3) / 1e9, "unit": "GVox/s",
+                          "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+                          "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                          "dtype": "f32" if args.image_type == "float" else "u16", "data": "synthetic",
+                          "config": {"workload": "get_apr by block (z tiles 128, ghost 16) of one uint16 %dx%dx%d "
+                                                 "(y,x,z) blob volume split by tiles over the GPUs" % (y, x, z),
+                                     "image_type": args.image_type, **PARAMS, "particles": P,
+                                     "parallelism": "z-tiles per rank, MAX all-reduce of the pyramid"}}))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -514,11 +575,15 @@ def main():
     ap.add_argument("--no-rl", action="store_true")
     ap.add_argument("--no-learned", action="store_true")
     ap.add_argument("--rl-shape", default="256,1024,1024", help="z,x,y of the deconvolution workload")
+    ap.add_argument("--split-volume", action="store_true",
+                    help="one volume's blocked construction split by z-tiles over the GPUs (strong scaling)")
     ap.add_argument("--image-type", default="float", choices=["float", "uint16"],
                     help="APRConverter ImageType; uint16 throws the reference's overflow error on this volume")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.split_volume:
+        return run_split(args)
 
     import torch
     import torch.distributed as dist
