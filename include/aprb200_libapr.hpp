@@ -9,6 +9,11 @@
  *
  *   aprb200::libapr::get_apr(conv, apr, img)        APRConverter<IT>::get_apr (APRConverter.hpp:69, 591-600)
  *   aprb200::libapr::sample_image(parts, apr, img)  ParticleData<T>::sample_image (ParticleData.hpp:123-127)
+ *   aprb200::libapr::get_apr_by_block(conv, apr, img)
+ *                                                   APRConverterBatch<IT>::get_apr (APRConverterBatch.hpp:48-64,
+ *                                                   114-175) with the volume in memory instead of a TIFF file
+ *   aprb200::libapr::sample_parts_from_img_blocked(parts, apr, img, z_block, ghost)
+ *                                                   ParticleData::sample_parts_from_img_blocked (ParticleData.hpp:140)
  *   aprb200::libapr::convolve_pencil(...)           APRFilter::convolve_pencil (APRFilter.hpp:139-149)
  *   aprb200::libapr::richardson_lucy(...)           APRNumerics::richardson_lucy (APRNumerics.hpp:132-134)
  *   aprb200::libapr::isotropic_convolve_333/555     isotropic_convolve_333/555 (APRIsoConvGPU333.hpp:37-51,
@@ -37,6 +42,9 @@
 #include "algorithm/APRConverter.hpp"
 #include "data_structures/APR/APR.hpp"
 #include "data_structures/APR/particles/ParticleData.hpp"
+#ifdef HAVE_LIBTIFF
+#include "algorithm/APRConverterBatch.hpp"
+#endif
 
 namespace aprb200 {
 namespace libapr {
@@ -135,6 +143,49 @@ void sample_image(ParticleData<T> &parts, APR &apr, PixelData<uint16_t> &img) {
     parts.data.resize(v.size());
     for (size_t i = 0; i < v.size(); ++i) parts.data[i] = (T)v[i];
 }
+
+/* ParticleData<T>::sample_parts_from_img_blocked (ParticleData.hpp:140-142,
+ * 288-372): every z-tile of z_block_size planes (ghost_z planes of overlap)
+ * samples its rows from its own pyramid; the volume comes from memory where
+ * the reference reads the tiles from a TIFF file. */
+template <typename T>
+void sample_parts_from_img_blocked(ParticleData<T> &parts, APR &apr, PixelData<uint16_t> &img,
+                                   int z_block_size = 256, int ghost_z = 32) {
+    Handle h;
+    handle_of(apr.linearAccess, h);
+    std::vector<uint16_t> v(apr.total_number_particles());
+    raise(aprb_sample_image_by_block(h.a, img.mesh.begin(), z_block_size, ghost_z, v.data()));
+    parts.data.resize(v.size());
+    for (size_t i = 0; i < v.size(); ++i) parts.data[i] = (T)v[i];
+}
+
+#ifdef HAVE_LIBTIFF
+/* APRConverterBatch<ImageType>::get_apr(APR&) (APRConverterBatch.hpp:48-64,
+ * 114-175): the pixel pipeline per z-tile of conv.z_block_size planes with
+ * conv.ghost_z planes of overlap (get_apr_method_patch :190-271), one global
+ * particle-cell tree, one pulling scheme; the volume comes from memory where
+ * the reference reads it tile by tile from par.input_dir +
+ * par.input_image_name.  The per-tile form (get_apr_method_patch on one
+ * ImagePatch) is aprb_pyramid_fill_tiles_device of the C ABI. */
+template <typename ImageType>
+bool get_apr_by_block(APRConverterBatch<ImageType> &conv, APR &apr, PixelData<uint16_t> &img) {
+    aprb_params p = params(conv.par);
+    aprb_converter *c = nullptr;
+    raise(aprb_converter_create(std::is_floating_point<ImageType>::value ? APRB_IMAGE_FLOAT : APRB_IMAGE_U16, &c));
+    Handle h;
+    const aprb_status s = aprb_get_apr_by_block(c, &p, img.mesh.begin(), img.y_num, img.x_num, img.z_num,
+                                                conv.z_block_size, conv.ghost_z, &h.a);
+    aprb_converter_destroy(c);
+    if (s == APRB_ERR_DIMENSIONS) return false;
+    raise(s);
+    aprb_params used;
+    raise(aprb_apr_get_parameters(h.a, &used));
+    conv.par.grad_th = used.grad_th;
+    conv.par.sigma_th = used.sigma_th;
+    fill_apr(apr, h.a, conv.par);
+    return true;
+}
+#endif
 
 namespace detail {
 template <typename S>

@@ -150,6 +150,9 @@ def bind_lib():
         L.bind_convolve.argtypes = [vp, C.POINTER(C.c_float), C.c_int, C.POINTER(C.c_float), C.POINTER(C.c_float),
                                     C.c_int, C.c_int, C.c_int, C.c_int]
         L.bind_rl.argtypes = [vp, u16p, C.POINTER(C.c_float), C.POINTER(C.c_float), C.c_int, C.c_int, C.c_int]
+        L.bind_get_apr_by_block.argtypes = [u16p, C.c_int, C.c_int, C.c_int, C.POINTER(OrcParams), C.c_int, C.c_int,
+                                            C.c_int, C.POINTER(vp), C.POINTER(C.c_uint64)]
+        L.bind_sample_blocked.argtypes = [vp, u16p, C.c_int, C.c_int, u16p]
         _bind = L
     return _bind
 

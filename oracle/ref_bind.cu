@@ -75,6 +75,48 @@ int bind_get_apr(const uint16_t *img, int y, int x, int z, const orc_params *p, 
 
 void bind_free(void *h) { delete (BindAPR *)h; }
 
+/* APRConverterBatch<IT>::get_apr through the binding, the volume from memory */
+int bind_get_apr_by_block(const uint16_t *img, int y, int x, int z, const orc_params *p, int image_type, int zblock,
+                          int ghost, void **out, uint64_t *P) {
+    std::unique_ptr<BindAPR> b(new BindAPR());
+    PixelData<uint16_t> in(y, x, z);
+    std::memcpy(in.mesh.begin(), img, sizeof(uint16_t) * (size_t)y * x * z);
+    try {
+        bool ok;
+        if (image_type == 1) {
+            APRConverterBatch<uint16_t> conv;
+            set_par(conv.par, p);
+            conv.z_block_size = zblock;
+            conv.ghost_z = ghost;
+            ok = aprb200::libapr::get_apr_by_block(conv, b->apr, in);
+        } else {
+            APRConverterBatch<float> conv;
+            set_par(conv.par, p);
+            conv.z_block_size = zblock;
+            conv.ghost_z = ghost;
+            ok = aprb200::libapr::get_apr_by_block(conv, b->apr, in);
+        }
+        if (!ok) return 1;
+    } catch (std::invalid_argument &) {
+        return 2;
+    } catch (std::exception &) {
+        return 3;
+    }
+    *P = b->apr.total_number_particles();
+    *out = b.release();
+    return 0;
+}
+
+int bind_sample_blocked(void *h, const uint16_t *img, int zblock, int ghost, uint16_t *parts) {
+    APR &apr = ((BindAPR *)h)->apr;
+    PixelData<uint16_t> in(apr.org_dims(0), apr.org_dims(1), apr.org_dims(2));
+    std::memcpy(in.mesh.begin(), img, sizeof(uint16_t) * in.mesh.size());
+    ParticleData<uint16_t> pd;
+    aprb200::libapr::sample_parts_from_img_blocked(pd, apr, in, zblock, ghost);
+    std::memcpy(parts, pd.data.begin(), sizeof(uint16_t) * pd.size());
+    return 0;
+}
+
 /* every particle's (level, z, x, y), walked with LibAPR's LinearIterator in
  * its storage order */
 int bind_particles(void *h, uint16_t *level, uint16_t *zz, uint16_t *xx, uint16_t *yy) {

@@ -15,7 +15,8 @@ from tests.helpers import gaussian_psf, oracle_params, random_stencil, volume
 
 needs_bind = pytest.mark.skipif(not B.bind_available(), reason="oracle/_ref/libaprbind.so not built")
 
-SYMBOLS = ["bind_get_apr", "bind_free", "bind_particles", "bind_sample", "bind_convolve", "bind_rl"]
+SYMBOLS = ["bind_get_apr", "bind_free", "bind_particles", "bind_sample", "bind_convolve", "bind_rl",
+           "bind_get_apr_by_block", "bind_sample_blocked"]
 
 
 @needs_bind
@@ -104,3 +105,31 @@ def test_get_apr_overflow_throws_invalid_argument_like_the_reference():
     img[10, 12, 14] = 65535 - 100
     img[0, 0, 0] = 0
     assert Bound(img, 1).status == 2
+
+
+@pytest.mark.gpu
+@needs_bind
+@pytest.mark.parametrize("shape,zb,ghost,image_type", [((100, 40, 48), 32, 8, 1), ((96, 30, 40), 20, 8, 0),
+                                                        ((200, 32, 32), 128, 16, 0)])
+def test_blocked_converter_and_sampling_fill_the_reference_objects(shape, zb, ghost, image_type):
+    """APRConverterBatch::get_apr and ParticleData::sample_parts_from_img_blocked
+    through the binding on LibAPR's own objects, against the oracle's blocked
+    converter and blocked sampling"""
+    L = B.bind_lib()
+    img = volume(shape, 30, 3)
+    z, x, y = shape
+    h, P = C.c_void_p(), C.c_uint64()
+    assert L.bind_get_apr_by_block(_ptr(img, C.c_uint16), y, x, z, C.byref(oracle_params()), image_type, zb, ghost,
+                                   C.byref(h), C.byref(P)) == 0
+    try:
+        e, acc = B.orc_get_apr_by_block(img, oracle_params(), image_type, zb, ghost)
+        assert e == 0 and int(P.value) == acc.P
+        a = [np.zeros(max(acc.P, 1), np.uint16) for _ in range(4)]
+        assert L.bind_particles(h, *(_ptr(v, C.c_uint16) for v in a)) == 0
+        ol, oz, ox, oy = acc.particle_coords()
+        assert all(np.array_equal(v[: acc.P].astype(np.int32), o) for v, o in zip(a, (ol, oz, ox, oy)))
+        parts = np.zeros(max(acc.P, 1), np.uint16)
+        assert L.bind_sample_blocked(h, _ptr(img, C.c_uint16), zb, ghost, _ptr(parts, C.c_uint16)) == 0
+        assert np.array_equal(parts[: acc.P], B.orc_sample_by_block(acc, img, zb, ghost))
+    finally:
+        L.bind_free(h)
