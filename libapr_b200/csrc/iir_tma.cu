@@ -300,7 +300,7 @@ void launch_tma_variant(const CUtensorMap &tm, float *work, int yn, int n, int m
                         const IIRDev &c, float2 *ckpt, unsigned *d_timeout, cudaStream_t s) {
     using Sh = TmaShape<BOXES, V, STAGES>;
     auto kern = iir_strided_tma_kernel<ZAXIS, BOXES, V, STAGES>;
-    APRB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::kSmem));
+    set_smem_once<iir_strided_tma_kernel<ZAXIS, BOXES, V, STAGES>>((int)Sh::kSmem);
     const unsigned blocks = (unsigned)((uint64_t)((yn + Sh::kY - 1) / Sh::kY) * (uint64_t)m);
     kern<<<blocks, Sh::kThreads, Sh::kSmem, s>>>(tm, work, yn, n, s1, s2, c, ckpt, (uint64_t)yn * (uint64_t)m,
                                                  d_timeout);

@@ -238,7 +238,7 @@ bool launch_iir_y_tma(const uint16_t *img, float *work, int yn, uint64_t nlines,
     if (!make_tensor_map_2d_sw128(&tout, work, true, d, (uint64_t)yn * 4, bout)) return false;
     constexpr int S = APRB_TMA_Y_STAGES;
     auto kern = iir_y_tma_kernel<S>;
-    APRB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)YShape<S>::kSmem));
+    set_smem_once<iir_y_tma_kernel<S>>((int)YShape<S>::kSmem);
     kern<<<(unsigned)((nlines + 31) / 32), 32, YShape<S>::kSmem, s>>>(tin, tout, img, yn, nlines, c, ckpt, d_timeout);
     count_launch();
     APRB_CHECK_LAUNCH();

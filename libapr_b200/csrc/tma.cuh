@@ -26,6 +26,19 @@ bool make_tensor_map_3d_f32(CUtensorMap *map, const void *base, const uint64_t d
 bool make_tensor_map_2d_sw128(CUtensorMap *map, const void *base, bool f32, const uint64_t d[2], uint64_t s1,
                               const uint32_t b[2]);
 
+// cudaFuncSetAttribute(KERN, MaxDynamicSharedMemorySize, bytes) once per
+// device for each kernel KERN (a launch needs it once per device)
+template <auto KERN>
+void set_smem_once(int bytes) {
+    static uint64_t done = 0;  // bit d: set on device d
+    int dev = 0;
+    APRB_CUDA(cudaGetDevice(&dev));
+    const uint64_t bit = dev < 64 ? (uint64_t(1) << dev) : 0;
+    if (bit && (__atomic_load_n(&done, __ATOMIC_ACQUIRE) & bit)) return;
+    APRB_CUDA(cudaFuncSetAttribute(KERN, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+    if (bit) __atomic_fetch_or(&done, bit, __ATOMIC_RELEASE);
+}
+
 // Iterations of a bounded mbarrier wait (each try_wait may suspend the thread
 // for a short, hardware-defined time); a wait that runs out reports failure.
 constexpr uint32_t kMbarWaitLimit = 1u << 20;
