@@ -358,6 +358,21 @@ aprb_status aprb_check_division_by_constant(float d, uint64_t *mismatches, uint3
 /* number of kernel launches this thread issued through the library so far */
 uint64_t aprb_kernel_launch_count(void);
 
+/* --- smoothing schedule (no counterpart in the reference: the kernel choice of the
+ * recursive smoothing, bspline_filt_rec_y/x/z, ComputeGradient.hpp:249-779) ---------
+ * For float ImageType the three passes run as one of several kernels, chosen per axis
+ * (0 y, 1 x, 2 z) and line-length bucket (n <= 128, 256, 512, 1024, 2048, longer: bucket
+ * 0 .. 5).  y: 0 cp.async-staged tiles, 1 / 2 TMA tiles with 2 / 3 stages in flight;
+ * x and z: 0 register-staged lines, 1 .. 4 TMA segments of (boxes of 256 y, lines per
+ * thread, stages) = (1, 2, 4), (2, 4, 3), (1, 1, 4), (2, 2, 3).  Every variant gives the
+ * same bits; the default is variant 1 everywhere, and a layout TMA cannot take uses
+ * variant 0.  libapr_b200.autotune times the variants on the device and persists the
+ * fastest (libapr_b200/data/smoothing_schedule.json, loaded by the Python package).
+ * The schedule is process-wide. */
+aprb_status aprb_smoothing_variants(int axis, int *count);
+aprb_status aprb_smoothing_schedule_set(int axis, int bucket, int variant);
+aprb_status aprb_smoothing_schedule_get(int axis, int bucket, int *variant);
+
 /* --- stage timing (the reference's APRTimer stages, APRConverter.hpp:61-65,
  * measured with CUDA events on the launching stream) -------------------------
  * When enabled, every pipeline stage records an event pair on its stream.

@@ -549,6 +549,39 @@ def auto_parameters_li_entropy(par, image, local_intensity_scale, grad, bspline_
     return par
 
 
+SCHEDULE_BUCKETS = (128, 256, 512, 1024, 2048, None)  # line-length bucket limits (None: longer)
+
+
+def smoothing_variants():
+    """Number of kernel variants of the smoothing passes per axis {"y", "x", "z"}."""
+    out = {}
+    for a, name in enumerate(_lib.AXES):
+        n = C.c_int()
+        check(lib().aprb_smoothing_variants(a, C.byref(n)))
+        out[name] = n.value
+    return out
+
+
+def smoothing_schedule():
+    """The process's smoothing schedule: {axis: [variant per line-length bucket]}."""
+    out = {}
+    for a, name in enumerate(_lib.AXES):
+        row = []
+        for b in range(len(SCHEDULE_BUCKETS)):
+            v = C.c_int()
+            check(lib().aprb_smoothing_schedule_get(a, b, C.byref(v)))
+            row.append(v.value)
+        out[name] = row
+    return out
+
+
+def set_smoothing_schedule(schedule):
+    """Sets {axis: [variant per bucket]} (every variant computes the same bits)."""
+    for a, name in enumerate(_lib.AXES):
+        for b, v in enumerate(schedule.get(name, [])):
+            check(lib().aprb_smoothing_schedule_set(a, b, int(v)))
+
+
 def kernel_launch_count():
     return int(lib().aprb_kernel_launch_count())
 

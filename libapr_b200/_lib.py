@@ -48,6 +48,9 @@ SIGNATURES = {
     "aprb_converter_destroy": ([_vp], _i),
     "aprb_converter_keep_intermediates": ([_vp, _i], _i),
     "aprb_converter_keep_input": ([_vp, _i], _i),
+    "aprb_smoothing_variants": ([_i, C.POINTER(_i)], _i),
+    "aprb_smoothing_schedule_set": ([_i, _i, _i], _i),
+    "aprb_smoothing_schedule_get": ([_i, _i, C.POINTER(_i)], _i),
     "aprb_get_apr": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, C.POINTER(_vp)], _i),
     "aprb_get_apr_device": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, _vp, C.POINTER(_vp)], _i),
     "aprb_get_apr_by_block": ([_vp, C.POINTER(aprb_params), _vp, _i, _i, _i, _i, _i, C.POINTER(_vp)], _i),
@@ -125,7 +128,31 @@ def lib():
             fn.argtypes = args
             fn.restype = res
         _lib = L
+        apply_schedule_file(L)
     return _lib
+
+
+# The smoothing schedule chosen by libapr_b200.autotune on the device
+# (aprb_smoothing_schedule_set): {"schedule": {"y": [variant per bucket], "x":
+# [...], "z": [...]}}, buckets n <= 128, 256, 512, 1024, 2048, longer.
+SCHEDULE_FILE = os.path.join(HERE, "data", "smoothing_schedule.json")
+AXES = ("y", "x", "z")
+
+
+def apply_schedule_file(L, path=SCHEDULE_FILE):
+    """Sets the library's smoothing schedule from the autotuner's file, when
+    there is one; returns the schedule applied (or None)."""
+    import json
+    if not path or not os.path.exists(path):
+        return None
+    with open(path) as f:
+        sched = json.load(f)["schedule"]
+    for a, name in enumerate(AXES):
+        for b, v in enumerate(sched.get(name, [])):
+            st = L.aprb_smoothing_schedule_set(a, b, int(v))
+            if st != APRB_OK:
+                raise APRBError(st, "smoothing schedule %s: bucket %d variant %s" % (name, b, v))
+    return sched
 
 
 class APRBError(RuntimeError):

@@ -834,6 +834,27 @@ aprb_status aprb_converter_intermediate(const aprb_converter *c, int stage, floa
     });
 }
 
+aprb_status aprb_smoothing_variants(int axis, int *count) {
+    return guarded([&] {
+        ARG_CHECK(count && axis >= 0 && axis <= 2, "axis must be 0 (y), 1 (x) or 2 (z)");
+        *count = smoothing_variants(axis);
+    });
+}
+
+aprb_status aprb_smoothing_schedule_set(int axis, int bucket, int variant) {
+    return guarded([&] {
+        ARG_CHECK(set_smoothing_variant(axis, bucket, variant), "axis, bucket or variant out of range");
+    });
+}
+
+aprb_status aprb_smoothing_schedule_get(int axis, int bucket, int *variant) {
+    return guarded([&] {
+        ARG_CHECK(variant && axis >= 0 && axis <= 2 && bucket >= 0 && bucket < kSchedBuckets,
+                  "axis or bucket out of range");
+        *variant = smoothing_variant(axis, bucket == 0 ? 1 : (64 << bucket) + 1);
+    });
+}
+
 aprb_status aprb_converter_level_margins(aprb_converter *c, double rel_tol, uint64_t *near_boundary,
                                          uint64_t *active) {
     return guarded([&] {

@@ -21,16 +21,13 @@
 #include "kernels.cuh"
 #include "tma.cuh"
 
-// boxes of 256 y per CTA, lines per thread, stages in flight.  Measured on
-// 2048x2048x512 (B200): 1 box, 2 lines, 4 stages (three 64 KB CTAs per SM)
-// x 4.27 / z 4.03 ms; 2 boxes, 4 lines, 3 stages 4.29 / 4.20; one CTA per SM
-// with 8 stages 5.5 - 7.3 ms (too few warps for the recurrences' latency).
-#ifndef APRB_TMA_Z_SHAPE
-#define APRB_TMA_Z_SHAPE 1, 2, 4
-#endif
-#ifndef APRB_TMA_X_SHAPE
-#define APRB_TMA_X_SHAPE 1, 2, 4
-#endif
+// Shapes of the TMA-staged x / z passes (boxes of 256 y per CTA, lines per
+// thread, stages in flight), chosen at run time per axis and line length by
+// the smoothing schedule (set_smoothing_variant; libapr_b200.autotune times
+// them and persists the choice).  Measured on 2048x2048x512 (B200): 1 box,
+// 2 lines, 4 stages (three 64 KB CTAs per SM) x 4.27 / z 4.03 ms; 2 boxes,
+// 4 lines, 3 stages 4.29 / 4.20; one CTA per SM with 8 stages 5.5 - 7.3 ms
+// (too few warps for the recurrences' latency).
 
 namespace aprb {
 
@@ -310,9 +307,33 @@ void launch_tma_variant(const CUtensorMap &tm, float *work, int yn, int n, int m
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// smoothing schedule: the kernel variant per axis and line-length bucket
+namespace {
+int g_sched[3][kSchedBuckets] = {{1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1}, {1, 1, 1, 1, 1, 1}};
+constexpr int kVariants[3] = {3, 5, 5};
+}  // namespace
+
+int sched_bucket(int n) {
+    int b = 0;
+    for (int lim = 128; b < kSchedBuckets - 1 && n > lim; lim *= 2) ++b;
+    return b;
+}
+int smoothing_variants(int axis) { return axis >= 0 && axis < 3 ? kVariants[axis] : 0; }
+int smoothing_variant(int axis, int n) {
+    return __atomic_load_n(&g_sched[axis][sched_bucket(n)], __ATOMIC_RELAXED);
+}
+bool set_smoothing_variant(int axis, int bucket, int v) {
+    if (axis < 0 || axis > 2 || bucket < 0 || bucket >= kSchedBuckets || v < 0 || v >= kVariants[axis]) return false;
+    __atomic_store_n(&g_sched[axis][bucket], v, __ATOMIC_RELAXED);
+    return true;
+}
+
 bool launch_strided_iir_tma(float *work, int yn, int xn, int zn, bool zaxis, const IIRDev &c, unsigned *d_timeout,
                             float2 *ckpt, uint64_t ckpt_elems, cudaStream_t s) {
     const int n = zaxis ? zn : xn, m = zaxis ? xn : zn;
+    const int variant = smoothing_variant(zaxis ? 2 : 1, n);
+    if (variant == 0) return false;  // the register-staged kernel
     if (yn % 4 != 0 || yn < kTBox || n < kTS || ((uintptr_t)work & 15) != 0 || ((uintptr_t)ckpt & 15) != 0)
         return false;
     if ((uint64_t)yn * (uint64_t)m * (uint64_t)((n + kTS - 1) / kTS) > ckpt_elems) return false;
@@ -321,10 +342,24 @@ bool launch_strided_iir_tma(float *work, int yn, int xn, int zn, bool zaxis, con
     const uint32_t box[3] = {(uint32_t)kTBox, zaxis ? 1u : (uint32_t)kTS, zaxis ? (uint32_t)kTS : 1u};
     if (!make_tensor_map_3d_f32(&tm, work, d, (uint64_t)yn * 4, (uint64_t)xn * yn * 4, box)) return false;
     const uint64_t s1 = zaxis ? (uint64_t)xn * yn : (uint64_t)yn, s2 = zaxis ? (uint64_t)yn : (uint64_t)xn * yn;
-    if (zaxis)
-        launch_tma_variant<true, APRB_TMA_Z_SHAPE>(tm, work, yn, n, m, s1, s2, c, ckpt, d_timeout, s);
-    else
-        launch_tma_variant<false, APRB_TMA_X_SHAPE>(tm, work, yn, n, m, s1, s2, c, ckpt, d_timeout, s);
+    // variants: 1 = (1 box, 2 lines, 4 stages), 2 = (2, 4, 3), 3 = (1, 1, 4), 4 = (2, 2, 3)
+#define APRB_TMA_LAUNCH(Z, B, V, S) launch_tma_variant<Z, B, V, S>(tm, work, yn, n, m, s1, s2, c, ckpt, d_timeout, s)
+    if (zaxis) {
+        switch (variant) {
+            case 2: APRB_TMA_LAUNCH(true, 2, 4, 3); break;
+            case 3: APRB_TMA_LAUNCH(true, 1, 1, 4); break;
+            case 4: APRB_TMA_LAUNCH(true, 2, 2, 3); break;
+            default: APRB_TMA_LAUNCH(true, 1, 2, 4); break;
+        }
+    } else {
+        switch (variant) {
+            case 2: APRB_TMA_LAUNCH(false, 2, 4, 3); break;
+            case 3: APRB_TMA_LAUNCH(false, 1, 1, 4); break;
+            case 4: APRB_TMA_LAUNCH(false, 2, 2, 3); break;
+            default: APRB_TMA_LAUNCH(false, 1, 2, 4); break;
+        }
+    }
+#undef APRB_TMA_LAUNCH
     return true;
 }
 

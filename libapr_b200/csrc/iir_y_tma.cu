@@ -16,12 +16,10 @@
 #include "kernels.cuh"
 #include "tma.cuh"
 
-// input stages in flight per warp.  Measured on 2048x2048x512 (B200): 2 stages
-// (17 KB per CTA, 13 warps per SM) 2.97 ms, 3 stages 3.00, 4 stages 3.31, 6
-// stages 3.94 (fewer resident warps); the cp.async-staged kernel 4.30 ms.
-#ifndef APRB_TMA_Y_STAGES
-#define APRB_TMA_Y_STAGES 2
-#endif
+// Input stages in flight per warp: 2 (variant 1) or 3 (variant 2) of the
+// smoothing schedule.  Measured on 2048x2048x512 (B200): 2 stages (17 KB per
+// CTA, 13 warps per SM) 2.97 ms, 3 stages 3.00, 4 stages 3.31, 6 stages 3.94
+// (fewer resident warps); the cp.async-staged kernel (variant 0) 4.30 ms.
 
 namespace aprb {
 
@@ -226,6 +224,8 @@ __global__ void __launch_bounds__(32)
 
 bool launch_iir_y_tma(const uint16_t *img, float *work, int yn, uint64_t nlines, const IIRDev &c, unsigned *d_timeout,
                       float2 *ckpt, uint64_t ckpt_elems, cudaStream_t s) {
+    const int variant = smoothing_variant(0, yn);
+    if (variant == 0) return false;  // the cp.async-staged kernel
     if (yn % 8 != 0 || yn < kYT || nlines < 32 || nlines > (uint64_t)INT32_MAX || ((uintptr_t)img & 15) != 0 ||
         ((uintptr_t)work & 15) != 0 || ((uintptr_t)ckpt & 7) != 0)
         return false;
@@ -236,10 +236,15 @@ bool launch_iir_y_tma(const uint16_t *img, float *work, int yn, uint64_t nlines,
     const uint32_t bin[2] = {(uint32_t)kYT, 32u}, bout[2] = {32u, 32u};
     if (!make_tensor_map_2d_sw128(&tin, img, false, d, (uint64_t)yn * 2, bin)) return false;
     if (!make_tensor_map_2d_sw128(&tout, work, true, d, (uint64_t)yn * 4, bout)) return false;
-    constexpr int S = APRB_TMA_Y_STAGES;
-    auto kern = iir_y_tma_kernel<S>;
-    set_smem_once<iir_y_tma_kernel<S>>((int)YShape<S>::kSmem);
-    kern<<<(unsigned)((nlines + 31) / 32), 32, YShape<S>::kSmem, s>>>(tin, tout, img, yn, nlines, c, ckpt, d_timeout);
+    if (variant == 2) {
+        set_smem_once<iir_y_tma_kernel<3>>((int)YShape<3>::kSmem);
+        iir_y_tma_kernel<3><<<(unsigned)((nlines + 31) / 32), 32, YShape<3>::kSmem, s>>>(tin, tout, img, yn, nlines, c,
+                                                                                        ckpt, d_timeout);
+    } else {
+        set_smem_once<iir_y_tma_kernel<2>>((int)YShape<2>::kSmem);
+        iir_y_tma_kernel<2><<<(unsigned)((nlines + 31) / 32), 32, YShape<2>::kSmem, s>>>(tin, tout, img, yn, nlines, c,
+                                                                                        ckpt, d_timeout);
+    }
     count_launch();
     APRB_CHECK_LAUNCH();
     return true;

@@ -27,6 +27,16 @@ struct LisBuffers {
 };
 
 // ---- iir_tma.cu
+// Smoothing schedule: the kernel variant of each axis (0 y, 1 x, 2 z) per
+// line-length bucket (n <= 128, 256, 512, 1024, 2048, longer).  y: 0 the
+// cp.async-staged kernel, 1 / 2 TMA tiles with 2 / 3 stages; x, z: 0 the
+// register-staged kernel, 1 .. 4 TMA segment shapes.  Variant 1 everywhere
+// unless set (a layout TMA cannot take falls back to variant 0).
+constexpr int kSchedBuckets = 6;
+int sched_bucket(int n);
+int smoothing_variants(int axis);
+int smoothing_variant(int axis, int n);
+bool set_smoothing_variant(int axis, int bucket, int v);
 // The x (zaxis false) or z pass of the recursive smoothing over a float image
 // with TMA-staged segments; false when the layout does not allow it (y_num not
 // a multiple of 4 or below 256, fewer than 16 samples along the axis, an

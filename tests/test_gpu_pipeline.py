@@ -209,3 +209,28 @@ def test_keep_input_samples_the_uploaded_copy():
     assert conv.get_apr(apr2, img)
     assert np.array_equal(A.ParticleData().sample_image(apr2, other).data,
                           A.ParticleData().sample_image(ref_apr, other).data)
+
+
+@pytest.fixture(scope="module")
+def tma_case():
+    shape = (37, 45, 600)  # takes the TMA kernels on every axis
+    img = volume(shape, 25, 21)
+    e, acc, (off, inter) = B.orc_get_apr(img, oracle_params(), 0)
+    assert e == 0
+    return img, acc, inter[0]
+
+
+@pytest.mark.parametrize("axis,variant", [("y", v) for v in range(3)] + [("x", v) for v in range(5)] +
+                         [("z", v) for v in range(5)])
+def test_every_smoothing_variant_bit_exact(tma_case, axis, variant):
+    """Each kernel variant of the smoothing schedule (the autotuner's choices)
+    gives the reference's smoothed image and structure bit for bit."""
+    img, acc, smoothed = tma_case
+    old = A.smoothing_schedule()
+    try:
+        A.set_smoothing_schedule({axis: [variant] * len(A.SCHEDULE_BUCKETS)})
+        conv, apr = gpu_apr(img, 0)
+        assert bits_equal(conv.intermediate(0, img.shape), smoothed)
+        assert np.array_equal(apr.linear_access()[2], acc.y_vec)
+    finally:
+        A.set_smoothing_schedule(old)
