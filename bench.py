@@ -895,6 +895,8 @@ def main():
                 "data": "synthetic",
                 "config": workload_config(args.image_type, P, world),
                 "gpu_launches": int(launches), "e2e": e2e, "cpu_baseline": cpu, **out, **conv_res}
+        line["smoothing_schedule"] = {"variants": A.smoothing_schedule(),
+                                      "source": "libapr_b200/data/smoothing_schedule.json (libapr_b200.autotune)"}
         if parity:
             line["parity"] = parity
         if auto_res:

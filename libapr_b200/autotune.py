@@ -3,7 +3,7 @@ B-spline smoothing (bspline_filt_rec_y/x/z, ComputeGradient.hpp:249-779) and
 every line-length bucket (n <= 128, 256, 512, 1024, 2048, longer), times each
 kernel variant of the library on the current GPU -- the pass's own stage time
 from the library's CUDA-event stage timer, median of a few get_apr calls on a
-seeded synthetic volume of about 2^27 voxels whose lines along that axis have
+seeded synthetic volume of about 2^29 voxels whose lines along that axis have
 the bucket's length -- and writes the fastest variant per (axis, bucket) with
 all timings to a JSON file, which the package applies when it loads the
 library.  Every variant computes the same bits, so the schedule changes only
@@ -22,7 +22,7 @@ from . import _lib
 
 LENGTHS = (128, 256, 512, 1024, 2048, 4096)  # one line length per bucket
 STAGE = {"y": "bspline_y", "x": "bspline_x", "z": "bspline_z"}
-TARGET = 1 << 27  # voxels of a timing volume
+TARGET = 1 << 29  # voxels of a timing volume
 
 
 def timing_shape(axis, n):
