@@ -401,7 +401,7 @@ PixelOut<IT> pixel_stages(aprb_converter *c, const aprb_params &p, const uint16_
     IT *grad = c->grad.as_on<IT>(nd, s);
     float *ids_raw = c->ids_raw.as_on<float>(nd, s);
     float *ids = c->ids.as_on<float>(nd, s);
-    launch_gradient<IT>(work, yn, xn, zn, grad, ids_raw, ids, yd, xd, zd, p, s);
+    launch_gradient<IT>(work, yn, xn, zn, grad, ids_raw, ids, yd, xd, zd, p, d_err + 1, s);
     float *lis = c->lis.as_on<float>(nd, s);
     launch_local_intensity_scale(ids, lis, yd, xd, zd, p, c->lisb, s);
     return PixelOut<IT>{grad, lis, ids, d_off, nd};

@@ -46,6 +46,17 @@ bool set_smoothing_variant(int axis, int bucket, int v);
 bool launch_strided_iir_tma(float *work, int yn, int xn, int zn, bool zaxis, const IIRDev &c, unsigned *d_timeout,
                             float2 *ckpt, uint64_t ckpt_elems, cudaStream_t s);
 
+// ---- inv_bspline_tma.cu
+// weights of the inverse B-spline filter [1/6, 4/6, 1/6] and the mirrored end weight a1 + a3
+struct InvB {
+    float a1, a2, a3, a13;
+};
+// calc_inv_bspline_y/x/z over the ds image with TMA-staged planes; false when
+// the layout does not allow it (y extent not a multiple of 4 or below 256, x
+// extent below 18, unaligned input), and the caller runs inv_bspline_kernel.
+bool launch_inv_bspline_tma(const float *in, float *O, int yd, int xd, int zd, int ony, int onx, int onz,
+                            const InvB &c, unsigned *d_timeout, cudaStream_t s);
+
 // ---- iir_y_tma.cu
 // The y pass of the recursive smoothing of a uint16 image into a float
 // working image with TMA-staged tiles; false when the layout does not allow
@@ -67,7 +78,7 @@ void launch_upload_smooth(const uint16_t *host, uint16_t *img, IT *work, int yn,
                           cudaStream_t s, cudaStream_t up);
 template <typename IT>
 void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *ids_raw, float *ids, int yd, int xd,
-                     int zd, const aprb_params &p, cudaStream_t s);
+                     int zd, const aprb_params &p, unsigned *d_timeout, cudaStream_t s);
 void launch_local_intensity_scale(const float *ids, float *lis, int yd, int xd, int zd, const aprb_params &p,
                                   LisBuffers &b, cudaStream_t s);
 template <typename IT>

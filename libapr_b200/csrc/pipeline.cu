@@ -1054,10 +1054,6 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
 // reference's expression with its operand order, so the columns reproduce
 // the whole-volume passes exactly.
 // ---------------------------------------------------------------------------
-struct InvB {
-    float a1, a2, a3, a13;
-};
-
 constexpr int kJX = 8, kJY = 256, kJZ = 32;
 constexpr int kJXH = kJX + 2, kJYH = kJY + 2;
 
@@ -1950,7 +1946,7 @@ void launch_upload_smooth(const uint16_t *host, uint16_t *img, IT *work, int yn,
 
 template <typename IT>
 void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *ids_raw, float *ids, int yd, int xd,
-                     int zd, const aprb_params &p, cudaStream_t s) {
+                     int zd, const aprb_params &p, unsigned *d_timeout, cudaStream_t s) {
     {
         APRB_PROF("gradient_ds", s);
         dim3 grid((yd + kGY - 1) / kGY, (xd + kGX - 1) / kGX, (zd + kGZ - 1) / kGZ);
@@ -1986,9 +1982,12 @@ void launch_gradient(const IT *work, int yn, int xn, int zn, IT *grad, float *id
     c.a3 = (float)(1.0 / 6.0);
     c.a13 = c.a1 + c.a3;
     dim3 grid((yd + kJY - 1) / kJY, (xd + kJX - 1) / kJX, (zd + kJZ - 1) / kJZ);
-    inv_bspline_kernel<<<grid, kJY, 0, s>>>(ids_raw, ids, yd, xd, zd, on && yn > 2, on && xn > 2, on && zn > 2, c);
-    count_launch();
-    APRB_CHECK_LAUNCH();
+    const int ony = on && yn > 2, onx = on && xn > 2, onz = on && zn > 2;
+    if (!launch_inv_bspline_tma(ids_raw, ids, yd, xd, zd, ony, onx, onz, c, d_timeout, s)) {
+        inv_bspline_kernel<<<grid, kJY, 0, s>>>(ids_raw, ids, yd, xd, zd, ony, onx, onz, c);
+        count_launch();
+        APRB_CHECK_LAUNCH();
+    }
 }
 
 template <int OFF>
@@ -2201,9 +2200,9 @@ template void launch_smooth<uint16_t>(const uint16_t *, uint16_t *, int, int, in
 template void launch_smooth<float>(const uint16_t *, float *, int, int, int, float, const float *, unsigned *,
                                    DevBuf &, cudaStream_t);
 template void launch_gradient<uint16_t>(const uint16_t *, int, int, int, uint16_t *, float *, float *, int, int, int,
-                                        const aprb_params &, cudaStream_t);
+                                        const aprb_params &, unsigned *, cudaStream_t);
 template void launch_gradient<float>(const float *, int, int, int, float *, float *, float *, int, int, int,
-                                     const aprb_params &, cudaStream_t);
+                                     const aprb_params &, unsigned *, cudaStream_t);
 template void launch_levels<uint16_t>(uint16_t *, float *, const float *, uint64_t, const float *, const aprb_params &,
                                       int, int, uint8_t *, uint8_t *, int, cudaStream_t);
 template void launch_levels<float>(float *, float *, const float *, uint64_t, const float *, const aprb_params &, int,

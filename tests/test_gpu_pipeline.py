@@ -52,9 +52,11 @@ def test_get_apr_bit_exact(shape, blobs, seed, image_type):
 # partial TMA boxes (y_num 600, 260), partial 16-sample segments, an x extent
 # below 16 that keeps the register-staged x pass; the y pass with y_num a
 # multiple of 8 and >= 64 and >= 32 lines -- one tile (64), a last tile of 8
-# or 24 samples (72, 600), line counts that are not multiples of 32
+# or 24 samples (72, 600), line counts that are not multiples of 32; the
+# inverse B-spline with a ds y extent that is a multiple of 4 and >= 256 and
+# an x extent >= 18 (600, 520: two y blocks, two x blocks, two z runs)
 TMA_SHAPES = [((37, 45, 600), 25, 21), ((16, 300, 260), 30, 22), ((130, 17, 512), 40, 23), ((20, 9, 256), 6, 24),
-              ((7, 11, 72), 4, 25), ((9, 5, 64), 3, 26), ((33, 40, 136), 12, 27)]
+              ((7, 11, 72), 4, 25), ((9, 5, 64), 3, 26), ((33, 40, 136), 12, 27), ((70, 40, 520), 30, 28)]
 
 
 @pytest.mark.parametrize("shape,blobs,seed", TMA_SHAPES)
@@ -65,6 +67,8 @@ def test_tma_smoothing_bit_exact(shape, blobs, seed, lam):
     assert e == 0
     conv, apr = gpu_apr(img, 0, lambda_=lam)
     assert bits_equal(conv.intermediate(0, shape), inter[0]), "smoothed image"
+    for w in range(1, 7):  # the TMA-staged inverse B-spline writes stage 2 where the ds image allows
+        assert bits_equal(conv.intermediate(w, STAGE_SHAPE_DS(shape)), inter[w]), "stage %d" % w
     lx, xe, yv = apr.linear_access()
     assert np.array_equal(xe, acc.xz_end) and np.array_equal(yv, acc.y_vec)
 
