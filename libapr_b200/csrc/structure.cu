@@ -139,6 +139,71 @@ __global__ void __launch_bounds__(256) dilate_kernel(uint8_t *__restrict__ st, L
     }
 }
 
+// The same dilation for rows of a multiple of 16 cells and 16-byte aligned
+// rows: a lane moves 16 consecutive cells as one 16-byte word, a warp reads
+// 512 y of a row in one load, and the shared mask holds per row and lane the
+// 16 bits of the lane's cells.
+constexpr int kD16Y = 512;
+template <int MODE>
+__global__ void __launch_bounds__(256) dilate16_kernel(uint8_t *__restrict__ st, LevelDims d) {
+    __shared__ uint16_t W[kDRows][32];
+    const int y0 = blockIdx.x * kD16Y, x0 = blockIdx.y * kDX, z0 = blockIdx.z * kDZ;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int y = y0 + 16 * lane;  // first of the lane's cells; yn % 16 == 0, so all 16 are in or out
+    for (int r = w; r < kDRows; r += 8) {
+        const int x = x0 - 1 + r % (kDX + 2), z = z0 - 1 + r / (kDX + 2);
+        const bool row_in = x >= 0 && x < d.xn && z >= 0 && z < d.zn;
+        const uint8_t *R = st + ((uint64_t)(row_in ? z : 0) * d.xn + (row_in ? x : 0)) * (uint64_t)d.yn;
+        const bool in = row_in && y < d.yn;
+        const uint4 v = in ? *reinterpret_cast<const uint4 *>(R + y) : make_uint4(0u, 0u, 0u, 0u);
+        const uint32_t vw[4] = {v.x, v.y, v.z, v.w};
+        unsigned p = 0;
+#pragma unroll
+        for (int e = 0; e < 16; ++e)
+            if (in && dil_source<MODE>((uint8_t)(vw[e >> 2] >> (8 * (e & 3))))) p |= 1u << e;
+        unsigned pl = (__shfl_up_sync(0xffffffffu, p, 1) >> 15) & 1u;
+        unsigned pr = __shfl_down_sync(0xffffffffu, p, 1) & 1u;
+        if (lane == 0) pl = row_in && y >= 1 && y - 1 < d.yn && dil_source<MODE>(R[y - 1]);
+        if (lane == 31) pr = row_in && y + 16 < d.yn && dil_source<MODE>(R[y + 16]);
+        W[r][lane] = (uint16_t)((p | (p << 1) | (p >> 1) | pl | (pr << 15)) & 0xFFFFu);
+    }
+    __syncthreads();
+    for (int task = w; task < kDX * kDZ; task += 8) {
+        const int xx = task % kDX, zz = task / kDX;
+        const int x = x0 + xx, z = z0 + zz;
+        if (x >= d.xn || z >= d.zn || y >= d.yn) continue;
+        unsigned m = 0;
+#pragma unroll
+        for (int dz = 0; dz < 3; ++dz)
+#pragma unroll
+            for (int dx = 0; dx < 3; ++dx) m |= W[(zz + dz) * (kDX + 2) + xx + dx][lane];
+        if (!m) continue;
+        uint4 *c = reinterpret_cast<uint4 *>(st + ((uint64_t)z * d.xn + x) * (uint64_t)d.yn + y);
+        const uint4 v = *c;
+        uint32_t nv[4] = {v.x, v.y, v.z, v.w};
+        bool changed = false;
+#pragma unroll
+        for (int e = 0; e < 16; ++e) {
+            if (!((m >> e) & 1u)) continue;
+            const uint32_t word = nv[e >> 2];
+            const int sh = 8 * (e & 3);
+            const uint8_t s = (uint8_t)(word >> sh);
+            uint8_t t = s;
+            if (MODE == 0) {
+                if (s == kEmpty) t = kAscendantNeighbour;
+                else if (s == kSeed) t = kPropagate;
+            } else {
+                if (s == kEmpty) t = kBoundary;
+            }
+            if (t != s) {
+                nv[e >> 2] = (word & ~(0xFFu << sh)) | ((uint32_t)t << sh);
+                changed = true;
+            }
+        }
+        if (changed) *c = make_uint4(nv[0], nv[1], nv[2], nv[3]);
+    }
+}
+
 // The same dilation for rows of a multiple of 4 cells: a lane moves 4
 // consecutive cells of a row as one 32-bit word, so a warp reads the block's
 // 128 y of a row in one load, and the shared mask holds per row and lane the
@@ -707,9 +772,13 @@ void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s, bool fill
     APRB_CHECK_LAUNCH();
     for (int l = top; l >= lmin; --l) {
         const dim3 dgrid((g.y_num[l] + kDY - 1) / kDY, (g.x_num[l] + kDX - 1) / kDX, (g.z_num[l] + kDZ - 1) / kDZ);
+        const dim3 dgrid16((g.y_num[l] + kD16Y - 1) / kD16Y, dgrid.y, dgrid.z);
+        const bool by16 = g.y_num[l] % 16 == 0 && ((uintptr_t)pm.status[l] & 15) == 0;
         const bool by4 = g.y_num[l] % 4 == 0 && ((uintptr_t)pm.status[l] & 3) == 0;
         if (l != top) {
-            if (by4)
+            if (by16)
+                dilate16_kernel<0><<<dgrid16, 256, 0, s>>>(pm.status[l], dims(g, l));
+            else if (by4)
                 dilate4_kernel<0><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
             else
                 dilate_kernel<0><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
@@ -722,7 +791,9 @@ void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s, bool fill
                                                                                   pm.status[l + 1], dims(g, l + 1));
             count_launch(2);
         }
-        if (by4)
+        if (by16)
+            dilate16_kernel<1><<<dgrid16, 256, 0, s>>>(pm.status[l], dims(g, l));
+        else if (by4)
             dilate4_kernel<1><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
         else
             dilate_kernel<1><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
