@@ -845,7 +845,7 @@ __device__ __forceinline__ void cp_async16(float *smem, const float *gmem) {
 // ImageType, yn a multiple of 4, 16-byte aligned image): tile rows arrive in
 // 16-byte copies.
 template <typename IT, bool PW2, bool VEC>
-__global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict__ im, int yn, int xn, int zn,
+__global__ void __launch_bounds__(kGThreads, 4) grad_ds_kernel(const IT *__restrict__ im, int yn, int xn, int zn,
                                                             IT *__restrict__ grad, float *__restrict__ ids, int yd,
                                                             int xd, int zd, float hx, float hy, float hz) {
     // six plane slots: the four planes a step reads and the two the next
@@ -1013,7 +1013,21 @@ __global__ void __launch_bounds__(kGThreads) grad_ds_kernel(const IT *__restrict
                     if (z1in) children(n2, n1.a1, n1.b1, d3a, d3b, f);
                 };
                 double smax = 0.0;  // every square is >= 0
-                all([&](double q) { smax = q > smax ? q : smax; });
+                auto upd = [&](double q) { smax = q > smax ? q : smax; };
+                if (y1in && x1in) {
+                    // away from the volume's y / x end every child exists:
+                    // straight-line code (the maximum is order-independent)
+                    auto four = [&](const Nb &C, float2 ua, float2 ub, float2 da, float2 db) {
+                        upd(gsq(C.m.x, C.b1.x, C.a0.y, C.a1.y, ua.x, da.x));
+                        upd(gsq(C.m.y, C.b1.y, C.a1.x, C.a2.x, ua.y, da.y));
+                        upd(gsq(C.a1.x, C.p.x, C.b0.y, C.b1.y, ub.x, db.x));
+                        upd(gsq(C.a1.y, C.p.y, C.b1.x, C.b2.x, ub.y, db.y));
+                    };
+                    four(n1, u0a, u0b, n2.a1, n2.b1);
+                    if (z1in) four(n2, n1.a1, n1.b1, d3a, d3b);
+                } else {
+                    all(upd);
+                }
                 if (sizeof(IT) == 4 || smax < 4294967296.0) {
                     const double root = sqrt(smax);
                     gmax = sizeof(IT) == 2 ? cvt_u16d(root) : (float)root;
