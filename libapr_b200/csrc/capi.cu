@@ -1212,6 +1212,7 @@ ConvPlan make_plan(const aprb_apr *a, const T *stencil, int ks, int ds, int norm
         o += sd * sd * sd;
     }
     plan.reflect = reflect != 0;
+    plan.values.assign(host.begin(), host.end());
     return plan;
 }
 
@@ -1280,6 +1281,7 @@ static void gradient_dim(aprb_apr *a, const float *in, float *out, int dim, int 
         plan.offsets.push_back(27 * d);
     }
     plan.reflect = true;
+    plan.values.assign(host.begin(), host.end());
     float *dst = scratch().stencils.as<float>(host.size());
     APRB_CUDA(cudaMemcpyAsync(dst, host.data(), host.size() * sizeof(float), cudaMemcpyHostToDevice, s));
     float *tree = scratch().tree_vals.as<float>(a->T ? a->T : 1);

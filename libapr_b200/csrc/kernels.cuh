@@ -157,6 +157,7 @@ struct ConvPlan {
     std::vector<int> sides;
     std::vector<int> offsets;
     int reflect = 1;
+    std::vector<double> values;  // the stencils on the host (exact for float and double), at offsets
 };
 // Row chunk index of every APR and tree level (built once per APR) and the
 // particle count of every APR level.
