@@ -1219,6 +1219,23 @@ __device__ __forceinline__ float sat_y_value(int i, int n, float d, float cm /*C
     return v;
 }
 
+// sat_y_value from the quotients qm = C[i-off-1] / d and qp = C[i+off] / d
+// (each the correctly rounded quotient; -cm / d == -(cm / d) exactly).
+template <int OFF>
+__device__ __forceinline__ float sat_y_value_q(int i, int n, float d, float qm, float qp, float clast) {
+    float v = (i <= OFF) ? 0.0f : -qm;
+    if (i < n - OFF) v = v + qp;
+    if (i >= n - OFF) {
+        float cnt = (float)(i - (n - OFF) + 1);
+        v = v * d;
+        v = v + clast;
+        v = (float)((double)v * (1.0 / (double)(d - cnt)));
+    }
+    if (i >= 1 && i <= OFF) v = (float)((double)v * ((double)d / ((double)i + (double)OFF + 1.0)));
+    if (i == 0) v = (float)((double)v * ((double)d / ((double)OFF + 1.0)));
+    return v;
+}
+
 // y box mean: one thread per y-line, cumulative sum carried in a register
 // shift window of 2*OFF+2 entries; tiles through shared memory as in the IIR.
 // absdiff_ref != nullptr makes the input |in - absdiff_ref| (calc_abs_diff,
@@ -1368,9 +1385,11 @@ __global__ void __launch_bounds__(32 * kSW) sat_y_async_kernel(const float *__re
         }
         cp_async_commit();
     };
-    float c[W];
+    // quotients C / d of the last W cumulative sums: the window's older end
+    // divided once, when it was the newest
+    float qr[W];
 #pragma unroll
-    for (int q = 0; q < W; ++q) c[q] = 0.0f;
+    for (int q = 0; q < W; ++q) qr[q] = 0.0f;
     float C = 0.0f;
     issue(0, 0);
     for (int t = 0; t < ntile; ++t) {
@@ -1391,11 +1410,11 @@ __global__ void __launch_bounds__(32 * kSW) sat_y_async_kernel(const float *__re
                     float v = T[lane][k];
                     if (REF) v = fabsf(v - R[lane][k]);
                     C = C + v;
+                    const float qn = div_const(C, d, rd);
 #pragma unroll
-                    for (int q = 0; q < W - 1; ++q) c[q] = c[q + 1];
-                    c[W - 1] = C;
-                    const float o = div_const(-c[0], d, rd);
-                    T[lane][k] = o + div_const(C, d, rd);
+                    for (int q = 0; q < W - 1; ++q) qr[q] = qr[q + 1];
+                    qr[W - 1] = qn;
+                    T[lane][k] = -qr[0] + qn;
                 }
             } else {
                 const int kend = min(kSY, n - y0);
@@ -1403,11 +1422,12 @@ __global__ void __launch_bounds__(32 * kSW) sat_y_async_kernel(const float *__re
                     float v = T[lane][k];
                     if (REF) v = fabsf(v - R[lane][k]);
                     C = C + v;
+                    const float qn = div_const(C, d, rd);
 #pragma unroll
-                    for (int q = 0; q < W - 1; ++q) c[q] = c[q + 1];
-                    c[W - 1] = C;
+                    for (int q = 0; q < W - 1; ++q) qr[q] = qr[q + 1];
+                    qr[W - 1] = qn;
                     const int i = y0 + k - OFF;
-                    if (i >= 0 && i < n - OFF) T[lane][k] = sat_y_value<OFF>(i, n, d, c[0], C, 0.0f);
+                    if (i >= 0 && i < n - OFF) T[lane][k] = sat_y_value_q<OFF>(i, n, d, qr[0], qn, 0.0f);
                 }
             }
         }
@@ -1430,11 +1450,11 @@ __global__ void __launch_bounds__(32 * kSW) sat_y_async_kernel(const float *__re
         for (int i = n - OFF; i < n; ++i) {
             if (i < 0) continue;
             const int back = (n - 1) - (i - OFF - 1);
-            float cm = 0.0f;
+            float qm = 0.0f;
 #pragma unroll
             for (int q = 0; q < W; ++q)
-                if (q == W - 1 - back) cm = c[q];
-            out[(line0 + lane) * (uint64_t)n + i] = sat_y_value<OFF>(i, n, d, cm, 0.0f, C);
+                if (q == W - 1 - back) qm = qr[q];
+            out[(line0 + lane) * (uint64_t)n + i] = sat_y_value_q<OFF>(i, n, d, qm, 0.0f, C);
         }
     }
 }
