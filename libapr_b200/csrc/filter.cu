@@ -117,6 +117,67 @@ __host__ __device__ constexpr int tree_tw() {
     return sizeof(T) == 8 ? 256 : 512;
 }
 
+// Stage elements [s, e) of one row (y values Y, values X) into the shared
+// row V / K (value, kind) at y - cy0.  With vec, whole aligned groups of four
+// elements move as one 8-byte y load and one 16-byte (two for double) value
+// load, two groups per lane in flight; the at most six elements in partial
+// groups at the ends go one per lane.
+template <typename T>
+__device__ __forceinline__ void stage_row(const uint16_t *__restrict__ Y, const T *__restrict__ X, uint64_t s,
+                                          uint64_t e, int cy0, T *V, uint8_t *K, uint8_t kind, int lane, int vec) {
+    const int n = (int)(e - s);
+    if (!vec) {
+#pragma unroll 4
+        for (int j = lane; j < n; j += 32) {
+            const int yv = (int)Y[s + j] - cy0;
+            V[yv] = X[s + j];
+            K[yv] = kind;
+        }
+        return;
+    }
+    const int g0 = (int)(s & 3);
+    const int gfirst = g0 ? 1 : 0, gend = (n + g0) >> 2;
+    const int hend = min(n, 4 * gfirst - g0), tbeg = max(hend, 4 * gend - g0);
+    if (lane < hend + (n - tbeg)) {
+        const int j = lane < hend ? lane : tbeg + lane - hend;
+        const int yv = (int)Y[s + j] - cy0;
+        V[yv] = X[s + j];
+        K[yv] = kind;
+    }
+    const uint64_t gb = s - (uint64_t)g0;  // element index of group 0 (a multiple of 4)
+    constexpr int B = 2;  // groups per lane in flight (more cost resident CTAs: 4.11 / 3.82 / 4.34 / 5.31 ms for 1 / 2 / 3 / 4 at 1.1e9 particles)
+    for (int gi0 = gfirst + lane; gi0 < gend; gi0 += 32 * B) {
+        uint2 yy[B];
+        T vv[B][4];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const int gi = gi0 + 32 * u;
+            if (gi >= gend) continue;
+            const uint64_t ge = gb + 4 * (uint64_t)gi;
+            yy[u] = *reinterpret_cast<const uint2 *>(Y + ge);
+            if constexpr (sizeof(T) == 4) {
+                const float4 v = *reinterpret_cast<const float4 *>(X + ge);
+                vv[u][0] = v.x, vv[u][1] = v.y, vv[u][2] = v.z, vv[u][3] = v.w;
+            } else {
+                const double2 v0 = *reinterpret_cast<const double2 *>(X + ge);
+                const double2 v1 = *reinterpret_cast<const double2 *>(X + ge + 2);
+                vv[u][0] = v0.x, vv[u][1] = v0.y, vv[u][2] = v1.x, vv[u][3] = v1.y;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            if (gi0 + 32 * u >= gend) continue;
+            const int y4[4] = {(int)(yy[u].x & 0xffffu), (int)(yy[u].x >> 16), (int)(yy[u].y & 0xffffu),
+                               (int)(yy[u].y >> 16)};
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                V[y4[q] - cy0] = vv[u][q];
+                K[y4[q] - cy0] = kind;
+            }
+        }
+    }
+}
+
 struct TreeLevelArgs {
     LD dt;                  // tree level t dims (== APR level t dims)
     LD dc;                  // child level dims
@@ -124,6 +185,7 @@ struct TreeLevelArgs {
     uint64_t c_row_base;    // APR level_xz[t+1]
     uint64_t ct_row_base;   // tree level_xz[t+1] (0 when t+1 has no tree level)
     const uint16_t *t_cidx, *c_cidx, *ct_cidx;
+    int vec;  // y arrays 8-byte and value arrays 16-byte aligned: group loads
 };
 
 template <typename T>
@@ -173,22 +235,12 @@ __global__ void __launch_bounds__(128 * kTR) tree_mean_kernel(TreeLevelArgs a, u
             const uint64_t s0 = r0 + CC[c0], e0 = r0 + CC[c1];
             T *V = sv[pr][q4];
             uint8_t *K = sk[pr][q4];
-#pragma unroll 4
-            for (uint64_t i = s0 + lane; i < e0; i += 32) {
-                const int yv = (int)y_vec[i] - cy0;
-                V[yv] = parts[i];
-                K[yv] = 1;
-            }
+            stage_row<T>(y_vec, parts, s0, e0, cy0, V, K, 1, lane, a.vec);
             if (a.ct_row_base) {
                 const uint16_t *CT = a.ct_cidx + row * (uint64_t)(ncc + 1);
                 const uint64_t r1 = t_xz_end[a.ct_row_base + row - 1];
                 const uint64_t s1 = r1 + CT[c0], e1 = r1 + CT[c1];
-#pragma unroll 4
-                for (uint64_t i = s1 + lane; i < e1; i += 32) {
-                    const int yv = (int)t_y_vec[i] - cy0;
-                    V[yv] = tree[i];
-                    K[yv] = 2;
-                }
+                stage_row<T>(t_y_vec, tree, s1, e1, cy0, V, K, 2, lane, a.vec);
             }
         }
     }
@@ -964,6 +1016,8 @@ static void tree_means_all(const Geom &g, const uint64_t *xz_end, const uint16_t
         ta.t_cidx = cbase + fi.tree_off[t];
         ta.c_cidx = cbase + fi.apr_off[l];
         ta.ct_cidx = (l <= tg.l_max) ? cbase + fi.tree_off[l] : nullptr;
+        auto al = [](const void *p, uintptr_t b) { return ((uintptr_t)p & (b - 1)) == 0; };
+        ta.vec = al(y_vec, 8) && al(t_y_vec, 8) && al(in, 16) && al(tree, 16);
         const uint64_t rows = (uint64_t)ta.dt.xn * ta.dt.zn;
         const unsigned ych = (unsigned)((ta.dt.yn + tree_tw<T>() - 1) / tree_tw<T>());
         if (rows == 0 || ych == 0) continue;
