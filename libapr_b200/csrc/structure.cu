@@ -436,44 +436,81 @@ __global__ void row_fill_kernel(const uint8_t *__restrict__ st, LevelDims d, con
     }
 }
 
-__global__ void row_fill_top_kernel(const uint8_t *__restrict__ st, LevelDims d, const uint64_t *__restrict__ xz_end,
-                                    uint64_t row_base, uint64_t row_base_m, int ylm, int xlm, int zlm,
-                                    uint16_t *__restrict__ y_vec, int min_type) {
+__global__ void __launch_bounds__(256) row_fill_top_kernel(const uint8_t *__restrict__ st, LevelDims d,
+                                                             const uint64_t *__restrict__ xz_end, uint64_t row_base,
+                                                             uint64_t row_base_m, int ylm, int xlm, int zlm,
+                                                             uint16_t *__restrict__ y_vec, int min_type, int vec4) {
+    // 128 cells of the row per step, four per lane: one scan of the packed
+    // per-lane counts (level l_max - 1 particles << 16 | level l_max outputs)
+    // places both; the step's l_max outputs are staged in shared memory and
+    // copied to the four child rows with coalesced stores
+    __shared__ uint16_t stage[8][256];
     const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
+    uint16_t *S = stage[threadIdx.x >> 5];
     if (row >= (uint64_t)d.xn * d.zn) return;
     const int x = (int)(row % (uint64_t)d.xn), z = (int)(row / (uint64_t)d.xn);
     const uint8_t *R = st + row * (uint64_t)d.yn;
     uint64_t o = xz_end[row_base + row - 1];
-    uint64_t om[4];
-    bool have[4];
+    uint16_t *Q[4];
+    int nq = 0;
+#pragma unroll
     for (int q = 0; q < 4; ++q) {
         const int zz = 2 * z + (q >> 1), xx = 2 * x + (q & 1);
-        have[q] = zz < zlm && xx < xlm;
-        om[q] = have[q] ? xz_end[row_base_m + (uint64_t)zz * xlm + xx - 1] : 0;
+        Q[q] = nullptr;
+        if (zz < zlm && xx < xlm) {
+            Q[q] = y_vec + xz_end[row_base_m + (uint64_t)zz * xlm + xx - 1];
+            nq = q + 1;
+        }
     }
-    uint64_t cm = 0;
-    const unsigned lt = (1u << lane) - 1u;
-    for (int y0 = 0; y0 < d.yn; y0 += 32) {
-        const int y = y0 + lane;
-        const uint8_t s = y < d.yn ? R[y] : 0;
-        const bool f = y < d.yn && is_particle(s, min_type);
-        const unsigned m = __ballot_sync(0xffffffffu, f);
-        if (f) y_vec[o + __popc(m & lt)] = (uint16_t)y;
-        o += __popc(m);
-        const unsigned cnt = (y < d.yn && is_seed(s, min_type)) ? 1u + (2 * y < ylm - 1) : 0u;
-        unsigned incl = cnt;
+    for (int y0 = 0; y0 < d.yn; y0 += 128) {
+        const int yb = y0 + 4 * lane;
+        uint8_t sv[4];
+        if (vec4 && yb + 4 <= d.yn) {
+            const uint32_t w = *reinterpret_cast<const uint32_t *>(R + yb);
+            sv[0] = w & 0xff, sv[1] = (w >> 8) & 0xff, sv[2] = (w >> 16) & 0xff, sv[3] = w >> 24;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) sv[k] = yb + k < d.yn ? R[yb + k] : 0;
+        }
+        int pc = 0, cc = 0;
+        int ck[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int y = yb + k;
+            pc += is_particle(sv[k], min_type) ? 1 : 0;
+            ck[k] = is_seed(sv[k], min_type) ? 1 + (2 * y < ylm - 1) : 0;
+            cc += ck[k];
+        }
+        const int mine = (pc << 16) | cc;
+        int incl = mine;
+#pragma unroll
         for (int k = 1; k < 32; k <<= 1) {
-            unsigned t = __shfl_up_sync(0xffffffffu, incl, k);
+            const int t = __shfl_up_sync(0xffffffffu, incl, k);
             if (lane >= k) incl += t;
         }
-        const unsigned excl = incl - cnt;
-        for (int q = 0; q < 4; ++q) {
-            if (!have[q] || cnt == 0) continue;
-            y_vec[om[q] + cm + excl] = (uint16_t)(2 * y);
-            if (cnt == 2) y_vec[om[q] + cm + excl + 1] = (uint16_t)(2 * y + 1);
+        const int tot = __shfl_sync(0xffffffffu, incl, 31);
+        const int excl = incl - mine;
+        int pp = excl >> 16, cp = excl & 0xffff;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int y = yb + k;
+            if (is_particle(sv[k], min_type)) y_vec[o + pp++] = (uint16_t)y;
+            if (ck[k]) {
+                S[cp++] = (uint16_t)(2 * y);
+                if (ck[k] == 2) S[cp++] = (uint16_t)(2 * y + 1);
+            }
         }
-        cm += __shfl_sync(0xffffffffu, incl, 31);
+        o += (uint64_t)(tot >> 16);
+        const int nc = tot & 0xffff;
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (q >= nq || Q[q] == nullptr) continue;
+            for (int j = lane; j < nc; j += 32) Q[q][j] = S[j];
+            Q[q] += nc;
+        }
+        __syncwarp();
     }
 }
 
@@ -851,9 +888,10 @@ void launch_linear_fill(const Geom &g, const Pyramid &pm, const uint64_t *xz_end
                                                               min_type);
         count_launch();
     }
+    const int vec4 = g.y_num[L - 1] % 4 == 0 && ((uintptr_t)pm.status[L - 1] & 3) == 0;
     row_fill_top_kernel<<<row_blocks(nrow(g, L - 1)), 256, 0, s>>>(pm.status[L - 1], dims(g, L - 1), xz_end,
                                                                   g.level_xz[L - 1], g.level_xz[L], g.y_num[L],
-                                                                  g.x_num[L], g.z_num[L], y_vec, min_type);
+                                                                  g.x_num[L], g.z_num[L], y_vec, min_type, vec4);
     count_launch();
     APRB_CHECK_LAUNCH();
 }
