@@ -181,6 +181,20 @@ struct aprb_apr {
     // used and released by the first sample_image from the same host buffer
     mutable DevBuf kept_img;
     mutable const uint16_t *kept_host = nullptr;
+    // No work on the APR can be pending on any stream: set at the end of the
+    // host-buffer get_apr / sample_image (each synchronises before it
+    // returns), cleared by every other call that touches the APR (device
+    // calls on the caller's streams, exported device pointers).  A quiet APR
+    // gives its pooled memory back in stream order without a device-wide
+    // synchronisation, so host threads converting other volumes at the same
+    // time are not stalled; otherwise freeing waits for the device, as
+    // cudaFree would.
+    mutable bool quiet = false;
+    ~aprb_apr() {
+        if (!quiet) return;
+        cudaStream_t s = cudaStreamPerThread;
+        for (DevBuf *b : {&xz_end, &y_vec, &t_xz_end, &t_y_vec, &cnn_rows, &kept_img}) b->release_idle(s);
+    }
 };
 
 struct aprb_converter {
@@ -777,6 +791,7 @@ aprb_status aprb_get_apr(aprb_converter *c, const aprb_params *p, const uint16_t
             (*out)->kept_img.swap(c->img);
             (*out)->kept_host = img;
         }
+        (*out)->quiet = true;  // get_apr_impl synchronised its streams
     });
 }
 
@@ -957,6 +972,7 @@ aprb_status aprb_apr_get_info(const aprb_apr *a, aprb_apr_info *info) {
 
 aprb_status aprb_apr_export(const aprb_apr *a, uint64_t *level_xz, uint64_t *xz_end, uint16_t *y_vec) {
     return guarded([&] {
+        if (a) a->quiet = false;
         ARG_CHECK(a, "null apr");
         if (level_xz) std::memcpy(level_xz, a->g.level_xz, sizeof(uint64_t) * (a->g.l_max + 2));
         if (xz_end) APRB_CUDA(cudaMemcpy(xz_end, a->xz_end.p, a->n_xz * sizeof(uint64_t), cudaMemcpyDeviceToHost));
@@ -967,6 +983,7 @@ aprb_status aprb_apr_export(const aprb_apr *a, uint64_t *level_xz, uint64_t *xz_
 aprb_status aprb_apr_device_arrays(const aprb_apr *a, const uint64_t **level_xz, const uint64_t **xz_end,
                                    const uint16_t **y_vec) {
     return guarded([&] {
+        if (a) a->quiet = false;
         ARG_CHECK(a, "null apr");
         if (level_xz) *level_xz = nullptr;  // level offsets are host-side geometry (aprb_apr_export)
         if (xz_end) *xz_end = (const uint64_t *)a->xz_end.p;
@@ -1003,6 +1020,7 @@ aprb_status aprb_apr_from_arrays(int y_num, int x_num, int z_num, const uint64_t
 
 aprb_status aprb_reconstruct_constant_u16(const aprb_apr *a, const uint16_t *parts, uint16_t *img) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && img && (parts || a->P == 0), "null argument");
         reconstruct_host<uint16_t>(a, parts, img, false);
@@ -1010,6 +1028,7 @@ aprb_status aprb_reconstruct_constant_u16(const aprb_apr *a, const uint16_t *par
 }
 aprb_status aprb_reconstruct_constant_f32(const aprb_apr *a, const float *parts, float *img) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && img && (parts || a->P == 0), "null argument");
         reconstruct_host<float>(a, parts, img, false);
@@ -1017,6 +1036,7 @@ aprb_status aprb_reconstruct_constant_f32(const aprb_apr *a, const float *parts,
 }
 aprb_status aprb_reconstruct_level(const aprb_apr *a, uint8_t *img) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && img, "null argument");
         reconstruct_host<uint8_t>(a, nullptr, img, true);
@@ -1025,6 +1045,7 @@ aprb_status aprb_reconstruct_level(const aprb_apr *a, uint8_t *img) {
 aprb_status aprb_reconstruct_constant_u16_device(const aprb_apr *a, const uint16_t *parts_dev, uint16_t *img_dev,
                                                  void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && img_dev && (parts_dev || a->P == 0), "null argument");
         reconstruct_device<uint16_t>(a, parts_dev, img_dev, false, (cudaStream_t)stream);
@@ -1033,6 +1054,7 @@ aprb_status aprb_reconstruct_constant_u16_device(const aprb_apr *a, const uint16
 aprb_status aprb_reconstruct_constant_f32_device(const aprb_apr *a, const float *parts_dev, float *img_dev,
                                                  void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && img_dev && (parts_dev || a->P == 0), "null argument");
         reconstruct_device<float>(a, parts_dev, img_dev, false, (cudaStream_t)stream);
@@ -1040,6 +1062,7 @@ aprb_status aprb_reconstruct_constant_f32_device(const aprb_apr *a, const float 
 }
 aprb_status aprb_reconstruct_level_device(const aprb_apr *a, uint8_t *img_dev, void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && img_dev, "null argument");
         reconstruct_device<uint8_t>(a, nullptr, img_dev, true, (cudaStream_t)stream);
@@ -1048,6 +1071,7 @@ aprb_status aprb_reconstruct_level_device(const aprb_apr *a, uint8_t *img_dev, v
 
 aprb_status aprb_sample_image_device(const aprb_apr *a, const uint16_t *img_dev, uint16_t *parts_dev, void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && img_dev && parts_dev, "null argument");
         launch_sample(a->g, (const uint64_t *)a->xz_end.p, (const uint16_t *)a->y_vec.p, img_dev, parts_dev, scratch().pyr,
@@ -1058,6 +1082,7 @@ aprb_status aprb_sample_image_device(const aprb_apr *a, const uint16_t *img_dev,
 aprb_status aprb_sample_image_by_block_device(const aprb_apr *a, const uint16_t *img_dev, int z_block_size,
                                               int ghost_z, uint16_t *parts_dev, void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && img_dev && parts_dev, "null argument");
         ARG_CHECK(z_block_size >= 1 && ghost_z >= 0, "z_block_size must be positive and ghost_z non-negative");
@@ -1069,6 +1094,7 @@ aprb_status aprb_sample_image_by_block_device(const aprb_apr *a, const uint16_t 
 aprb_status aprb_sample_image_by_block(const aprb_apr *a, const uint16_t *img, int z_block_size, int ghost_z,
                                        uint16_t *parts) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && img && parts, "null argument");
         ARG_CHECK(z_block_size >= 1 && ghost_z >= 0, "z_block_size must be positive and ghost_z non-negative");
@@ -1086,6 +1112,7 @@ aprb_status aprb_sample_image_by_block(const aprb_apr *a, const uint16_t *img, i
 
 aprb_status aprb_sample_image(const aprb_apr *a, const uint16_t *img, uint16_t *parts) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && img && parts, "null argument");
         cudaStream_t s = cudaStreamPerThread;
@@ -1102,8 +1129,11 @@ aprb_status aprb_sample_image(const aprb_apr *a, const uint16_t *img, uint16_t *
             launch_sample(g, xz, yv, (const uint16_t *)a->kept_img.p, dp, scratch().pyr, s);
             if (a->P) APRB_CUDA(cudaMemcpyAsync(parts, dp, a->P * sizeof(uint16_t), cudaMemcpyDeviceToHost, s));
             APRB_CUDA(cudaStreamSynchronize(s));
-            a->kept_img.release();
+            // the copy's upload finished before get_apr returned and this
+            // stream is drained: nothing can still read it
+            a->kept_img.release_idle(s);
             a->kept_host = nullptr;
+            a->quiet = true;
             return;
         }
         uint16_t *di = scratch().io_in.as<uint16_t>(n);
@@ -1361,6 +1391,7 @@ extern "C" {
 
 aprb_status aprb_apr_init_tree(aprb_apr *a) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a, "null apr");
         ensure_tree(a, cudaStreamPerThread);
@@ -1369,6 +1400,7 @@ aprb_status aprb_apr_init_tree(aprb_apr *a) {
 
 aprb_status aprb_apr_export_tree(aprb_apr *a, uint64_t *level_xz, uint64_t *xz_end, uint16_t *y_vec) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a, "null apr");
         ensure_tree(a, cudaStreamPerThread);
@@ -1380,6 +1412,7 @@ aprb_status aprb_apr_export_tree(aprb_apr *a, uint64_t *level_xz, uint64_t *xz_e
 
 aprb_status aprb_fill_tree_mean_device(aprb_apr *a, const float *parts_dev, float *tree_dev, void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && parts_dev && tree_dev, "null argument");
         cudaStream_t s = (cudaStream_t)stream;
@@ -1392,6 +1425,7 @@ aprb_status aprb_fill_tree_mean_device(aprb_apr *a, const float *parts_dev, floa
 
 aprb_status aprb_fill_tree_mean(aprb_apr *a, const float *parts, float *tree) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && parts && tree, "null argument");
         cudaStream_t s = cudaStreamPerThread;
@@ -1410,6 +1444,7 @@ aprb_status aprb_fill_tree_mean(aprb_apr *a, const float *parts, float *tree) {
 aprb_status aprb_convolve_device(aprb_apr *a, const float *stencil, int ksize, const float *in_dev, float *out_dev,
                                  int reflect, int use_stencil_downsample, int normalize, void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && stencil && in_dev && out_dev, "null argument");
         convolve_impl(a, stencil, ksize, in_dev, out_dev, reflect, use_stencil_downsample, normalize,
@@ -1419,6 +1454,7 @@ aprb_status aprb_convolve_device(aprb_apr *a, const float *stencil, int ksize, c
 
 aprb_status aprb_gradient(aprb_apr *a, const float *in, float *out, int dimension, float delta, int sobel) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && out && (in || a->P == 0), "null argument");
         ARG_CHECK(dimension >= 0 && dimension <= 2, "dimension must be 0 (y), 1 (x) or 2 (z)");
@@ -1435,6 +1471,7 @@ aprb_status aprb_gradient(aprb_apr *a, const float *in, float *out, int dimensio
 aprb_status aprb_gradient_device(aprb_apr *a, const float *in_dev, float *out_dev, int dimension, float delta,
                                  int sobel, void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && out_dev && (in_dev || a->P == 0), "null argument");
         ARG_CHECK(dimension >= 0 && dimension <= 2, "dimension must be 0 (y), 1 (x) or 2 (z)");
@@ -1444,6 +1481,7 @@ aprb_status aprb_gradient_device(aprb_apr *a, const float *in_dev, float *out_de
 
 aprb_status aprb_gradient_magnitude(aprb_apr *a, const float *in, float *out, const float *deltas, int sobel) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && out && deltas && (in || a->P == 0), "null argument");
         cudaStream_t s = cudaStreamPerThread;
@@ -1459,6 +1497,7 @@ aprb_status aprb_gradient_magnitude(aprb_apr *a, const float *in, float *out, co
 aprb_status aprb_gradient_magnitude_device(aprb_apr *a, const float *in_dev, float *out_dev, const float *deltas,
                                            int sobel, void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && out_dev && deltas && (in_dev || a->P == 0), "null argument");
         gradient_magnitude(a, in_dev, out_dev, deltas, sobel, (cudaStream_t)stream);
@@ -1468,6 +1507,7 @@ aprb_status aprb_gradient_magnitude_device(aprb_apr *a, const float *in_dev, flo
 aprb_status aprb_convolve(aprb_apr *a, const float *stencil, int ksize, const float *in, float *out, int reflect,
                           int use_stencil_downsample, int normalize) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && stencil && in && out, "null argument");
         cudaStream_t s = cudaStreamPerThread;
@@ -1484,6 +1524,7 @@ aprb_status aprb_richardson_lucy_device(aprb_apr *a, const uint16_t *in_dev, flo
                                         int ksize, int niter, int use_stencil_downsample, int normalize, int resume,
                                         void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && in_dev && out_dev && psf && niter >= 0, "invalid argument");
         rl_impl<float>(a, in_dev, out_dev, psf, ksize, niter, use_stencil_downsample, normalize, resume,
@@ -1494,6 +1535,7 @@ aprb_status aprb_richardson_lucy_device(aprb_apr *a, const uint16_t *in_dev, flo
 aprb_status aprb_richardson_lucy(aprb_apr *a, const uint16_t *in, float *out, const float *psf, int ksize, int niter,
                                  int use_stencil_downsample, int normalize, int resume) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && in && out && psf && niter >= 0, "invalid argument");
         cudaStream_t s = cudaStreamPerThread;
@@ -1511,6 +1553,7 @@ aprb_status aprb_richardson_lucy_fp64_device(aprb_apr *a, const uint16_t *in_dev
                                              int ksize, int niter, int use_stencil_downsample, int normalize,
                                              int resume, void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && in_dev && out_dev && psf && niter >= 0, "invalid argument");
         rl_impl<double>(a, in_dev, out_dev, psf, ksize, niter, use_stencil_downsample, normalize, resume,
@@ -1521,6 +1564,7 @@ aprb_status aprb_richardson_lucy_fp64_device(aprb_apr *a, const uint16_t *in_dev
 aprb_status aprb_richardson_lucy_fp64(aprb_apr *a, const uint16_t *in, double *out, const float *psf, int ksize,
                                       int niter, int use_stencil_downsample, int normalize, int resume) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && in && out && psf && niter >= 0, "invalid argument");
         cudaStream_t s = cudaStreamPerThread;
@@ -1573,6 +1617,7 @@ extern "C" {
 aprb_status aprb_cnn_layer_forward_device(aprb_apr *a, const float *in, const float *W, const float *bias, int relu,
                                           float *out, void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && in && W && bias && out, "null argument");
         cudaStream_t s = (cudaStream_t)stream;
@@ -1585,6 +1630,7 @@ aprb_status aprb_cnn_layer_backward_device(aprb_apr *a, const float *in, const f
                                            const float *g_out, int relu, float *g_in, float *dW, float *db,
                                            void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && in && W && out && g_out && g_in && dW && db, "null argument");
         cudaStream_t s = (cudaStream_t)stream;
@@ -1596,6 +1642,7 @@ aprb_status aprb_cnn_layer_backward_device(aprb_apr *a, const float *in, const f
 aprb_status aprb_cnn_features_device(const aprb_apr *a, const float *u, const float *ratio, const uint16_t *raw,
                                      float *features, void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && u && ratio && raw && features, "null argument");
         cnn_features(u, ratio, raw, features, a->P, (cudaStream_t)stream);
@@ -1605,6 +1652,7 @@ aprb_status aprb_cnn_features_device(const aprb_apr *a, const float *u, const fl
 aprb_status aprb_cnn_loss_device(const aprb_apr *a, const float *pred, const float *u0, const float *u1, float *g_pred,
                                  double *loss_dev, void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && pred && u0 && u1 && g_pred && loss_dev, "null argument");
         cnn_loss(pred, u0, u1, g_pred, a->P, loss_dev, (cudaStream_t)stream);
@@ -1613,6 +1661,7 @@ aprb_status aprb_cnn_loss_device(const aprb_apr *a, const float *pred, const flo
 
 aprb_status aprb_cnn_apply_device(const aprb_apr *a, const float *pred, float *u, void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && pred && u, "null argument");
         cnn_apply(pred, u, a->P, (cudaStream_t)stream);
@@ -1632,6 +1681,7 @@ aprb_status aprb_rl_ratio_device(aprb_apr *a, const uint16_t *in_dev, const floa
                                  const float *psf, int ksize, int use_stencil_downsample, int normalize,
                                  void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && in_dev && u_dev && ratio_dev && psf, "null argument");
         cudaStream_t s = (cudaStream_t)stream;
@@ -1654,6 +1704,7 @@ aprb_status aprb_rl_objective_device(aprb_apr *a, const uint16_t *in_dev, const 
                                      int ksize, int use_stencil_downsample, int normalize, double *objective,
                                      void *stream) {
     return guarded([&] {
+        if (a) a->quiet = false;
         require_device();
         ARG_CHECK(a && in_dev && u_dev && psf && objective, "null argument");
         cudaStream_t s = (cudaStream_t)stream;

@@ -132,6 +132,19 @@ struct DevBuf {
         cap = 0;
         pooled = false;
     }
+    // Back to the pool in the order of stream s, without waiting for the
+    // device: only for a block that no stream can still be using.
+    void release_idle(cudaStream_t s) {
+        if (p) {
+            if (pooled)
+                cudaFreeAsync(p, s);
+            else
+                cudaFree(p);
+        }
+        p = nullptr;
+        cap = 0;
+        pooled = false;
+    }
     void swap(DevBuf &o) {
         std::swap(p, o.p);
         std::swap(cap, o.cap);
