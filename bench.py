@@ -881,10 +881,11 @@ def main():
 
     # Two volumes in flight: a second converter on a second host thread, each
     # thread taking every other step (get_apr + sample_image of one volume).
-    # The get_apr calls (upload and construction) take turns, so one volume's
-    # sampling and particle download overlap the next one's upload (PCIe
-    # carries both directions at once).  Every step still moves its own image
-    # up and its own particles down inside the timed region.
+    # The library lets one host-buffer upload at a time cross PCIe, so the
+    # uploads run back to back while the other volume's construction,
+    # sampling and particle download proceed (PCIe carries both directions at
+    # once).  Every step still moves its own image up and its own particles
+    # down inside the timed region.
     import threading
     conv2 = A.APRConverter(args.image_type)
     hparts2 = torch.empty(max(P, 1), dtype=torch.int16, pin_memory=True)
@@ -893,15 +894,12 @@ def main():
     for cv in convs:
         _lib.check(L.aprb_converter_keep_input(cv._h, 1))
 
-    upload = threading.Lock()  # one get_apr (the image upload) at a time
-
     def worker(i, count, errs):
         try:
             torch.cuda.set_device(local)
             for _ in range(count):
                 h = C.c_void_p()
-                with upload:
-                    _lib.check(L.aprb_get_apr(convs[i]._h, C.byref(par), hp, y, x, z, C.byref(h)))
+                _lib.check(L.aprb_get_apr(convs[i]._h, C.byref(par), hp, y, x, z, C.byref(h)))
                 _lib.check(L.aprb_sample_image(h, hp, outs[i]))
                 L.aprb_apr_free(h)
         except Exception as e:  # noqa: BLE001 -- reported after the join
@@ -931,8 +929,8 @@ def main():
            "one_volume_in_flight": {"value": N * world / te1 / 1e9, "ms_per_step": te1 * 1e3},
            "note": "aprb_get_apr + aprb_sample_image on pinned host buffers, converter keep_input on (the "
                    "image crosses PCIe once per step, in z-chunks overlapped with smoothing; the particles "
-                   "come back once); two converters on two host threads take alternate steps, their "
-                   "get_apr calls in turn, so one volume's download overlaps the next one's upload; "
+                   "come back once); two converters on two host threads take alternate steps, the uploads "
+                   "in turn, so one volume's construction and download overlap the next one's upload; "
                    "one_volume_in_flight: the same calls on one thread"}
     cpu, parity = None, None
     if not args.no_cpu and world == 1 and shape == SHAPE:

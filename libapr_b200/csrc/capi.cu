@@ -210,7 +210,35 @@ struct aprb_converter {
     aprb_params last_par{};  // parameters of the last get_apr after the automatic ones
     int last_l_max = 0;
     DevBuf margins;
+    // host-buffer get_apr: the device's upload lock while this call's image
+    // is still crossing PCIe, and the event that marks its last chunk landed
+    std::unique_lock<std::mutex> *upload_lock = nullptr;
+    cudaEvent_t up_done = nullptr;
+    ~aprb_converter() {
+        if (up_done) cudaEventDestroy(up_done);
+    }
 };
+
+// One host-buffer upload at a time per device: concurrent host get_apr calls
+// (other converters on other host threads) would share the link anyway; in
+// turn, each call's smoothing, construction and the other calls' particle
+// downloads overlap the next call's upload.
+static std::mutex &upload_mutex() {
+    static std::mutex mu[64];
+    int dev = 0;
+    APRB_CUDA(cudaGetDevice(&dev));
+    return mu[dev & 63];
+}
+
+// Called once a host-buffer get_apr has enqueued all its upload chunks and
+// before its first blocking wait: waits for the last chunk and lets the next
+// caller's upload start.
+static void release_upload(aprb_converter *c) {
+    if (!c->upload_lock) return;
+    APRB_CUDA(cudaEventSynchronize(c->up_done));
+    c->upload_lock->unlock();
+    c->upload_lock = nullptr;
+}
 
 // reconstruct_constant / reconstruct_level on device buffers
 template <typename V>
@@ -408,6 +436,10 @@ PixelOut<IT> pixel_stages(aprb_converter *c, const aprb_params &p, const uint16_
     if (host) {
         launch_upload_smooth<IT>(host, const_cast<uint16_t *>(img), work, yn, xn, zn, p.lambda, mm, d_off,
                                  is_u16 && p.lambda > 0, d_err, c->iir_ckpt, s, up);
+        if (c->upload_lock) {
+            if (!c->up_done) APRB_CUDA(cudaEventCreateWithFlags(&c->up_done, cudaEventDisableTiming));
+            APRB_CUDA(cudaEventRecord(c->up_done, up));  // after the last chunk's copy
+        }
     } else {
         launch_minmax_offset(img, n, mm, d_off, is_u16 && p.lambda > 0, s);
         launch_smooth<IT>(img, work, yn, xn, zn, p.lambda, d_off, d_err, c->iir_ckpt, s);
@@ -440,6 +472,7 @@ void throw_if_overflow(aprb_converter *c, cudaStream_t s) {
 // (generateDatastructures, APRConverter.hpp:339-363); reads the overflow
 // flag before the particle count is trusted.
 void build_structure(aprb_converter *c, const aprb_params &p, Pyramid &pm, aprb_apr *a, cudaStream_t s) {
+    release_upload(c);
     const Geom &g = a->g;
     const int L = g.l_max;
     uint64_t *xz_end = a->xz_end.as_pooled<uint64_t>(a->n_xz, s);
@@ -781,12 +814,16 @@ aprb_status aprb_get_apr(aprb_converter *c, const aprb_params *p, const uint16_t
         // the copy goes in z-chunks on the transfer stream, overlapped with
         // the smoothing of the chunks already on the device
         cudaStream_t up = transfer_streams().up;
+        std::unique_lock<std::mutex> lk(upload_mutex());  // released once this call's upload has landed
+        c->upload_lock = &lk;
         try {
             get_apr_impl(c, p, d, y_num, x_num, z_num, s, out, img, up);
         } catch (...) {
+            c->upload_lock = nullptr;
             cudaStreamSynchronize(up);  // no copy from the caller's buffer outlives the call
             throw;
         }
+        c->upload_lock = nullptr;
         if (c->keep_input) {
             (*out)->kept_img.swap(c->img);
             (*out)->kept_host = img;
