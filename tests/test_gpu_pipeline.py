@@ -238,3 +238,57 @@ def test_every_smoothing_variant_bit_exact(tma_case, axis, variant):
         assert np.array_equal(apr.linear_access()[2], acc.y_vec)
     finally:
         A.set_smoothing_schedule(old)
+
+
+def test_host_calls_from_two_threads_match_one_thread():
+    """Two host threads, each with its own converter (keep_input on), convert
+    and sample different volumes through the host-buffer calls at the same
+    time: their uploads take turns on the device and their APRs are freed
+    without a device-wide wait.  Every structure and every particle equals
+    the one-thread result of the same volume."""
+    import threading
+
+    import torch
+
+    shape = (40, 512, 512)
+    vols = []
+    for seed in (31, 32, 33, 34):
+        dev = torch.empty(shape, dtype=torch.int16, device="cuda")
+        A.synth_blobs_device(dev, 300, sigma=(2.0, 6.0), amp=(500.0, 6000.0), seed=seed)
+        torch.cuda.synchronize()
+        vols.append(np.ascontiguousarray(dev.cpu().numpy().view(np.uint16)))
+
+    def convert(conv, img):
+        apr = A.APR()
+        assert conv.get_apr(apr, img)
+        parts = A.ParticleData().sample_image(apr, img).data.copy()
+        return [a.copy() for a in apr.linear_access()], parts
+
+    ref_conv = A.APRConverter("float")
+    ref_conv.par = lib_params()
+    ref = [convert(ref_conv, v) for v in vols]
+
+    results = [None] * len(vols)
+    errors = []
+
+    def worker(t):
+        try:
+            torch.cuda.set_device(0)
+            conv = A.APRConverter("float")
+            conv.par = lib_params()
+            conv.keep_input(True)
+            for k in range(t, len(vols), 2):
+                results[k] = convert(conv, vols[k])
+        except Exception as e:  # noqa: BLE001 -- reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=(t,)) for t in range(2)]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    assert not errors, errors
+    for (sr, pr), (s, p) in zip(ref, results):
+        for u, v in zip(sr, s):
+            assert np.array_equal(u, v)
+        assert np.array_equal(pr, p)
