@@ -712,6 +712,86 @@ def main():
                                     "frac": pipe_b / (ms_all / 1e3) / 1e9 / hbm}
         out["stages_ms_per_step"] = {k: v[0] / args.steps for k, v in stages.items()}
 
+    # --- end to end through the host-buffer C ABI, on every rank (before the
+    # other workloads, as a process that converts a stream of volumes runs it)
+    e2e = None
+    host = torch.empty(shape, dtype=torch.int16, pin_memory=True)
+    host.copy_(img)
+    hparts = torch.empty(max(P, 1), dtype=torch.int16, pin_memory=True)
+    hp = C.c_void_p(host.data_ptr())
+    hpp = C.c_void_p(hparts.data_ptr())
+
+    def e2e_step():
+        h = C.c_void_p()
+        _lib.check(L.aprb_get_apr(conv._h, C.byref(par), hp, y, x, z, C.byref(h)))
+        _lib.check(L.aprb_sample_image(h, hp, hpp))
+        L.aprb_apr_free(h)
+
+    # the image goes to the GPU once per step: get_apr hands its device copy
+    # to the APR and sample_image of the same host buffer uses it
+    _lib.check(L.aprb_converter_keep_input(conv._h, 1))
+    e2e_step()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    te1 = max_over_ranks((time.perf_counter() - t0) / args.steps, world, "cuda")
+    _lib.check(L.aprb_converter_keep_input(conv._h, 0))
+
+    # Two volumes in flight: a second converter on a second host thread, each
+    # thread taking every other step (get_apr + sample_image of one volume).
+    # The library lets one host-buffer upload at a time cross PCIe, so the
+    # uploads run back to back while the other volume's construction,
+    # sampling and particle download proceed (PCIe carries both directions at
+    # once).  Every step still moves its own image up and its own particles
+    # down inside the timed region.
+    import threading
+    conv2 = A.APRConverter(args.image_type)
+    hparts2 = torch.empty(max(P, 1), dtype=torch.int16, pin_memory=True)
+    outs = [hpp, C.c_void_p(hparts2.data_ptr())]
+    convs = [conv, conv2]
+    for cv in convs:
+        _lib.check(L.aprb_converter_keep_input(cv._h, 1))
+
+    def worker(i, count, errs):
+        try:
+            torch.cuda.set_device(local)
+            for _ in range(count):
+                h = C.c_void_p()
+                _lib.check(L.aprb_get_apr(convs[i]._h, C.byref(par), hp, y, x, z, C.byref(h)))
+                _lib.check(L.aprb_sample_image(h, hp, outs[i]))
+                L.aprb_apr_free(h)
+        except Exception as e:  # noqa: BLE001 -- reported after the join
+            errs.append(e)
+
+    def run_pair(counts):
+        errs = []
+        ths = [threading.Thread(target=worker, args=(i, counts[i], errs)) for i in range(2)]
+        for t in ths:
+            t.start()
+        for t in ths:
+            t.join()
+        if errs:
+            raise errs[0]
+
+    run_pair([1, 1])  # each thread's first call sets up its streams and scratch
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    run_pair([(args.steps + 1) // 2, args.steps // 2])
+    torch.cuda.synchronize()
+    te = max_over_ranks((time.perf_counter() - t0) / args.steps, world, "cuda")
+    for cv in convs:
+        _lib.check(L.aprb_converter_keep_input(cv._h, 0))
+    del conv2
+    e2e = {"value": N * world / te / 1e9, "unit": "GVox/s", "h2d_bytes_per_step": 2 * N,
+           "d2h_bytes_per_step": 2 * P, "ms_per_step": te * 1e3,
+           "one_volume_in_flight": {"value": N * world / te1 / 1e9, "ms_per_step": te1 * 1e3},
+           "note": "aprb_get_apr + aprb_sample_image on pinned host buffers, converter keep_input on (the "
+                   "image crosses PCIe once per step, in z-chunks overlapped with smoothing; the particles "
+                   "come back once); two converters on two host threads take alternate steps, the uploads "
+                   "in turn, so one volume's construction and download overlap the next one's upload; "
+                   "one_volume_in_flight: the same calls on one thread"}
     # --- convolution over the particles of the last step (float intensities)
     conv_res = {}
     if not args.no_conv:
@@ -853,85 +933,6 @@ def main():
     if not args.no_rl and world == 1:
         rl_res = bench_rl(A, L, _lib, torch, stream, sptr, args)
 
-    # --- end to end through the host-buffer C ABI, on every rank
-    e2e = None
-    host = torch.empty(shape, dtype=torch.int16, pin_memory=True)
-    host.copy_(img)
-    hparts = torch.empty(max(P, 1), dtype=torch.int16, pin_memory=True)
-    hp = C.c_void_p(host.data_ptr())
-    hpp = C.c_void_p(hparts.data_ptr())
-
-    def e2e_step():
-        h = C.c_void_p()
-        _lib.check(L.aprb_get_apr(conv._h, C.byref(par), hp, y, x, z, C.byref(h)))
-        _lib.check(L.aprb_sample_image(h, hp, hpp))
-        L.aprb_apr_free(h)
-
-    # the image goes to the GPU once per step: get_apr hands its device copy
-    # to the APR and sample_image of the same host buffer uses it
-    _lib.check(L.aprb_converter_keep_input(conv._h, 1))
-    e2e_step()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        e2e_step()
-    torch.cuda.synchronize()
-    te1 = max_over_ranks((time.perf_counter() - t0) / args.steps, world, "cuda")
-    _lib.check(L.aprb_converter_keep_input(conv._h, 0))
-
-    # Two volumes in flight: a second converter on a second host thread, each
-    # thread taking every other step (get_apr + sample_image of one volume).
-    # The library lets one host-buffer upload at a time cross PCIe, so the
-    # uploads run back to back while the other volume's construction,
-    # sampling and particle download proceed (PCIe carries both directions at
-    # once).  Every step still moves its own image up and its own particles
-    # down inside the timed region.
-    import threading
-    conv2 = A.APRConverter(args.image_type)
-    hparts2 = torch.empty(max(P, 1), dtype=torch.int16, pin_memory=True)
-    outs = [hpp, C.c_void_p(hparts2.data_ptr())]
-    convs = [conv, conv2]
-    for cv in convs:
-        _lib.check(L.aprb_converter_keep_input(cv._h, 1))
-
-    def worker(i, count, errs):
-        try:
-            torch.cuda.set_device(local)
-            for _ in range(count):
-                h = C.c_void_p()
-                _lib.check(L.aprb_get_apr(convs[i]._h, C.byref(par), hp, y, x, z, C.byref(h)))
-                _lib.check(L.aprb_sample_image(h, hp, outs[i]))
-                L.aprb_apr_free(h)
-        except Exception as e:  # noqa: BLE001 -- reported after the join
-            errs.append(e)
-
-    def run_pair(counts):
-        errs = []
-        ths = [threading.Thread(target=worker, args=(i, counts[i], errs)) for i in range(2)]
-        for t in ths:
-            t.start()
-        for t in ths:
-            t.join()
-        if errs:
-            raise errs[0]
-
-    run_pair([1, 1])  # each thread's first call sets up its streams and scratch
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    run_pair([(args.steps + 1) // 2, args.steps // 2])
-    torch.cuda.synchronize()
-    te = max_over_ranks((time.perf_counter() - t0) / args.steps, world, "cuda")
-    for cv in convs:
-        _lib.check(L.aprb_converter_keep_input(cv._h, 0))
-    del conv2
-    e2e = {"value": N * world / te / 1e9, "unit": "GVox/s", "h2d_bytes_per_step": 2 * N,
-           "d2h_bytes_per_step": 2 * P, "ms_per_step": te * 1e3,
-           "one_volume_in_flight": {"value": N * world / te1 / 1e9, "ms_per_step": te1 * 1e3},
-           "note": "aprb_get_apr + aprb_sample_image on pinned host buffers, converter keep_input on (the "
-                   "image crosses PCIe once per step, in z-chunks overlapped with smoothing; the particles "
-                   "come back once); two converters on two host threads take alternate steps, the uploads "
-                   "in turn, so one volume's construction and download overlap the next one's upload; "
-                   "one_volume_in_flight: the same calls on one thread"}
     cpu, parity = None, None
     if not args.no_cpu and world == 1 and shape == SHAPE:
         hv = host.numpy().view(np.uint16)
