@@ -801,6 +801,9 @@ def main():
         _lib.check(L.aprb_apr_get_info(last, C.byref(info)))
         T = int(info.tree_total_number_particles)
         rng = np.random.default_rng(7)
+        # FP32 FMA peak of this GPU, measured (the measured-peaks file has none)
+        fp32_peak = C.c_double(0.0)
+        _lib.check(L.aprb_measure_fp32_fma_peak(sptr, C.byref(fp32_peak)))
         for ks in (3, 5):
             st = rng.uniform(-1, 1, ks ** 3).astype(np.float32)
             st = (st / st.sum()).astype(np.float32)
@@ -836,7 +839,12 @@ def main():
                 "value": P / (cms / 1e3) / 1e9, "unit": "Gpart/s", "ms": cms, "particles": P, "tree_nodes": T,
                 "roofline": {"bound": "hbm", "achieved": ab / (cms / 1e3) / 1e9, "peak": hbm, "unit": "GB/s",
                              "frac": ab / (cms / 1e3) / 1e9 / hbm, "algorithmic_bytes": ab},
-                "gflops": flops / (cms / 1e3) / 1e9, "stages_ms": cstages}
+                "gflops": flops / (cms / 1e3) / 1e9, "stages_ms": cstages,
+                "fp32": {"achieved_tflops": flops / (cms / 1e3) / 1e12, "peak_tflops": fp32_peak.value,
+                         "frac": flops / (cms / 1e3) / 1e12 / fp32_peak.value if fp32_peak.value else None,
+                         "peak_source": "measured here: independent FP32 FMA chains (aprb_measure_fp32_fma_peak)",
+                         "note": "2 ks^3 flops per particle; the bit-exact taps are a separate multiply "
+                                 "and add, so 0.5 is the ceiling of this fraction"}}
         # gradient magnitude on the particles (APRNumerics::gradient_magnitude_cfd
         # and _sobel): three directional 3x3x3 convolutions, squares and a root
         deltas = (C.c_float * 3)(1.0, 1.0, 1.0)

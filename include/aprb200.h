@@ -355,6 +355,12 @@ aprb_status aprb_synth_blobs_f32(float *img_dev, int y_num, int x_num, int z_num
  * results differ in their bits (NaNs compare equal) and the first such input. */
 aprb_status aprb_check_division_by_constant(float d, uint64_t *mismatches, uint32_t *first_bits);
 
+/* --- FP32 arithmetic peak (a measurement helper; no counterpart in the reference) ---
+ * Times a kernel of independent fused multiply-add chains on the current
+ * device and stream and returns its rate in TFLOP/s (two flops per FMA): the
+ * denominator for the arithmetic rate of the convolutions. */
+aprb_status aprb_measure_fp32_fma_peak(void *stream, double *tflops);
+
 /* number of kernel launches this thread issued through the library so far */
 uint64_t aprb_kernel_launch_count(void);
 

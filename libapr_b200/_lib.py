@@ -109,6 +109,7 @@ SIGNATURES = {
     "aprb_reconstruct_constant_f32_device": ([_vp, _vp, _vp, _vp], _i),
     "aprb_reconstruct_level_device": ([_vp, _vp, _vp], _i),
     "aprb_check_division_by_constant": ([C.c_float, C.POINTER(C.c_uint64), C.POINTER(C.c_uint32)], _i),
+    "aprb_measure_fp32_fma_peak": ([_vp, C.POINTER(C.c_double)], _i),
     "aprb_profile_enable": ([_i], _i),
     "aprb_profile_reset": ([], _i),
     "aprb_profile_read": ([C.POINTER(C.c_char_p), C.POINTER(C.c_double), C.POINTER(C.c_uint64), _i], _i),

@@ -285,6 +285,14 @@ const char *aprb_status_string(aprb_status s) {
 const char *aprb_last_error(void) { return g_last_error.c_str(); }
 uint64_t aprb_kernel_launch_count(void) { return g_launches; }
 
+aprb_status aprb_measure_fp32_fma_peak(void *stream, double *tflops) {
+    return guarded([&] {
+        require_device();
+        ARG_CHECK(tflops, "null argument");
+        *tflops = measure_fp32_fma_tflops((cudaStream_t)stream);
+    });
+}
+
 aprb_status aprb_check_division_by_constant(float d, uint64_t *mismatches, uint32_t *first_bits) {
     return guarded([&] {
         require_device();

@@ -66,6 +66,11 @@ bool launch_inv_bspline_tma(const float *in, float *O, int yd, int xd, int zd, i
 bool launch_iir_y_tma(const uint16_t *img, float *work, int yn, uint64_t nlines, const IIRDev &c, unsigned *d_timeout,
                       float2 *ckpt, uint64_t ckpt_elems, cudaStream_t s);
 
+// ---- peaks.cu
+// FP32 fused multiply-add throughput of the current device (TFLOP/s, two
+// flops per FMA), measured on stream s
+double measure_fp32_fma_tflops(cudaStream_t s);
+
 // ---- pipeline.cu
 void launch_check_div_const(float d, unsigned long long *out, cudaStream_t s);
 void launch_minmax_offset(const uint16_t *img, uint64_t n, unsigned *mm, float *offset, int apply, cudaStream_t s);
