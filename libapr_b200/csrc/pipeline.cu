@@ -1202,25 +1202,11 @@ __global__ void pad_reflect_kernel(const float *__restrict__ in, int yn, int xn,
     out[g] = in[idx3(ry, rx, rz, yn, xn)];
 }
 
-// One output of calc_sat_mean_y (:311-362) given the line's cumulative sums.
-template <int OFF>
-__device__ __forceinline__ float sat_y_value(int i, int n, float d, float cm /*C[i-off-1]*/, float cp /*C[i+off]*/,
-                                             float clast /*C[n-1]*/) {
-    float v = (i <= OFF) ? 0.0f : -cm / d;
-    if (i < n - OFF) v = v + cp / d;
-    if (i >= n - OFF) {
-        float cnt = (float)(i - (n - OFF) + 1);
-        v = v * d;
-        v = v + clast;
-        v = (float)((double)v * (1.0 / (double)(d - cnt)));
-    }
-    if (i >= 1 && i <= OFF) v = (float)((double)v * ((double)d / ((double)i + (double)OFF + 1.0)));
-    if (i == 0) v = (float)((double)v * ((double)d / ((double)OFF + 1.0)));
-    return v;
-}
-
-// sat_y_value from the quotients qm = C[i-off-1] / d and qp = C[i+off] / d
-// (each the correctly rounded quotient; -cm / d == -(cm / d) exactly).
+// Output i of the y box mean (calc_sat_mean_y, LocalIntensityScale.hpp:
+// 311-362) from the quotients qm = C[i-off-1] / d and qp = C[i+off] / d of the
+// cumulative sums (each the correctly rounded quotient, and -cm / d ==
+// -(cm / d) exactly) and the last sum C[n-1]: the edge windows rescaled as
+// the reference does.
 template <int OFF>
 __device__ __forceinline__ float sat_y_value_q(int i, int n, float d, float qm, float qp, float clast) {
     float v = (i <= OFF) ? 0.0f : -qm;
@@ -1236,10 +1222,6 @@ __device__ __forceinline__ float sat_y_value_q(int i, int n, float d, float qm, 
     return v;
 }
 
-// y box mean: one thread per y-line, cumulative sum carried in a register
-// shift window of 2*OFF+2 entries; tiles through shared memory as in the IIR.
-// absdiff_ref != nullptr makes the input |in - absdiff_ref| (calc_abs_diff,
-// :188-196) on the fly.
 // Reads of the padded image folded into the first y pass: padded (y, x, z)
 // maps to the unpadded image by reflection about the edge sample (paddPixels,
 // PixelData.hpp:1071-1178).  on_in maps the input, on_ref the |in - ref| operand.
@@ -1250,85 +1232,12 @@ struct PadMap {
 
 __device__ __forceinline__ int reflect101(int i, int n) { return i < 0 ? -i : (i > n - 1 ? 2 * (n - 1) - i : i); }
 
-template <int OFF>
-__global__ void __launch_bounds__(kYWarps * 32) sat_y_kernel(const float *__restrict__ in,
-                                                              const float *__restrict__ absdiff_ref,
-                                                              float *__restrict__ out, int n, uint64_t nlines,
-                                                              PadMap pm) {
-    constexpr int W = 2 * OFF + 2;
-    __shared__ float tin[kYWarps][kTile][kTile + 1];
-    __shared__ float tout[kYWarps][kTile][kTile + 1];
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint64_t line0 = ((uint64_t)blockIdx.x * kYWarps + w) * kTile;
-    if (line0 >= nlines) return;
-    const bool valid = line0 + lane < nlines;
-    const float d = (float)(2 * OFF + 1);
-    float c[W];
-#pragma unroll
-    for (int q = 0; q < W; ++q) c[q] = 0.0f;
-    float C = 0.0f;
-    // unpadded row start of line line0 + lane when the reads are reflected
-    uint64_t mbase = 0;
-    if ((pm.on_in | pm.on_ref) && valid) {
-        const uint64_t ln = line0 + lane;
-        const int xp = (int)(ln % (uint64_t)pm.px), zp = (int)(ln / (uint64_t)pm.px);
-        mbase = idx3(0, reflect101(xp - pm.sx, pm.xd), reflect101(zp - pm.sz, pm.zd), pm.yd, pm.xd);
-    }
-    for (int y0 = 0; y0 < n; y0 += kTile) {
-        const int my = (pm.on_in | pm.on_ref) ? reflect101(y0 + lane - pm.sy, pm.yd) : 0;
-        // partial unrolling: 8 loads in flight per thread at a register count
-        // that keeps 48 warps per SM resident
-#pragma unroll 8
-        for (int j = 0; j < kTile; ++j) {
-            const uint64_t ln = line0 + j;
-            const uint64_t bj = __shfl_sync(0xffffffffu, mbase, j);
-            if (ln < nlines && y0 + lane < n) {
-                const uint64_t a = ln * (uint64_t)n + y0 + lane;
-                const uint64_t am = bj + (uint64_t)my;
-                float v = in[pm.on_in ? am : a];
-                if (absdiff_ref) v = fabsf(v - absdiff_ref[pm.on_ref ? am : a]);
-                tin[w][j][lane] = v;
-            }
-        }
-        __syncwarp();
-        if (valid) {
-            const int kend = min(kTile, n - y0);
-            for (int k = 0; k < kend; ++k) {
-                const int j = y0 + k;
-                C = C + tin[w][lane][k];
-#pragma unroll
-                for (int q = 0; q < W - 1; ++q) c[q] = c[q + 1];
-                c[W - 1] = C;
-                const int i = j - OFF;
-                if (i >= 0 && i < n - OFF) tout[w][lane][k] = sat_y_value<OFF>(i, n, d, c[0], C, 0.0f);
-            }
-        }
-        __syncwarp();
-#pragma unroll 8
-        for (int j = 0; j < kTile; ++j) {
-            uint64_t ln = line0 + j;
-            int i = y0 + lane - OFF;
-            if (ln < nlines && y0 + lane < n && i >= 0 && i < n - OFF) out[ln * (uint64_t)n + i] = tout[w][j][lane];
-        }
-        __syncwarp();
-    }
-    if (valid) {
-        // right-hand tail: outputs n-OFF .. n-1 need C[n-1] (= c[W-1])
-        for (int i = n - OFF; i < n; ++i) {
-            if (i < 0) continue;
-            const int back = (n - 1) - (i - OFF - 1);  // distance from C[n-1] to C[i-off-1]
-            float cm = 0.0f;
-#pragma unroll
-            for (int q = 0; q < W; ++q)
-                if (q == W - 1 - back) cm = c[q];
-            out[(line0 + lane) * (uint64_t)n + i] = sat_y_value<OFF>(i, n, d, cm, 0.0f, C);
-        }
-    }
-}
-
-// The same y box mean with the samples staged by cp.async one tile ahead of
-// the recurrence: a warp owns 32 lines and walks them in tiles of kSY
-// samples, so no registers hold the prefetch and more warps stay resident.
+// y box mean: one thread per y-line, the cumulative sum carried in a register
+// and the quotients of the last 2*OFF+2 sums in a register shift window; REF
+// makes the input |in - ref| (calc_abs_diff, :188-196) on the fly.  The
+// samples are staged by cp.async one tile ahead of the recurrence: a warp
+// owns 32 lines and walks them in tiles of kSY samples, so no registers hold
+// the prefetch and more warps stay resident.
 // 32-sample tiles (a warp's copies and stores are 128-byte runs of a line),
 // one warp per block.
 // In tiles that touch neither end of the line the recurrence runs fully
