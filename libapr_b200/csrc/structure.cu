@@ -48,6 +48,41 @@ __global__ void pyramid_fill_kernel(const uint8_t *__restrict__ lev_in, LevelDim
     status[g] = seed ? kSeed : kEmpty;
 }
 
+// The same for four output cells per thread (row grid as the row kernels
+// below): each of the four input rows of a 2x2 (x, z) block arrives as one
+// 8-byte load (input y extent a multiple of 8, so no y clamp).
+__global__ void pyramid_fill4_kernel(const uint8_t *__restrict__ lev_in, LevelDims di, uint8_t *__restrict__ lev_out,
+                                     uint8_t *__restrict__ status, LevelDims d, int level, int is_min) {
+    const int gidx = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y, z = blockIdx.z;
+    if (gidx >= d.yn / 4) return;
+    const int y0 = 4 * gidx;
+    const int x1 = min(2 * x + 1, di.xn - 1), z1 = min(2 * z + 1, di.zn - 1);
+    const int xs[2] = {2 * x, x1}, zs[2] = {2 * z, z1};
+    uint32_t mlo = 0, mhi = 0;  // byte-wise maxima of the four rows
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const uint2 v = *reinterpret_cast<const uint2 *>(lev_in + idx3(2 * y0, xs[b], zs[a], di.yn, di.xn));
+            mlo = __vmaxu4(mlo, v.x);
+            mhi = __vmaxu4(mhi, v.y);
+        }
+    // output k = max of input bytes 2k and 2k + 1
+    uint32_t out = 0, st = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint32_t w = k < 2 ? mlo : mhi;
+        const int sh = 16 * (k & 1);
+        const uint32_t m = max((w >> sh) & 0xffu, (w >> (sh + 8)) & 0xffu);
+        out |= m << (8 * k);
+        const bool seed = is_min ? (m <= (uint32_t)level) : (m == (uint32_t)level);
+        st |= (uint32_t)(seed ? kSeed : kEmpty) << (8 * k);
+    }
+    const uint64_t o = ((uint64_t)z * d.xn + x) * d.yn + y0;
+    *reinterpret_cast<uint32_t *>(lev_out + o) = out;
+    if (status) *reinterpret_cast<uint32_t *>(status + o) = st;
+}
+
 // PullingScheme::fill_patch (PullingScheme.hpp:175-247) for a z-tile: the
 // tile's level image at one pct level (tile-local planes zlo..zhi-1) marks
 // SEED cells of the global level at plane z + offz.  mode 0: level >= k (top),
@@ -286,14 +321,23 @@ __global__ void fill_parent_kernel(const uint8_t *__restrict__ child, LevelDims 
 // the same per-cell rules as the scalar kernels.
 __device__ __forceinline__ uint8_t byte_of(uint64_t v, int b) { return (uint8_t)(v >> (8 * b)); }
 
+// Grid of the row kernels below (set_filler8, fill_parent4): (groups of a row
+// / blockDim.x, x, z), so a thread finds its row without integer division.
+__device__ __forceinline__ bool row_group(int groups, int xn, int &gidx, int &x, int &z, uint64_t &row) {
+    gidx = blockIdx.x * blockDim.x + threadIdx.x;
+    x = blockIdx.y;
+    z = blockIdx.z;
+    row = (uint64_t)z * xn + x;
+    return gidx < groups;
+}
+
 __global__ void set_filler8_kernel(const uint8_t *__restrict__ parent, LevelDims dp, uint8_t *__restrict__ child,
                                    LevelDims dc) {
     const int groups = dc.yn / 8;
-    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (uint64_t)dc.xn * dc.zn * groups) return;
-    const uint64_t row = t / (uint64_t)groups;
-    const int y0 = (int)(t % (uint64_t)groups) * 8;
-    const int x = (int)(row % (uint64_t)dc.xn), z = (int)(row / (uint64_t)dc.xn);
+    int gidx, x, z;
+    uint64_t row;
+    if (!row_group(groups, dc.xn, gidx, x, z, row)) return;
+    const int y0 = gidx * 8;
     uint2 *cp = reinterpret_cast<uint2 *>(child + row * (uint64_t)dc.yn + y0);
     const uint2 cv = *cp;
     uint64_t c = ((uint64_t)cv.y << 32) | cv.x;
@@ -338,11 +382,10 @@ __global__ void eqopt8_kernel(const uint8_t *__restrict__ parent, LevelDims dp, 
 __global__ void fill_parent4_kernel(const uint8_t *__restrict__ child, LevelDims dc, uint8_t *__restrict__ parent,
                                     LevelDims dp) {
     const int groups = dp.yn / 4;
-    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (uint64_t)dp.xn * dp.zn * groups) return;
-    const uint64_t row = t / (uint64_t)groups;
-    const int y0 = (int)(t % (uint64_t)groups) * 4;
-    const int x = (int)(row % (uint64_t)dp.xn), z = (int)(row / (uint64_t)dp.xn);
+    int gidx, x, z;
+    uint64_t row;
+    if (!row_group(groups, dp.xn, gidx, x, z, row)) return;
+    const int y0 = gidx * 4;
     uint32_t *pp = reinterpret_cast<uint32_t *>(parent + row * (uint64_t)dp.yn + y0);
     const uint32_t pv = *pp;
     uint32_t hit = 0;  // bit b: parent y0 + b has a SEED / PROPOGATE / ASCENDANT child
@@ -762,6 +805,12 @@ LevelDims dims(const Geom &g, int l) { return LevelDims{g.y_num[l], g.x_num[l], 
 uint64_t ncell(const Geom &g, int l) { return (uint64_t)g.y_num[l] * g.x_num[l] * g.z_num[l]; }
 uint64_t nrow(const Geom &g, int l) { return (uint64_t)g.x_num[l] * g.z_num[l]; }
 unsigned row_blocks(uint64_t rows) { return blocks_for(rows * 32, 256); }
+// (groups of a row / kRowThreads, x, z) of level l: the grid of the row kernels
+constexpr int kRowThreads = 128;
+dim3 row_grid(int groups, const Geom &g, int l) {
+    return dim3((unsigned)std::max((groups + kRowThreads - 1) / kRowThreads, 1), (unsigned)g.x_num[l],
+                (unsigned)g.z_num[l]);
+}
 
 }  // namespace
 
@@ -802,8 +851,15 @@ void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s, bool fill
     if (top < lmin) return;
     APRB_PROF("pulling_scheme", s);
     for (int l = top - 1; l >= lmin && fill_pyramid; --l) {
-        pyramid_fill_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(pm.level[l + 1], dims(g, l + 1), pm.level[l],
-                                                                        pm.status[l], dims(g, l), l, l == lmin);
+        const bool v4 = g.y_num[l + 1] % 8 == 0 && g.y_num[l] % 4 == 0 && ((uintptr_t)pm.level[l + 1] & 7) == 0 &&
+                        ((uintptr_t)pm.level[l] & 3) == 0 && ((uintptr_t)pm.status[l] & 3) == 0;
+        if (v4)
+            pyramid_fill4_kernel<<<row_grid(g.y_num[l] / 4, g, l), kRowThreads, 0, s>>>(
+                pm.level[l + 1], dims(g, l + 1), pm.level[l], pm.status[l], dims(g, l), l, l == lmin);
+        else
+            pyramid_fill_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(pm.level[l + 1], dims(g, l + 1),
+                                                                            pm.level[l], pm.status[l], dims(g, l), l,
+                                                                            l == lmin);
         count_launch();
     }
     APRB_CHECK_LAUNCH();
@@ -820,9 +876,8 @@ void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s, bool fill
             else
                 dilate_kernel<0><<<dgrid, 256, 0, s>>>(pm.status[l], dims(g, l));
             if (g.y_num[l + 1] % 8 == 0)
-                set_filler8_kernel<<<blocks_for(ncell(g, l + 1) / 8, 256), 256, 0, s>>>(pm.status[l], dims(g, l),
-                                                                                       pm.status[l + 1],
-                                                                                       dims(g, l + 1));
+                set_filler8_kernel<<<row_grid(g.y_num[l + 1] / 8, g, l + 1), kRowThreads, 0, s>>>(
+                    pm.status[l], dims(g, l), pm.status[l + 1], dims(g, l + 1));
             else
                 set_filler_kernel<<<blocks_for(ncell(g, l + 1), 256), 256, 0, s>>>(pm.status[l], dims(g, l),
                                                                                   pm.status[l + 1], dims(g, l + 1));
@@ -837,7 +892,7 @@ void launch_pulling_scheme(const Geom &g, Pyramid &pm, cudaStream_t s, bool fill
         count_launch();
         if (l - 1 >= lmin) {
             if (g.y_num[l] % 8 == 0)
-                fill_parent4_kernel<<<blocks_for(ncell(g, l - 1) / 4, 256), 256, 0, s>>>(
+                fill_parent4_kernel<<<row_grid(g.y_num[l - 1] / 4, g, l - 1), kRowThreads, 0, s>>>(
                     pm.status[l], dims(g, l), pm.status[l - 1], dims(g, l - 1));
             else
                 fill_parent_kernel<<<blocks_for(ncell(g, l - 1), 256), 256, 0, s>>>(pm.status[l], dims(g, l),
