@@ -703,12 +703,11 @@ __global__ void pyr_mean_u16_kernel(const uint16_t *__restrict__ in, LevelDims d
 // reads 4 x uint2 (4 samples each) and writes two outputs as one uint32.
 __global__ void pyr_mean_u16x2_kernel(const uint16_t *__restrict__ in, LevelDims di, uint16_t *__restrict__ out,
                                       LevelDims d) {
-    const int groups = d.yn / 2;
-    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (uint64_t)d.xn * d.zn * groups) return;
-    const uint64_t row = t / (uint64_t)groups;
-    const int y = (int)(t % (uint64_t)groups) * 2;
-    const int x = (int)(row % (uint64_t)d.xn), z = (int)(row / (uint64_t)d.xn);
+    // grid (pairs of a row / blockDim.x, x, z): no integer division
+    const int gidx = blockIdx.x * blockDim.x + threadIdx.x, x = blockIdx.y, z = blockIdx.z;
+    if (gidx >= d.yn / 2) return;
+    const uint64_t row = (uint64_t)z * d.xn + x;
+    const int y = 2 * gidx;
     const int x1 = min(2 * x + 1, di.xn - 1), z1 = min(2 * z + 1, di.zn - 1);
     const int xs[2] = {2 * x, x1}, zs[2] = {2 * z, z1};
     unsigned s0 = 0, s1 = 0;
@@ -807,10 +806,10 @@ uint64_t nrow(const Geom &g, int l) { return (uint64_t)g.x_num[l] * g.z_num[l]; 
 unsigned row_blocks(uint64_t rows) { return blocks_for(rows * 32, 256); }
 // (groups of a row / kRowThreads, x, z) of level l: the grid of the row kernels
 constexpr int kRowThreads = 128;
-dim3 row_grid(int groups, const Geom &g, int l) {
-    return dim3((unsigned)std::max((groups + kRowThreads - 1) / kRowThreads, 1), (unsigned)g.x_num[l],
-                (unsigned)g.z_num[l]);
+dim3 row_grid(int groups, int xn, int zn) {
+    return dim3((unsigned)std::max((groups + kRowThreads - 1) / kRowThreads, 1), (unsigned)xn, (unsigned)zn);
 }
+dim3 row_grid(int groups, const Geom &g, int l) { return row_grid(groups, g.x_num[l], g.z_num[l]); }
 
 }  // namespace
 
@@ -976,7 +975,7 @@ void launch_sample(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec,
     for (int l = L - 1; l >= lmin; --l) {
         uint16_t *o = base + off[l];
         if (g.y_num[l + 1] % 4 == 0 && (l + 1 < L || ((uintptr_t)img & 7) == 0))
-            pyr_mean_u16x2_kernel<<<blocks_for(ncell(g, l) / 2, 256), 256, 0, s>>>(lev[l + 1], dims(g, l + 1), o,
+            pyr_mean_u16x2_kernel<<<row_grid(g.y_num[l] / 2, g, l), kRowThreads, 0, s>>>(lev[l + 1], dims(g, l + 1), o,
                                                                                 dims(g, l));
         else
             pyr_mean_u16_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(lev[l + 1], dims(g, l + 1), o,
@@ -1015,7 +1014,7 @@ void launch_sample_slab(const Geom &g, const uint64_t *xz_end, const uint16_t *y
         uint16_t *o = pyr_top + (uint64_t)(z0 / 2) * d.yn * d.xn;
         const uint64_t nout = (uint64_t)d.yn * d.xn * d.zn;
         if (di.yn % 4 == 0 && ((uintptr_t)slab & 7) == 0)
-            pyr_mean_u16x2_kernel<<<blocks_for(nout / 2, 256), 256, 0, s>>>(slab, di, o, d);
+            pyr_mean_u16x2_kernel<<<row_grid(d.yn / 2, d.xn, d.zn), kRowThreads, 0, s>>>(slab, di, o, d);
         else
             pyr_mean_u16_kernel<<<blocks_for(nout, 256), 256, 0, s>>>(slab, di, o, d);
         count_launch();
@@ -1034,7 +1033,8 @@ void launch_sample_coarse(const Geom &g, const uint64_t *xz_end, const uint16_t 
         uint16_t *o = base + off[l];
         const uint16_t *in = base + off[l + 1];
         if (g.y_num[l + 1] % 4 == 0)
-            pyr_mean_u16x2_kernel<<<blocks_for(ncell(g, l) / 2, 256), 256, 0, s>>>(in, dims(g, l + 1), o, dims(g, l));
+            pyr_mean_u16x2_kernel<<<row_grid(g.y_num[l] / 2, g, l), kRowThreads, 0, s>>>(in, dims(g, l + 1), o,
+                                                                                       dims(g, l));
         else
             pyr_mean_u16_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(in, dims(g, l + 1), o, dims(g, l));
         count_launch();
