@@ -174,10 +174,59 @@ __global__ void __launch_bounds__(256) dilate_kernel(uint8_t *__restrict__ st, L
     }
 }
 
+// Byte-parallel helpers on 32-bit words of four cells (byte j = cell j).
+// bytes_eq: 0x80 in each byte equal to the corresponding byte of c4, 0 in the
+// others; exact, since (t & 0x7F) + 0x7F never carries out of its byte.
+__device__ __forceinline__ uint32_t bytes_eq(uint32_t w, uint32_t c4) {
+    const uint32_t t = w ^ c4;
+    return ~((((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) | 0x7F7F7F7Fu);
+}
+// The high bits of the four bytes of h (h holds no other bits) as bits 0..3:
+// the product's partial sums land on distinct bits, so nothing carries.
+__device__ __forceinline__ unsigned high_bits4(uint32_t h) { return (h * 0x00204081u) >> 28; }
+// Bits 0..3 of n (n < 16) as 0x80 / 0x00 in bytes 0..3.
+__device__ __forceinline__ uint32_t nibble_high_bytes(unsigned n) { return ((n * 0x00204081u) & 0x01010101u) << 7; }
+// 0x80 in each byte b of w with 1 <= b <= m (0 <= m < 128), 0 in the others:
+// (b | 0x80) - (m + 1) never borrows across bytes, and its high bit is clear
+// exactly when b < m + 1 (for b < 128).
+__device__ __forceinline__ uint32_t bytes_in_1_to(uint32_t w, int m) {
+    const uint32_t lt = ~(((w | 0x80808080u) - (uint32_t)(m + 1) * 0x01010101u) | w) & 0x80808080u;
+    return lt & ~bytes_eq(w, 0u);
+}
+
+template <int MODE>
+__device__ __forceinline__ uint32_t dil_source4(uint32_t w) {
+    return MODE == 0 ? bytes_eq(w, kAscendant * 0x01010101u)
+                     : bytes_eq(w, kSeed * 0x01010101u) | bytes_eq(w, kPropagate * 0x01010101u);
+}
+
+template <int MODE>
+__device__ __forceinline__ unsigned dil_bits16(const uint4 v) {
+    return high_bits4(dil_source4<MODE>(v.x)) | high_bits4(dil_source4<MODE>(v.y)) << 4 |
+           high_bits4(dil_source4<MODE>(v.z)) << 8 | high_bits4(dil_source4<MODE>(v.w)) << 12;
+}
+
+// The targets among the four cells of w whose bits in n (0..3) are set:
+// MODE 0 turns EMPTY into ASCENDANTNEIGHBOUR and SEED into PROPOGATE, MODE 1
+// EMPTY into BOUNDARY.  Each selected byte gains the difference of the two
+// status values, which never carries into the next byte.
+static_assert(kEmpty == 0 && kPropagate > kSeed, "EMPTY and SEED targets are formed by adding to the byte");
+template <int MODE>
+__device__ __forceinline__ uint32_t dil_target4(uint32_t w, unsigned n) {
+    const uint32_t sel = nibble_high_bytes(n);
+    const uint32_t e = bytes_eq(w, 0u) & sel;
+    if (MODE == 0) {
+        const uint32_t sd = bytes_eq(w, kSeed * 0x01010101u) & sel;
+        return w + (e >> 7) * kAscendantNeighbour + (sd >> 7) * (uint32_t)(kPropagate - kSeed);
+    }
+    return w + (e >> 7) * kBoundary;
+}
+
 // The same dilation for rows of a multiple of 16 cells and 16-byte aligned
 // rows: a lane moves 16 consecutive cells as one 16-byte word, a warp reads
 // 512 y of a row in one load, and the shared mask holds per row and lane the
-// 16 bits of the lane's cells.
+// 16 bits of the lane's cells.  Sources and targets are found four cells at
+// a time with byte-parallel arithmetic on 32-bit words, not cell by cell.
 constexpr int kD16Y = 512;
 template <int MODE>
 __global__ void __launch_bounds__(256) dilate16_kernel(uint8_t *__restrict__ st, LevelDims d) {
@@ -191,11 +240,7 @@ __global__ void __launch_bounds__(256) dilate16_kernel(uint8_t *__restrict__ st,
         const uint8_t *R = st + ((uint64_t)(row_in ? z : 0) * d.xn + (row_in ? x : 0)) * (uint64_t)d.yn;
         const bool in = row_in && y < d.yn;
         const uint4 v = in ? *reinterpret_cast<const uint4 *>(R + y) : make_uint4(0u, 0u, 0u, 0u);
-        const uint32_t vw[4] = {v.x, v.y, v.z, v.w};
-        unsigned p = 0;
-#pragma unroll
-        for (int e = 0; e < 16; ++e)
-            if (in && dil_source<MODE>((uint8_t)(vw[e >> 2] >> (8 * (e & 3))))) p |= 1u << e;
+        const unsigned p = dil_bits16<MODE>(v);
         unsigned pl = (__shfl_up_sync(0xffffffffu, p, 1) >> 15) & 1u;
         unsigned pr = __shfl_down_sync(0xffffffffu, p, 1) & 1u;
         if (lane == 0) pl = row_in && y >= 1 && y - 1 < d.yn && dil_source<MODE>(R[y - 1]);
@@ -215,27 +260,9 @@ __global__ void __launch_bounds__(256) dilate16_kernel(uint8_t *__restrict__ st,
         if (!m) continue;
         uint4 *c = reinterpret_cast<uint4 *>(st + ((uint64_t)z * d.xn + x) * (uint64_t)d.yn + y);
         const uint4 v = *c;
-        uint32_t nv[4] = {v.x, v.y, v.z, v.w};
-        bool changed = false;
-#pragma unroll
-        for (int e = 0; e < 16; ++e) {
-            if (!((m >> e) & 1u)) continue;
-            const uint32_t word = nv[e >> 2];
-            const int sh = 8 * (e & 3);
-            const uint8_t s = (uint8_t)(word >> sh);
-            uint8_t t = s;
-            if (MODE == 0) {
-                if (s == kEmpty) t = kAscendantNeighbour;
-                else if (s == kSeed) t = kPropagate;
-            } else {
-                if (s == kEmpty) t = kBoundary;
-            }
-            if (t != s) {
-                nv[e >> 2] = (word & ~(0xFFu << sh)) | ((uint32_t)t << sh);
-                changed = true;
-            }
-        }
-        if (changed) *c = make_uint4(nv[0], nv[1], nv[2], nv[3]);
+        const uint4 nv = make_uint4(dil_target4<MODE>(v.x, m & 15u), dil_target4<MODE>(v.y, (m >> 4) & 15u),
+                                    dil_target4<MODE>(v.z, (m >> 8) & 15u), dil_target4<MODE>(v.w, m >> 12));
+        if (nv.x != v.x || nv.y != v.y || nv.z != v.z || nv.w != v.w) *c = nv;
     }
 }
 
@@ -319,7 +346,6 @@ __global__ void fill_parent_kernel(const uint8_t *__restrict__ child, LevelDims 
 // levels whose rows are multiples of 8 cells (child) / 4 cells (parent): a
 // thread moves 8 child cells (uint2) or 4 parent cells (uint32) at once, with
 // the same per-cell rules as the scalar kernels.
-__device__ __forceinline__ uint8_t byte_of(uint64_t v, int b) { return (uint8_t)(v >> (8 * b)); }
 
 // Grid of the row kernels below (set_filler8, fill_parent4): (groups of a row
 // / blockDim.x, x, z), so a thread finds its row without integer division.
@@ -340,43 +366,32 @@ __global__ void set_filler8_kernel(const uint8_t *__restrict__ parent, LevelDims
     const int y0 = gidx * 8;
     uint2 *cp = reinterpret_cast<uint2 *>(child + row * (uint64_t)dc.yn + y0);
     const uint2 cv = *cp;
-    uint64_t c = ((uint64_t)cv.y << 32) | cv.x;
     const uint32_t pv = *reinterpret_cast<const uint32_t *>(parent + idx3(y0 / 2, x / 2, z / 2, dp.yn, dp.xn));
-    uint64_t nc = c;
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-        const uint8_t ps = (uint8_t)(pv >> (8 * (b / 2)));
-        if (byte_of(c, b) == kEmpty && (ps == kAscendantNeighbour || ps == kPropagate))
-            nc = (nc & ~(0xffull << (8 * b))) | ((uint64_t)kFiller << (8 * b));
-    }
-    if (nc != c) *cp = make_uint2((uint32_t)nc, (uint32_t)(nc >> 32));
+    // parents ASCENDANTNEIGHBOUR or PROPOGATE, each byte spread over its two child cells
+    const uint32_t pt = bytes_eq(pv, kAscendantNeighbour * 0x01010101u) | bytes_eq(pv, kPropagate * 0x01010101u);
+    const uint32_t lo = bytes_eq(cv.x, 0u) & __byte_perm(pt, 0u, 0x1100u);
+    const uint32_t hi = bytes_eq(cv.y, 0u) & __byte_perm(pt, 0u, 0x3322u);
+    if (lo | hi) *cp = make_uint2(cv.x + (lo >> 7) * kFiller, cv.y + (hi >> 7) * kFiller);  // EMPTY -> FILLER
 }
 
+// Grid (groups x rows of a plane / 256, z): one 32-bit division per thread
+// finds the row; the many threads whose parents hold no seed end at once, so
+// blocks of 256 keep the block count low.
 __global__ void eqopt8_kernel(const uint8_t *__restrict__ parent, LevelDims dp, uint8_t *__restrict__ st,
                               LevelDims d, int min_type) {
-    const int groups = d.yn / 8;
-    const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (uint64_t)d.xn * d.zn * groups) return;
-    const uint64_t row = t / (uint64_t)groups;
-    const int y0 = (int)(t % (uint64_t)groups) * 8;
-    const int x = (int)(row % (uint64_t)d.xn), z = (int)(row / (uint64_t)d.xn);
+    const unsigned groups = (unsigned)d.yn / 8u;
+    const unsigned t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= groups * (unsigned)d.xn) return;
+    const int x = (int)(t / groups), z = blockIdx.y;
+    const int y0 = (int)(t - (unsigned)x * groups) * 8;
     const uint32_t pv = *reinterpret_cast<const uint32_t *>(parent + idx3(y0 / 2, x / 2, z / 2, dp.yn, dp.xn));
-    bool any = false;
-#pragma unroll
-    for (int b = 0; b < 4; ++b) {
-        const uint8_t ps = (uint8_t)(pv >> (8 * b));
-        any = any || (ps > 0 && ps <= min_type);
-    }
-    if (!any) return;
-    uint2 *cp = reinterpret_cast<uint2 *>(st + row * (uint64_t)d.yn + y0);
+    const uint32_t seeds = bytes_in_1_to(pv, min_type);
+    if (!seeds) return;
+    uint2 *cp = reinterpret_cast<uint2 *>(st + idx3(y0, x, z, d.yn, d.xn));
     const uint2 cv = *cp;
-    uint64_t c = ((uint64_t)cv.y << 32) | cv.x;
-#pragma unroll
-    for (int b = 0; b < 8; ++b) {
-        const uint8_t ps = (uint8_t)(pv >> (8 * (b / 2)));
-        if (ps > 0 && ps <= min_type) c = (c & ~(0xffull << (8 * b))) | ((uint64_t)kUpsamplingSeed << (8 * b));
-    }
-    *cp = make_uint2((uint32_t)c, (uint32_t)(c >> 32));
+    const uint32_t lo = (__byte_perm(seeds, 0u, 0x1100u) >> 7) * 0xFFu, hi = (__byte_perm(seeds, 0u, 0x3322u) >> 7) * 0xFFu;
+    const uint32_t up = kUpsamplingSeed * 0x01010101u;
+    *cp = make_uint2((cv.x & ~lo) | (up & lo), (cv.y & ~hi) | (up & hi));
 }
 
 __global__ void fill_parent4_kernel(const uint8_t *__restrict__ child, LevelDims dc, uint8_t *__restrict__ parent,
@@ -388,22 +403,27 @@ __global__ void fill_parent4_kernel(const uint8_t *__restrict__ child, LevelDims
     const int y0 = gidx * 4;
     uint32_t *pp = reinterpret_cast<uint32_t *>(parent + row * (uint64_t)dp.yn + y0);
     const uint32_t pv = *pp;
-    uint32_t hit = 0;  // bit b: parent y0 + b has a SEED / PROPOGATE / ASCENDANT child
-    for (int cz = 2 * z; cz < min(2 * z + 2, dc.zn); ++cz)
-        for (int cx = 2 * x; cx < min(2 * x + 2, dc.xn); ++cx) {
-            const uint2 cv = *reinterpret_cast<const uint2 *>(child + idx3(2 * y0, cx, cz, dc.yn, dc.xn));
-            const uint64_t c = ((uint64_t)cv.y << 32) | cv.x;
+    uint2 cv[4];  // the (up to) four child rows under the parent row, all loaded before any is used
 #pragma unroll
-            for (int b = 0; b < 8; ++b) {
-                const uint8_t q = byte_of(c, b);
-                if (q == kSeed || q == kPropagate || q == kAscendant) hit |= 1u << (b / 2);
-            }
-        }
-    uint32_t nv = pv;
+    for (int k = 0; k < 4; ++k) {
+        const int cz = 2 * z + (k >> 1), cx = 2 * x + (k & 1);
+        cv[k] = cz < dc.zn && cx < dc.xn ? *reinterpret_cast<const uint2 *>(child + idx3(2 * y0, cx, cz, dc.yn, dc.xn))
+                                         : make_uint2(0u, 0u);
+    }
+    uint32_t lo = 0, hi = 0;  // 0x80 in the child bytes 0..3 / 4..7 that are SEED, PROPOGATE or ASCENDANT in a row
 #pragma unroll
-    for (int b = 0; b < 4; ++b)
-        if ((hit >> b & 1) && (uint8_t)(pv >> (8 * b)) != kSeed)
-            nv = (nv & ~(0xffu << (8 * b))) | ((uint32_t)kAscendant << (8 * b));
+    for (int k = 0; k < 4; ++k) {
+        lo |= bytes_eq(cv[k].x, kSeed * 0x01010101u) | bytes_eq(cv[k].x, kPropagate * 0x01010101u) |
+              bytes_eq(cv[k].x, kAscendant * 0x01010101u);
+        hi |= bytes_eq(cv[k].y, kSeed * 0x01010101u) | bytes_eq(cv[k].y, kPropagate * 0x01010101u) |
+              bytes_eq(cv[k].y, kAscendant * 0x01010101u);
+    }
+    lo |= lo >> 8;  // bytes 0 and 2: either child of parents 0 and 1
+    hi |= hi >> 8;
+    const unsigned hit = ((lo >> 7) & 1u) | ((lo >> 22) & 2u) | ((hi >> 5) & 4u) | ((hi >> 20) & 8u);
+    // parents with such a child, unless SEED, become ASCENDANT
+    const uint32_t m = ((nibble_high_bytes(hit) & ~bytes_eq(pv, kSeed * 0x01010101u)) >> 7) * 0xFFu;
+    const uint32_t nv = (pv & ~m) | (kAscendant * 0x01010101u & m);
     if (nv != pv) *pp = nv;
 }
 
@@ -928,9 +948,10 @@ uint64_t launch_linear_counts(const Geom &g, Pyramid &pm, uint64_t *xz_end, uint
     const int L = g.l_max, lmin = g.l_min;
     APRB_CUDA(cudaMemsetAsync(xz_end, 0, n_xz * sizeof(uint64_t), s));
     for (int l = lmin + 1; l < L; ++l) {
-        if (g.y_num[l] % 8 == 0)
-            eqopt8_kernel<<<blocks_for(ncell(g, l) / 8, 256), 256, 0, s>>>(pm.status[l - 1], dims(g, l - 1),
-                                                                          pm.status[l], dims(g, l), min_type);
+        const uint64_t plane8 = (uint64_t)(g.y_num[l] / 8) * (uint64_t)g.x_num[l];
+        if (g.y_num[l] % 8 == 0 && plane8 < (1ull << 31))
+            eqopt8_kernel<<<dim3((unsigned)((plane8 + 255) / 256), (unsigned)g.z_num[l]), 256, 0, s>>>(
+                pm.status[l - 1], dims(g, l - 1), pm.status[l], dims(g, l), min_type);
         else
             eqopt_kernel<<<blocks_for(ncell(g, l), 256), 256, 0, s>>>(pm.status[l - 1], dims(g, l - 1), pm.status[l],
                                                                      dims(g, l), min_type);
