@@ -548,23 +548,22 @@ __global__ void __launch_bounds__(256) row_fill_top_kernel(const uint8_t *__rest
     }
     for (int y0 = 0; y0 < d.yn; y0 += 128) {
         const int yb = y0 + 4 * lane;
-        uint8_t sv[4];
+        uint32_t w = 0;  // the lane's four cells, zero (EMPTY) beyond the row
         if (vec4 && yb + 4 <= d.yn) {
-            const uint32_t w = *reinterpret_cast<const uint32_t *>(R + yb);
-            sv[0] = w & 0xff, sv[1] = (w >> 8) & 0xff, sv[2] = (w >> 16) & 0xff, sv[3] = w >> 24;
+            w = *reinterpret_cast<const uint32_t *>(R + yb);
         } else {
 #pragma unroll
-            for (int k = 0; k < 4; ++k) sv[k] = yb + k < d.yn ? R[yb + k] : 0;
+            for (int k = 0; k < 4; ++k)
+                if (yb + k < d.yn) w |= (uint32_t)R[yb + k] << (8 * k);
         }
-        int pc = 0, cc = 0;
-        int ck[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int y = yb + k;
-            pc += is_particle(sv[k], min_type) ? 1 : 0;
-            ck[k] = is_seed(sv[k], min_type) ? 1 + (2 * y < ylm - 1) : 0;
-            cc += ck[k];
-        }
+        // 0x80 in the bytes of seeds (1..min_type) and of particles (min_type < s <= UPSAMPLING_SEED)
+        const uint32_t seedm = bytes_in_1_to(w, min_type);
+        const uint32_t partm = bytes_in_1_to(w, kUpsamplingSeed) & ~seedm;
+        // a seed cell y has the level l_max children 2y and 2y + 1, the second
+        // only where 2y + 1 < ylm, i.e. below y = ylm / 2
+        const int kcut = (ylm >> 1) - yb;
+        const uint32_t one_child = kcut <= 0 ? 0x80808080u : (kcut >= 4 ? 0u : 0x80808080u << (8 * kcut));
+        const int pc = __popc(partm), cc = 2 * __popc(seedm) - __popc(seedm & one_child);
         const int mine = (pc << 16) | cc;
         int incl = mine;
 #pragma unroll
@@ -578,10 +577,10 @@ __global__ void __launch_bounds__(256) row_fill_top_kernel(const uint8_t *__rest
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int y = yb + k;
-            if (is_particle(sv[k], min_type)) y_vec[o + pp++] = (uint16_t)y;
-            if (ck[k]) {
+            if ((partm >> (8 * k + 7)) & 1u) y_vec[o + pp++] = (uint16_t)y;
+            if ((seedm >> (8 * k + 7)) & 1u) {
                 S[cp++] = (uint16_t)(2 * y);
-                if (ck[k] == 2) S[cp++] = (uint16_t)(2 * y + 1);
+                if (2 * y + 1 < ylm) S[cp++] = (uint16_t)(2 * y + 1);
             }
         }
         o += (uint64_t)(tot >> 16);
