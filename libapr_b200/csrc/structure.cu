@@ -788,6 +788,28 @@ __global__ void gather_kernel(const uint16_t *__restrict__ im, LevelDims d, cons
     for (uint64_t i = b + lane; i < e; i += 32) parts[i] = R[y_vec[i]];
 }
 
+// The same gather with four particles per lane and step (8-byte y and value
+// accesses, four independent image reads in flight per lane); the particles
+// before the first index that is a multiple of four and after the last whole
+// group of four go one per lane.  y_vec and parts must be 8-byte aligned.
+__global__ void gather4_kernel(const uint16_t *__restrict__ im, LevelDims d, const uint64_t *__restrict__ xz_end,
+                               uint64_t row_base, const uint16_t *__restrict__ y_vec, uint16_t *__restrict__ parts) {
+    const uint64_t row = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (row >= (uint64_t)d.xn * d.zn) return;
+    const uint64_t b = xz_end[row_base + row - 1], e = xz_end[row_base + row];
+    const uint16_t *R = im + row * (uint64_t)d.yn;
+    const uint64_t i0 = min((b + 3) & ~uint64_t(3), e), i1 = i0 + ((e - i0) & ~uint64_t(3));
+    if ((uint64_t)lane < i0 - b) parts[b + lane] = R[y_vec[b + lane]];
+    for (uint64_t i = i0 + 4 * (uint64_t)lane; i < i1; i += 128) {
+        const uint2 yv = *reinterpret_cast<const uint2 *>(y_vec + i);
+        const uint32_t v0 = R[yv.x & 0xffffu], v1 = R[yv.x >> 16], v2 = R[yv.y & 0xffffu], v3 = R[yv.y >> 16];
+        *reinterpret_cast<uint2 *>(parts + i) = make_uint2(v0 | v1 << 16, v2 | v3 << 16);
+    }
+    if ((uint64_t)lane < e - i1) parts[i1 + lane] = R[y_vec[i1 + lane]];
+}
+
+
 // ---------------------------------------------------------------------------
 // APR tree (APR.hpp:633-689, LinearAccess.hpp:67-122)
 // ---------------------------------------------------------------------------
@@ -843,6 +865,15 @@ LevelDims dims(const Geom &g, int l) { return LevelDims{g.y_num[l], g.x_num[l], 
 uint64_t ncell(const Geom &g, int l) { return (uint64_t)g.y_num[l] * g.x_num[l] * g.z_num[l]; }
 uint64_t nrow(const Geom &g, int l) { return (uint64_t)g.x_num[l] * g.z_num[l]; }
 unsigned row_blocks(uint64_t rows) { return blocks_for(rows * 32, 256); }
+
+void launch_gather(const uint16_t *im, LevelDims d, const uint64_t *xz_end, uint64_t row_base, const uint16_t *y_vec,
+                   uint16_t *parts, uint64_t rows, cudaStream_t s) {
+    if ((((uintptr_t)y_vec | (uintptr_t)parts) & 7) == 0)
+        gather4_kernel<<<row_blocks(rows), 256, 0, s>>>(im, d, xz_end, row_base, y_vec, parts);
+    else
+        gather_kernel<<<row_blocks(rows), 256, 0, s>>>(im, d, xz_end, row_base, y_vec, parts);
+}
+
 // (groups of a row / kRowThreads, x, z) of level l: the grid of the row kernels
 constexpr int kRowThreads = 128;
 dim3 row_grid(int groups, int xn, int zn) {
@@ -1025,7 +1056,7 @@ void launch_sample(const Geom &g, const uint64_t *xz_end, const uint16_t *y_vec,
         lev[l] = o;
     }
     for (int l = lmin; l <= L; ++l) {
-        gather_kernel<<<row_blocks(nrow(g, l)), 256, 0, s>>>(lev[l], dims(g, l), xz_end, g.level_xz[l], y_vec, parts);
+        launch_gather(lev[l], dims(g, l), xz_end, g.level_xz[l], y_vec, parts, nrow(g, l), s);
         count_launch();
     }
     APRB_CHECK_LAUNCH();
@@ -1061,8 +1092,7 @@ void launch_sample_slab(const Geom &g, const uint64_t *xz_end, const uint16_t *y
         count_launch();
     }
     const uint64_t rows = (uint64_t)(z1 - z0) * di.xn;
-    gather_kernel<<<row_blocks(rows), 256, 0, s>>>(slab, di, xz_end, g.level_xz[L] + (uint64_t)z0 * di.xn, y_vec,
-                                                   parts);
+    launch_gather(slab, di, xz_end, g.level_xz[L] + (uint64_t)z0 * di.xn, y_vec, parts, rows, s);
     count_launch();
     APRB_CHECK_LAUNCH();
 }
@@ -1081,8 +1111,7 @@ void launch_sample_coarse(const Geom &g, const uint64_t *xz_end, const uint16_t 
         count_launch();
     }
     for (int l = lmin; l < L; ++l) {
-        gather_kernel<<<row_blocks(nrow(g, l)), 256, 0, s>>>(base + off[l], dims(g, l), xz_end, g.level_xz[l], y_vec,
-                                                            parts);
+        launch_gather(base + off[l], dims(g, l), xz_end, g.level_xz[l], y_vec, parts, nrow(g, l), s);
         count_launch();
     }
     APRB_CHECK_LAUNCH();
