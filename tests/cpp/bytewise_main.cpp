@@ -1,9 +1,11 @@
-// Checks, on the host, the byte-parallel forms of the pulling-scheme,
+// Checks, on the host, the multi-cell forms of the pulling-scheme,
 // equivalence-step and sampling kernels against their per-cell forms: the
-// helpers against the per-byte rules for every byte value in every position,
-// and whole launches (every thread of the grid in turn) of set_filler8,
-// eqopt8, fill_parent4 and gather4 against set_filler, eqopt, fill_parent and
-// gather on random levels.  Prints the mismatch count; exit status 1 on any.
+// byte-parallel helpers against the per-byte rules for every byte value in
+// every position, and whole launches (every thread of the grid in turn) of
+// set_filler8, eqopt8, fill_parent4, pyramid_fill4, pyr_mean_u16x2 and
+// gather4 against set_filler, eqopt, fill_parent, pyramid_fill, pyr_mean_u16
+// and gather on random levels.  Prints the mismatch counts; exit status 1 on
+// any.
 
 template <class F>
 static void launch_1d(uint64_t threads, unsigned block, F f) {
@@ -119,6 +121,38 @@ static long check_pulling(std::mt19937 &g, long &cases) {
     return bad;
 }
 
+// One pyramid step from level di down to d = (di.yn / 2, ceil(di.xn / 2),
+// ceil(di.zn / 2)), under the vector kernels' launch conditions.
+static long check_pyramids(std::mt19937 &g, long &cases) {
+    long bad = 0;
+    for (int it = 0; it < 200; ++it) {
+        LevelDims di, d;
+        di.yn = 8 * (1 + (int)(g() % 24));
+        di.xn = 1 + (int)(g() % 9);
+        di.zn = 1 + (int)(g() % 7);
+        d.yn = di.yn / 2;
+        d.xn = (di.xn + 1) / 2;
+        d.zn = (di.zn + 1) / 2;
+        const size_t ni = (size_t)di.yn * di.xn * di.zn, no = (size_t)d.yn * d.xn * d.zn;
+        std::vector<uint8_t> lev(ni);
+        for (auto &v : lev) v = (uint8_t)(g() % 14);
+        const int level = (int)(g() % 14), is_min = (int)(g() % 2);
+        std::vector<uint8_t> o1(no), s1(no), o2(no), s2(no);
+        launch_1d(no, 256, [&] { pyramid_fill_kernel(lev.data(), di, o1.data(), s1.data(), d, level, is_min); });
+        launch_3d((unsigned)std::max((d.yn / 4 + 127) / 128, 1), d.xn, d.zn, 128,
+                  [&] { pyramid_fill4_kernel(lev.data(), di, o2.data(), s2.data(), d, level, is_min); });
+        bad += o1 != o2 || s1 != s2;
+        std::vector<uint16_t> img(ni), m1(no), m2(no);
+        for (auto &v : img) v = (uint16_t)g();
+        launch_1d(no, 256, [&] { pyr_mean_u16_kernel(img.data(), di, m1.data(), d); });
+        launch_3d((unsigned)std::max((d.yn / 2 + 127) / 128, 1), d.xn, d.zn, 128,
+                  [&] { pyr_mean_u16x2_kernel(img.data(), di, m2.data(), d); });
+        bad += m1 != m2;
+        cases += 2;
+    }
+    return bad;
+}
+
 static long check_gather(std::mt19937 &g, long &cases) {
     long bad = 0;
     for (int it = 0; it < 600; ++it) {
@@ -152,7 +186,8 @@ static long check_gather(std::mt19937 &g, long &cases) {
 int main() {
     std::mt19937 g(20261203);
     long cases = 0;
-    const long h = check_helpers(g), p = check_pulling(g, cases), q = check_gather(g, cases);
-    std::printf("helpers %ld, launches %ld of %ld + gathers %ld mismatched\n", h, p, cases, q);
-    return (h || p || q) ? 1 : 0;
+    const long h = check_helpers(g), p = check_pulling(g, cases), m = check_pyramids(g, cases),
+               q = check_gather(g, cases);
+    std::printf("helpers %ld, launches %ld + pyramids %ld of %ld + gathers %ld mismatched\n", h, p, m, cases, q);
+    return (h || p || m || q) ? 1 : 0;
 }

@@ -9,6 +9,7 @@
 #include <random>
 #include <vector>
 
+using std::max;
 using std::min;
 
 struct HostDim3 {
@@ -37,6 +38,13 @@ inline uint32_t __byte_perm(uint32_t x, uint32_t y, uint32_t s) {
     const uint64_t v = ((uint64_t)y << 32) | x;
     uint32_t r = 0;
     for (int i = 0; i < 4; ++i) r |= (uint32_t)((v >> (8 * ((s >> (4 * i)) & 7u))) & 0xFFu) << (8 * i);
+    return r;
+}
+
+// __vmaxu4(a, b): byte-wise unsigned maximum.
+inline uint32_t __vmaxu4(uint32_t a, uint32_t b) {
+    uint32_t r = 0;
+    for (int i = 0; i < 4; ++i) r |= std::max((a >> (8 * i)) & 0xFFu, (b >> (8 * i)) & 0xFFu) << (8 * i);
     return r;
 }
 

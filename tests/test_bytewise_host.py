@@ -1,13 +1,15 @@
-"""Byte-parallel kernels of the pulling scheme, the equivalence step and the
-sampling gather, checked on the CPU against the library's own per-cell forms.
+"""Multi-cell kernels of the particle-cell and sampling pyramids, the pulling
+scheme, the equivalence step and the sampling gather, checked on the CPU
+against the library's own per-cell forms.
 
 The helpers and kernels are taken verbatim from libapr_b200/csrc/structure.cu
 (and the status codes and idx3 from kernels.cuh / common.cuh), compiled with
 g++ behind the host stand-ins of tests/cpp/bytewise_prelude.hpp, and run
 thread by thread by tests/cpp/bytewise_main.cpp: the word-wide status tests
 against the per-byte rules for every byte value in every position, and whole
-launches of set_filler8, eqopt8 (both min types), fill_parent4 and gather4
-against set_filler, eqopt, fill_parent and gather on random levels.  The GPU
+launches of set_filler8, eqopt8 (both min types), fill_parent4,
+pyramid_fill4, pyr_mean_u16x2 and gather4 against set_filler, eqopt,
+fill_parent, pyramid_fill, pyr_mean_u16 and gather on random levels.  The GPU
 parity tests compare the same kernels with the oracle on real volumes; this
 test also covers status bytes and row shapes those volumes never produce.
 """
@@ -65,6 +67,10 @@ def _translation_unit():
         "__global__ void eqopt8_kernel(",
         "__global__ void fill_parent_kernel(",
         "__global__ void fill_parent4_kernel(",
+        "__global__ void pyramid_fill_kernel(",
+        "__global__ void pyramid_fill4_kernel(",
+        "__global__ void pyr_mean_u16_kernel(",
+        "__global__ void pyr_mean_u16x2_kernel(",
         "__global__ void gather_kernel(",
         "__global__ void gather4_kernel(",
     )]
@@ -83,4 +89,4 @@ def test_byte_parallel_kernels_match_per_cell_kernels(tmp_path):
     subprocess.run(["g++", "-std=c++17", "-O2", "-o", exe, str(src)], check=True)
     r = subprocess.run([exe], capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "helpers 0, launches 0 of" in r.stdout and "gathers 0 mismatched" in r.stdout, r.stdout
+    assert "helpers 0, launches 0 + pyramids 0 of" in r.stdout and "gathers 0 mismatched" in r.stdout, r.stdout
